@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Throughput of pot's per-timestep particle loop on B200.
+
+Metric: particle-steps/s (plasma particles x base time steps; ions keep the
+reference's sub-cycling, pot.c:4157-4159) for the 1,000,001-particle plasma
+(Te/Ti = 10, Mach-1 ion drift, R = 10 Debye lengths, grain 0.2 Debye
+lengths, theta = 0.5), fast form (FP32 leaf-grouped walk, FP64 positions and
+push, leaf size 16).  Synthetic data: particles initialised on the device by
+the reference's init_particles sampler with a fixed seed.
+
+Our arm (default):
+  * value: K device-timed steps with every input resident in HBM, CUDA events
+    around each step on the library's stream, L2 flushed (a 256 MiB write)
+    between steps outside the timed intervals; max over ranks;
+  * e2e: the drop-in call pot_gpu_move_particles on pinned host buffers in
+    the reference's Particle layout (upload, step, download every step),
+    wall-clock around the loop;
+  * plain_fp64: the same workload with the plain FP64 form (the reference's
+    arithmetic, leaf size 1);
+  * roofline: the dominant kernel's algorithmic bytes per launch over its
+    CUDA-event duration, against MEASURED_PEAKS.json;
+  * cpu_baseline: the reference program itself (oracle/_ref, one core, one
+    MPI rank) for one step of the same configuration.
+Reference arm (--impl reference): the compiled reference on the host cores,
+P processes each playing one MPI rank of a P-rank run (full tree build,
+its own block of particles pushed), max over ranks per step.
+
+Multi-GPU (--gpus N under torchrun): independent replicas, one per GPU,
+different seeds, no collective in the data path (the run has a global tree
+dependency and does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200 vs plain GPU & CPU; batch p99 latency @1% charge err"
+UNIT = "particle-steps/s"
+WORKLOAD = ("1m plasma: 1,000,001 particles (grain + 500,000 ions + 500,000 electrons), Te/Ti = 10, "
+            "Mach-1 ion drift along x, R = 10 lambda_De, a = 0.2 lambda_De, theta = 0.5, "
+            "SCEPTIC reinjection, dt = 0.005/omega_pe")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def reduce_max(x: float, device=None) -> float:
+    """Max over ranks of a per-rank timing (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = "/tmp/pot_bench_clocks_%d.csv" % os.getpid()
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_baseline_reference(cfg_name: str):
+    """One step of the reference program (compiled from its own sources,
+    one MPI rank on one core) on the same configuration."""
+    from oracle.oracle import RefLib, RunParams
+    from pot_b200.configs import CONFIGS
+    c = dict(CONFIGS[cfg_name])
+    steps, leaf = c.pop("steps"), c.pop("leaf_size")
+    p = RunParams(**c)
+    kind = "reference"
+    try:
+        ref = RefLib("sceptic", build=False)
+    except Exception:
+        ref = None
+    if ref is not None:
+        t0 = time.perf_counter()
+        ref.setup(p, seed=1)
+        t_init = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.step()
+        t_step = time.perf_counter() - t0
+        n_plasma = p.N - 1
+        return {"value": n_plasma / t_step, "unit": UNIT, "cores": 1, "kind": kind,
+                "sample": "one step (t = 1: tree over %d particles, %d electrons pushed) of the %s config by the "
+                          "reference pot.c compiled with gcc -O2 and a single-rank MPI stand-in, after its own "
+                          "init_particles (%.1f s); step took %.1f s" % (p.N, n_plasma // 2, cfg_name, t_init,
+                                                                         t_step)}
+    from oracle.oracle import Oracle
+    o = Oracle(p, mode="reference", seed=1)
+    t0 = time.perf_counter()
+    o.step()
+    t_step = time.perf_counter() - t0
+    return {"value": (p.N - 1) / t_step, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "one step of the %s config by the C restatement (reference not built here)" % cfg_name}
+
+
+def _ref_rank_worker(args):
+    cfg_name, nprocs, rank, n_steps, q = args
+    from oracle.oracle import RefLib, RunParams
+    from pot_b200.configs import CONFIGS
+    c = dict(CONFIGS[cfg_name])
+    c.pop("steps")
+    c.pop("leaf_size")
+    p = RunParams(**c)
+    ref = RefLib("sceptic", build=False)
+    ref.setup(p, seed=1, nprocs=nprocs, rank=rank)
+    times = []
+    for _ in range(n_steps):
+        t0 = time.perf_counter()
+        ref.step()
+        times.append(time.perf_counter() - t0)
+    q.put((rank, times))
+
+
+def run_reference_arm(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    try:
+        import psutil
+        mem_gb = psutil.virtual_memory().available / 2 ** 30
+    except Exception:
+        mem_gb = 64.0
+    from pot_b200.configs import CONFIGS
+    N = CONFIGS[args.config]["N"]
+    per_proc_gb = N * (56 * 2 + 9 * 130 + 48 + 24) / 2 ** 30 + 0.1
+    cores = len(os.sched_getaffinity(0))
+    P = max(1, min(cores, int(mem_gb * 0.6 / per_proc_gb), 64))
+    # each step is a bounded sample: at most a few minutes for the whole run
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    n = args.warmup + args.steps
+    procs = [ctx.Process(target=_ref_rank_worker, args=((args.config, P, r, n, q),)) for r in range(P)]
+    for pr in procs:
+        pr.start()
+    res = {}
+    for _ in range(P):
+        r, times = q.get()
+        res[r] = times
+    for pr in procs:
+        pr.join()
+    per_step = [max(res[r][k] for r in range(P)) for k in range(n)][args.warmup:]
+    t = sum(per_step)
+    value = (N - 1) * args.steps / t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/x87",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "N": N},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": "reference",
+                             "sample": "%d processes, each one MPI rank of a %d-rank run of the reference pot.c "
+                                       "(gcc -O2, single-rank MPI stand-in): full tree build plus its own block "
+                                       "of ~%d particles per step; step time = max over ranks; no MPI "
+                                       "communication counted" % (P, P, N // P)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from pot_b200.configs import CONFIGS, run_config
+    from pot_b200.gpu import PARTICLE_DTYPE, Run
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    # a dedicated stream: the library launches on it and the events are recorded on it
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
+    cfgd = CONFIGS[args.config]
+    cfg = run_config(args.config)
+    N = cfg.N
+    n_plasma = N - 1
+    hbm_peak, peak_kind = peaks()
+
+    run = Run(cfg, form=args.form, leaf_size=args.leaf or cfgd["leaf_size"], seed=1 + rank, device=local,
+              stream=stream.cuda_stream, timing=True)
+    run.init_particles()
+    # warm-up
+    for _ in range(args.warmup):
+        run.step_async(1)
+    run.sync()
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device=dev)
+    run.reset_kernel_times()
+    l0 = run.launch_count()
+    st0 = run.step(0)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(local)
+    clocks.start()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        run.step_async(1)
+        ev[k][1].record(stream)
+        flush.zero_()
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    run.sync()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    launches = run.launch_count() - l0
+    kt = run.kernel_times()
+    st = run.step(0)
+    t_ms = reduce_max(t_ms, dev)
+    value = n_plasma * ws * args.steps / (t_ms / 1e3)
+
+    # dominant kernel and its roofline (algorithmic bytes per launch)
+    dom = max(kt.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_n) = dom
+    n_e = n_plasma - (N - 1) // 2
+    tss_ion = int((cfg.Te * 1836.15 / cfg.Ti) ** 0.5)
+    pushes_per_step = n_e + ((N - 1) // 2) / tss_ion  # average due particles per step
+    per_launch_s = dom_ms / dom_n / 1e3
+    if dom_name.startswith("walk_push"):
+        alg_bytes = pushes_per_step * 96.0  # FP64 state read + write per push
+    elif dom_name.startswith("sort"):
+        alg_bytes = N * 24.0 * 2
+    else:
+        alg_bytes = N * 48.0
+    achieved = alg_bytes / per_launch_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(dom_name)
+        except Exception:
+            traffic = None
+    inter = st["interactions"]  # last timed step
+
+    # plain FP64 form on the same workload (fewer steps: it is the slow form)
+    plain = None
+    if args.plain_steps > 0:
+        runp = Run(cfg, form="plain", seed=1 + rank, device=local, stream=stream.cuda_stream, timing=False)
+        runp.init_particles()
+        runp.step_async(1)
+        runp.sync()
+        evp = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.plain_steps)]
+        torch.cuda.synchronize(dev)
+        for k in range(args.plain_steps):
+            evp[k][0].record(stream)
+            runp.step_async(1)
+            evp[k][1].record(stream)
+            flush.zero_()
+        torch.cuda.synchronize(dev)
+        runp.sync()
+        tp = sum(a.elapsed_time(b) for a, b in evp)
+        plain = {"value": n_plasma * args.plain_steps / (tp / 1e3), "unit": UNIT,
+                 "ms_per_step": tp / args.plain_steps, "steps": args.plain_steps, "form": "plain FP64, leaf 1"}
+        runp.close()
+
+    # end to end: drop-in call on pinned host buffers
+    host = torch.empty(N * PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+    parts = host.numpy().view(PARTICLE_DTYPE)
+    P, g = run.download()
+    parts[:] = P
+    grain = g
+    run.move_particles(parts, grain)  # warm
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        grain, _ = run.move_particles(parts, grain)
+    torch.cuda.synchronize(dev)
+    t_e2e = time.perf_counter() - t0
+    e2e = {"value": n_plasma * args.e2e_steps / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": int(N * PARTICLE_DTYPE.itemsize + 96),
+           "d2h_bytes_per_step": int(N * PARTICLE_DTYPE.itemsize + 96 + 88),
+           "steps": args.e2e_steps, "timing": "wall clock around pot_gpu_move_particles calls"}
+    if ws > 1:
+        e2e["value"] = n_plasma * ws * args.e2e_steps / reduce_max(t_e2e, dev)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_reference(args.config)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 force / f64 state", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "N": N, "form": args.form, "leaf_size": args.leaf or cfgd["leaf_size"],
+                       "l2": "flushed between timed steps (256 MiB write outside the events)",
+                       "parallelism": "replicas" if ws > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm_peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                         "ms_per_launch": per_launch_s * 1e3,
+                         "share_of_step": dom_ms / t_ms if t_ms else None},
+            "interactions_per_s": (inter * ws / (t_ms / args.steps / 1e3)) if inter else None,
+            "kernels_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
+            "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
+            "status": st["status"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    run.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--config", default="1m")
+    ap.add_argument("--form", choices=("fast", "plain"), default="fast")
+    ap.add_argument("--leaf", type=int, default=0)
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

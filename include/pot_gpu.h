@@ -1,0 +1,208 @@
+/*
+ * pot_gpu.h -- C ABI of the B200 (sm_100a) implementation of pot's
+ * per-timestep particle loop.
+ *
+ * The reference (drewthomas/pot, pot.c) runs one time step as two C calls
+ * inside run()'s loop:
+ *     build_tree(Proc*, Run)                          pot.c:4308 -> 1457-1643
+ *     move_particles(Proc*, Run, Tree*, ..., t)       pot.c:4386 -> 2330-2934
+ * on a host array of `Particle` records (pot.c:295-303) replicated on every
+ * MPI rank.  This library replaces both calls, and the MPI decomposition
+ * around them, with one GPU: particles live in HBM in Morton order, and a
+ * step is a fixed sequence of CUDA kernels (Morton keys, radix sort, octree
+ * build, upward moments, Barnes-Hut walk fused with the Boris push,
+ * grain absorption with an integer tally, boundary reinjection, grain
+ * update).  The host keeps ownership of its arrays; every pointer in this
+ * header is a plain host pointer.
+ *
+ * Every function returns POT_OK (0) or a negative POT_E_* status and never
+ * aborts; the reference's fatal paths (abort() at pot.c:1651 and 1802,
+ * NULL from build_tree at pot.c:1498 and 1583) map to status codes, with
+ * pot_gpu_strerror() giving a message.  A context is used by one host
+ * thread at a time.
+ */
+#ifndef POT_GPU_H
+#define POT_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define POT_OK 0
+#define POT_E_ARG (-1)          /* invalid argument or configuration */
+#define POT_E_CUDA (-2)         /* CUDA runtime error (no device, launch failure) */
+#define POT_E_NOMEM (-3)        /* device allocation failed */
+#define POT_E_DOMAIN (-4)       /* particle outside the root cell: build_tree's NULL, pot.c:1491-1500 */
+#define POT_E_COINCIDENT (-5)   /* two particles at one position, pot.c:1578-1586 / 1800-1802 */
+#define POT_E_WALK (-6)         /* walk stack overflow, pot.c:1647-1652 */
+#define POT_E_NONFINITE (-7)    /* NaN position, pot.c:1434-1446 */
+#define POT_E_ITER (-8)         /* an iteration cap in a sampler was reached */
+#define POT_E_CAPACITY (-9)     /* tree larger than the node arrays */
+#define POT_E_STATE (-10)       /* call out of order (e.g. step before upload) */
+
+/* ---- records shared with the reference --------------------------------- */
+
+/* Byte-compatible with pot.c:295-303 on x86-64 (56 bytes). */
+typedef struct pot_particle {
+	double x, y, z;
+	double vx, vy, vz;
+	int32_t species; /* 0 dust grain, 1 ion, 2 electron (pot.c:286-290) */
+	int32_t pad;
+} pot_particle;
+
+/* Run settings: the reference's `Run` (pot.c:335-358, spherical domain)
+   plus the compile-time switches of pot.c:25-196 that the hot path reads. */
+typedef struct pot_run_cfg {
+	uint64_t N;       /* particles incl. the grain at index 0 (-N) */
+	uint32_t r;       /* domain radius in pixels (-r) */
+	uint32_t flags;   /* POT_CFG_* */
+	double dt;        /* time step, s (-d) */
+	double mpp;       /* metres per pixel (-m) */
+	double soft;      /* softening length, m (-s) */
+	double Te, Ti;    /* injection temperatures, K (-E, -I) */
+	double x_drift;   /* drift velocity along x, m/s (-x) */
+	double a;         /* grain radius, m (-a) */
+	double settle;    /* settling time before absorption starts, s (-e) */
+	double theta;     /* opening angle OAP (pot.c:97) */
+	double B[3];      /* EXTERNAL_B_X/Y/Z, tesla (pot.c:55-57) */
+	double A;         /* spheroid aspect ratio (-A of pot-spheroid.c); 0 = sphere */
+} pot_run_cfg;
+
+#define POT_CFG_SCEPTIC 0x1u        /* SCEPTIC_REINJECTION (pot.c:181): flux-weighted reinjection */
+#define POT_CFG_DISABLE_GRAIN 0x2u  /* DISABLE_GRAIN (pot.c:30): no absorption */
+
+/* Execution options (no counterpart in the reference). */
+typedef struct pot_gpu_opts {
+	uint32_t form;        /* POT_FORM_PLAIN or POT_FORM_FAST */
+	uint32_t leaf_size;   /* particles per leaf; 1 in POT_FORM_PLAIN (the reference's tree) */
+	uint32_t group_size;  /* POT_FORM_FAST: targets per warp group (32 or 64); 0 = default */
+	uint32_t flags;       /* POT_OPT_* */
+	int32_t device;       /* CUDA device ordinal */
+	uint32_t pad;
+	uint64_t seed;        /* key of the Philox streams used for (re)injection */
+	void* stream;         /* cudaStream_t to launch on; NULL = a private stream */
+} pot_gpu_opts;
+
+#define POT_FORM_PLAIN 0u  /* FP64 walk per target, leaf size 1: the reference's arithmetic */
+#define POT_FORM_FAST 1u   /* FP32 leaf-grouped warp walk, FP64 positions and push */
+
+#define POT_OPT_TIMING 0x1u  /* record CUDA events around each kernel (pot_gpu_kernel_times) */
+
+/* Grain state: the reference keeps it in Proc (pot.c:370-371, 397) and in
+   parts[0] (pot.c:890-899). */
+typedef struct pot_grain_state {
+	int64_t q;            /* net charge, elementary charges (Proc.dust_grain_q) */
+	double m;             /* mass, kg (Proc.dust_grain_m) */
+	double x, y, z;       /* position, m */
+	double vx, vy, vz;    /* velocity, m/s */
+	uint64_t tot_absor_e; /* electrons absorbed so far (Proc.tot_absor_e) */
+	uint64_t t_steps;     /* steps taken so far (Proc.t_steps) */
+	double chi_b;         /* normalised edge potential (Proc.chi_b, SCEPTIC) */
+} pot_grain_state;
+
+/* Per-step results, written by pot_gpu_step for the last step it ran. */
+typedef struct pot_step_stats {
+	uint64_t t_steps;      /* step index after the step */
+	int64_t grain_q;       /* grain charge after the step */
+	int64_t dq;            /* charge absorbed this step (pot.c:2663) */
+	uint64_t de;           /* electrons absorbed this step */
+	uint64_t n_absorbed;   /* particles absorbed this step */
+	uint64_t n_reinjected; /* reinjections this step (absorption + boundary) */
+	uint64_t n_pushed;     /* particles advanced this step */
+	uint64_t interactions; /* cell + pair interactions evaluated this step */
+	uint64_t n_nodes;      /* internal tree nodes this step */
+	double chi_b;          /* edge potential in force after the step */
+	int32_t status;        /* POT_OK or the first device-side error */
+	uint32_t pad;
+} pot_step_stats;
+
+typedef struct pot_gpu_ctx pot_gpu_ctx;
+
+/* ---- life cycle -------------------------------------------------------- */
+
+/* Allocate device state for one run of cfg->N particles.  Replaces the
+   allocations of main() and run() (pot.c:5117-5130, 4115-4146). */
+int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx** out);
+void pot_gpu_destroy(pot_gpu_ctx* ctx);
+const char* pot_gpu_strerror(int status);
+
+/* Copy a host particle array (reference order: grain, ions, electrons) and
+   the grain state to the device.  Replaces the per-step MPI_Bcast of all
+   particles (pot.c:4299).  grain may be NULL (charge 0, mass 1.67e-12 kg,
+   t_steps 0, as main() starts a run, pot.c:5184-5190). */
+int pot_gpu_upload(pot_gpu_ctx* ctx, const pot_particle* parts, uint64_t N,
+                   const pot_grain_state* grain);
+
+/* init_particles (pot.c:887-996) on the device: grain at the centre,
+   (N-1)/2 ions then electrons, positions uniform in the shell a < r < R,
+   Maxwellian velocities, each particle drawing from its own Philox stream. */
+int pot_gpu_init_particles(pot_gpu_ctx* ctx);
+
+/* Run nsteps steps (each: t_steps++, build_tree, move_particles).  `flags`
+   is reserved (0).  `out` (may be NULL) receives the last step's stats. */
+int pot_gpu_step(pot_gpu_ctx* ctx, uint32_t nsteps, uint32_t flags, pot_step_stats* out);
+
+/* Enqueue nsteps steps on the context's stream and return without waiting.
+   Device-side errors surface at the next pot_gpu_sync / pot_gpu_step /
+   pot_gpu_download, which return the first status recorded. */
+int pot_gpu_step_async(pot_gpu_ctx* ctx, uint32_t nsteps);
+
+/* Copy particles back in reference order (index = original position), and
+   the grain state.  Either pointer may be NULL. */
+int pot_gpu_download(pot_gpu_ctx* ctx, pot_particle* parts, pot_grain_state* grain);
+
+/* Drop-in for one iteration of run()'s hot path (pot.c:4299-4386): upload
+   `parts` (N records, reference order) and `grain`, t_steps++, build the
+   tree, move the particles, download both back into the same arrays. */
+int pot_gpu_move_particles(pot_gpu_ctx* ctx, pot_particle* parts, uint64_t N,
+                           pot_grain_state* grain, pot_step_stats* out);
+
+/* ---- inspection (parity tests) ----------------------------------------- */
+
+/* Build the tree from the current device particles without stepping
+   (build_tree, pot.c:1457-1643).  Returns the number of internal nodes in
+   *n_nodes. */
+int pot_gpu_build_tree(pot_gpu_ctx* ctx, uint64_t* n_nodes);
+
+/* Canonical dump of the last tree built: internal nodes and leaves, each
+   labelled by (level, octal-digit path from the root); the same format as
+   the oracle's dump of the reference's pointer tree.  Leaves report the
+   original particle index of each occupant (leaf_size 1). */
+int pot_gpu_tree_dump(pot_gpu_ctx* ctx, uint64_t max_nodes,
+                      uint64_t* n_int, int32_t* int_level, uint64_t* int_path, int32_t* int_q,
+                      uint32_t* int_aq, double* int_c, double* int_w,
+                      uint64_t* n_leaf, uint32_t* leaf_part, int32_t* leaf_level,
+                      uint64_t* leaf_path);
+
+/* E field (V/m) at n points xyz[3k..3k+2], each for the target particle
+   with original index idx[k] (excluded from its own field), over the last
+   tree built: field_particle_feels_at (pot.c:1696-1808) for many targets. */
+int pot_gpu_field_at(pot_gpu_ctx* ctx, uint64_t n, const uint32_t* idx, const double* xyz,
+                     double* E);
+
+/* Potential (V) at n points over the last tree built, every particle
+   included: phi_at (pot.c:1818-1901). */
+int pot_gpu_phi_at(pot_gpu_ctx* ctx, uint64_t n, const double* xyz, double* phi);
+
+/* Accumulated per-kernel device time since creation or the last reset
+   (requires POT_OPT_TIMING).  Writes up to `max` entries; returns the count
+   of kernels known (names are static strings). */
+int pot_gpu_kernel_times(pot_gpu_ctx* ctx, int max, const char** names, double* ms,
+                         uint64_t* launches);
+int pot_gpu_reset_kernel_times(pot_gpu_ctx* ctx);
+
+/* Number of CUDA kernels this context has enqueued since creation. */
+int pot_gpu_launch_count(pot_gpu_ctx* ctx, uint64_t* n);
+
+/* Block the calling thread until all work queued on the context's stream
+   has finished; returns the first device-side status seen. */
+int pot_gpu_sync(pot_gpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

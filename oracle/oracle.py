@@ -100,7 +100,7 @@ class RefLib:
         L.potref_setup.argtypes = [C.c_ulong, C.c_uint, C.c_double, C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_double, C.c_double,
-                                   C.c_void_p, C.c_int]
+                                   C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.potref_setup.restype = C.c_int
         L.potref_build_tree.restype = C.c_int
         L.potref_step.argtypes = [C.c_int]
@@ -142,11 +142,13 @@ class RefLib:
         assert L.potref_sizeof_particle() == 56
 
     # -- set-up ---------------------------------------------------------------
-    def setup(self, p: RunParams, seed: int = 1, init: bool = True):
+    def setup(self, p: RunParams, seed: int = 1, init: bool = True, nprocs: int = 1, rank: int = 0):
+        """Set up a run; with nprocs > 1 this process plays MPI rank `rank`
+        (it builds the whole tree and steps only its own block)."""
         words = splitmix64_words(seed)
         rc = self.lib.potref_setup(p.N, p.r, p.dt, p.mpp, p.soft, p.Te, p.Ti, p.x_drift, p.a,
                                    p.settle, p.theta, p.B[0], p.B[1], p.B[2], _ptr(words),
-                                   1 if init else 0)
+                                   1 if init else 0, int(nprocs), int(rank))
         if rc != 0:
             raise RuntimeError("potref_setup failed: %d" % rc)
         self.N = p.N
@@ -338,6 +340,8 @@ class Oracle:
         self.cfg = cfg
         self.params = p
         self.mode = mode
+        self.seed = seed
+        self.sceptic = sceptic
         self.N = p.N
         self.h = L.pto_create(C.byref(cfg))
         if not self.h:

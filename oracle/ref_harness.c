@@ -59,7 +59,7 @@ static void h_free(void)
 int potref_setup(unsigned long N, unsigned int r, double dt, double mpp, double soft,
                  double Te, double Ti, double x_drift, double a, double settle,
                  double oap, double bx, double by, double bz,
-                 const uint32_t* seed16, int init)
+                 const uint32_t* seed16, int init, int nprocs, int rank)
 {
 	h_free();
 	memset(&R, 0, sizeof(R));
@@ -84,8 +84,12 @@ int potref_setup(unsigned long N, unsigned int r, double dt, double mpp, double 
 	pot_ref_bz = bz;
 
 	memset(&H, 0, sizeof(H));
-	H.rank = 0;
-	H.num_procs = 1;
+	/* One rank of an nprocs-rank run: the block decomposition of
+	   set_up_workers_for_assignments (pot.c:2936-2998) and the per-block
+	   species layout of init_particles (pot.c:908-930) are the reference's;
+	   MPI traffic is absent, so this rank steps only its own block. */
+	H.rank = rank;
+	H.num_procs = nprocs > 0 ? nprocs : 1;
 	if (set_up_workers_for_assignments(&H, R)) return -1;
 	H.parts = malloc(sizeof(Particle) * N);
 	H.new_parts = malloc(sizeof(Particle) * N);
@@ -93,7 +97,7 @@ int potref_setup(unsigned long N, unsigned int r, double dt, double mpp, double 
 	H.prev_x = malloc(3 * sizeof(double) * N);
 	H.tr_alloc = 9 * N;
 	H.root = malloc(sizeof(Tree) * H.tr_alloc);
-	H.starts = malloc(sizeof(unsigned int) * 1);
+	H.starts = malloc(sizeof(unsigned int) * (H.num_procs > 0 ? H.num_procs : 1));
 	if (!H.parts || !H.new_parts || !H.a_x1 || !H.prev_x || !H.root || !H.starts) return -2;
 	H.a_y1 = &(H.a_x1[N]);
 	H.a_z1 = &(H.a_x1[2 * N]);

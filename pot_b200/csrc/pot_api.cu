@@ -1,0 +1,820 @@
+// C ABI (include/pot_gpu.h): run context, host <-> device transfers, the
+// per-step launch sequence, inspection queries and the kernel timer.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "pot_tree.cuh"
+
+using namespace pot;
+
+struct pot_gpu_ctx {
+	pot_run_cfg cfg;
+	pot_gpu_opts opts;
+	Params P;
+	cudaStream_t stream = nullptr;
+	bool own_stream = false;
+	int device = 0;
+	uint32_t n = 0;
+	double4* pos[2] = { nullptr, nullptr };
+	double4* vel[2] = { nullptr, nullptr };
+	uint32_t* pid[2] = { nullptr, nullptr };
+	int cur = 0;
+	double4* src64 = nullptr;
+	float4* src32 = nullptr;
+	uint64_t* keys[2] = { nullptr, nullptr };
+	uint32_t* vals[2] = { nullptr, nullptr };
+	uint32_t* counts = nullptr;
+	uint32_t* block_sums = nullptr;
+	uint8_t* due = nullptr;
+	uint32_t* due_list = nullptr;
+	uint32_t* due_prefix = nullptr;  // n + 1
+	uint2* groups = nullptr;
+	uint32_t* rein_list = nullptr;
+	uint32_t* inv = nullptr;
+	pot_particle* aos = nullptr;
+	TreeDev T {};
+	RunRec* rec = nullptr;
+	StepHist* hist = nullptr;
+	// query scratch
+	double* q_xyz = nullptr;
+	double* q_out = nullptr;
+	uint32_t* q_idx = nullptr;
+	uint32_t* q_slot = nullptr;
+	size_t q_cap = 0;
+	bool uploaded = false;
+	bool tree_valid = false;
+	int sticky = POT_OK;
+	Timer timer;
+	std::vector<void*> allocs;
+};
+
+// ---------------------------------------------------------------------------
+// Timer
+// ---------------------------------------------------------------------------
+namespace pot {
+
+cudaEvent_t Timer::take()
+{
+	if (!pool_.empty()) {
+		cudaEvent_t e = pool_.back();
+		pool_.pop_back();
+		return e;
+	}
+	cudaEvent_t e = nullptr;
+	cudaEventCreate(&e);
+	return e;
+}
+
+int Timer::kind_of(const char* name)
+{
+	for (size_t i = 0; i < names_.size(); i++)
+		if (std::strcmp(names_[i], name) == 0) return (int)i;
+	names_.push_back(name);
+	ms_.push_back(0.0);
+	count_.push_back(0);
+	return (int)names_.size() - 1;
+}
+
+void Timer::begin(const char* name)
+{
+	if (!enabled || open_kind_ >= 0) return;  // nested scopes: the outer one times
+	open_kind_ = kind_of(name);
+	open_a_ = take();
+	cudaEventRecord(open_a_, stream);
+}
+
+void Timer::end()
+{
+	if (!enabled || open_kind_ < 0) return;
+	cudaEvent_t b = take();
+	cudaEventRecord(b, stream);
+	pending_.push_back({ open_kind_, open_a_, b });
+	open_kind_ = -1;
+	open_a_ = nullptr;
+}
+
+void Timer::resolve()
+{
+	for (auto& p : pending_) {
+		float ms = 0.f;
+		if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+			ms_[p.kind] += ms;
+			count_[p.kind] += 1;
+		}
+		pool_.push_back(p.a);
+		pool_.push_back(p.b);
+	}
+	pending_.clear();
+}
+
+void Timer::reset()
+{
+	resolve();
+	for (auto& m : ms_) m = 0.0;
+	for (auto& c : count_) c = 0;
+}
+
+int Timer::report(int max, const char** names, double* ms, uint64_t* launches) const
+{
+	const int n = (int)names_.size();
+	for (int i = 0; i < n && i < max; i++) {
+		if (names) names[i] = names_[i];
+		if (ms) ms[i] = ms_[i];
+		if (launches) launches[i] = count_[i];
+	}
+	return n;
+}
+
+Timer::~Timer()
+{
+	for (auto& p : pending_) {
+		cudaEventDestroy(p.a);
+		cudaEventDestroy(p.b);
+	}
+	for (auto e : pool_) cudaEventDestroy(e);
+}
+
+}  // namespace pot
+
+// ---------------------------------------------------------------------------
+// small kernels: layout conversion, inverse permutation
+// ---------------------------------------------------------------------------
+__global__ void k_from_aos(const pot_particle* __restrict__ aos, uint32_t n, double4* __restrict__ pos,
+                           double4* __restrict__ vel, uint32_t* __restrict__ pid, RunRec* rec)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const pot_particle p = aos[i];
+	int sp = p.species;
+	if (sp < 0 || sp > 2) {
+		set_status(rec, POT_E_ARG);
+		sp = SP_E;
+	}
+	pos[i] = make_double4(p.x, p.y, p.z, (double)sp);
+	vel[i] = make_double4(p.vx, p.vy, p.vz, 0.0);
+	pid[i] = i;
+}
+
+__global__ void k_to_aos(const double4* __restrict__ pos, const double4* __restrict__ vel,
+                         const uint32_t* __restrict__ pid, uint32_t n, pot_particle* __restrict__ aos)
+{
+	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= n) return;
+	const double4 p = pos[s];
+	const double4 v = vel[s];
+	pot_particle o;
+	o.x = p.x; o.y = p.y; o.z = p.z;
+	o.vx = v.x; o.vy = v.y; o.vz = v.z;
+	o.species = (int32_t)p.w;
+	o.pad = 0;
+	aos[pid[s]] = o;
+}
+
+__global__ void k_inverse(const uint32_t* __restrict__ pid, uint32_t n, uint32_t* __restrict__ inv)
+{
+	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s < n) inv[pid[s]] = s;
+}
+
+__global__ void k_map_slots(const uint32_t* __restrict__ inv, const uint32_t* __restrict__ idx, uint32_t nq,
+                            uint32_t n, uint32_t* __restrict__ slot)
+{
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < nq) slot[k] = idx[k] < n ? inv[idx[k]] : 0xFFFFFFFFu;
+}
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+#define CK(call)                                                        \
+	do {                                                                \
+		cudaError_t e_ = (call);                                        \
+		if (e_ != cudaSuccess) {                                        \
+			fprintf(stderr, "pot_gpu: %s: %s\n", #call, cudaGetErrorString(e_)); \
+			return e_ == cudaErrorMemoryAllocation ? POT_E_NOMEM : POT_E_CUDA; \
+		}                                                               \
+	} while (0)
+
+template <typename T>
+static int dalloc(pot_gpu_ctx* c, T** p, size_t count)
+{
+	*p = nullptr;
+	if (count == 0) count = 1;
+	cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+	if (e != cudaSuccess) {
+		*p = nullptr;
+		return e == cudaErrorMemoryAllocation ? POT_E_NOMEM : POT_E_CUDA;
+	}
+	c->allocs.push_back((void*)*p);
+	return POT_OK;
+}
+
+static inline uint32_t nblk(size_t n, int t) { return (uint32_t)((n + t - 1) / t); }
+
+static int fill_params(pot_gpu_ctx* c)
+{
+	const pot_run_cfg& r = c->cfg;
+	Params& P = c->P;
+	std::memset(&P, 0, sizeof(P));
+	P.n = (uint32_t)r.N;
+	P.n_total = (uint32_t)r.N;
+	P.n_ions = (uint32_t)((r.N - 1) / 2);
+	P.r_pix = r.r;
+	P.leaf_size = c->opts.leaf_size;
+	P.flags = r.flags;
+	P.form = c->opts.form;
+	P.seed = c->opts.seed;
+	const long double m_ion = (long double)MASS_ION, m_e = (long double)MASS_E, m_d = (long double)MASS_DUST;
+	// species time-step multiples, pot.c:4157-4159
+	P.tss[SP_E] = 1;
+	P.tss[SP_ION] = (uint32_t)(int)std::sqrt((double)(r.Te * m_ion / (r.Ti * m_e)));
+	P.tss[SP_DUST] = P.tss[SP_ION] * (uint32_t)(int)std::sqrt((double)(0.1 * m_d / m_ion));
+	if (P.tss[SP_ION] == 0 || P.tss[SP_DUST] == 0) return POT_E_ARG;
+	P.dt = r.dt;
+	P.mpp = r.mpp;
+	P.rad = r.r * r.mpp;           // pot.c:2032
+	P.root_w = 2.0 * r.r * r.mpp;  // pot.c:1476
+	P.inv_rad = 1.0 / P.rad;
+	P.soft = r.soft;
+	P.soft2 = r.soft * r.soft;
+	P.a = r.a;
+	P.Te = r.Te;
+	P.Ti = r.Ti;
+	P.x_drift = r.x_drift;
+	P.oap2 = r.theta * r.theta;
+	P.k4 = 4 * PI_REF * EPSILON0;
+	P.Bmag = std::sqrt(r.B[0] * r.B[0] + r.B[1] * r.B[1] + r.B[2] * r.B[2]);
+	for (int k = 0; k < 3; k++) P.bhat[k] = P.Bmag != 0.0 ? r.B[k] / P.Bmag : 0.0;
+	P.oap2_f = (float)P.oap2;
+	P.soft2_f = (float)((r.soft * P.inv_rad) * (r.soft * P.inv_rad));
+	// sigma = sqrt(KB T / MASS) with the division in long double, pot.c:675-681
+	P.sigma_i = std::sqrt((double)((long double)(KB * r.Ti) / m_ion));
+	P.sigma_e = std::sqrt((double)((long double)(KB * r.Te) / m_e));
+	// v_n of pot.c:517-524: (2 KB / MASS) rounded to double, times T
+	{
+		double vi = (double)((long double)(2.0 * KB) / m_ion);
+		double ve = (double)((long double)(2.0 * KB) / m_e);
+		P.vn_i = std::sqrt(vi * r.Ti);
+		P.vn_e = std::sqrt(ve * r.Te);
+	}
+	// Rol of pot.c:577-579
+	{
+		double Rol = QE * QE * (r.N - 1) / 2.0;
+		Rol /= (4.0 * PI_REF / 3.0) * r.mpp * r.r * EPSILON0 * KB * r.Te;
+		P.Rol = std::sqrt(Rol);
+	}
+	// absorption starts at the first step with t * dt > settle (long double, pot.c:2644)
+	{
+		const long double dtl = (long double)r.dt, st = (long double)r.settle;
+		unsigned long long t0 = 1;
+		if (st > 0.0L) {
+			const long double g = st / dtl;
+			t0 = g > 2.0L ? (unsigned long long)(g - 2.0L) : 1ull;
+			if (t0 < 1) t0 = 1;
+			while ((long double)t0 * dtl <= st) t0++;
+		} else {
+			while ((long double)t0 * dtl <= st) t0++;
+		}
+		P.t_settle = t0;
+	}
+	return POT_OK;
+}
+
+static void tree_ptrs_fast(pot_gpu_ctx* c, bool fast)
+{
+	if (!fast) {
+		c->T.f = nullptr;
+		c->T.r2 = nullptr;
+		c->T.lf = nullptr;
+		c->T.lr2 = nullptr;
+	}
+}
+
+static int sync_status(pot_gpu_ctx* c)
+{
+	cudaError_t e = cudaStreamSynchronize(c->stream);
+	if (e != cudaSuccess) {
+		fprintf(stderr, "pot_gpu: %s\n", cudaGetErrorString(e));
+		return POT_E_CUDA;
+	}
+	c->timer.resolve();
+	int st = 0;
+	e = cudaMemcpy(&st, &c->rec->status, sizeof(int), cudaMemcpyDeviceToHost);
+	if (e != cudaSuccess) return POT_E_CUDA;
+	if (st != POT_OK && c->sticky == POT_OK) c->sticky = st;
+	return st;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+template <typename T>
+static int fetch(std::vector<T>& v, const T* d, size_t n)
+{
+	v.resize(n);
+	if (n == 0) return POT_OK;
+	CK(cudaMemcpy(v.data(), d, sizeof(T) * n, cudaMemcpyDeviceToHost));
+	return POT_OK;
+}
+
+extern "C" {
+
+const char* pot_gpu_strerror(int s)
+{
+	switch (s) {
+	case POT_OK: return "ok";
+	case POT_E_ARG: return "invalid argument";
+	case POT_E_CUDA: return "CUDA error";
+	case POT_E_NOMEM: return "out of device memory";
+	case POT_E_DOMAIN: return "particle not in simulation area (tree building failed)";
+	case POT_E_COINCIDENT: return "multiple particles at one location";
+	case POT_E_WALK: return "particle tree path length exceeded";
+	case POT_E_NONFINITE: return "particle has a NaN position";
+	case POT_E_ITER: return "sampler iteration cap reached";
+	case POT_E_CAPACITY: return "tree larger than its node arrays";
+	case POT_E_STATE: return "call out of order";
+	default: return "unknown status";
+	}
+}
+
+void pot_gpu_destroy(pot_gpu_ctx* c)
+{
+	if (!c) return;
+	cudaSetDevice(c->device);
+	if (c->stream) cudaStreamSynchronize(c->stream);
+	for (void* p : c->allocs) cudaFree(p);
+	if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+	delete c;
+}
+
+int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx** out)
+{
+	if (!cfg || !out) return POT_E_ARG;
+	*out = nullptr;
+	pot_gpu_opts o {};
+	if (opts) o = *opts;
+	if (o.form != POT_FORM_PLAIN && o.form != POT_FORM_FAST) return POT_E_ARG;
+	if (o.leaf_size == 0) o.leaf_size = o.form == POT_FORM_PLAIN ? 1 : 16;
+	if (o.form == POT_FORM_PLAIN && o.leaf_size != 1) return POT_E_ARG;
+	if (o.leaf_size > 64) return POT_E_ARG;
+	if (cfg->N < 2 || cfg->N > (1ull << 24) || cfg->N <= o.leaf_size) return POT_E_ARG;  // scans cover 2^24
+	if (cfg->r == 0 || !(cfg->mpp > 0.0) || !(cfg->dt > 0.0) || !(cfg->a > 0.0) || cfg->soft < 0.0 ||
+	    !(cfg->theta > 0.0) || cfg->Te < 0.0 || cfg->Ti <= 0.0)
+		return POT_E_ARG;
+	if (cfg->A != 0.0 && cfg->A != 1.0) return POT_E_ARG;  // spheroidal grains are not in this build
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return POT_E_CUDA;
+	if (o.device < 0 || o.device >= ndev) return POT_E_ARG;
+	pot_gpu_ctx* c = new (std::nothrow) pot_gpu_ctx();
+	if (!c) return POT_E_NOMEM;
+	c->cfg = *cfg;
+	c->opts = o;
+	c->device = o.device;
+	if (cudaSetDevice(c->device) != cudaSuccess) {
+		delete c;
+		return POT_E_CUDA;
+	}
+	int rc = fill_params(c);
+	if (rc) {
+		delete c;
+		return rc;
+	}
+	if (o.stream) {
+		c->stream = (cudaStream_t)o.stream;
+	} else {
+		if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+			delete c;
+			return POT_E_CUDA;
+		}
+		c->own_stream = true;
+	}
+	c->timer.enabled = (o.flags & POT_OPT_TIMING) != 0;
+	c->timer.stream = c->stream;
+	const uint32_t n = (uint32_t)cfg->N;
+	c->n = n;
+	const bool fast = o.form == POT_FORM_FAST;
+	const uint32_t L = o.leaf_size;
+	const uint32_t cap = (L == 1 ? 4u * n : (4u * n) / L + 8u * n / 64u) + 4096u;
+	const size_t nsum = std::max(scan_blocks(radix_counts_words(n)), scan_blocks(n)) + 16;
+#define AL(ptr, count)                         \
+	do {                                       \
+		if ((rc = dalloc(c, &(ptr), (count)))) { \
+			pot_gpu_destroy(c);                \
+			return rc;                         \
+		}                                      \
+	} while (0)
+	for (int b = 0; b < 2; b++) {
+		AL(c->pos[b], n);
+		AL(c->vel[b], n);
+		AL(c->pid[b], n);
+		AL(c->keys[b], n);
+		AL(c->vals[b], n);
+	}
+	AL(c->src64, n);
+	if (fast) AL(c->src32, n);
+	AL(c->counts, radix_counts_words(n));
+	AL(c->block_sums, nsum);
+	AL(c->due, n);
+	AL(c->due_list, n);
+	AL(c->due_prefix, (size_t)n + 1);
+	if (fast) AL(c->groups, n);
+	AL(c->rein_list, 2 * (size_t)n);
+	AL(c->inv, n);
+	AL(c->rec, 1);
+	AL(c->hist, HIST);
+	TreeDev& T = c->T;
+	T.cap = cap;
+	AL(T.lvl8, n);
+	AL(T.cnt, n);
+	AL(T.base, n);
+	AL(T.first, cap);
+	AL(T.last, cap);
+	AL(T.level, cap);
+	AL(T.child, 8ull * cap);
+	AL(T.parent, cap);
+	AL(T.nint, cap);
+	AL(T.ctr, cap);
+	AL(T.q, cap);
+	AL(T.aq, cap);
+	AL(T.cq, cap);
+	AL(T.w2, cap);
+	AL(T.ovf, OVF_CAP);
+	if (fast) {
+		AL(T.f, cap);
+		AL(T.r2, cap);
+		if (L > 1) {
+			AL(T.lf, 8ull * cap);
+			AL(T.lr2, 8ull * cap);
+			AL(T.lrange, 8ull * cap);
+		}
+	}
+	if (!fast || L == 1) {
+		T.lf = nullptr;
+		T.lr2 = nullptr;
+		if (!T.lrange) T.lrange = nullptr;
+	}
+	tree_ptrs_fast(c, fast);
+#undef AL
+	RunRec r0;
+	std::memset(&r0, 0, sizeof(r0));
+	r0.grain_m = MASS_DUST;
+	r0.grain_slot = 0xFFFFFFFFu;
+	if (cudaMemcpy(c->rec, &r0, sizeof(r0), cudaMemcpyHostToDevice) != cudaSuccess) {
+		pot_gpu_destroy(c);
+		return POT_E_CUDA;
+	}
+	*out = c;
+	return POT_OK;
+}
+
+static int set_rec_from_grain(pot_gpu_ctx* c, const pot_grain_state* g, const double4& g_pos, const double4& g_vel)
+{
+	RunRec r;
+	std::memset(&r, 0, sizeof(r));
+	if (g) {
+		r.grain_q = g->q;
+		r.grain_m = g->m;
+		r.grain_pos[0] = g->x; r.grain_pos[1] = g->y; r.grain_pos[2] = g->z;
+		r.grain_vel[0] = g->vx; r.grain_vel[1] = g->vy; r.grain_vel[2] = g->vz;
+		r.tot_absor_e = g->tot_absor_e;
+		r.t_steps = g->t_steps;
+		r.chi_b = g->chi_b;
+	} else {
+		r.grain_q = 0;
+		r.grain_m = MASS_DUST;
+		r.grain_pos[0] = g_pos.x; r.grain_pos[1] = g_pos.y; r.grain_pos[2] = g_pos.z;
+		r.grain_vel[0] = g_vel.x; r.grain_vel[1] = g_vel.y; r.grain_vel[2] = g_vel.z;
+	}
+	r.grain_slot = 0xFFFFFFFFu;
+	CK(cudaMemcpyAsync(c->rec, &r, sizeof(r), cudaMemcpyHostToDevice, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	c->sticky = POT_OK;
+	return POT_OK;
+}
+
+int pot_gpu_upload(pot_gpu_ctx* c, const pot_particle* parts, uint64_t N, const pot_grain_state* grain)
+{
+	if (!c || !parts || N != c->cfg.N) return POT_E_ARG;
+	if (parts[0].species != SP_DUST) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	if (!c->aos) {
+		const int ra = dalloc(c, &c->aos, c->n);
+		if (ra) return ra;
+	}
+	CK(cudaMemcpyAsync(c->aos, parts, sizeof(pot_particle) * c->n, cudaMemcpyHostToDevice, c->stream));
+	c->cur = 0;
+	k_from_aos<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->aos, c->n, c->pos[0], c->vel[0], c->pid[0], c->rec);
+	CK(cudaGetLastError());
+	const double4 gp = make_double4(parts[0].x, parts[0].y, parts[0].z, 0.0);
+	const double4 gv = make_double4(parts[0].vx, parts[0].vy, parts[0].vz, 0.0);
+	int rc = set_rec_from_grain(c, grain, gp, gv);
+	if (rc) return rc;
+	c->uploaded = true;
+	c->tree_valid = false;
+	return POT_OK;
+}
+
+int pot_gpu_init_particles(pot_gpu_ctx* c)
+{
+	if (!c) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	RunRec r;
+	std::memset(&r, 0, sizeof(r));
+	r.grain_m = MASS_DUST;
+	r.grain_pos[0] = r.grain_pos[1] = r.grain_pos[2] = c->P.rad;
+	r.grain_slot = 0xFFFFFFFFu;
+	CK(cudaMemcpyAsync(c->rec, &r, sizeof(r), cudaMemcpyHostToDevice, c->stream));
+	c->cur = 0;
+	launch_init(c->pos[0], c->vel[0], c->pid[0], c->P, c->rec, c->stream, c->timer);
+	CK(cudaGetLastError());
+	c->sticky = POT_OK;
+	int st = sync_status(c);
+	if (st != POT_OK) return st;
+	c->uploaded = true;
+	c->tree_valid = false;
+	return POT_OK;
+}
+
+// Keys, sort, reorder (+ due flags) and tree for the current state.
+static void enqueue_tree(pot_gpu_ctx* c, int begin_step)
+{
+	Params& P = c->P;
+	cudaStream_t s = c->stream;
+	launch_keys(c->pos[c->cur], c->keys[0], c->vals[0], P, c->rec, begin_step, s, c->timer);
+	radix_sort_pairs(c->keys, c->vals, c->n, c->counts, c->block_sums, s, c->timer);
+	const int nx = c->cur ^ 1;
+	launch_reorder(c->vals[0], c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->pos[nx], c->vel[nx], c->pid[nx],
+	               c->src64, c->src32, c->due, P, c->rec, s, c->timer);
+	c->cur = nx;
+	launch_build(c->keys[0], c->T, c->src64, P, c->rec, c->block_sums, s, c->timer);
+}
+
+static void enqueue_step(pot_gpu_ctx* c)
+{
+	Params& P = c->P;
+	cudaStream_t s = c->stream;
+	enqueue_tree(c, 1);
+	compact_flags(c->due, c->n, c->due_list, c->block_sums, &c->rec->n_due, s, c->timer, c->due_prefix);
+	if (P.form == POT_FORM_FAST) launch_groups(c->T, c->due_prefix, c->groups, P, c->rec, s, c->timer);
+	launch_chi_b(c->T, c->src64, P, c->rec, 0, s, c->timer);
+	launch_push(c->pos[c->cur], c->vel[c->cur], c->T, c->src64, c->src32, c->due_list, c->groups, c->rein_list, P,
+	            c->rec, s, c->timer);
+	launch_absorb_late(c->pos[c->cur], c->vel[c->cur], c->src64, c->due_list, c->rein_list, P, c->rec, s, c->timer);
+	launch_reinject(c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->rein_list, P, c->rec, s, c->timer);
+	launch_grain_end(c->pos[c->cur], c->vel[c->cur], c->hist, P, c->rec, s, c->timer);
+}
+
+int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats* out)
+{
+	(void)flags;
+	if (!c) return POT_E_ARG;
+	if (!c->uploaded) return POT_E_STATE;
+	if (c->sticky != POT_OK) return c->sticky;
+	CK(cudaSetDevice(c->device));
+	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c);
+	CK(cudaGetLastError());
+	c->tree_valid = true;
+	const int st = sync_status(c);
+	if (out) {
+		RunRec r;
+		CK(cudaMemcpy(&r, c->rec, sizeof(r), cudaMemcpyDeviceToHost));
+		StepHist h;
+		CK(cudaMemcpy(&h, &c->hist[r.t_steps % HIST], sizeof(h), cudaMemcpyDeviceToHost));
+		std::memset(out, 0, sizeof(*out));
+		out->t_steps = r.t_steps;
+		out->grain_q = r.grain_q;
+		out->dq = h.dq;
+		out->de = h.de;
+		out->n_absorbed = h.n_absorbed;
+		out->n_reinjected = h.n_reinjected;
+		out->n_pushed = h.n_pushed;
+		out->interactions = h.interactions;
+		out->n_nodes = h.n_nodes;
+		out->chi_b = r.chi_b;
+		out->status = r.status;
+	}
+	return st;
+}
+
+int pot_gpu_step_async(pot_gpu_ctx* c, uint32_t nsteps)
+{
+	if (!c) return POT_E_ARG;
+	if (!c->uploaded) return POT_E_STATE;
+	if (c->sticky != POT_OK) return c->sticky;
+	CK(cudaSetDevice(c->device));
+	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c);
+	CK(cudaGetLastError());
+	c->tree_valid = true;
+	return POT_OK;
+}
+
+int pot_gpu_download(pot_gpu_ctx* c, pot_particle* parts, pot_grain_state* grain)
+{
+	if (!c) return POT_E_ARG;
+	if (!c->uploaded) return POT_E_STATE;
+	CK(cudaSetDevice(c->device));
+	if (parts) {
+		if (!c->aos) {
+			const int ra = dalloc(c, &c->aos, c->n);
+			if (ra) return ra;
+		}
+		k_to_aos<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->n,
+		                                                   c->aos);
+		CK(cudaGetLastError());
+		CK(cudaMemcpyAsync(parts, c->aos, sizeof(pot_particle) * c->n, cudaMemcpyDeviceToHost, c->stream));
+	}
+	RunRec r;
+	CK(cudaMemcpyAsync(&r, c->rec, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	if (grain) {
+		grain->q = r.grain_q;
+		grain->m = r.grain_m;
+		grain->x = r.grain_pos[0]; grain->y = r.grain_pos[1]; grain->z = r.grain_pos[2];
+		grain->vx = r.grain_vel[0]; grain->vy = r.grain_vel[1]; grain->vz = r.grain_vel[2];
+		grain->tot_absor_e = r.tot_absor_e;
+		grain->t_steps = r.t_steps;
+		grain->chi_b = r.chi_b;
+	}
+	return r.status;
+}
+
+int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_grain_state* grain,
+                           pot_step_stats* out)
+{
+	int rc = pot_gpu_upload(c, parts, N, grain);
+	if (rc) return rc;
+	rc = pot_gpu_step(c, 1, 0, out);
+	if (rc) return rc;
+	return pot_gpu_download(c, parts, grain);
+}
+
+int pot_gpu_build_tree(pot_gpu_ctx* c, uint64_t* n_nodes)
+{
+	if (!c) return POT_E_ARG;
+	if (!c->uploaded) return POT_E_STATE;
+	CK(cudaSetDevice(c->device));
+	enqueue_tree(c, 0);
+	CK(cudaGetLastError());
+	const int st = sync_status(c);
+	if (n_nodes) {
+		unsigned int m = 0;
+		CK(cudaMemcpy(&m, &c->rec->n_nodes, sizeof(m), cudaMemcpyDeviceToHost));
+		*n_nodes = m;
+	}
+	c->tree_valid = st == POT_OK;
+	return st;
+}
+
+int pot_gpu_tree_dump(pot_gpu_ctx* c, uint64_t max_nodes, uint64_t* n_int, int32_t* int_level, uint64_t* int_path,
+                      int32_t* int_q, uint32_t* int_aq, double* int_c, double* int_w, uint64_t* n_leaf,
+                      uint32_t* leaf_part, int32_t* leaf_level, uint64_t* leaf_path)
+{
+	if (!c || !n_int || !n_leaf) return POT_E_ARG;
+	if (!c->tree_valid) return POT_E_STATE;
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	unsigned int M = 0;
+	CK(cudaMemcpy(&M, &c->rec->n_nodes, sizeof(M), cudaMemcpyDeviceToHost));
+	std::vector<uint64_t> keys;
+	std::vector<uint32_t> first, pid;
+	std::vector<uint8_t> level;
+	std::vector<int32_t> child, q;
+	std::vector<uint32_t> aq;
+	std::vector<double4> cq;
+	std::vector<double> w2;
+	std::vector<uint2> lrange;
+	int rc;
+	if ((rc = fetch(keys, c->keys[0], c->n)) || (rc = fetch(first, c->T.first, M)) ||
+	    (rc = fetch(pid, c->pid[c->cur], c->n)) || (rc = fetch(level, c->T.level, M)) ||
+	    (rc = fetch(child, c->T.child, 8ull * M)) || (rc = fetch(q, c->T.q, M)) || (rc = fetch(aq, c->T.aq, M)) ||
+	    (rc = fetch(cq, c->T.cq, M)) || (rc = fetch(w2, c->T.w2, M)))
+		return rc;
+	if (c->P.leaf_size > 1 && (rc = fetch(lrange, c->T.lrange, 8ull * M))) return rc;
+	std::vector<uint2> ovf;
+	if (c->P.leaf_size == 1 && (rc = fetch(ovf, c->T.ovf, (size_t)OVF_CAP))) return rc;
+	uint64_t ni = 0, nl = 0;
+	for (uint32_t k = 0; k < M; k++) {
+		const int l = level[k];
+		const uint64_t pfx = l == 0 ? 0ull : keys[first[k]] >> (63 - 3 * l);
+		if (ni >= max_nodes) return POT_E_ARG;
+		if (int_level) int_level[ni] = l;
+		if (int_path) int_path[ni] = pfx;
+		if (int_q) int_q[ni] = q[k];
+		if (int_aq) int_aq[ni] = aq[k];
+		if (int_c) {
+			int_c[3 * ni] = cq[k].x;
+			int_c[3 * ni + 1] = cq[k].y;
+			int_c[3 * ni + 2] = cq[k].z;
+		}
+		if (int_w) int_w[ni] = std::sqrt(w2[k]);
+		ni++;
+		for (int d = 0; d < 8; d++) {
+			const int32_t code = child[8ull * k + d];
+			if (code >= CH_EMPTY) continue;
+			const uint32_t e = leaf_payload(code);
+			uint32_t s0 = e, cnt = 1;
+			if (c->P.leaf_size > 1) {
+				s0 = lrange[e].x;
+				cnt = lrange[e].y;
+			} else if (e >= c->n) {
+				s0 = ovf[e - c->n].x;
+				cnt = ovf[e - c->n].y;
+			}
+			for (uint32_t j = 0; j < cnt; j++) {
+				if (nl >= max_nodes) return POT_E_ARG;
+				if (leaf_part) leaf_part[nl] = pid[s0 + j];
+				if (leaf_level) leaf_level[nl] = l + 1;
+				if (leaf_path) leaf_path[nl] = (pfx << 3) | (uint64_t)d;
+				nl++;
+			}
+		}
+	}
+	*n_int = ni;
+	*n_leaf = nl;
+	return POT_OK;
+}
+
+static int ensure_query(pot_gpu_ctx* c, size_t n)
+{
+	if (n <= c->q_cap) return POT_OK;
+	for (void* p : { (void*)c->q_xyz, (void*)c->q_out, (void*)c->q_idx, (void*)c->q_slot }) {
+		if (!p) continue;
+		for (auto& a : c->allocs)
+			if (a == p) a = nullptr;
+		cudaFree(p);
+	}
+	int rc;
+	if ((rc = dalloc(c, &c->q_xyz, 3 * n)) || (rc = dalloc(c, &c->q_out, 3 * n)) || (rc = dalloc(c, &c->q_idx, n)) ||
+	    (rc = dalloc(c, &c->q_slot, n)))
+		return rc;
+	c->q_cap = n;
+	return POT_OK;
+}
+
+int pot_gpu_field_at(pot_gpu_ctx* c, uint64_t n, const uint32_t* idx, const double* xyz, double* E)
+{
+	if (!c || !idx || !xyz || !E) return POT_E_ARG;
+	if (!c->tree_valid) return POT_E_STATE;
+	if (n == 0) return POT_OK;
+	CK(cudaSetDevice(c->device));
+	int rc = ensure_query(c, n);
+	if (rc) return rc;
+	CK(cudaMemcpyAsync(c->q_xyz, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+	CK(cudaMemcpyAsync(c->q_idx, idx, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
+	k_inverse<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->pid[c->cur], c->n, c->inv);
+	k_map_slots<<<nblk(n, 256), 256, 0, c->stream>>>(c->inv, c->q_idx, (uint32_t)n, c->n, c->q_slot);
+	launch_field_query(c->T, c->src64, c->src32, c->q_xyz, c->q_slot, (uint32_t)n, c->q_out, c->P, c->rec,
+	                   c->stream, c->timer);
+	CK(cudaGetLastError());
+	CK(cudaMemcpyAsync(E, c->q_out, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+	return sync_status(c);
+}
+
+int pot_gpu_phi_at(pot_gpu_ctx* c, uint64_t n, const double* xyz, double* phi)
+{
+	if (!c || !xyz || !phi) return POT_E_ARG;
+	if (!c->tree_valid) return POT_E_STATE;
+	if (n == 0) return POT_OK;
+	CK(cudaSetDevice(c->device));
+	int rc = ensure_query(c, n);
+	if (rc) return rc;
+	CK(cudaMemcpyAsync(c->q_xyz, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+	launch_phi_query(c->T, c->src64, c->q_xyz, (uint32_t)n, c->q_out, c->P, c->rec, c->stream, c->timer);
+	CK(cudaGetLastError());
+	CK(cudaMemcpyAsync(phi, c->q_out, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+	return sync_status(c);
+}
+
+int pot_gpu_kernel_times(pot_gpu_ctx* c, int max, const char** names, double* ms, uint64_t* launches)
+{
+	if (!c) return POT_E_ARG;
+	c->timer.resolve();
+	return c->timer.report(max, names, ms, launches);
+}
+
+int pot_gpu_reset_kernel_times(pot_gpu_ctx* c)
+{
+	if (!c) return POT_E_ARG;
+	CK(cudaStreamSynchronize(c->stream));
+	c->timer.reset();
+	return POT_OK;
+}
+
+int pot_gpu_launch_count(pot_gpu_ctx* c, uint64_t* n)
+{
+	if (!c || !n) return POT_E_ARG;
+	*n = c->timer.launches;
+	return POT_OK;
+}
+
+int pot_gpu_sync(pot_gpu_ctx* c)
+{
+	if (!c) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	return sync_status(c);
+}
+
+}  // extern "C"

@@ -1,0 +1,327 @@
+// Initial injection and boundary reinjection on the device.
+//
+// Each (re)injected particle draws from its own Philox4x32-10 stream keyed
+// by (run seed, original particle index, step, attempt), so the result does
+// not depend on thread scheduling or on which other particles are reinjected
+// in the same step.  The samplers are the reference's:
+//   * inject (pot.c:658-765, spherical domain): uniform in the shell
+//     a < r < R at start (cube-root transform), on the sphere r = R at
+//     reinjection with the inward radial velocity component, Maxwellian
+//     components, drift added along x;
+//   * sceptically_reinject (pot.c:496-652): flux-weighted drifting
+//     Maxwellian at infinity through the inverse CDFs of Hutchinson 2003
+//     (prng.c:138-214, Newton), entry point on the sphere from the OML orbit
+//     angle alpha (integrate_for_alpha, pot.c:433-492).
+// Every loop that the reference leaves unbounded (Newton iterations, the
+// u^2 < chi_b rejection, the retry on NaN alpha) has a cap here; reaching one
+// sets POT_E_ITER and leaves the particle at a valid boundary state.
+#include "pot_tree.cuh"
+
+namespace pot {
+
+constexpr int NEWTON_CAP = 200;
+constexpr int REJECT_CAP = 10000;
+constexpr int RETRY_CAP = 1000;
+constexpr int SIMPSON_CAP = 100000;
+
+__device__ double d_u_no_flow_icdf(double chi, double q, bool& ok)
+{
+	const double omc = 1.0 - chi;
+	double u = 1.29951, p;
+	int it = 0;
+	do {
+		const double usq = u * u;
+		p = 1.0 - ((usq + omc) * exp(-usq) / omc) - q;
+		u -= p / (2.0 * u * exp(-usq) * (chi - usq) / -omc);
+	} while ((p * p) > 1e-16 && ++it < NEWTON_CAP);
+	if (it >= NEWTON_CAP) ok = false;
+	return u;
+}
+
+__device__ double d_u_icdf(double U, double chi, double q, bool& ok)
+{
+	const double Usq = U * U;
+	const double psi = SQRT_PI_REF * (1.0 + (2.0 * (Usq - chi))) / 2.0;
+	const double p_den = 2.0 * ((U * exp(-Usq)) + (psi * erf(U)));
+	const double dp_den = 2.0 * SQRT_PI_REF * (U + (psi * exp(Usq) * erf(U)));
+	double u = (U > 2.1) ? U + (1.0 / U) : 1.2586147 + (0.221 * U) + (0.1903312 * U * U);
+	double p;
+	int it = 0;
+	do {
+		const double usq = u * u;
+		const double temp = -(U + u) * (U + u);
+		double p_num = (U - u) * exp(temp);
+		p_num += (U + u) * exp((4.0 * U * u) + temp);
+		p_num += psi * (erf(U - u) + erf(U + u));
+		p = 1.0 - (p_num / p_den) - q;
+		double dp_num = (SQRT_PI_REF * (1.0 + (2.0 * (Usq - usq)))) - (2.0 * psi);
+		dp_num *= exp(-u * ((2.0 * U) + u)) - exp((2.0 * U * u) - usq);
+		u -= p / (dp_num / dp_den);
+	} while ((p * p) > 1e-16 && ++it < NEWTON_CAP);
+	if (it >= NEWTON_CAP) ok = false;
+	return u;
+}
+
+__device__ double d_integrate_for_alpha(double s, double chi_b, double u2, double Rol, bool& ok)
+{
+	const double chu2 = chi_b / u2;
+	const double s2 = s * s;
+	const double y_one = s / sqrt(1.0 - chu2 - s2);
+	double alpha = 0.0;
+	double xi0 = 0.0, xi1, xi2, y0 = s, y1, y2;
+	int guard = 0;
+	if (s == 0.0) return 0.0;
+	do {
+		xi2 = 1.0;
+		y2 = y_one;
+		xi1 = (xi0 + xi2) / 2.0;
+		y1 = 1.0 - (chu2 * xi1 * exp(Rol * (1.0 - (1.0 / xi1))));
+		y1 = 1.0 / sqrt((y1 / s2) - (xi1 * xi1));
+		while (fabs(y2 - y1 - (y1 - y0)) > 0.01) {
+			xi2 = xi1;
+			y2 = y1;
+			xi1 = (xi0 + xi2) / 2.0;
+			y1 = 1.0 - (chu2 * xi1 * exp(Rol * (1.0 - (1.0 / xi1))));
+			y1 = 1.0 / sqrt((y1 / s2) - (xi1 * xi1));
+			if (++guard > SIMPSON_CAP) { ok = false; return 0.0; }
+		}
+		alpha += (xi2 - xi0) * (y0 + (4.0 * y1) + y2) / 6.0;
+		xi0 = xi2;
+		y0 = y2;
+		if (++guard > SIMPSON_CAP) { ok = false; return 0.0; }
+	} while (xi2 < 1.0);
+	return alpha;
+}
+
+// rotate_vec_about_xy_dir, coord.c:22-37
+__device__ __forceinline__ void rot_xy(double d0, double d1, double s, double c, double& x, double& y, double& z,
+                                       double offset)
+{
+	const double omc = 1.0 - c;
+	double t0 = d0 * ((d0 * x) + (d1 * y)) * omc;
+	t0 += (x * c) + (d1 * z * s);
+	double t1 = d1 * ((d0 * x) + (d1 * y)) * omc;
+	t1 += (y * c) - (d0 * z * s);
+	double t2 = z * c;
+	t2 += ((d0 * y) - (d1 * x)) * s;
+	x = offset + t0;
+	y = offset + t1;
+	z = offset + t2;
+}
+
+// velocity_in_cartesian_coords, coord.c:6-14
+__device__ __forceinline__ void vel_cart(double v0, double v1, double v2, double phi, double theta, double& vx,
+                                         double& vy, double& vz)
+{
+	double sp, cp, st, ct;
+	sincos(phi, &sp, &cp);
+	sincos(theta, &st, &ct);
+	vx = (v0 * cp * st) - (v1 * sp) + (v2 * cp * ct);
+	vy = (v0 * sp * st) + (v1 * cp) + (v2 * sp * ct);
+	vz = (v0 * ct) - (v2 * st);
+}
+
+// nrv_pair, prng.c:32-47
+__device__ __forceinline__ void nrv_pair(Stream& st, double sd, double& a, double& b)
+{
+	const double urv2 = st.rnd(1.0);
+	double urv1;
+	int guard = 0;
+	do {
+		urv1 = st.rnd(1.0);
+	} while (urv1 == 0.0 && ++guard < 64);
+	const double r = sqrt(-2.0 * log(urv1));
+	const double theta = 2.0 * PI_REF * urv2;
+	double s, c;
+	sincos(theta, &s, &c);
+	a = sd * r * c;
+	b = sd * r * s;
+}
+
+// sceptically_reinject, pot.c:496-652
+__device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Params& P, double4& p, double4& v,
+                                 bool& ok)
+{
+	const double v_n = sp == SP_E ? P.vn_e : P.vn_i;
+	double chi_b = chi_b_in;
+	double u_mag = 0.0, u2 = 0.0, cz = 0.0, b = 0.0, alpha = 0.0, u[3];
+	for (int attempt = 0;; attempt++) {
+		chi_b = chi_b_in;
+		if (sp == SP_E) chi_b *= -P.Ti / P.Te;
+		if (P.x_drift != 0.0) {
+			const double U = P.x_drift / v_n;
+			int k = 0;
+			do {
+				u_mag = d_u_icdf(U, chi_b, st.rnd(1.0), ok);
+				u2 = u_mag * u_mag;
+			} while (u2 < chi_b && ++k < REJECT_CAP);
+			if (k >= REJECT_CAP) ok = false;
+			const double q = st.rnd(1.0);
+			cz = log(q + (1.0 - q) * exp(-4.0 * u_mag * U)) / (2.0 * u_mag * U);
+			cz += 1.0;
+		} else {
+			int k = 0;
+			do {
+				u_mag = d_u_no_flow_icdf(chi_b, st.rnd(1.0), ok);
+				u2 = u_mag * u_mag;
+			} while (u2 < chi_b && ++k < REJECT_CAP);
+			if (k >= REJECT_CAP) ok = false;
+			cz = st.rnd(2.0) - 1.0;
+		}
+		u[0] = 0.0;
+		u[1] = 0.0;
+		u[2] = u_mag;
+		rot_xy(0.0, 1.0, cz, sqrt(1.0 - (cz * cz)), u[0], u[1], u[2], 0.0);
+		const double psi = st.rnd(2.0 * PI_REF);
+		double sps, cps;
+		sincos(psi, &sps, &cps);
+		rot_xy(1.0, 0.0, sps, cps, u[0], u[1], u[2], 0.0);
+		b = sqrt(st.rnd(1.0 - (chi_b / u2)));
+		alpha = d_integrate_for_alpha(b, chi_b, u2, P.Rol, ok);
+		if (!isnan(alpha) || attempt + 1 >= RETRY_CAP) break;
+	}
+	if (isnan(alpha)) {
+		ok = false;
+		alpha = 0.0;
+	}
+	const double phi = st.rnd(2.0 * PI_REF);
+	double sa, ca, sph, cph;
+	sincos(alpha, &sa, &ca);
+	sincos(phi, &sph, &cph);
+	double x = P.mpp * P.r_pix * sa * cph;
+	double y = P.mpp * P.r_pix * sa * sph;
+	double z = P.mpp * P.r_pix * ca;
+	const double nrm = sqrt((u[0] * u[0]) + (u[1] * u[1]));
+	const double a0 = u[1] / nrm, a1 = -u[0] / nrm;
+	const double co_z = u[2] / u_mag;
+	const double si_z = sin(acos(co_z));
+	rot_xy(a0, a1, si_z, co_z, x, y, z, P.mpp * P.r_pix);
+	const double vz_ = u_mag * b;
+	const double vr = -sqrt(u2 - chi_b - (vz_ * vz_));
+	double vx, vy, vz;
+	vel_cart(vr, 0.0, vz_, phi, alpha, vx, vy, vz);
+	rot_xy(a0, a1, si_z, co_z, vx, vy, vz, 0.0);
+	p = make_double4(x, y, z, p.w);
+	v = make_double4(vx * v_n, vy * v_n, vz * v_n, 0.0);
+}
+
+// inject, pot.c:658-765 (spherical domain, grain enabled)
+__device__ void inject(Stream& st, int sp, bool reinjection, double chi_b, const Params& P, double4& p, double4& v,
+                       bool& ok)
+{
+	double sigma = sp == SP_ION ? P.sigma_i : P.sigma_e;
+	const bool sceptic = (P.flags & FLAG_SCEPTIC) != 0;
+	if (!sceptic && !reinjection) sigma *= 0.85;
+	double r;
+	if (!reinjection) {
+		const double rmax3 = (double)(P.r_pix * P.r_pix * P.r_pix);
+		r = P.mpp * cbrt(st.rnd(rmax3));
+		int guard = 0;
+		while (r <= P.a && ++guard < REJECT_CAP) r = P.mpp * cbrt(st.rnd(rmax3));
+		if (guard >= REJECT_CAP) ok = false;
+	} else {
+		r = P.mpp * P.r_pix;
+	}
+	if (sceptic && reinjection) {
+		sceptic_reinject(st, sp, chi_b, P, p, v, ok);
+		return;
+	}
+	const double phi = st.rnd(2.0 * PI_REF);
+	const double theta = acos(st.rnd(2.0) - 1.0);
+	double sth, cth, sph, cph;
+	sincos(theta, &sth, &cth);
+	sincos(phi, &sph, &cph);
+	const double c = P.mpp * P.r_pix;
+	p = make_double4(c + (r * sth * cph), c + (r * sth * sph), c + (r * cth), p.w);
+	double vx, vy, vz;
+	if (!reinjection) {
+		nrv_pair(st, sigma, vx, vy);
+		double d;
+		nrv_pair(st, sigma, d, vz);
+	} else {
+		double v0, v1, v2, d;
+		nrv_pair(st, sigma, v0, v1);
+		nrv_pair(st, sigma, d, v2);
+		if (v0 > 0.0) v0 = -v0;
+		vel_cart(v0, v1, v2, phi, theta, vx, vy, vz);
+	}
+	v = make_double4(vx + P.x_drift, vy, vz, 0.0);
+}
+
+__device__ __forceinline__ bool outside_sphere(const double4& p, const Params& P)
+{
+	return sqrt(dsq3(dsub(p.x, P.rad), dsub(p.y, P.rad), dsub(p.z, P.rad))) > P.rad;
+}
+
+// Reinjection list entries: slot | reason << 30, reason 1 = absorbed by
+// the grain (reinjected, then tested against the boundary once more, as
+// pot.c:2676 followed by pot.c:2691), 2 = left the domain.
+__global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel, const uint32_t* __restrict__ pid,
+                           const uint32_t* __restrict__ list, Params P, RunRec* rec)
+{
+	if (rec->status != POT_OK) return;
+	const uint32_t n = rec->n_rein;
+	const uint32_t t = (uint32_t)rec->t_steps;
+	const double chi_b = rec->chi_b;
+	for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+		const uint32_t w = list[e];
+		const uint32_t s = w & 0x3FFFFFFFu;
+		const uint32_t reason = w >> 30;
+		const uint32_t id = pid[s];
+		double4 p = pos[s];
+		double4 v = vel[s];
+		const int sp = (int)p.w;
+		bool ok = true;
+		uint32_t attempt = 0;
+		Stream st;
+		st.init(P.seed, id, t, 0x10000u | attempt++);
+		inject(st, sp, true, chi_b, P, p, v, ok);
+		if ((reason & 1u) && outside_sphere(p, P)) {
+			st.init(P.seed, id, t, 0x10000u | attempt++);
+			inject(st, sp, true, chi_b, P, p, v, ok);
+		}
+		if (!ok) set_status(rec, POT_E_ITER);
+		pos[s] = p;
+		vel[s] = v;
+	}
+}
+
+// init_particles for one rank (pot.c:887-935), reference order: slot i holds
+// particle i.
+__global__ void k_init(double4* __restrict__ pos, double4* __restrict__ vel, uint32_t* __restrict__ pid, Params P,
+                       RunRec* rec)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= P.n_total) return;
+	pid[i] = i;
+	if (i == 0) {
+		pos[0] = make_double4(P.rad, P.rad, P.rad, (double)SP_DUST);
+		vel[0] = make_double4(0.0, 0.0, 0.0, 0.0);
+		return;
+	}
+	const int sp = species_of_id(i, P.n_ions);
+	double4 p = make_double4(0.0, 0.0, 0.0, (double)sp), v;
+	bool ok = true;
+	Stream st;
+	st.init(P.seed, i, 0u, 0x20000u);
+	inject(st, sp, false, 0.0, P, p, v, ok);
+	if (!ok) set_status(rec, POT_E_ITER);
+	pos[i] = p;
+	vel[i] = v;
+}
+
+void launch_reinject(double4* pos, double4* vel, const uint32_t* pid, const uint32_t* rein_list,
+                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+{
+	ScopedKernel k(tm, "reinject");
+	k_reinject<<<148, 64, 0, s>>>(pos, vel, pid, rein_list, P, rec);
+}
+
+void launch_init(double4* pos, double4* vel, uint32_t* pid, const Params& P, RunRec* rec, cudaStream_t s,
+                 Timer& tm)
+{
+	ScopedKernel k(tm, "init");
+	k_init<<<(P.n_total + 127) / 128, 128, 0, s>>>(pos, vel, pid, P, rec);
+}
+
+}  // namespace pot

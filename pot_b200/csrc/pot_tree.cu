@@ -1,0 +1,399 @@
+// Morton keys, per-step reorder, octree build and upward moments.
+//
+// Topology.  The reference inserts particles one by one into a pointer
+// octree whose root is [0, 2 r mpp]^3 and whose cells split at the midpoint
+// (x1 + x2) / 2 of their faces until every leaf holds one particle
+// (pot.c:1457-1643).  The final tree does not depend on insertion order: a
+// cell is internal exactly when two or more particles lie in it.  So it is
+// rebuilt here from sorted keys:
+//   * key = 21 levels x 3 bits of the comparisons `x < mid` the reference's
+//     descent makes (pot.c:1522-1553), computed with the same midpoint
+//     arithmetic, so cell membership is bit-identical;
+//   * with keys sorted, the cell of level l containing particle i holds
+//     more than L particles iff keys i and i + L share its 3l-bit prefix;
+//     pair i = (i, i + L) "owns" the cells whose first particle is i, i.e.
+//     the levels (lvl[i-1], lvl[i]], which numbers cells in pre-order;
+//   * a cell's last particle and its 8 children are found by binary search
+//     over its key range.
+// Leaf size L = 1 reproduces the reference's tree; L > 1 gives bucket leaves.
+//
+// Moments.  Net charge q, absolute charge aq and the |q|-weighted centre of
+// a cell are the reference's running update over its children in the
+// member order gxlylz, gxlygz, lxlylz, lxlygz, lxgylz, lxgygz, gxgylz, gxgygz
+// (pot.c:1290-1402), evaluated bottom-up with arrival counters and unfused
+// double operations, which makes them bit-identical too.
+#include "pot_tree.cuh"
+
+namespace pot {
+
+// 63-bit key: level 1 in bits 62..60, digit = gx << 2 | gy << 1 | gz.
+__device__ __forceinline__ uint64_t morton_key(double x, double y, double z, double w)
+{
+	double lx = 0.0, hx = w, ly = 0.0, hy = w, lz = 0.0, hz = w;
+	uint64_t key = 0;
+#pragma unroll 3
+	for (int l = 0; l < MAX_LEVELS; l++) {
+		const double mx = dmul(dadd(lx, hx), 0.5);
+		const double my = dmul(dadd(ly, hy), 0.5);
+		const double mz = dmul(dadd(lz, hz), 0.5);
+		const uint32_t bx = (x < mx) ? 0u : 1u;
+		const uint32_t by = (y < my) ? 0u : 1u;
+		const uint32_t bz = (z < mz) ? 0u : 1u;
+		if (bx) lx = mx; else hx = mx;
+		if (by) ly = my; else hy = my;
+		if (bz) lz = mz; else hz = mz;
+		key = (key << 3) | (uint64_t)((bx << 2) | (by << 1) | bz);
+	}
+	return key;
+}
+
+__global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ keys,
+                       uint32_t* __restrict__ vals, Params P, RunRec* rec, int begin_step)
+{
+	if (begin_step && blockIdx.x == 0 && threadIdx.x == 0) {
+		const unsigned long long t = rec->t_steps + 1;
+		rec->t_steps = t;
+		rec->n_due = 0;
+		rec->n_rein = 0;
+		rec->n_nodes = 0;
+		rec->work_ctr = 0;
+		rec->grain_due = (t % P.tss[SP_DUST]) == 0 ? 1u : 0u;
+		rec->dq = 0;
+		rec->de = 0;
+		rec->nabs_ion = 0;
+		rec->nabs_e = 0;
+		for (int k = 0; k < 3; k++) { rec->sumv_ion[k] = 0; rec->sumv_e[k] = 0; }
+		rec->interactions = 0;
+		rec->n_pushed = 0;
+		rec->grain_slot = 0xFFFFFFFFu;
+	}
+	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= P.n) return;
+	const double4 p = pos[s];
+	if (isnan(p.x) || isnan(p.y) || isnan(p.z)) {
+		set_status(rec, POT_E_NONFINITE);
+	} else if (p.x < 0.0 || p.x > P.root_w || p.y < 0.0 || p.y > P.root_w || p.z < 0.0 || p.z > P.root_w) {
+		set_status(rec, POT_E_DOMAIN);  // build_tree returns NULL, pot.c:1491-1500
+	}
+	keys[s] = morton_key(p.x, p.y, p.z, P.root_w);
+	vals[s] = s;
+}
+
+// Gather the state into the new Morton order, write the tree sources and
+// mark the particles due this step (electrons every step, ions every
+// tss[ION] steps, the grain every tss[DUST] steps, pot.c:2430-2434).
+__global__ void k_reorder(const uint32_t* __restrict__ perm, const double4* __restrict__ pos_in,
+                          const double4* __restrict__ vel_in, const uint32_t* __restrict__ pid_in,
+                          double4* __restrict__ pos_out, double4* __restrict__ vel_out,
+                          uint32_t* __restrict__ pid_out, double4* __restrict__ src64,
+                          float4* __restrict__ src32, uint8_t* __restrict__ due, Params P, RunRec* rec)
+{
+	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= P.n) return;
+	const uint32_t j = perm[s];
+	const double4 p = pos_in[j];
+	const double4 v = vel_in[j];
+	const uint32_t id = pid_in[j];
+	const int sp = (int)p.w;
+	const double q = sp == SP_DUST ? (double)rec->grain_q : (sp == SP_ION ? 1.0 : -1.0);
+	pos_out[s] = p;
+	vel_out[s] = v;
+	pid_out[s] = id;
+	src64[s] = make_double4(p.x, p.y, p.z, q);
+	if (src32) {
+		src32[s] = make_float4((float)((p.x - P.rad) * P.inv_rad), (float)((p.y - P.rad) * P.inv_rad),
+		                       (float)((p.z - P.rad) * P.inv_rad), (float)q);
+	}
+	due[s] = (rec->t_steps % P.tss[sp]) == 0 ? 1 : 0;
+	if (sp == SP_DUST) rec->grain_slot = s;
+}
+
+__device__ __forceinline__ int lcp_levels(uint64_t a, uint64_t b)
+{
+	const uint64_t x = a ^ b;
+	if (x == 0) return MAX_LEVELS;
+	return (__clzll((long long)x) - 1) / 3;
+}
+
+// lvl8[i] = common levels of keys i and i + L (capped at 20: a level-21
+// cell cannot split); cnt[i] = number of cells pair i owns.
+__global__ void k_pairs(const uint64_t* __restrict__ keys, const double4* __restrict__ src64, uint32_t n,
+                        uint32_t n_pairs, uint32_t L, int8_t* __restrict__ lvl8, uint32_t* __restrict__ cnt,
+                        RunRec* rec)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	// Two particles at one position: the reference's insertion would split
+	// forever (pot.c:1466-1470) or fail at a reallocation (pot.c:1578-1586).
+	if (i + 1 < n && keys[i] == keys[i + 1]) {
+		const double4 a = src64[i], b = src64[i + 1];
+		if (a.x == b.x && a.y == b.y && a.z == b.z) set_status(rec, POT_E_COINCIDENT);
+	}
+	if (i >= n_pairs) return;
+	const int li = lcp_levels(keys[i], keys[i + L]);
+	if (li == MAX_LEVELS) atomicOr(&rec->warn, 1u);
+	const int hi = li < MAX_LEVELS - 1 ? li : MAX_LEVELS - 1;
+	int prev = -1;
+	if (i > 0) {
+		const int lp = lcp_levels(keys[i - 1], keys[i - 1 + L]);
+		prev = lp < MAX_LEVELS - 1 ? lp : MAX_LEVELS - 1;
+	}
+	lvl8[i] = (int8_t)hi;
+	cnt[i] = hi > prev ? (uint32_t)(hi - prev) : 0u;
+}
+
+__global__ void k_fill_nodes(const int8_t* __restrict__ lvl8, const uint32_t* __restrict__ base,
+                             uint32_t n_pairs, TreeDev T, RunRec* rec)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n_pairs) return;
+	const int hi = lvl8[i];
+	const int lo = i == 0 ? 0 : lvl8[i - 1] + 1;
+	for (int l = lo; l <= hi; l++) {
+		const uint32_t k = base[i] + (uint32_t)(l - lo);
+		if (k >= T.cap) {
+			set_status(rec, POT_E_CAPACITY);
+			return;
+		}
+		T.first[k] = i;
+		T.level[k] = (uint8_t)l;
+	}
+}
+
+// first index in [a, b) whose child digit at `shift` is >= c (digits are
+// non-decreasing over a cell's sorted key range)
+__device__ __forceinline__ uint32_t lower_digit(const uint64_t* __restrict__ keys, uint32_t a, uint32_t b,
+                                                int shift, uint32_t c)
+{
+	while (a < b) {
+		const uint32_t m = a + ((b - a) >> 1);
+		if (((keys[m] >> shift) & 7u) < c) a = m + 1; else b = m;
+	}
+	return a;
+}
+
+__global__ void k_finish_nodes(const uint64_t* __restrict__ keys, uint32_t n, uint32_t L,
+                               const int8_t* __restrict__ lvl8, const uint32_t* __restrict__ base,
+                               TreeDev T, Params P, RunRec* rec)
+{
+	const uint32_t M = rec->n_nodes;
+	if (M > T.cap) {
+		if (blockIdx.x == 0 && threadIdx.x == 0) set_status(rec, POT_E_CAPACITY);
+		return;
+	}
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+		const uint32_t f = T.first[k];
+		const int l = T.level[k];
+		const int shift = 63 - 3 * l;
+		const uint64_t pfx = keys[f] >> shift;
+		// last particle of the cell: gallop, then bisect
+		uint32_t good = f, step = 1, probe = f + 1;
+		while (probe < n && (keys[probe] >> shift) == pfx) {
+			good = probe;
+			step <<= 1;
+			probe = f + step;
+		}
+		uint32_t a = good + 1, b = probe < n ? probe : n;
+		while (a < b) {
+			const uint32_t m = a + ((b - a) >> 1);
+			if ((keys[m] >> shift) == pfx) a = m + 1; else b = m;
+		}
+		const uint32_t last = a - 1;
+		T.last[k] = last;
+		// children by digit at the next level
+		const int cshift = shift - 3;
+		uint32_t s[9];
+		s[0] = f;
+		s[8] = last + 1;
+#pragma unroll
+		for (int c = 1; c < 8; c++) s[c] = lower_digit(keys, s[c - 1], last + 1, cshift, (uint32_t)c);
+		int nint = 0;
+#pragma unroll
+		for (int c = 0; c < 8; c++) {
+			const uint32_t cnt = s[c + 1] - s[c];
+			int32_t code;
+			if (cnt == 0) {
+				code = CH_EMPTY;
+			} else if (cnt <= L || l + 1 >= MAX_LEVELS) {
+				if (L == 1 && cnt == 1) {
+					code = leaf_code(s[c]);
+				} else if (L == 1) {
+					const uint32_t j = atomicAdd(&rec->n_overflow, 1u);
+					atomicOr(&rec->warn, 1u);
+					if (j < OVF_CAP) {
+						T.ovf[j] = make_uint2(s[c], cnt);
+						code = leaf_code(n + j);
+					} else {
+						set_status(rec, POT_E_CAPACITY);
+						code = CH_EMPTY;
+					}
+				} else {
+					const uint32_t e = 8u * k + (uint32_t)c;
+					code = leaf_code(e);
+					T.lrange[e] = make_uint2(s[c], cnt);
+				}
+			} else {
+				const uint32_t sc = s[c];
+				const int lo = sc == 0 ? 0 : lvl8[sc - 1] + 1;
+				const uint32_t kc = base[sc] + (uint32_t)(l + 1 - lo);
+				if (sc + L >= n || kc >= M || kc <= k) {
+					// cannot happen for a consistent key order; never write out of range
+					set_status(rec, POT_E_CAPACITY);
+					code = CH_EMPTY;
+				} else {
+					code = (int32_t)kc;
+					T.parent[kc] = (int32_t)k;
+					nint++;
+				}
+			}
+			T.child[8u * k + (uint32_t)c] = code;
+		}
+		T.nint[k] = (uint8_t)nint;
+		T.ctr[k] = 0;
+		if (k == 0) T.parent[0] = -1;
+		// x-extent of the cell by the reference's halving (pot.c:1262)
+		double lo = 0.0, hi = P.root_w;
+		for (int lev = 1; lev <= l; lev++) {
+			const uint32_t bit = (uint32_t)(pfx >> (3 * (l - lev) + 2)) & 1u;
+			const double mid = dmul(dadd(lo, hi), 0.5);
+			if (bit) lo = mid; else hi = mid;
+		}
+		const double w = dsub(hi, lo);
+		T.w2[k] = dmul(w, w);
+	}
+}
+
+// running |q|-weighted update of pot.c:1290-1310
+__device__ __forceinline__ void add_moment(int& q, uint32_t& aq, double& cx, double& cy, double& cz, int cq,
+                                           uint32_t caq, double ccx, double ccy, double ccz)
+{
+	const double a0 = (double)aq, a1 = (double)caq, den = (double)(aq + caq);
+	cx = ddiv(dadd(dmul(a0, cx), dmul(a1, ccx)), den);
+	cy = ddiv(dadd(dmul(a0, cy), dmul(a1, ccy)), den);
+	cz = ddiv(dadd(dmul(a0, cz), dmul(a1, ccz)), den);
+	q += cq;
+	aq += caq;
+}
+
+__global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec)
+{
+	const uint32_t M = rec->n_nodes;
+	if (M > T.cap) return;
+	const uint32_t L = P.leaf_size;
+	for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < M; k0 += gridDim.x * blockDim.x) {
+	if (T.nint[k0] != 0) continue;
+	uint32_t k = k0;
+	for (;;) {
+		int q = 0;
+		uint32_t aq = 0;
+		double cx = 0.0, cy = 0.0, cz = 0.0;
+		const float w_child = 0.5f * (float)(sqrt(T.w2[k]) * P.inv_rad);
+		for (int s = 0; s < 8; s++) {
+			const int d = slot_digit(s);
+			const int32_t code = T.child[8u * k + (uint32_t)d];
+			if (code == CH_EMPTY) continue;
+			int cq;
+			uint32_t caq;
+			double ccx, ccy, ccz;
+			if (code >= 0) {
+				cq = __ldcg(&T.q[code]);
+				caq = __ldcg(&T.aq[code]);
+				const double2* cp2 = reinterpret_cast<const double2*>(&T.cq[code]);
+				const double2 c01 = __ldcg(cp2), c23 = __ldcg(cp2 + 1);
+				const double4 c = make_double4(c01.x, c01.y, c23.x, c23.y);
+				ccx = c.x; ccy = c.y; ccz = c.z;
+			} else if (L == 1 && leaf_payload(code) < P.n) {
+				const double4 sp = src64[leaf_payload(code)];
+				cq = (int)sp.w;
+				caq = (uint32_t)abs(cq);
+				ccx = sp.x; ccy = sp.y; ccz = sp.z;
+			} else {
+				// bucket leaf: its own running moments over its particles
+				const uint32_t e = leaf_payload(code);
+				const uint2 r = L == 1 ? T.ovf[e - P.n] : T.lrange[e];
+				cq = 0;
+				caq = 0;
+				ccx = ccy = ccz = 0.0;
+				for (uint32_t j = r.x; j < r.x + r.y; j++) {
+					const double4 sp = src64[j];
+					const int pq = (int)sp.w;
+					const uint32_t paq = (uint32_t)abs(pq);
+					if (paq) add_moment(cq, caq, ccx, ccy, ccz, pq, paq, sp.x, sp.y, sp.z);
+				}
+				if (T.lf && L > 1) {
+					T.lf[e] = make_float4((float)((ccx - P.rad) * P.inv_rad), (float)((ccy - P.rad) * P.inv_rad),
+					                      (float)((ccz - P.rad) * P.inv_rad), (float)cq);
+					T.lr2[e] = w_child * w_child / P.oap2_f;
+				}
+			}
+			if (caq) add_moment(q, aq, cx, cy, cz, cq, caq, ccx, ccy, ccz);
+		}
+		T.q[k] = q;
+		T.aq[k] = aq;
+		T.cq[k] = make_double4(cx, cy, cz, (double)q);
+		if (T.f) {
+			T.f[k] = make_float4((float)((cx - P.rad) * P.inv_rad), (float)((cy - P.rad) * P.inv_rad),
+			                     (float)((cz - P.rad) * P.inv_rad), (float)q);
+			T.r2[k] = (float)(T.w2[k] * P.inv_rad * P.inv_rad / P.oap2);
+		}
+		if (k == 0) break;
+		const int32_t p = T.parent[k];
+		if (p < 0 || (uint32_t)p >= k) {  // parents precede children in pre-order
+			set_status(rec, POT_E_CAPACITY);
+			break;
+		}
+		__threadfence();
+		const uint32_t arrived = atomicAdd(&T.ctr[p], 1u) + 1u;
+		if (arrived != T.nint[p]) break;
+		__threadfence();
+		k = (uint32_t)p;
+	}
+	}
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static inline uint32_t blocks_for(size_t n, int threads) { return (uint32_t)((n + threads - 1) / threads); }
+
+void launch_keys(const double4* pos, uint64_t* keys, uint32_t* vals, const Params& P, RunRec* rec,
+                 int begin_step, cudaStream_t s, Timer& tm)
+{
+	ScopedKernel k(tm, "keys");
+	k_keys<<<blocks_for(P.n, 256), 256, 0, s>>>(pos, keys, vals, P, rec, begin_step);
+}
+
+void launch_reorder(const uint32_t* perm, const double4* pos_in, const double4* vel_in, const uint32_t* pid_in,
+                    double4* pos_out, double4* vel_out, uint32_t* pid_out, double4* src64, float4* src32,
+                    uint8_t* due, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+{
+	ScopedKernel k(tm, "reorder");
+	k_reorder<<<blocks_for(P.n, 256), 256, 0, s>>>(perm, pos_in, vel_in, pid_in, pos_out, vel_out, pid_out,
+	                                               src64, src32, due, P, rec);
+}
+
+void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const Params& P, RunRec* rec,
+                  uint32_t* block_sums, cudaStream_t s, Timer& tm)
+{
+	const uint32_t n = P.n, L = P.leaf_size;
+	const uint32_t n_pairs = n - L;  // n > L is checked at creation
+	cudaMemsetAsync(&rec->n_overflow, 0, sizeof(unsigned int), s);
+	{
+		ScopedKernel k(tm, "tree_pairs");
+		k_pairs<<<blocks_for(n - 1, 256), 256, 0, s>>>(keys, src64, n, n_pairs, L, T.lvl8, T.cnt, rec);
+	}
+	scan_exclusive(T.cnt, T.base, n_pairs, block_sums, &rec->n_nodes, s, tm);
+	{
+		ScopedKernel k(tm, "tree_fill");
+		k_fill_nodes<<<blocks_for(n_pairs, 256), 256, 0, s>>>(T.lvl8, T.base, n_pairs, T, rec);
+	}
+	{
+		ScopedKernel k(tm, "tree_finish");
+		k_finish_nodes<<<blocks_for(n, 256), 256, 0, s>>>(keys, n, L, T.lvl8, T.base, T, P, rec);
+	}
+	{
+		ScopedKernel k(tm, "tree_moments");
+		k_moments<<<blocks_for(n, 256), 256, 0, s>>>(T, src64, P, rec);
+	}
+}
+
+}  // namespace pot

@@ -1,0 +1,67 @@
+// Tree storage and launchers shared by the tree and walk translation units.
+#pragma once
+
+#include "pot_host.h"
+
+namespace pot {
+
+// Internal nodes in pre-order, structure of arrays; `cap` entries each
+// (the leaf table of bucket leaves has 8 * cap entries).
+struct TreeDev {
+	uint32_t cap;
+	int8_t* lvl8;      // [n] common levels of pair (i, i + L), capped at 20
+	uint32_t* cnt;     // [n] cells owned by pair i
+	uint32_t* base;    // [n] exclusive scan of cnt: index of pair i's first cell
+	uint32_t* first;   // first particle (Morton slot)
+	uint32_t* last;    // last particle
+	uint8_t* level;    // depth (root 0)
+	int32_t* child;    // [8 * cap] child codes by octal digit
+	int32_t* parent;
+	uint8_t* nint;     // internal children
+	uint32_t* ctr;     // arrivals in the upward pass
+	int32_t* q;        // net charge (Tree.q)
+	uint32_t* aq;      // absolute charge (Tree.aq)
+	double4* cq;       // centre of |q| and q
+	double* w2;        // (x2 - x1)^2
+	// FP32 walk (fast form only; null otherwise)
+	float4* f;         // centre relative to the domain centre, q
+	float* r2;         // w2 / OAP^2: accepted when d^2 > r2
+	float4* lf;        // [8 * cap] bucket-leaf moments
+	float* lr2;        // [8 * cap] bucket-leaf critical radius^2
+	uint2* lrange;     // [8 * cap] bucket-leaf (first slot, count)
+	uint2* ovf;        // [OVF_CAP] leaf-size-1 overflow buckets (first slot, count)
+};
+
+void launch_keys(const double4* pos, uint64_t* keys, uint32_t* vals, const Params& P, RunRec* rec,
+                 int begin_step, cudaStream_t s, Timer& tm);
+void launch_reorder(const uint32_t* perm, const double4* pos_in, const double4* vel_in, const uint32_t* pid_in,
+                    double4* pos_out, double4* vel_out, uint32_t* pid_out, double4* src64, float4* src32,
+                    uint8_t* due, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const Params& P, RunRec* rec,
+                  uint32_t* block_sums, cudaStream_t s, Timer& tm);
+
+// walk.cu
+void launch_chi_b(const TreeDev& T, const double4* src64, const Params& P, RunRec* rec, int force,
+                  cudaStream_t s, Timer& tm);
+void launch_push(double4* pos, double4* vel, const TreeDev& T, const double4* src64, const float4* src32,
+                 const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P, RunRec* rec,
+                 cudaStream_t s, Timer& tm);
+void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const Params& P, RunRec* rec,
+                   cudaStream_t s, Timer& tm);
+void launch_absorb_late(double4* pos, double4* vel, const double4* src64, const uint32_t* due_list,
+                        uint32_t* rein_list, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+void launch_grain_end(double4* pos, double4* vel, StepHist* hist, const Params& P, RunRec* rec, cudaStream_t s,
+                      Timer& tm);
+void launch_field_query(const TreeDev& T, const double4* src64, const float4* src32, const double* xyz,
+                        const uint32_t* self_slot, uint32_t nq, double* E, const Params& P, RunRec* rec,
+                        cudaStream_t s, Timer& tm);
+void launch_phi_query(const TreeDev& T, const double4* src64, const double* xyz, uint32_t nq, double* phi,
+                      const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+
+// inject.cu
+void launch_reinject(double4* pos, double4* vel, const uint32_t* pid, const uint32_t* rein_list,
+                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+void launch_init(double4* pos, double4* vel, uint32_t* pid, const Params& P, RunRec* rec, cudaStream_t s,
+                 Timer& tm);
+
+}  // namespace pot

@@ -1,0 +1,406 @@
+// Barnes-Hut walks fused with the Boris push, grain absorption and the
+// boundary test; edge potential (chi_b); grain update.
+//
+// Plain form (POT_FORM_PLAIN): one thread per target, FP64, leaf size 1, the
+// reference's stack discipline (children pushed in member order, popped
+// last-first, pot.c:1755-1772), opening test and force expressions
+// (pot.c:1719-1803) with unfused products so every accept/open decision is
+// the reference's.  The reference accumulates in x87 long double; here the
+// accumulation is FP64 with fused multiply-adds.
+//
+// Fast form (POT_FORM_FAST): see pot_walk_fast.cu.
+#include "pot_push.cuh"
+
+namespace pot {
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// E (V/m) at (x, y, z) for the particle in Morton slot `self`:
+// field_particle_feels_at, pot.c:1696-1808 (monopole cells).
+__device__ int field_plain(uint32_t self, double x, double y, double z, const TreeDev& T,
+                           const double4* __restrict__ src64, const Params& P, double E[3],
+                           uint32_t& n_inter)
+{
+	int32_t stack[WALK_STACK];
+	int len = 1;
+	stack[0] = 0;
+	double ex = 0.0, ey = 0.0, ez = 0.0;
+	while (len) {
+		const int32_t code = stack[--len];
+		if (code >= 0) {
+			const double4 c = T.cq[code];
+			const double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
+			const double dist2 = dsq3(dx, dy, dz);
+			if (T.w2[code] < dmul(P.oap2, dist2)) {
+				if (c.w != 0.0) {
+					const double dist = sqrt(dist2);
+					const double es = dmul(ddiv(QE, dmul(dmul(P.k4, dist2), dist)), c.w);
+					ex = fma(es, dx, ex);
+					ey = fma(es, dy, ey);
+					ez = fma(es, dz, ez);
+					n_inter++;
+				}
+			} else {
+				if (len + 8 > WALK_STACK) {
+					E[0] = E[1] = E[2] = 0.0;
+					return POT_E_WALK;
+				}
+				const int32_t* ch = &T.child[8u * (uint32_t)code];
+#pragma unroll
+				for (int s = 0; s < 8; s++) {
+					const int32_t cc = ch[slot_digit(s)];
+					if (cc != CH_EMPTY) stack[len++] = cc;
+				}
+			}
+		} else {
+			const uint32_t e = leaf_payload(code);
+			uint32_t j0 = e, j1 = e + 1;
+			if (e >= P.n) {  // overflow bucket (see OVF_CAP)
+				const uint2 r = T.ovf[e - P.n];
+				j0 = r.x;
+				j1 = r.x + r.y;
+			}
+			for (uint32_t slot = j0; slot < j1; slot++) {
+				if (slot == self) continue;
+				const double4 p = src64[slot];
+				const double dx = dsub(x, p.x), dy = dsub(y, p.y), dz = dsub(z, p.z);
+				double dist2 = dsq3(dx, dy, dz);
+				if (dist2 == 0.0) {
+					E[0] = E[1] = E[2] = 0.0;
+					return POT_E_COINCIDENT;
+				}
+				dist2 = dadd(dist2, P.soft2);
+				const double dist = sqrt(dist2);
+				const double es = ddiv(dmul(QE, p.w), dmul(dmul(P.k4, dist2), dist));
+				ex = fma(es, dx, ex);
+				ey = fma(es, dy, ey);
+				ez = fma(es, dz, ez);
+				n_inter++;
+			}
+		}
+	}
+	E[0] = ex;
+	E[1] = ey;
+	E[2] = ez;
+	return POT_OK;
+}
+
+__device__ __forceinline__ void warp_add_u64(unsigned long long* dst, unsigned long long v)
+{
+#pragma unroll
+	for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	if (lane_id() == 0 && v) atomicAdd(dst, v);
+}
+
+__global__ void __launch_bounds__(128) k_push_plain(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T,
+                                                    const double4* __restrict__ src64,
+                                                    const uint32_t* __restrict__ due_list,
+                                                    uint32_t* __restrict__ rein_list, Params P, RunRec* rec)
+{
+	if (rec->status != POT_OK) return;
+	const uint32_t n_due = rec->n_due;
+	const unsigned long long t = rec->t_steps;
+	const bool grain_due = rec->grain_due != 0;
+	const bool absorb_on = !(P.flags & FLAG_NO_GRAIN) && t >= P.t_settle;
+	const double gx = rec->grain_pos[0], gy = rec->grain_pos[1], gz = rec->grain_pos[2];
+	const double qg = (double)rec->grain_q;
+	unsigned long long n_inter = 0, n_push = 0;
+	for (;;) {
+		uint32_t base = 0;
+		if (lane_id() == 0) base = atomicAdd(&rec->work_ctr, 32u);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if (base >= n_due) break;
+		const uint32_t i = base + lane_id();
+		if (i >= n_due) continue;
+		const uint32_t s = due_list[i];
+		const double4 p = pos[s];
+		double4 v = vel[s];
+		const int sp = (int)p.w;
+		const double dt = P.dt * (double)P.tss[sp];
+		const double half = 0.5 * dt;
+		const double3 h = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
+		double E[3];
+		uint32_t ni = 0;
+		const int rc = field_plain(s, h.x, h.y, h.z, T, src64, P, E, ni);
+		if (rc != POT_OK) set_status(rec, rc);
+		n_inter += ni;
+		n_push++;
+		const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
+		const double qom = (QE * charge) / mass_of(sp);
+		double3 xn;
+		boris(v, h, E, qom, dt, P, xn);
+		uint32_t reason = 0;
+		if (!grain_due) reason = after_push(sp, p, xn, v, P, rec, absorb_on, gx, gy, gz);
+		pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
+		vel[s] = v;
+		if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
+	}
+	warp_add_u64(&rec->interactions, n_inter);
+	warp_add_u64(&rec->n_pushed, n_push);
+}
+
+// Steps where the grain itself moves (t a multiple of tss[DUST]): the
+// reference tests absorption against the grain's new position
+// (new_parts[0], pot.c:2641-2652), so the tests run after all pushes.
+__global__ void k_absorb_late(double4* __restrict__ pos, double4* __restrict__ vel,
+                              const double4* __restrict__ src64, const uint32_t* __restrict__ due_list,
+                              uint32_t* __restrict__ rein_list, Params P, RunRec* rec)
+{
+	if (rec->status != POT_OK || !rec->grain_due) return;
+	const uint32_t n_due = rec->n_due;
+	const bool absorb_on = !(P.flags & FLAG_NO_GRAIN) && rec->t_steps >= P.t_settle;
+	const double4 g = pos[rec->grain_slot];
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_due; i += gridDim.x * blockDim.x) {
+		const uint32_t s = due_list[i];
+		const double4 p = pos[s];
+		const double4 v = vel[s];
+		const double4 p_old = src64[s];
+		const int sp = (int)p.w;
+		const uint32_t reason =
+		    after_push(sp, p_old, make_double3(p.x, p.y, p.z), v, P, rec, absorb_on, g.x, g.y, g.z);
+		if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
+	}
+}
+
+// Grain update of pot.c:2825-2848 and the step's statistics.
+__global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel, StepHist* hist, Params P,
+                            RunRec* rec)
+{
+	if (threadIdx.x != 0 || blockIdx.x != 0) return;
+	const double dm = (double)rec->nabs_ion * MASS_ION + (double)rec->nabs_e * MASS_E;
+	const double m = rec->grain_m + dm;
+	double dp[3];
+	for (int k = 0; k < 3; k++) {
+		dp[k] = MASS_E * ((double)rec->sumv_e[k] / VFIX) + MASS_ION * ((double)rec->sumv_ion[k] / VFIX);
+	}
+	const uint32_t gs = rec->grain_slot;
+	double gv[3] = { rec->grain_vel[0], rec->grain_vel[1], rec->grain_vel[2] };
+	if (gs < P.n) {
+		const double4 v = vel[gs];
+		gv[0] = v.x; gv[1] = v.y; gv[2] = v.z;
+	}
+	for (int k = 0; k < 3; k++) gv[k] += dp[k] / m;
+	if (gs < P.n) {
+		vel[gs] = make_double4(gv[0], gv[1], gv[2], 0.0);
+		if (rec->grain_due) {
+			const double4 p = pos[gs];
+			rec->grain_pos[0] = p.x; rec->grain_pos[1] = p.y; rec->grain_pos[2] = p.z;
+		}
+	}
+	for (int k = 0; k < 3; k++) rec->grain_vel[k] = gv[k];
+	rec->grain_m = m;
+	rec->grain_q += rec->dq;
+	rec->tot_absor_e += rec->de;
+	StepHist h;
+	h.t_steps = rec->t_steps;
+	h.grain_q = rec->grain_q;
+	h.dq = rec->dq;
+	h.de = rec->de;
+	h.n_absorbed = rec->nabs_ion + rec->nabs_e;
+	h.n_reinjected = rec->n_rein;
+	h.n_pushed = rec->n_pushed;
+	h.interactions = rec->interactions;
+	h.n_nodes = rec->n_nodes;
+	h.chi_b = rec->chi_b;
+	h.status = rec->status;
+	h.pad = (int)rec->warn;
+	hist[rec->t_steps % HIST] = h;
+}
+
+// ---------------------------------------------------------------------------
+// potential: warp-cooperative phi_at (pot.c:1818-1901)
+// ---------------------------------------------------------------------------
+constexpr int PHI_STACK = 2048;
+
+// One warp evaluates the potential at (x, y, z); `stack` is this warp's
+// shared-memory stack.  Nodes are processed 32 at a time; children of opened
+// cells are pushed with a warp prefix sum.  Returns NaN on stack overflow.
+__device__ double warp_phi(double x, double y, double z, const TreeDev& T, const double4* __restrict__ src64,
+                           const Params& P, int32_t* stack)
+{
+	const uint32_t lane = lane_id();
+	int len = 1;
+	if (lane == 0) stack[0] = 0;
+	__syncwarp();
+	double acc = 0.0;
+	bool overflow = false;
+	while (len > 0) {
+		const int take = len < 32 ? len : 32;
+		const int32_t code = (int)lane < take ? stack[len - 1 - (int)lane] : CH_EMPTY;
+		__syncwarp();
+		len -= take;
+		int32_t ch[8];
+		int nch = 0;
+		if (code >= 0) {
+			const double4 c = T.cq[code];
+			const double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
+			const double dist2 = dsq3(dx, dy, dz);
+			if (T.w2[code] < dmul(P.oap2, dist2)) {
+				if (c.w != 0.0) acc += ddiv(dmul(QE, c.w), dmul(P.k4, sqrt(dist2)));
+			} else {
+				const int32_t* cp = &T.child[8u * (uint32_t)code];
+#pragma unroll
+				for (int s = 0; s < 8; s++) {
+					const int32_t cc = cp[slot_digit(s)];
+					if (cc != CH_EMPTY) ch[nch++] = cc;
+				}
+			}
+		} else if (code != CH_EMPTY) {
+			const uint32_t e = leaf_payload(code);
+			uint32_t j0 = e, j1 = e + 1;
+			if (P.leaf_size > 1 || e >= P.n) {
+				const uint2 r = P.leaf_size > 1 ? T.lrange[e] : T.ovf[e - P.n];
+				j0 = r.x;
+				j1 = r.x + r.y;
+			}
+			for (uint32_t j = j0; j < j1; j++) {
+				const double4 p = src64[j];
+				const double d2 = dsq3(dsub(x, p.x), dsub(y, p.y), dsub(z, p.z));
+				acc += ddiv(dmul(QE, p.w), dmul(P.k4, sqrt(dadd(d2, P.soft2))));
+			}
+		}
+		int incl = nch;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int tv = __shfl_up_sync(0xffffffffu, incl, o);
+			if ((int)lane >= o) incl += tv;
+		}
+		const int total = __shfl_sync(0xffffffffu, incl, 31);
+		if (len + total > PHI_STACK) {
+			overflow = true;
+			break;
+		}
+		const int off = len + incl - nch;
+		for (int j = 0; j < nch; j++) stack[off + j] = ch[j];
+		__syncwarp();
+		len += total;
+	}
+#pragma unroll
+	for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+	return overflow ? __longlong_as_double(0x7ff8000000000000ll) : acc;
+}
+
+// measure_chi_b (pot.c:2251-2279) for one rank: azimuth 0 in the x-y plane
+// through the grain, every 20 steps (pot.c:2409).
+__global__ void k_chi_b(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec, int force)
+{
+	__shared__ int32_t stack[PHI_STACK];
+	if (!(P.flags & FLAG_SCEPTIC) || rec->status != POT_OK) return;
+	if (!force && (rec->t_steps % 20) != 0) return;
+	const double zen = PI_REF / 2.0;
+	const double r = P.rad;
+	const double x = rec->grain_pos[0] + (r * cos(0.0) * sin(zen));
+	const double y = rec->grain_pos[1] + (r * sin(0.0) * sin(zen));
+	const double z = rec->grain_pos[2] + (r * cos(zen));
+	const double phi = warp_phi(x, y, z, T, src64, P, stack);
+	if (lane_id() == 0) {
+		if (isnan(phi)) set_status(rec, POT_E_WALK);
+		else rec->chi_b = phi / (KB * P.Ti / (1 * QE));
+	}
+}
+
+__global__ void k_phi_query(TreeDev T, const double4* __restrict__ src64, const double* __restrict__ xyz,
+                            uint32_t nq, double* __restrict__ phi, Params P, RunRec* rec)
+{
+	__shared__ int32_t stack[4][PHI_STACK];
+	const uint32_t w = threadIdx.x >> 5;
+	for (uint32_t q = blockIdx.x * 4 + w; q < nq; q += gridDim.x * 4) {
+		const double v = warp_phi(xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2], T, src64, P, stack[w]);
+		if (lane_id() == 0) {
+			phi[q] = v;
+			if (isnan(v)) set_status(rec, POT_E_WALK);
+		}
+	}
+}
+
+__global__ void k_field_query_plain(TreeDev T, const double4* __restrict__ src64, const double* __restrict__ xyz,
+                                    const uint32_t* __restrict__ self_slot, uint32_t nq, double* __restrict__ E,
+                                    Params P, RunRec* rec)
+{
+	const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+	if (q >= nq) return;
+	double e[3];
+	uint32_t ni = 0;
+	const int rc = field_plain(self_slot[q], xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2], T, src64, P, e, ni);
+	if (rc != POT_OK) set_status(rec, rc);
+	E[3 * q] = e[0];
+	E[3 * q + 1] = e[1];
+	E[3 * q + 2] = e[2];
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,
+                      const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P,
+                      RunRec* rec, cudaStream_t s, Timer& tm);
+void launch_field_query_fast(const TreeDev& T, const float4* src32, const double* xyz, const uint32_t* self_slot,
+                             uint32_t nq, double* E, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+
+static int sm_count()
+{
+	static int n = 0;
+	if (!n) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+		if (n <= 0) n = 148;
+	}
+	return n;
+}
+
+void launch_chi_b(const TreeDev& T, const double4* src64, const Params& P, RunRec* rec, int force,
+                  cudaStream_t s, Timer& tm)
+{
+	if (!(P.flags & FLAG_SCEPTIC)) return;
+	ScopedKernel k(tm, "chi_b");
+	k_chi_b<<<1, 32, 0, s>>>(T, src64, P, rec, force);
+}
+
+void launch_push(double4* pos, double4* vel, const TreeDev& T, const double4* src64, const float4* src32,
+                 const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P, RunRec* rec,
+                 cudaStream_t s, Timer& tm)
+{
+	if (P.form == POT_FORM_FAST) {
+		launch_push_fast(pos, vel, T, src32, src64, due_list, groups, rein_list, P, rec, s, tm);
+		return;
+	}
+	ScopedKernel k(tm, "walk_push_plain");
+	k_push_plain<<<sm_count() * 8, 128, 0, s>>>(pos, vel, T, src64, due_list, rein_list, P, rec);
+}
+
+void launch_absorb_late(double4* pos, double4* vel, const double4* src64, const uint32_t* due_list,
+                        uint32_t* rein_list, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+{
+	ScopedKernel k(tm, "absorb_late");
+	k_absorb_late<<<sm_count(), 256, 0, s>>>(pos, vel, src64, due_list, rein_list, P, rec);
+}
+
+void launch_grain_end(double4* pos, double4* vel, StepHist* hist, const Params& P, RunRec* rec, cudaStream_t s,
+                      Timer& tm)
+{
+	ScopedKernel k(tm, "grain_end");
+	k_grain_end<<<1, 32, 0, s>>>(pos, vel, hist, P, rec);
+}
+
+void launch_field_query(const TreeDev& T, const double4* src64, const float4* src32, const double* xyz,
+                        const uint32_t* self_slot, uint32_t nq, double* E, const Params& P, RunRec* rec,
+                        cudaStream_t s, Timer& tm)
+{
+	if (P.form == POT_FORM_FAST) {
+		launch_field_query_fast(T, src32, xyz, self_slot, nq, E, P, rec, s, tm);
+		return;
+	}
+	ScopedKernel k(tm, "field_query");
+	k_field_query_plain<<<(nq + 127) / 128, 128, 0, s>>>(T, src64, xyz, self_slot, nq, E, P, rec);
+}
+
+void launch_phi_query(const TreeDev& T, const double4* src64, const double* xyz, uint32_t nq, double* phi,
+                      const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+{
+	ScopedKernel k(tm, "phi_query");
+	const uint32_t nb = (nq + 3) / 4;
+	k_phi_query<<<nb < 4096 ? nb : 4096, 128, 0, s>>>(T, src64, xyz, nq, phi, P, rec);
+}
+
+}  // namespace pot

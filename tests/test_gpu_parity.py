@@ -1,0 +1,259 @@
+"""GPU parity tests: the CUDA path through the C ABI against the oracle.
+
+Bars: integers (tree topology, cell charges, absorption tallies, grain
+charge) bit-exact; the tree's FP64 centres of charge bit-exact (same
+unfused operations in the same order as pot.c:1290-1402); FP64 plain-form
+fields within 1e-12 of the oracle's x87 long-double walk relative to the
+field magnitude; positions after a step within 1e-12 of the domain radius;
+FP32 fast-form fields within the stated error budget of an FP64 direct sum.
+"""
+import numpy as np
+import pytest
+
+from common import SMALL, STRESS, by_cell, canonical_dump, ld, oracle_snapshot, params, run_config
+from oracle.oracle import DUST, ELECTRON, ION, PARTICLE_DTYPE, Oracle
+from pot_b200.gpu import PotError, Run
+
+pytestmark = pytest.mark.gpu
+
+
+def grain_of(o: Oracle) -> dict:
+    g = o.grain()
+    P = o.particles()
+    return dict(q=g["q"], m=g["m"], pos=(P[0]["x"], P[0]["y"], P[0]["z"]), vel=(P[0]["vx"], P[0]["vy"], P[0]["vz"]),
+                tot_absor_e=g["tot_absor_e"], t_steps=g["t_steps"], chi_b=g["chi_b"])
+
+
+def gpu_from_oracle(d, o: Oracle, form="plain", sceptic=True, **kw):
+    """A GPU run holding the oracle's state, with the same Philox key."""
+    kw.setdefault("seed", o.seed)
+    r = Run(run_config(d, sceptic=sceptic), form=form, **kw)
+    r.upload(o.particles(), grain_of(o))
+    return r
+
+
+@pytest.mark.parametrize("q_grain", [0, -317])
+def test_tree_topology_and_moments_bit_exact_small(q_grain):
+    o = oracle_snapshot(SMALL, seed=1, mode="reference")
+    o.set_grain(q=q_grain)
+    o.build_tree()
+    od = o.tree_dump()
+    with gpu_from_oracle(SMALL, o) as r:
+        n_nodes = r.build_tree()
+        gd = r.tree_dump()
+    assert n_nodes == len(od["int_level"])
+    assert canonical_dump(gd) == canonical_dump(od)
+    assert by_cell(gd) == by_cell(od)  # q, aq, centre of |q| and width, bit for bit
+
+
+def test_tree_topology_bit_exact_200k():
+    d = dict(SMALL, N=200001)
+    o = oracle_snapshot(d, seed=5, mode="gpu")
+    o.set_grain(q=-1500)
+    o.build_tree()
+    od = o.tree_dump()
+    with gpu_from_oracle(d, o) as r:
+        r.build_tree()
+        gd = r.tree_dump()
+    assert canonical_dump(gd) == canonical_dump(od)
+    assert by_cell(gd) == by_cell(od)
+
+
+def _half_drifted(o: Oracle, idx):
+    P = o.particles()
+    tss = o.tss()
+    dt = o.params.dt * tss[P["species"][idx]]
+    return np.stack([P["x"][idx] + 0.5 * dt * P["vx"][idx], P["y"][idx] + 0.5 * dt * P["vy"][idx],
+                     P["z"][idx] + 0.5 * dt * P["vz"][idx]], axis=1)
+
+
+@pytest.mark.parametrize("d", [SMALL, STRESS], ids=["small", "stress"])
+def test_field_plain_matches_oracle(d):
+    o = oracle_snapshot(d, seed=3, mode="gpu", steps=3)
+    o.set_grain(q=-250)
+    o.build_tree()
+    rng = np.random.default_rng(0)
+    idx = rng.choice(np.arange(1, d["N"]), size=512, replace=False).astype(np.uint32)
+    idx = np.concatenate([[0], idx]).astype(np.uint32)  # include the grain as a target
+    xyz = _half_drifted(o, idx)
+    hi, lo = o.field_many(idx, xyz)
+    E_ref = ld(hi, lo)
+    with gpu_from_oracle(d, o) as r:
+        r.build_tree()
+        E = r.field_at(idx, xyz)
+    mag = np.sqrt((E_ref.astype(np.float64) ** 2).sum(1))
+    err = np.abs(E - E_ref.astype(np.float64)).max(1) / mag
+    assert np.all(np.isfinite(E))
+    assert err.max() < 1e-12, err.max()
+
+
+def test_phi_and_chi_b_match_oracle():
+    o = oracle_snapshot(SMALL, seed=2, mode="gpu", steps=2)
+    o.set_grain(q=-400)
+    o.build_tree()
+    R = SMALL["r"] * SMALL["mpp"]
+    rng = np.random.default_rng(1)
+    pts = R + rng.uniform(-0.9 * R, 0.9 * R, size=(64, 3))
+    ref = np.array([o.phi_at(*p) for p in pts])
+    with gpu_from_oracle(SMALL, o) as r:
+        r.build_tree()
+        phi = r.phi_at(pts)
+    assert np.max(np.abs(phi - ref) / np.abs(ref).max()) < 1e-12
+    # chi_b is refreshed on steps that are multiples of 20 (pot.c:2409)
+    g = o.grain()
+    o.set_grain(q=g["q"], m=g["m"], tot_absor_e=g["tot_absor_e"], t_steps=19, chi_b=0.0)
+    chi_ref = None
+    o2 = Oracle(params(SMALL), mode="gpu", seed=2, init=False)
+    o2.set_particles(o.particles())
+    o2.set_grain(q=g["q"], m=g["m"], tot_absor_e=g["tot_absor_e"], t_steps=19, chi_b=0.0)
+    o2.build_tree()
+    chi_ref = o2.measure_chi_b()
+    with gpu_from_oracle(SMALL, o2) as r:
+        st = r.step(1)
+    assert st["t_steps"] == 20
+    assert abs(st["chi_b"] - chi_ref) <= 1e-12 * abs(chi_ref)
+
+
+def _compare_step(d, o_before: Oracle, sceptic=True):
+    with gpu_from_oracle(d, o_before, sceptic=sceptic) as r:
+        st = r.step(1)
+        Pg, gg = r.download()
+    o_before.step()
+    Po = o_before.particles()
+    go = o_before.grain()
+    so = o_before.last_step_stats()
+    return st, Pg, gg, Po, go, so
+
+
+@pytest.mark.parametrize("d,sceptic,steps", [(SMALL, True, 2), (STRESS, True, 30), (STRESS, False, 30)],
+                         ids=["small-sceptic", "stress-sceptic", "stress-plain-reinjection"])
+def test_one_step_plain_vs_oracle(d, sceptic, steps):
+    o = oracle_snapshot(d, seed=11, mode="gpu", steps=steps, sceptic=sceptic)
+    st, Pg, gg, Po, go, so = _compare_step(d, o, sceptic=sceptic)
+    assert st["status"] == 0
+    # integer tallies, bit-exact
+    assert st["dq"] == so["dq"]
+    assert st["de"] == so["de"]
+    assert st["n_absorbed"] == so["n_absorbed"]
+    assert st["n_reinjected"] == so["n_reinjected"]
+    assert st["n_pushed"] == so["n_pushed"]
+    assert gg["q"] == go["q"]
+    assert gg["tot_absor_e"] == go["tot_absor_e"]
+    assert np.array_equal(Pg["species"], Po["species"])
+    R = d["r"] * d["mpp"]
+    pos_g = np.stack([Pg["x"], Pg["y"], Pg["z"]], 1)
+    pos_o = np.stack([Po["x"], Po["y"], Po["z"]], 1)
+    vel_g = np.stack([Pg["vx"], Pg["vy"], Pg["vz"]], 1)
+    vel_o = np.stack([Po["vx"], Po["vy"], Po["vz"]], 1)
+    vscale = np.abs(vel_o).max()
+    assert np.abs(pos_g - pos_o).max() < 1e-12 * R
+    assert np.abs(vel_g - vel_o).max() < 1e-9 * vscale
+    assert abs(gg["m"] - go["m"]) <= 1e-15 * go["m"]
+
+
+def test_absorption_happens_and_matches():
+    """Many steps of the stress case with a big grain: absorptions occur and
+    the charge tally matches the oracle step by step while the states agree."""
+    o = oracle_snapshot(STRESS, seed=21, mode="gpu", steps=5)
+    total = 0
+    for _ in range(6):
+        st, Pg, gg, Po, go, so = _compare_step(STRESS, o)
+        assert st["dq"] == so["dq"] and st["de"] == so["de"]
+        total += st["n_absorbed"]
+    assert total > 0
+
+
+def test_init_particles_distribution():
+    """Device init_particles (pot.c:887-935) vs the oracle's with the same
+    Philox streams: identical species layout; positions and velocities equal
+    to FP64 rounding of the transcendental functions."""
+    d = dict(SMALL, N=20001)
+    o = Oracle(params(d), mode="gpu", seed=9)
+    Po = o.particles()
+    with Run(run_config(d), seed=9) as r:
+        r.init_particles()
+        Pg, g = r.download()
+    assert np.array_equal(Pg["species"], Po["species"])
+    assert (Pg["species"] == ION).sum() == (d["N"] - 1) // 2
+    R = d["r"] * d["mpp"]
+    for k in ("x", "y", "z"):
+        assert np.abs(Pg[k] - Po[k]).max() < 1e-12 * R
+    for k in ("vx", "vy", "vz"):
+        assert np.abs(Pg[k] - Po[k]).max() < 1e-9 * np.abs(Po[k]).max()
+
+
+@pytest.mark.parametrize("leaf", [1, 8, 16])
+def test_fast_field_accuracy_vs_direct_sum(leaf):
+    """FP32 grouped walk: per-particle relative error against an FP64
+    (long double) direct sum on sampled particles, as pot.c:2197-2238 checks
+    its own tree.  Bar: no worse than the reference's own FP64 tree at the
+    same opening angle (plus 1e-3 for FP32), and RMS below 2 %."""
+    d = dict(SMALL, N=40001)
+    o = oracle_snapshot(d, seed=4, mode="gpu", steps=1)
+    o.set_grain(q=-600)
+    rng = np.random.default_rng(2)
+    idx = np.sort(rng.choice(np.arange(1, d["N"]), size=2048, replace=False)).astype(np.uint32)
+    P = o.particles()
+    xyz = np.stack([P["x"][idx], P["y"][idx], P["z"][idx]], 1)
+    # every pair softened, as the tree's near field is
+    hi, lo = o.field_direct_many(idx, xyz, soften_all=True)
+    E_dir = ld(hi, lo).astype(np.float64)
+    o.build_tree()
+    hi, lo = o.field_many(idx, xyz)
+    E_tree = ld(hi, lo).astype(np.float64)
+    with gpu_from_oracle(d, o, form="fast", leaf_size=leaf) as r:
+        r.build_tree()
+        E = r.field_at(idx, xyz)
+
+    def rms_rel(a):
+        rel = np.sqrt(((a - E_dir) ** 2).sum(1) / (E_dir ** 2).sum(1))
+        return np.sqrt(np.mean(rel ** 2))
+
+    ref_err, fast_err = rms_rel(E_tree), rms_rel(E)
+    assert fast_err <= ref_err + 1e-3, (fast_err, ref_err)
+    assert fast_err < 2e-2
+
+
+def test_fast_step_runs_and_conserves():
+    d = dict(STRESS, N=20001, theta=0.5)
+    o = oracle_snapshot(d, seed=8, mode="gpu", steps=1)
+    with gpu_from_oracle(d, o, form="fast", leaf_size=16) as r:
+        q0 = r.download()[1]["q"]
+        tot_dq = 0
+        for _ in range(10):
+            st = r.step(1)
+            tot_dq += st["dq"]
+            assert st["status"] == 0
+        P, g = r.download()
+    assert g["q"] == q0 + tot_dq
+    assert (P["species"] == ION).sum() == (d["N"] - 1) // 2
+    R = d["r"] * d["mpp"]
+    rr = np.sqrt((P["x"] - R) ** 2 + (P["y"] - R) ** 2 + (P["z"] - R) ** 2)
+    assert rr.max() <= R * (1 + 1e-12)
+
+
+def test_domain_error_status():
+    o = oracle_snapshot(SMALL, seed=1, mode="gpu")
+    P = o.particles()
+    P[7]["x"] = -1e-9  # outside the root cell [0, 2R]: build_tree's NULL
+    with Run(run_config(SMALL)) as r:
+        r.upload(P)
+        with pytest.raises(PotError) as e:
+            r.step(1)
+        assert e.value.status == -4
+
+
+def test_coincident_error_status():
+    """Two electrons at one position: the reference's build_tree cannot
+    separate them (pot.c:1578-1586) and its walk aborts (pot.c:1800-1802)."""
+    o = oracle_snapshot(SMALL, seed=1, mode="gpu")
+    P = o.particles()
+    a, b = 8000, 8001
+    assert P[a]["species"] == ELECTRON and P[b]["species"] == ELECTRON
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        P[b][k] = P[a][k]
+    with Run(run_config(SMALL)) as r:
+        r.upload(P)
+        with pytest.raises(PotError) as e:
+            r.step(1)
+        assert e.value.status == -5
