@@ -26,6 +26,7 @@ struct pot_gpu_ctx {
 	float4* src32 = nullptr;
 	uint64_t* keys[2] = { nullptr, nullptr };
 	uint32_t* vals[2] = { nullptr, nullptr };
+	int kb = 0;  // which key buffer holds the sorted keys
 	uint32_t* counts = nullptr;
 	uint32_t* block_sums = nullptr;
 	uint8_t* due = nullptr;
@@ -226,6 +227,9 @@ static int fill_params(pot_gpu_ctx* c)
 	P.leaf_size = c->opts.leaf_size;
 	P.flags = r.flags;
 	P.form = c->opts.form;
+	P.max_level = c->opts.form == POT_FORM_FAST ? 16u : (uint32_t)MAX_LEVELS;
+	P.key_bits = c->opts.form == POT_FORM_FAST ? 63u - 3u * P.max_level : 0u;
+	P.group_max = c->opts.group_size == 64 ? 64u : 32u;
 	P.seed = c->opts.seed;
 	const long double m_ion = (long double)MASS_ION, m_e = (long double)MASS_E, m_d = (long double)MASS_DUST;
 	// species time-step multiples, pot.c:4157-4159
@@ -360,6 +364,7 @@ int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx
 	if (o.leaf_size == 0) o.leaf_size = o.form == POT_FORM_PLAIN ? 1 : 16;
 	if (o.form == POT_FORM_PLAIN && o.leaf_size != 1) return POT_E_ARG;
 	if (o.leaf_size > 64) return POT_E_ARG;
+	if (o.group_size != 0 && o.group_size != 32 && o.group_size != 64) return POT_E_ARG;
 	if (cfg->N < 2 || cfg->N > (1ull << 24) || cfg->N <= o.leaf_size) return POT_E_ARG;  // scans cover 2^24
 	if (cfg->r == 0 || !(cfg->mpp > 0.0) || !(cfg->dt > 0.0) || !(cfg->a > 0.0) || cfg->soft < 0.0 ||
 	    !(cfg->theta > 0.0) || cfg->Te < 0.0 || cfg->Ti <= 0.0)
@@ -445,6 +450,8 @@ int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx
 	if (fast) {
 		AL(T.f, cap);
 		AL(T.r2, cap);
+		AL(T.mom_pre, 5 * mom_prefix_entries(n));
+		AL(T.mom_blk, 5 * mom_block_entries(n));
 		if (L > 1) {
 			AL(T.lf, 8ull * cap);
 			AL(T.lr2, 8ull * cap);
@@ -544,12 +551,14 @@ static void enqueue_tree(pot_gpu_ctx* c, int begin_step)
 	Params& P = c->P;
 	cudaStream_t s = c->stream;
 	launch_keys(c->pos[c->cur], c->keys[0], c->vals[0], P, c->rec, begin_step, s, c->timer);
-	radix_sort_pairs(c->keys, c->vals, c->n, c->counts, c->block_sums, s, c->timer);
+	const int kb = radix_sort_pairs(c->keys, c->vals, c->n, c->counts, c->block_sums, (int)P.key_bits, s, c->timer,
+	                                &c->rec->status);
+	c->kb = kb;
 	const int nx = c->cur ^ 1;
-	launch_reorder(c->vals[0], c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->pos[nx], c->vel[nx], c->pid[nx],
+	launch_reorder(c->vals[kb], c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->pos[nx], c->vel[nx], c->pid[nx],
 	               c->src64, c->src32, c->due, P, c->rec, s, c->timer);
 	c->cur = nx;
-	launch_build(c->keys[0], c->T, c->src64, P, c->rec, c->block_sums, s, c->timer);
+	launch_build(c->keys[kb], c->T, c->src64, P, c->rec, c->block_sums, s, c->timer);
 }
 
 static void enqueue_step(pot_gpu_ctx* c)
@@ -687,7 +696,7 @@ int pot_gpu_tree_dump(pot_gpu_ctx* c, uint64_t max_nodes, uint64_t* n_int, int32
 	std::vector<double> w2;
 	std::vector<uint2> lrange;
 	int rc;
-	if ((rc = fetch(keys, c->keys[0], c->n)) || (rc = fetch(first, c->T.first, M)) ||
+	if ((rc = fetch(keys, c->keys[c->kb], c->n)) || (rc = fetch(first, c->T.first, M)) ||
 	    (rc = fetch(pid, c->pid[c->cur], c->n)) || (rc = fetch(level, c->T.level, M)) ||
 	    (rc = fetch(child, c->T.child, 8ull * M)) || (rc = fetch(q, c->T.q, M)) || (rc = fetch(aq, c->T.aq, M)) ||
 	    (rc = fetch(cq, c->T.cq, M)) || (rc = fetch(w2, c->T.w2, M)))

@@ -69,9 +69,10 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, size_t n, uint32_t* block
 void compact_flags(const uint8_t* flags, size_t n, uint32_t* list, uint32_t* block_sums,
                    unsigned int* count, cudaStream_t s, Timer& tm, uint32_t* prefix = nullptr);
 size_t radix_counts_words(size_t n);
-// LSD radix sort of (keys, vals) on bits [0, 64): 8 passes of 8 bits,
-// result in keys[0]/vals[0].
-void radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* counts,
-                      uint32_t* block_sums, cudaStream_t s, Timer& tm);
+// LSD radix sort of (keys, vals) on bits [low_bit, 64) in 8-bit passes;
+// result in keys[0]/vals[0] when the number of passes is even, keys[1]/vals[1]
+// otherwise (returns the index).
+int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* counts, uint32_t* block_sums,
+                     int low_bit, cudaStream_t s, Timer& tm, int* err);
 
 }  // namespace pot

@@ -55,8 +55,8 @@ constexpr int WALK_STACK = 400;    // MAX_PATH_LEN, pot.c:196
 // than 2R / 2^21 in every axis); such a level-21 cell becomes a bucket in a
 // small overflow table, leaf payload n + j, and sets warn bit 0.
 constexpr uint32_t OVF_CAP = 4096;
-// Fast form: targets per warp group (one per lane).
-constexpr uint32_t GROUP_MAX = 32;
+// Fast form: largest target group per warp (two targets per lane).
+constexpr uint32_t GROUP_MAX = 64;
 constexpr uint32_t FLAG_SCEPTIC = POT_CFG_SCEPTIC;
 constexpr uint32_t FLAG_NO_GRAIN = POT_CFG_DISABLE_GRAIN;
 
@@ -119,6 +119,9 @@ struct Params {
 	uint32_t flags;
 	uint32_t tss[3];
 	uint32_t form;
+	uint32_t max_level;  // deepest level (leaf cells): 21 in the plain form, 16 in the fast form
+	uint32_t key_bits;   // low key bits left unsorted: 0 plain, 15 fast (levels 17-21)
+	uint32_t group_max;  // fast form: targets per warp group, 32 or 64
 	uint64_t seed;
 	unsigned long long t_settle;  // first step with t*dt > settle (long double test on the host)
 	double dt, mpp, rad, root_w;  // rad = r*mpp, root_w = 2.0*r*mpp (pot.c:1476)

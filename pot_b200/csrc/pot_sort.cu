@@ -144,64 +144,103 @@ void compact_flags(const uint8_t* flags, size_t n, uint32_t* list, uint32_t* blo
 }
 
 // ---------------------------------------------------------------------------
-// radix sort
+// radix sort: one kernel per 8-bit pass with decoupled look-back
 // ---------------------------------------------------------------------------
-// Per-tile digit histogram, written digit-major: counts[d * nb + b].
-__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t* __restrict__ keys, size_t n, int shift,
-                                                        uint32_t* __restrict__ counts, uint32_t nb)
+// Tiles of OS_TILE keys.  A block takes the next tile index from a counter
+// (so tiles start in index order), ranks its keys stably per digit, publishes
+// its per-digit counts, and obtains the exclusive prefix of each digit over
+// all earlier tiles by looking back at their published words (aggregate or
+// inclusive prefix).  Every wait has an iteration cap; reaching it records
+// POT_E_ITER and the pass completes with wrong order but without hanging.
+// The keys are then staged in shared memory in digit order and written out
+// contiguously per digit.
+constexpr int OS_THREADS = 256;
+constexpr int OS_ITEMS = 8;
+constexpr int OS_TILE = OS_THREADS * OS_ITEMS;
+constexpr int OS_MAX_PASSES = 8;
+constexpr uint32_t OS_FLAG_AGG = 1u << 30;
+constexpr uint32_t OS_FLAG_PRE = 2u << 30;
+constexpr uint32_t OS_COUNT = (1u << 30) - 1u;
+constexpr long OS_SPIN_CAP = 1L << 24;
+
+// Digit counts of every pass in one read of the keys: hist[p * 256 + d].
+__global__ void __launch_bounds__(OS_THREADS) k_os_hist(const uint64_t* __restrict__ keys, size_t n, int low_bit,
+                                                        int npass, uint32_t* __restrict__ hist)
 {
-	__shared__ uint32_t h[8][RS_BINS];
-	const int w = threadIdx.x >> 5;
-	for (int i = threadIdx.x; i < 8 * RS_BINS; i += RS_THREADS) (&h[0][0])[i] = 0;
+	__shared__ uint32_t h[OS_MAX_PASSES][RS_BINS];
+	for (int i = threadIdx.x; i < OS_MAX_PASSES * RS_BINS; i += OS_THREADS) (&h[0][0])[i] = 0;
 	__syncthreads();
-	const size_t base = (size_t)blockIdx.x * RS_TILE + threadIdx.x;
-#pragma unroll 4
-	for (int r = 0; r < RS_ITEMS; r++) {
-		const size_t i = base + (size_t)r * RS_THREADS;
-		if (i < n) atomicAdd(&h[w][(keys[i] >> shift) & 0xFF], 1u);
+	for (size_t i = (size_t)blockIdx.x * OS_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * OS_THREADS) {
+		const uint64_t k = keys[i];
+		for (int p = 0; p < npass; p++) atomicAdd(&h[p][(k >> (low_bit + 8 * p)) & 0xFF], 1u);
 	}
 	__syncthreads();
-	const int d = threadIdx.x;  // RS_THREADS == RS_BINS
-	uint32_t c = 0;
-#pragma unroll
-	for (int k = 0; k < 8; k++) c += h[k][d];
-	counts[(size_t)d * nb + blockIdx.x] = c;
+	for (int p = 0; p < npass; p++) {
+		const uint32_t c = h[p][threadIdx.x];
+		if (c) atomicAdd(&hist[p * RS_BINS + threadIdx.x], c);
+	}
 }
 
-// Stable scatter: tile processed in RS_ITEMS rounds of RS_THREADS keys in
-// index order; within a round the rank of a key among equal digits is
-// (earlier rounds) + (earlier warps this round) + (earlier lanes).
-__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t* __restrict__ kin,
-                                                           const uint32_t* __restrict__ vin, size_t n,
-                                                           int shift, const uint32_t* __restrict__ offsets,
-                                                           uint32_t nb, uint64_t* __restrict__ kout,
-                                                           uint32_t* __restrict__ vout)
+// In place: hist[p * 256 + d] <- exclusive prefix over digits (one block).
+__global__ void __launch_bounds__(RS_BINS) k_os_offsets(uint32_t* __restrict__ hist, int npass)
 {
-	__shared__ uint32_t s_base[RS_BINS];
-	__shared__ uint32_t s_tot[RS_BINS];
+	for (int p = 0; p < npass; p++) {
+		uint32_t tot;
+		const uint32_t v = hist[p * RS_BINS + threadIdx.x];
+		const uint32_t e = block_excl_scan(v, &tot);
+		hist[p * RS_BINS + threadIdx.x] = e;
+		__syncthreads();
+	}
+}
+
+__global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restrict__ kin,
+                                                        const uint32_t* __restrict__ vin, size_t n, int shift,
+                                                        const uint32_t* __restrict__ goff,
+                                                        uint32_t* __restrict__ status,
+                                                        unsigned int* __restrict__ tile_ctr,
+                                                        uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                        int* __restrict__ err)
+{
+	__shared__ uint32_t s_tile;
+	__shared__ uint32_t s_run[RS_BINS];       // running per-digit count in this tile
 	__shared__ uint32_t s_wcnt[8][RS_BINS];
 	__shared__ uint32_t s_wpre[8][RS_BINS];
+	__shared__ uint32_t s_loc[RS_BINS];       // digit start inside the staged tile
+	__shared__ uint32_t s_glob[RS_BINS];      // digit start in the output
+	__shared__ uint64_t s_key[OS_TILE];
+	__shared__ uint32_t s_val[OS_TILE];
 	const int t = threadIdx.x, w = t >> 5, lane = t & 31;
 	const uint32_t lt_mask = (1u << lane) - 1u;
-	s_base[t] = offsets[(size_t)t * nb + blockIdx.x];
+	if (t == 0) s_tile = atomicAdd(tile_ctr, 1u);
+	s_run[t] = 0;
 #pragma unroll
 	for (int k = 0; k < 8; k++) s_wcnt[k][t] = 0;
 	__syncthreads();
-	const size_t base = (size_t)blockIdx.x * RS_TILE;
-	for (int r = 0; r < RS_ITEMS; r++) {
-		const size_t i = base + (size_t)r * RS_THREADS + t;
-		const bool valid = i < n;
-		uint64_t key = 0;
-		uint32_t val = 0;
-		int d = RS_BINS;  // sentinel for the ragged tail
-		if (valid) {
-			key = kin[i];
-			val = vin[i];
-			d = (int)((key >> shift) & 0xFF);
+	const uint32_t tile = s_tile;
+	const size_t base = (size_t)tile * OS_TILE;
+	uint64_t key[OS_ITEMS];
+	uint32_t val[OS_ITEMS];
+	uint32_t rank[OS_ITEMS];
+	int dig[OS_ITEMS];
+#pragma unroll
+	for (int r = 0; r < OS_ITEMS; r++) {
+		const size_t i = base + (size_t)r * OS_THREADS + t;
+		dig[r] = RS_BINS;
+		key[r] = 0;
+		val[r] = 0;
+		if (i < n) {
+			key[r] = kin[i];
+			val[r] = vin[i];
+			dig[r] = (int)((key[r] >> shift) & 0xFF);
 		}
+	}
+	// stable local ranks: rounds in index order, then warps, then lanes
+#pragma unroll
+	for (int r = 0; r < OS_ITEMS; r++) {
+		const int d = dig[r];
 		const uint32_t peers = __match_any_sync(0xffffffffu, d);
 		const uint32_t lrank = __popc(peers & lt_mask);
-		if (valid && lrank == 0) s_wcnt[w][d] = __popc(peers);
+		if (d < RS_BINS && lrank == 0) s_wcnt[w][d] = __popc(peers);
 		__syncthreads();
 		{
 			uint32_t run = 0;
@@ -212,46 +251,100 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t* __res
 				s_wpre[k][t] = run;
 				run += c;
 			}
-			s_tot[t] = run;
+			s_loc[t] = run;  // this round's count of digit t
 		}
 		__syncthreads();
-		if (valid) {
-			const uint32_t pos = s_base[d] + s_wpre[w][d] + lrank;
-			kout[pos] = key;
-			vout[pos] = val;
-		}
+		if (d < RS_BINS) rank[r] = s_run[d] + s_wpre[w][d] + lrank;
 		__syncthreads();
-		s_base[t] += s_tot[t];
+		s_run[t] += s_loc[t];
+	}
+	__syncthreads();
+	// publish this tile's count of digit t, then look back for its prefix
+	const uint32_t cnt = s_run[t];
+	volatile uint32_t* st = status;
+	st[(size_t)tile * RS_BINS + t] = (tile == 0 ? OS_FLAG_PRE : OS_FLAG_AGG) | cnt;
+	uint32_t excl = 0;
+	if (tile > 0) {
+		long spins = 0;
+		for (int64_t j = (int64_t)tile - 1; j >= 0;) {
+			const uint32_t v = st[(size_t)j * RS_BINS + t];
+			const uint32_t flag = v & ~OS_COUNT;
+			if (flag == 0) {
+				if (++spins > OS_SPIN_CAP) {
+					atomicCAS(err, 0, POT_E_ITER);
+					break;
+				}
+				continue;
+			}
+			excl += v & OS_COUNT;
+			if (flag == OS_FLAG_PRE) break;
+			j--;
+		}
+		st[(size_t)tile * RS_BINS + t] = OS_FLAG_PRE | (excl + cnt);
+	}
+	s_glob[t] = goff[t] + excl;
+	// digit starts inside the tile
+	{
+		uint32_t tot;
+		const uint32_t e = block_excl_scan(cnt, &tot);
+		s_loc[t] = e;
+	}
+	__syncthreads();
+#pragma unroll
+	for (int r = 0; r < OS_ITEMS; r++) {
+		if (dig[r] < RS_BINS) {
+			const uint32_t p = s_loc[dig[r]] + rank[r];
+			s_key[p] = key[r];
+			s_val[p] = val[r];
+		}
+	}
+	__syncthreads();
+	const uint32_t nt = (uint32_t)((n - base) < (size_t)OS_TILE ? (n - base) : (size_t)OS_TILE);
+	for (uint32_t i = t; i < nt; i += OS_THREADS) {
+		const uint64_t k = s_key[i];
+		const int d = (int)((k >> shift) & 0xFF);
+		const uint32_t o = s_glob[d] + (i - s_loc[d]);
+		kout[o] = k;
+		vout[o] = s_val[i];
 	}
 }
+
+static inline int os_passes(int low_bit) { return (63 - low_bit + 7) / 8; }
 
 size_t radix_counts_words(size_t n)
 {
-	const size_t nb = (n + RS_TILE - 1) / RS_TILE;
-	return (size_t)RS_BINS * (nb ? nb : 1);
+	const size_t tiles = (n + OS_TILE - 1) / OS_TILE;
+	return (size_t)OS_MAX_PASSES * (tiles ? tiles : 1) * RS_BINS + (size_t)OS_MAX_PASSES * RS_BINS + OS_MAX_PASSES;
 }
 
-void radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* counts,
-                      uint32_t* block_sums, cudaStream_t s, Timer& tm)
+int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* counts, uint32_t* block_sums,
+                     int low_bit, cudaStream_t s, Timer& tm, int* err)
 {
-	if (n == 0) return;
-	const uint32_t nb = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
-	const size_t nc = (size_t)RS_BINS * nb;
+	(void)block_sums;
+	if (n == 0) return 0;
+	const uint32_t tiles = (uint32_t)((n + OS_TILE - 1) / OS_TILE);
+	const int npass = os_passes(low_bit);
+	uint32_t* status = counts;
+	uint32_t* hist = counts + (size_t)OS_MAX_PASSES * tiles * RS_BINS;
+	unsigned int* ctr = hist + OS_MAX_PASSES * RS_BINS;
+	const size_t words = (size_t)npass * tiles * RS_BINS;
+	cudaMemsetAsync(status, 0, sizeof(uint32_t) * words, s);
+	cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (OS_MAX_PASSES * RS_BINS + OS_MAX_PASSES), s);
+	{
+		ScopedKernel k(tm, "sort_hist", 2);
+		uint32_t nb = tiles < 1024 ? tiles : 1024;
+		k_os_hist<<<nb, OS_THREADS, 0, s>>>(keys[0], n, low_bit, npass, hist);
+		k_os_offsets<<<1, RS_BINS, 0, s>>>(hist, npass);
+	}
 	int src = 0;
-	for (int pass = 0; pass < 8; pass++) {
-		const int shift = 8 * pass;
-		{
-			ScopedKernel k(tm, "sort_hist");
-			k_rs_hist<<<nb, RS_THREADS, 0, s>>>(keys[src], n, shift, counts, nb);
-		}
-		scan_exclusive(counts, counts, nc, block_sums, nullptr, s, tm);
-		{
-			ScopedKernel k(tm, "sort_scatter");
-			k_rs_scatter<<<nb, RS_THREADS, 0, s>>>(keys[src], vals[src], n, shift, counts, nb,
-			                                       keys[src ^ 1], vals[src ^ 1]);
-		}
+	for (int p = 0; p < npass; p++) {
+		ScopedKernel k(tm, "sort_pass");
+		k_os_pass<<<tiles, OS_THREADS, 0, s>>>(keys[src], vals[src], n, low_bit + 8 * p, hist + p * RS_BINS,
+		                                      status + (size_t)p * tiles * RS_BINS, ctr + p, keys[src ^ 1],
+		                                      vals[src ^ 1], err);
 		src ^= 1;
 	}
+	return src;
 }
 
 }  // namespace pot

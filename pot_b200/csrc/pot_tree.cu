@@ -118,8 +118,8 @@ __device__ __forceinline__ int lcp_levels(uint64_t a, uint64_t b)
 // lvl8[i] = common levels of keys i and i + L (capped at 20: a level-21
 // cell cannot split); cnt[i] = number of cells pair i owns.
 __global__ void k_pairs(const uint64_t* __restrict__ keys, const double4* __restrict__ src64, uint32_t n,
-                        uint32_t n_pairs, uint32_t L, int8_t* __restrict__ lvl8, uint32_t* __restrict__ cnt,
-                        RunRec* rec)
+                        uint32_t n_pairs, uint32_t L, int max_level, int8_t* __restrict__ lvl8,
+                        uint32_t* __restrict__ cnt, RunRec* rec)
 {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	// Two particles at one position: the reference's insertion would split
@@ -130,12 +130,12 @@ __global__ void k_pairs(const uint64_t* __restrict__ keys, const double4* __rest
 	}
 	if (i >= n_pairs) return;
 	const int li = lcp_levels(keys[i], keys[i + L]);
-	if (li == MAX_LEVELS) atomicOr(&rec->warn, 1u);
-	const int hi = li < MAX_LEVELS - 1 ? li : MAX_LEVELS - 1;
+	if (li == MAX_LEVELS && max_level == MAX_LEVELS) atomicOr(&rec->warn, 1u);
+	const int hi = li < max_level - 1 ? li : max_level - 1;
 	int prev = -1;
 	if (i > 0) {
 		const int lp = lcp_levels(keys[i - 1], keys[i - 1 + L]);
-		prev = lp < MAX_LEVELS - 1 ? lp : MAX_LEVELS - 1;
+		prev = lp < max_level - 1 ? lp : max_level - 1;
 	}
 	lvl8[i] = (int8_t)hi;
 	cnt[i] = hi > prev ? (uint32_t)(hi - prev) : 0u;
@@ -213,7 +213,7 @@ __global__ void k_finish_nodes(const uint64_t* __restrict__ keys, uint32_t n, ui
 			int32_t code;
 			if (cnt == 0) {
 				code = CH_EMPTY;
-			} else if (cnt <= L || l + 1 >= MAX_LEVELS) {
+			} else if (cnt <= L || l + 1 >= (int)P.max_level) {
 				if (L == 1 && cnt == 1) {
 					code = leaf_code(s[c]);
 				} else if (L == 1) {
@@ -350,6 +350,251 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 	}
 }
 
+// Fast form: the same bottom-up pass with plain sums, sum |q| x / sum |q|
+// divided once per cell, and bucket leaves summed directly.
+__global__ void k_moments_fast(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec)
+{
+	const uint32_t M = rec->n_nodes;
+	if (M > T.cap) return;
+	const uint32_t L = P.leaf_size;
+	for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < M; k0 += gridDim.x * blockDim.x) {
+		if (T.nint[k0] != 0) continue;
+		uint32_t k = k0;
+		for (;;) {
+			int q = 0;
+			uint32_t aq = 0;
+			double sx = 0.0, sy = 0.0, sz = 0.0;
+			const float w_child = 0.5f * (float)(sqrt(T.w2[k]) * P.inv_rad);
+			const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * k]);
+			const int4 c0 = cp[0], c1 = cp[1];
+			const int32_t cc[8] = { c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w };
+#pragma unroll
+			for (int d = 0; d < 8; d++) {
+				const int32_t code = cc[d];
+				if (code == CH_EMPTY) continue;
+				if (code >= 0) {
+					const int cq = __ldcg(&T.q[code]);
+					const uint32_t caq = __ldcg(&T.aq[code]);
+					const double2* p2 = reinterpret_cast<const double2*>(&T.cq[code]);
+					const double2 a01 = __ldcg(p2), a23 = __ldcg(p2 + 1);
+					q += cq;
+					aq += caq;
+					sx = fma((double)caq, a01.x, sx);
+					sy = fma((double)caq, a01.y, sy);
+					sz = fma((double)caq, a23.x, sz);
+					continue;
+				}
+				const uint32_t e = leaf_payload(code);
+				uint32_t j0 = e, j1 = e + 1;
+				if (L > 1) {
+					const uint2 r = T.lrange[e];
+					j0 = r.x;
+					j1 = r.x + r.y;
+				} else if (e >= P.n) {
+					const uint2 r = T.ovf[e - P.n];
+					j0 = r.x;
+					j1 = r.x + r.y;
+				}
+				int lq = 0;
+				uint32_t laq = 0;
+				double lx = 0.0, ly = 0.0, lz = 0.0;
+				for (uint32_t j = j0; j < j1; j++) {
+					const double4 sp = src64[j];
+					const int pq = (int)sp.w;
+					const double pa = (double)abs(pq);
+					lq += pq;
+					laq += (uint32_t)abs(pq);
+					lx = fma(pa, sp.x, lx);
+					ly = fma(pa, sp.y, ly);
+					lz = fma(pa, sp.z, lz);
+				}
+				if (L > 1 && T.lf) {
+					const double inv = laq ? 1.0 / (double)laq : 0.0;
+					T.lf[e] = make_float4((float)((lx * inv - P.rad) * P.inv_rad), (float)((ly * inv - P.rad) * P.inv_rad),
+					                      (float)((lz * inv - P.rad) * P.inv_rad), (float)lq);
+					T.lr2[e] = w_child * w_child / P.oap2_f;
+				}
+				q += lq;
+				aq += laq;
+				sx += lx;
+				sy += ly;
+				sz += lz;
+			}
+			const double inv = aq ? 1.0 / (double)aq : 0.0;
+			const double cx = sx * inv, cy = sy * inv, cz = sz * inv;
+			T.q[k] = q;
+			T.aq[k] = aq;
+			T.cq[k] = make_double4(cx, cy, cz, (double)q);
+			T.f[k] = make_float4((float)((cx - P.rad) * P.inv_rad), (float)((cy - P.rad) * P.inv_rad),
+			                     (float)((cz - P.rad) * P.inv_rad), (float)q);
+			T.r2[k] = (float)(T.w2[k] * P.inv_rad * P.inv_rad / P.oap2);
+			if (k == 0) break;
+			const int32_t p = T.parent[k];
+			if (p < 0 || (uint32_t)p >= k) {
+				set_status(rec, POT_E_CAPACITY);
+				break;
+			}
+			__threadfence();
+			const uint32_t arrived = atomicAdd(&T.ctr[p], 1u) + 1u;
+			if (arrived != T.nint[p]) break;
+			__threadfence();
+			k = (uint32_t)p;
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Fast form moments from prefix sums.  With particles in Morton order every
+// cell and bucket leaf is a contiguous slot range [a, b), so its net charge,
+// absolute charge and |q|-weighted position sums are differences of
+// exclusive prefix sums P[b] - P[a] of (q, |q|, |q|(x - c), |q|(y - c),
+// |q|(z - c)), c the domain centre.  FP64 sums: with |x - c| <= R the
+// cancellation error of a difference is ~1e-16 of the largest prefix, far
+// below the FP32 resolution the fast walk uses.
+// ---------------------------------------------------------------------------
+struct Mom5 {
+	double q, a, x, y, z;
+};
+
+__device__ __forceinline__ Mom5 mom_add(const Mom5& u, const Mom5& v)
+{
+	return Mom5 { u.q + v.q, u.a + v.a, u.x + v.x, u.y + v.y, u.z + v.z };
+}
+
+__device__ __forceinline__ Mom5 mom_of(const double4& p, double c)
+{
+	const double a = fabs(p.w);
+	return Mom5 { p.w, a, a * (p.x - c), a * (p.y - c), a * (p.z - c) };
+}
+
+__device__ __forceinline__ Mom5 mom_shfl_up(const Mom5& m, int o)
+{
+	return Mom5 { __shfl_up_sync(0xffffffffu, m.q, o), __shfl_up_sync(0xffffffffu, m.a, o),
+	              __shfl_up_sync(0xffffffffu, m.x, o), __shfl_up_sync(0xffffffffu, m.y, o),
+	              __shfl_up_sync(0xffffffffu, m.z, o) };
+}
+
+constexpr int MOM_THREADS = 256;
+constexpr int MOM_ITEMS = 16;
+constexpr int MOM_TILE = MOM_THREADS * MOM_ITEMS;
+
+// exclusive block scan of one Mom5 per thread; *tot = block total
+__device__ Mom5 mom_block_excl(Mom5 v, Mom5* tot)
+{
+	__shared__ Mom5 wsum[MOM_THREADS / 32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	Mom5 inc = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const Mom5 t = mom_shfl_up(inc, o);
+		if (lane >= o) inc = mom_add(inc, t);
+	}
+	if (lane == 31) wsum[w] = inc;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		Mom5 run = Mom5 { 0, 0, 0, 0, 0 };
+		for (int k = 0; k < MOM_THREADS / 32; k++) {
+			const Mom5 t = wsum[k];
+			wsum[k] = run;
+			run = mom_add(run, t);
+		}
+		*tot = run;
+	}
+	__syncthreads();
+	const Mom5 excl = mom_add(wsum[w], Mom5 { inc.q - v.q, inc.a - v.a, inc.x - v.x, inc.y - v.y, inc.z - v.z });
+	__syncthreads();
+	return excl;
+}
+
+__global__ void __launch_bounds__(MOM_THREADS) k_mom_reduce(const double4* __restrict__ src64, uint32_t n, double c,
+                                                           Mom5* __restrict__ bsum)
+{
+	__shared__ Mom5 tot;
+	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)threadIdx.x * MOM_ITEMS;
+	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
+	for (int k = 0; k < MOM_ITEMS; k++)
+		if (base + k < n) s = mom_add(s, mom_of(src64[base + k], c));
+	mom_block_excl(s, &tot);
+	if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(MOM_THREADS) k_mom_top(Mom5* __restrict__ bsum, uint32_t nb)
+{
+	__shared__ Mom5 tot;
+	__shared__ Mom5 carry;
+	if (threadIdx.x == 0) carry = Mom5 { 0, 0, 0, 0, 0 };
+	__syncthreads();
+	for (uint32_t base = 0; base < nb; base += MOM_THREADS) {
+		const uint32_t i = base + threadIdx.x;
+		const Mom5 v = i < nb ? bsum[i] : Mom5 { 0, 0, 0, 0, 0 };
+		const Mom5 e = mom_block_excl(v, &tot);
+		const Mom5 c = carry;
+		if (i < nb) bsum[i] = mom_add(c, e);
+		__syncthreads();
+		if (threadIdx.x == 0) carry = mom_add(c, tot);
+		__syncthreads();
+	}
+}
+
+__global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restrict__ src64, uint32_t n, double c,
+                                                         const Mom5* __restrict__ bsum, Mom5* __restrict__ pre)
+{
+	__shared__ Mom5 tot;
+	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)threadIdx.x * MOM_ITEMS;
+	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
+	for (int k = 0; k < MOM_ITEMS; k++)
+		if (base + k < n) s = mom_add(s, mom_of(src64[base + k], c));
+	Mom5 run = mom_add(bsum[blockIdx.x], mom_block_excl(s, &tot));
+	for (int k = 0; k < MOM_ITEMS; k++) {
+		if (base + k < n) {
+			pre[base + k] = run;
+			run = mom_add(run, mom_of(src64[base + k], c));
+			if (base + k + 1 == n) pre[n] = run;
+		}
+	}
+}
+
+__device__ __forceinline__ Mom5 mom_range(const Mom5* __restrict__ pre, uint32_t a, uint32_t b)
+{
+	const Mom5 u = pre[b], v = pre[a];
+	return Mom5 { u.q - v.q, u.a - v.a, u.x - v.x, u.y - v.y, u.z - v.z };
+}
+
+__global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, Params P, RunRec* rec)
+{
+	const uint32_t M = rec->n_nodes;
+	if (M > T.cap) return;
+	const uint32_t L = P.leaf_size;
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+		const Mom5 m = mom_range(pre, T.first[k], T.last[k] + 1);
+		const double inv = m.a > 0.0 ? 1.0 / m.a : 0.0;
+		const double cx = m.x * inv, cy = m.y * inv, cz = m.z * inv;  // relative to the centre
+		const int q = (int)llrint(m.q);
+		T.q[k] = q;
+		T.aq[k] = (uint32_t)llrint(m.a);
+		T.cq[k] = make_double4(cx + P.rad, cy + P.rad, cz + P.rad, (double)q);
+		T.f[k] = make_float4((float)(cx * P.inv_rad), (float)(cy * P.inv_rad), (float)(cz * P.inv_rad), (float)q);
+		T.r2[k] = (float)(T.w2[k] * P.inv_rad * P.inv_rad / P.oap2);
+		if (L > 1) {
+			const float w_child = 0.5f * (float)(sqrt(T.w2[k]) * P.inv_rad);
+			for (int d = 0; d < 8; d++) {
+				const int32_t code = T.child[8u * k + (uint32_t)d];
+				if (code >= CH_EMPTY) continue;
+				const uint32_t e = leaf_payload(code);
+				const uint2 r = T.lrange[e];
+				const Mom5 lm = mom_range(pre, r.x, r.x + r.y);
+				const double li = lm.a > 0.0 ? 1.0 / lm.a : 0.0;
+				T.lf[e] = make_float4((float)(lm.x * li * P.inv_rad), (float)(lm.y * li * P.inv_rad),
+				                      (float)(lm.z * li * P.inv_rad), (float)llrint(lm.q));
+				T.lr2[e] = w_child * w_child / P.oap2_f;
+			}
+		}
+	}
+}
+
+size_t mom_prefix_entries(size_t n) { return n + 1; }
+size_t mom_block_entries(size_t n) { return (n + MOM_TILE - 1) / MOM_TILE + 1; }
+
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
@@ -379,7 +624,8 @@ void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const 
 	cudaMemsetAsync(&rec->n_overflow, 0, sizeof(unsigned int), s);
 	{
 		ScopedKernel k(tm, "tree_pairs");
-		k_pairs<<<blocks_for(n - 1, 256), 256, 0, s>>>(keys, src64, n, n_pairs, L, T.lvl8, T.cnt, rec);
+		k_pairs<<<blocks_for(n - 1, 256), 256, 0, s>>>(keys, src64, n, n_pairs, L, (int)P.max_level, T.lvl8,
+		                                               T.cnt, rec);
 	}
 	scan_exclusive(T.cnt, T.base, n_pairs, block_sums, &rec->n_nodes, s, tm);
 	{
@@ -392,7 +638,19 @@ void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const 
 	}
 	{
 		ScopedKernel k(tm, "tree_moments");
-		k_moments<<<blocks_for(n, 256), 256, 0, s>>>(T, src64, P, rec);
+		if (P.form == POT_FORM_FAST && T.mom_pre) {
+			const uint32_t nb = (uint32_t)((n + MOM_TILE - 1) / MOM_TILE);
+			Mom5* pre = reinterpret_cast<Mom5*>(T.mom_pre);
+			Mom5* bs = reinterpret_cast<Mom5*>(T.mom_blk);
+			k_mom_reduce<<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs);
+			k_mom_top<<<1, MOM_THREADS, 0, s>>>(bs, nb);
+			k_mom_down<<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs, pre);
+			k_moments_prefix<<<blocks_for(n / 4 + 1, 256), 256, 0, s>>>(T, pre, P, rec);
+		} else if (P.form == POT_FORM_FAST) {
+			k_moments_fast<<<blocks_for(n, 256), 256, 0, s>>>(T, src64, P, rec);
+		} else {
+			k_moments<<<blocks_for(n, 256), 256, 0, s>>>(T, src64, P, rec);
+		}
 	}
 }
 

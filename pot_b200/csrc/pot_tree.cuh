@@ -30,8 +30,13 @@ struct TreeDev {
 	float* lr2;        // [8 * cap] bucket-leaf critical radius^2
 	uint2* lrange;     // [8 * cap] bucket-leaf (first slot, count)
 	uint2* ovf;        // [OVF_CAP] leaf-size-1 overflow buckets (first slot, count)
+	// fast form: exclusive prefix sums of (q, |q|, |q| x, |q| y, |q| z), 5 doubles each
+	double* mom_pre;   // [n + 1]
+	double* mom_blk;   // [blocks + 1]
 };
 
+size_t mom_prefix_entries(size_t n);
+size_t mom_block_entries(size_t n);
 void launch_keys(const double4* pos, uint64_t* keys, uint32_t* vals, const Params& P, RunRec* rec,
                  int begin_step, cudaStream_t s, Timer& tm);
 void launch_reorder(const uint32_t* perm, const double4* pos_in, const double4* vel_in, const uint32_t* pid_in,

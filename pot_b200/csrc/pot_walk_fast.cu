@@ -1,32 +1,39 @@
 // Fast form (POT_FORM_FAST): leaf-grouped, warp-cooperative Barnes-Hut walk
 // in FP32, fused with the FP64 Boris push, absorption and boundary test.
 //
-// A warp owns a group of 32 consecutive due particles in Morton order (one
-// per lane) and walks the tree once for the whole group:
+// Groups.  Targets are the particles due this step, in Morton order.  A group
+// is a run of at most GROUP_MAX (64) of them lying inside one tree cell (see
+// k_groups), so its bounding box is compact.  A warp owns one group, two
+// targets per lane (lane l holds group members l and l + 32).
+//
+// Walk.  The warp walks the tree once for the whole group:
 //   * opening test per cell against the group's bounding box: accept when
 //     the squared distance from the box to the cell's centre of charge
 //     exceeds (x2 - x1)^2 / OAP^2.  Every target in the box is at least that
 //     far, so each accepted cell also passes the reference's per-target test
-//     (pot.c:1729); the group list refines every member's list;
-//   * accepted cells (monopoles, unsoftened as pot.c:1737-1749) and opened
-//     leaves (particle ranges, Plummer-softened as pot.c:1789-1798, the
-//     target excluded by slot) are staged in shared memory and flushed:
-//     every lane evaluates its own target against each staged entry, which
-//     all lanes read at once;
+//     (pot.c:1729): the group's list refines every member's list;
+//   * accepted cells (monopoles, unsoftened as pot.c:1737-1749) are staged in
+//     shared memory; opened leaves (particle ranges, Plummer-softened as
+//     pot.c:1789-1798, the target excluded by slot) are staged as ranges and
+//     their particles gathered 32 at a time into shared memory;
+//   * flushes: every lane evaluates its two targets against each staged
+//     entry, which all lanes read at once (shared-memory broadcast);
 //   * the stack of cells still to test lives in shared memory; children of
 //     opened cells are appended with a warp prefix sum.
 // Positions are FP32 relative to the domain centre in units of the domain
-// radius; the FP32 sum is scaled to V/m in FP64 once per target.
+// radius; the FP32 sums are scaled to V/m in FP64 once per target.
 #include "pot_push.cuh"
 
 namespace pot {
 
 constexpr int FW_WARPS = 4;        // warps per block
+constexpr int FW_TPL_MAX = 2;      // targets per lane (1 or 2; groups of 32 or 64)
 constexpr int FW_STACK = 1536;     // cells awaiting a test, per warp
 constexpr int FW_CELLS = 96;       // staged monopoles (flush at >= 64)
 constexpr int FW_CELL_FLUSH = 64;
 constexpr int FW_LEAVES = 64;      // staged leaf ranges (flush at >= 32)
 constexpr int FW_LEAF_FLUSH = 32;
+static_assert(GROUP_MAX == 32 * FW_TPL_MAX, "one group per warp, at most FW_TPL_MAX targets per lane");
 
 struct FastSmem {
 	int32_t stack[FW_STACK];
@@ -59,21 +66,51 @@ __device__ __forceinline__ int warp_excl(int v, int& total)
 	return incl - v;
 }
 
-// Group walk.  t = target (relative units), self = own slot (or 0xFFFFFFFF),
-// valid = lane holds a target.  Returns E in units of q / R^2 (multiply by
-// QE / (4 pi eps0 R^2) for V/m) and the number of entries evaluated.
-__device__ float3 group_walk(float3 t, uint32_t self, bool valid, const TreeDev& T,
-                             const float4* __restrict__ src32, const Params& P, FastSmem& sm,
-                             uint32_t& n_eval, int& err)
+template <int TPL>
+struct Targets {
+	float3 t[TPL];
+	uint32_t self[TPL];  // slot, 0xFFFFFFFF for none
+	bool valid[TPL];
+};
+
+template <int TPL>
+struct Field {
+	float x[TPL], y[TPL], z[TPL];
+};
+
+// monopole (eps2 = 0) or softened pair contribution of source q to every target
+template <int TPL>
+__device__ __forceinline__ void accumulate(Field<TPL>& E, const Targets<TPL>& T, float4 q, float eps2, uint32_t qslot)
+{
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		const float dx = T.t[k].x - q.x, dy = T.t[k].y - q.y, dz = T.t[k].z - q.z;
+		const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+		const float ri = rsqrtf(r2);
+		const float w = (qslot == T.self[k]) ? 0.f : q.w * (ri * ri) * ri;
+		E.x[k] = fmaf(w, dx, E.x[k]);
+		E.y[k] = fmaf(w, dy, E.y[k]);
+		E.z[k] = fmaf(w, dz, E.z[k]);
+	}
+}
+
+// Group walk.  Returns the fields in units of q / R^2 (multiply by
+// QE / (4 pi eps0 R^2) for V/m) and the number of entries evaluated per
+// target.
+template <int TPL>
+__device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const float4* __restrict__ src32,
+                                 const Params& P, FastSmem& sm, uint32_t& n_eval, int& err)
 {
 	const uint32_t lane = lane_f();
-	// group bounding box over valid lanes
-	const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
-	const int src_lane = vmask ? __ffs(vmask) - 1 : 0;
-	float3 ref = make_float3(__shfl_sync(0xffffffffu, t.x, src_lane), __shfl_sync(0xffffffffu, t.y, src_lane),
-	                         __shfl_sync(0xffffffffu, t.z, src_lane));
-	float3 q = valid ? t : ref;
-	float3 bmin = q, bmax = q;
+	// bounding box of the valid targets
+	float3 bmin = make_float3(3.0e38f, 3.0e38f, 3.0e38f), bmax = make_float3(-3.0e38f, -3.0e38f, -3.0e38f);
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		if (tg.valid[k]) {
+			bmin = make_float3(fminf(bmin.x, tg.t[k].x), fminf(bmin.y, tg.t[k].y), fminf(bmin.z, tg.t[k].z));
+			bmax = make_float3(fmaxf(bmax.x, tg.t[k].x), fmaxf(bmax.y, tg.t[k].y), fmaxf(bmax.z, tg.t[k].z));
+		}
+	}
 #pragma unroll
 	for (int o = 16; o; o >>= 1) {
 		bmin.x = fminf(bmin.x, __shfl_xor_sync(0xffffffffu, bmin.x, o));
@@ -85,7 +122,9 @@ __device__ float3 group_walk(float3 t, uint32_t self, bool valid, const TreeDev&
 	}
 	const float eps2 = P.soft2_f;
 	const bool single_leaves = P.leaf_size == 1;
-	float ex = 0.f, ey = 0.f, ez = 0.f;
+	Field<TPL> E;
+#pragma unroll
+	for (int k = 0; k < TPL; k++) E.x[k] = E.y[k] = E.z[k] = 0.f;
 	int len = 1, ncell = 0, nleaf = 0;
 	uint32_t n_cells_ev = 0, n_parts_ev = 0;
 	if (lane == 0) sm.stack[0] = 0;
@@ -148,23 +187,13 @@ __device__ float3 group_walk(float3 t, uint32_t self, bool valid, const TreeDev&
 		// flush staged monopoles
 		if (ncell >= FW_CELL_FLUSH || (done && ncell > 0)) {
 #pragma unroll 4
-			for (int j = 0; j < ncell; j++) {
-				const float4 c = sm.cells[j];
-				const float dx = t.x - c.x, dy = t.y - c.y, dz = t.z - c.z;
-				const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-				const float ri = rsqrtf(r2);
-				const float w = c.w * ri * ri * ri;
-				ex = fmaf(w, dx, ex);
-				ey = fmaf(w, dy, ey);
-				ez = fmaf(w, dz, ez);
-			}
+			for (int j = 0; j < ncell; j++) accumulate(E, tg, sm.cells[j], 0.f, 0xFFFFFFFEu);
 			n_cells_ev += ncell;
 			ncell = 0;
 			__syncwarp();
 		}
 		// flush staged leaves: their particles are gathered 32 at a time into
-		// shared memory (dense, by a prefix sum over the leaf sizes) and every
-		// lane evaluates its target against each of them
+		// shared memory (dense, by a prefix sum over the leaf sizes)
 		if (nleaf >= FW_LEAF_FLUSH || (done && nleaf > 0)) {
 			const uint32_t c0 = (int)lane < nleaf ? sm.leaves[lane].y : 0u;
 			const uint32_t c1 = (int)lane + 32 < nleaf ? sm.leaves[lane + 32].y : 0u;
@@ -180,28 +209,19 @@ __device__ float3 group_walk(float3 t, uint32_t self, bool valid, const TreeDev&
 				float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
 				uint32_t id = 0xFFFFFFFFu;
 				if (g < total) {
-					int lo = 0, hi = nleaf - 1;
-					while (lo < hi) {  // last staged leaf whose offset <= g
-						const int mid = (lo + hi + 1) >> 1;
-						if (sm.loff[mid] <= g) lo = mid; else hi = mid - 1;
+					int a = 0, b = nleaf - 1;
+					while (a < b) {  // last staged leaf whose offset <= g
+						const int mid = (a + b + 1) >> 1;
+						if (sm.loff[mid] <= g) a = mid; else b = mid - 1;
 					}
-					id = sm.leaves[lo].x + (g - sm.loff[lo]);
+					id = sm.leaves[a].x + (g - sm.loff[a]);
 					p = __ldg(&src32[id]);
 				}
 				sm.pbuf[lane] = p;
 				sm.pidx[lane] = id;
 				__syncwarp();
 #pragma unroll 8
-				for (int m = 0; m < 32; m++) {
-					const float4 q = sm.pbuf[m];
-					const float dx = t.x - q.x, dy = t.y - q.y, dz = t.z - q.z;
-					const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-					const float ri = rsqrtf(r2);
-					const float w = (sm.pidx[m] == self) ? 0.f : q.w * ri * ri * ri;
-					ex = fmaf(w, dx, ex);
-					ey = fmaf(w, dy, ey);
-					ez = fmaf(w, dz, ez);
-				}
+				for (int m = 0; m < 32; m++) accumulate(E, tg, sm.pbuf[m], eps2, sm.pidx[m]);
 				__syncwarp();
 			}
 			n_parts_ev += total;
@@ -210,8 +230,8 @@ __device__ float3 group_walk(float3 t, uint32_t self, bool valid, const TreeDev&
 		}
 		if (done) break;
 	}
-	n_eval = valid ? n_cells_ev + n_parts_ev : 0u;
-	return make_float3(ex, ey, ez);
+	n_eval = n_cells_ev + n_parts_ev;
+	return E;
 }
 
 // Slot range [a, b) of a child code.
@@ -239,10 +259,11 @@ __device__ __forceinline__ void child_range(const TreeDev& T, int32_t code, cons
 	}
 }
 
-__device__ __forceinline__ void emit_groups(RunRec* rec, uint2* groups, uint32_t start, uint32_t count)
+__device__ __forceinline__ void emit_groups(RunRec* rec, uint2* groups, uint32_t start, uint32_t count,
+                                            uint32_t gmax)
 {
 	while (count > 0) {
-		const uint32_t c = count < GROUP_MAX ? count : GROUP_MAX;
+		const uint32_t c = count < gmax ? count : gmax;
 		groups[atomicAdd(&rec->n_groups, 1u)] = make_uint2(start, c);
 		start += c;
 		count -= c;
@@ -259,12 +280,13 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 {
 	if (rec->status != POT_OK) return;
 	const uint32_t M = rec->n_nodes;
+	const uint32_t gmax = P.group_max;
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
 		const uint32_t a = T.first[k], b = T.last[k] + 1;
 		const uint32_t d = dpre[b] - dpre[a];
 		if (d == 0) continue;
-		if (d <= GROUP_MAX) {
-			if (k == 0) emit_groups(rec, groups, dpre[a], d);
+		if (d <= gmax) {
+			if (k == 0) emit_groups(rec, groups, dpre[a], d, gmax);
 			continue;
 		}
 		uint32_t run_start = 0, run = 0;
@@ -275,22 +297,23 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 			child_range(T, code, P, ca, cb);
 			const uint32_t dc = dpre[cb] - dpre[ca];
 			if (dc == 0) continue;
-			if (code >= 0 && dc > GROUP_MAX) {
-				emit_groups(rec, groups, run_start, run);
+			if (code >= 0 && dc > gmax) {
+				emit_groups(rec, groups, run_start, run, gmax);
 				run = 0;
 				continue;
 			}
-			if (run + dc > GROUP_MAX) {
-				emit_groups(rec, groups, run_start, run);
+			if (run + dc > gmax) {
+				emit_groups(rec, groups, run_start, run, gmax);
 				run = 0;
 			}
 			if (run == 0) run_start = dpre[ca];
 			run += dc;
 		}
-		emit_groups(rec, groups, run_start, run);
+		emit_groups(rec, groups, run_start, run, gmax);
 	}
 }
 
+template <int TPL>
 __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel,
                                                             TreeDev T, const float4* __restrict__ src32,
                                                             const uint32_t* __restrict__ due_list,
@@ -315,45 +338,54 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict
 		g = __shfl_sync(0xffffffffu, g, 0);
 		if (g >= n_groups) break;
 		const uint2 grp = groups[g];
-		const uint32_t i = grp.x + lane_f();
-		const bool valid = lane_f() < grp.y;
-		uint32_t s = 0xFFFFFFFFu;
-		double4 p = make_double4(P.rad, P.rad, P.rad, 0.0), v = make_double4(0.0, 0.0, 0.0, 0.0);
-		int sp = SP_E;
-		double dt = P.dt, half = 0.5 * P.dt;
-		double3 h = make_double3(P.rad, P.rad, P.rad);
-		if (valid) {
-			s = due_list[i];
-			p = pos[s];
-			v = vel[s];
-			sp = (int)p.w;
-			dt = P.dt * (double)P.tss[sp];
-			half = 0.5 * dt;
-			h = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
+		Targets<TPL> tg;
+		uint32_t slot[TPL];
+		double3 h[TPL];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			const uint32_t m = lane_f() + 32u * k;
+			tg.valid[k] = m < grp.y;
+			slot[k] = 0xFFFFFFFFu;
+			h[k] = make_double3(P.rad, P.rad, P.rad);
+			if (tg.valid[k]) {
+				slot[k] = due_list[grp.x + m];
+				const double4 p = pos[slot[k]];
+				const double4 v = vel[slot[k]];
+				const double half = 0.5 * (P.dt * (double)P.tss[(int)p.w]);
+				h[k] = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
+			}
+			tg.self[k] = slot[k];
+			tg.t[k] = make_float3((float)((h[k].x - P.rad) * P.inv_rad), (float)((h[k].y - P.rad) * P.inv_rad),
+			                      (float)((h[k].z - P.rad) * P.inv_rad));
 		}
-		const float3 tf = make_float3((float)((h.x - P.rad) * P.inv_rad), (float)((h.y - P.rad) * P.inv_rad),
-		                              (float)((h.z - P.rad) * P.inv_rad));
 		uint32_t ne = 0;
 		int err = POT_OK;
-		const float3 ef = group_walk(tf, s, valid, T, src32, P, sm, ne, err);
+		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, err);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
 			break;
 		}
-		if (!valid) continue;
-		n_inter += ne;
-		n_push++;
-		const double E[3] = { (double)ef.x * escale, (double)ef.y * escale, (double)ef.z * escale };
-		const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
-		const double mass = sp == SP_DUST ? MASS_DUST : (sp == SP_ION ? MASS_ION : MASS_E);
-		const double qom = (QE * charge) / mass;
-		double3 xn;
-		boris(v, h, E, qom, dt, P, xn);
-		uint32_t reason = 0;
-		if (!grain_due) reason = after_push(sp, p, xn, v, P, rec, absorb_on, gx, gy, gz);
-		pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
-		vel[s] = v;
-		if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			if (!tg.valid[k]) continue;
+			const uint32_t s = slot[k];
+			const double4 p = pos[s];
+			double4 v = vel[s];
+			const int sp = (int)p.w;
+			const double dt = P.dt * (double)P.tss[sp];
+			n_inter += ne;
+			n_push++;
+			const double E[3] = { (double)ef.x[k] * escale, (double)ef.y[k] * escale, (double)ef.z[k] * escale };
+			const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
+			const double qom = (QE * charge) / mass_of(sp);
+			double3 xn;
+			boris(v, h[k], E, qom, dt, P, xn);
+			uint32_t reason = 0;
+			if (!grain_due) reason = after_push(sp, p, xn, v, P, rec, absorb_on, gx, gy, gz);
+			pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
+			vel[s] = v;
+			if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
+		}
 	}
 	unsigned long long a = n_inter, b = n_push;
 #pragma unroll
@@ -367,6 +399,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict
 	}
 }
 
+template <int TPL>
 __global__ void __launch_bounds__(FW_WARPS * 32) k_field_query_fast(TreeDev T, const float4* __restrict__ src32,
                                                                    const double* __restrict__ xyz,
                                                                    const uint32_t* __restrict__ self_slot,
@@ -375,26 +408,37 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_field_query_fast(TreeDev T, c
 {
 	__shared__ FastSmem smem[FW_WARPS];
 	FastSmem& sm = smem[threadIdx.x >> 5];
-	const uint32_t n_groups = (nq + 31) / 32;
+	const uint32_t gsize = 32u * TPL;
+	const uint32_t n_groups = (nq + gsize - 1) / gsize;
 	const double escale = QE / (P.k4 * P.rad * P.rad);
 	for (uint32_t g = blockIdx.x * FW_WARPS + (threadIdx.x >> 5); g < n_groups; g += gridDim.x * FW_WARPS) {
-		const uint32_t q = g * 32 + lane_f();
-		const bool valid = q < nq;
-		float3 tf = make_float3(0.f, 0.f, 0.f);
-		uint32_t self = 0xFFFFFFFFu;
-		if (valid) {
-			tf = make_float3((float)((xyz[3 * q] - P.rad) * P.inv_rad), (float)((xyz[3 * q + 1] - P.rad) * P.inv_rad),
-			                 (float)((xyz[3 * q + 2] - P.rad) * P.inv_rad));
-			self = self_slot[q];
+		Targets<TPL> tg;
+		uint32_t q[TPL];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			q[k] = g * gsize + lane_f() + 32u * k;
+			tg.valid[k] = q[k] < nq;
+			tg.t[k] = make_float3(0.f, 0.f, 0.f);
+			tg.self[k] = 0xFFFFFFFFu;
+			if (tg.valid[k]) {
+				const uint32_t j = q[k];
+				tg.t[k] = make_float3((float)((xyz[3 * j] - P.rad) * P.inv_rad),
+				                      (float)((xyz[3 * j + 1] - P.rad) * P.inv_rad),
+				                      (float)((xyz[3 * j + 2] - P.rad) * P.inv_rad));
+				tg.self[k] = self_slot[j];
+			}
 		}
 		uint32_t ne = 0;
 		int err = POT_OK;
-		const float3 ef = group_walk(tf, self, valid, T, src32, P, sm, ne, err);
+		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, err);
 		if (err != POT_OK && lane_f() == 0) set_status(rec, err);
-		if (valid) {
-			E[3 * q] = (double)ef.x * escale;
-			E[3 * q + 1] = (double)ef.y * escale;
-			E[3 * q + 2] = (double)ef.z * escale;
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			if (!tg.valid[k]) continue;
+			const uint32_t j = q[k];
+			E[3 * j] = (double)ef.x[k] * escale;
+			E[3 * j + 1] = (double)ef.y[k] * escale;
+			E[3 * j + 2] = (double)ef.z[k] * escale;
 		}
 	}
 }
@@ -425,18 +469,28 @@ void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4
 {
 	(void)src64;
 	ScopedKernel k(tm, "walk_push_fast");
-	k_push_fast<<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list, P,
-	                                                         rec);
+	if (P.group_max > 32) {
+		k_push_fast<2><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list,
+		                                                            P, rec);
+	} else {
+		k_push_fast<1><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list,
+		                                                            P, rec);
+	}
 }
 
 void launch_field_query_fast(const TreeDev& T, const float4* src32, const double* xyz, const uint32_t* self_slot,
                              uint32_t nq, double* E, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
 {
 	ScopedKernel k(tm, "field_query_fast");
-	const uint32_t groups = (nq + 31) / 32;
+	const uint32_t gsize = P.group_max > 32 ? 64u : 32u;
+	const uint32_t groups = (nq + gsize - 1) / gsize;
 	uint32_t nb = (groups + FW_WARPS - 1) / FW_WARPS;
 	if (nb == 0) nb = 1;
-	k_field_query_fast<<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
+	if (gsize == 64) {
+		k_field_query_fast<2><<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
+	} else {
+		k_field_query_fast<1><<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
+	}
 }
 
 }  // namespace pot
