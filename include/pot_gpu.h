@@ -42,6 +42,7 @@ extern "C" {
 #define POT_E_ITER (-8)         /* an iteration cap in a sampler was reached */
 #define POT_E_CAPACITY (-9)     /* tree larger than the node arrays */
 #define POT_E_STATE (-10)       /* call out of order (e.g. step before upload) */
+#define POT_E_LIMIT (-11)       /* request larger than a non-allocating entry point's fixed scratch */
 
 /* ---- records shared with the reference --------------------------------- */
 
@@ -182,6 +183,20 @@ int pot_gpu_tree_dump(pot_gpu_ctx* ctx, uint64_t max_nodes,
    tree built: field_particle_feels_at (pot.c:1696-1808) for many targets. */
 int pot_gpu_field_at(pot_gpu_ctx* ctx, uint64_t n, const uint32_t* idx, const double* xyz,
                      double* E);
+
+/* pot_gpu_field_at without allocation (no counterpart in the reference,
+   which has no device memory).  For callers that must not allocate device
+   memory while they run, e.g. a host program that owns the device heap
+   through its own pool, or a step loop in which cudaMalloc is not allowed.
+   The staging buffers live in one fixed array of about 3.5 MiB that every
+   device which loads the library holds until the process exits; hence at
+   most POT_NOALLOC_MAX_POINTS points per call, larger n returns
+   POT_E_LIMIT.  The first call on each device looks the array's device
+   address up (make that call before any stream capture).  All calls on a
+   device share the array: calls whose work overlaps on the GPU race. */
+#define POT_NOALLOC_MAX_POINTS 65536u
+int pot_gpu_field_at_noalloc(pot_gpu_ctx* ctx, uint64_t n, const uint32_t* idx, const double* xyz,
+                             double* E);
 
 /* Potential (V) at n points over the last tree built, every particle
    included: phi_at (pot.c:1818-1901). */

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "pot_tree.cuh"
@@ -340,6 +341,7 @@ const char* pot_gpu_strerror(int s)
 	case POT_E_ITER: return "sampler iteration cap reached";
 	case POT_E_CAPACITY: return "tree larger than its node arrays";
 	case POT_E_STATE: return "call out of order";
+	case POT_E_LIMIT: return "request larger than the fixed scratch of a non-allocating entry point";
 	default: return "unknown status";
 	}
 }
@@ -779,6 +781,80 @@ int pot_gpu_field_at(pot_gpu_ctx* c, uint64_t n, const uint32_t* idx, const doub
 	                   c->stream, c->timer);
 	CK(cudaGetLastError());
 	CK(cudaMemcpyAsync(E, c->q_out, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+	return sync_status(c);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Field query without allocation.
+//
+// pot_gpu_field_at stages its points, target slots and results in device
+// buffers that it allocates on first use (and grows).  Callers that may not
+// allocate device memory while they run -- a host program that owns the
+// device heap through its own pool, a step loop that must not call
+// cudaMalloc between its iterations -- use pot_gpu_field_at_noalloc, which
+// stages everything in this fixed array instead: at most
+// POT_NOALLOC_MAX_POINTS points per call, about 3.5 MiB held on every device
+// that loads the library until the process exits.  Every call on a device
+// shares the array and overwrites all of it that it reads (nothing needs to
+// start at zero); calls whose work overlaps on the GPU, from any context on
+// that device, race on it.
+// ---------------------------------------------------------------------------
+struct NoAllocScratch {
+	double xyz[3 * POT_NOALLOC_MAX_POINTS];
+	double E[3 * POT_NOALLOC_MAX_POINTS];
+	uint32_t idx[POT_NOALLOC_MAX_POINTS];
+	uint32_t slot[POT_NOALLOC_MAX_POINTS];
+};
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// Device address of g_noalloc_scratch on `device` (the current device),
+// looked up once per device.  In host code the symbol names a host-side
+// stand-in, never device memory, so kernels only ever get this address.
+static int noalloc_scratch(int device, NoAllocScratch** out)
+{
+	static std::mutex mu;
+	static void* addr[256] = { nullptr };
+	if (device < 0 || device >= 256) return POT_E_ARG;
+	std::lock_guard<std::mutex> lock(mu);
+	if (!addr[device]) {
+		void* p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p) {
+			fprintf(stderr, "pot_gpu: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
+			return POT_E_CUDA;
+		}
+		addr[device] = p;
+	}
+	*out = static_cast<NoAllocScratch*>(addr[device]);
+	return POT_OK;
+}
+
+extern "C" {
+
+int pot_gpu_field_at_noalloc(pot_gpu_ctx* c, uint64_t n, const uint32_t* idx, const double* xyz, double* E)
+{
+	if (!c || !idx || !xyz || !E) return POT_E_ARG;
+	if (n > POT_NOALLOC_MAX_POINTS) {
+		fprintf(stderr, "pot_gpu_field_at_noalloc: %llu points requested, at most %u per call\n",
+		        (unsigned long long)n, (unsigned)POT_NOALLOC_MAX_POINTS);
+		return POT_E_LIMIT;
+	}
+	if (!c->tree_valid) return POT_E_STATE;
+	if (n == 0) return POT_OK;
+	CK(cudaSetDevice(c->device));
+	NoAllocScratch* sc = nullptr;
+	int rc = noalloc_scratch(c->device, &sc);
+	if (rc) return rc;
+	CK(cudaMemcpyAsync(sc->xyz, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+	CK(cudaMemcpyAsync(sc->idx, idx, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
+	k_inverse<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->pid[c->cur], c->n, c->inv);
+	k_map_slots<<<nblk(n, 256), 256, 0, c->stream>>>(c->inv, sc->idx, (uint32_t)n, c->n, sc->slot);
+	launch_field_query(c->T, c->src64, c->src32, sc->xyz, sc->slot, (uint32_t)n, sc->E, c->P, c->rec, c->stream,
+	                   c->timer);
+	CK(cudaGetLastError());
+	CK(cudaMemcpyAsync(E, sc->E, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
 	return sync_status(c);
 }
 

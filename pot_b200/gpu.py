@@ -34,7 +34,8 @@ DUST, ION, ELECTRON = 0, 1, 2
 POT_OK = 0
 STATUS_NAMES = {0: "POT_OK", -1: "POT_E_ARG", -2: "POT_E_CUDA", -3: "POT_E_NOMEM", -4: "POT_E_DOMAIN",
                 -5: "POT_E_COINCIDENT", -6: "POT_E_WALK", -7: "POT_E_NONFINITE", -8: "POT_E_ITER",
-                -9: "POT_E_CAPACITY", -10: "POT_E_STATE"}
+                -9: "POT_E_CAPACITY", -10: "POT_E_STATE", -11: "POT_E_LIMIT"}
+NOALLOC_MAX_POINTS = 65536
 FORM_PLAIN, FORM_FAST = 0, 1
 CFG_SCEPTIC, CFG_DISABLE_GRAIN = 0x1, 0x2
 OPT_TIMING = 0x1
@@ -115,6 +116,7 @@ def load_library(path: str = LIB_PATH, build_if_stale: bool = True):
     L.pot_gpu_build_tree.argtypes = [vp, C.POINTER(u64)]
     L.pot_gpu_tree_dump.argtypes = [vp, u64, C.POINTER(u64), vp, vp, vp, vp, vp, vp, C.POINTER(u64), vp, vp, vp]
     L.pot_gpu_field_at.argtypes = [vp, u64, vp, vp, vp]
+    L.pot_gpu_field_at_noalloc.argtypes = [vp, u64, vp, vp, vp]
     L.pot_gpu_phi_at.argtypes = [vp, u64, vp, vp]
     L.pot_gpu_kernel_times.argtypes = [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
                                        C.POINTER(u64)]
@@ -292,6 +294,16 @@ class Run:
         out = np.zeros_like(xyz)
         self._check(self.lib.pot_gpu_field_at(self.h, len(idx), _ptr(idx), _ptr(xyz), _ptr(out)),
                     "pot_gpu_field_at")
+        return out
+
+    def field_at_noalloc(self, idx, xyz) -> np.ndarray:
+        """field_at through the entry point that allocates no device memory
+        (at most NOALLOC_MAX_POINTS points per call)."""
+        idx = np.ascontiguousarray(idx, np.uint32)
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        out = np.zeros_like(xyz)
+        self._check(self.lib.pot_gpu_field_at_noalloc(self.h, len(idx), _ptr(idx), _ptr(xyz), _ptr(out)),
+                    "pot_gpu_field_at_noalloc")
         return out
 
     def phi_at(self, xyz) -> np.ndarray:
