@@ -93,6 +93,96 @@ __device__ double d_integrate_for_alpha(double s, double chi_b, double u2, doubl
 	return alpha;
 }
 
+// The same integral with a warp: for the interval starting at xi0 the
+// reference halves [xi0, 1] until the integrand looks linear, re-evaluating
+// one point per halving.  Here lane k evaluates the k-th halving's end point
+// e_k (e_0 = 1, e_{k+1} = (xi0 + e_k) / 2, the reference's recursion) at
+// once, and a ballot picks the first k that passes the linearity test -- the
+// interval the sequential loop stops at, with the same values.  All lanes
+// return the same alpha.
+__device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, double Rol, bool& ok)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	const double chu2 = chi_b / u2;
+	const double s2 = s * s;
+	const double y_one = s / sqrt(1.0 - chu2 - s2);
+	if (s == 0.0) return 0.0;
+	double alpha = 0.0, xi0 = 0.0, y0 = s;
+	int intervals = 0;
+	for (;;) {
+		// end points e_0 .. e_32 (lane k holds e_{k+1} and its integrand)
+		double e = 1.0, ek1 = 0.0;
+		for (uint32_t k = 0; k <= lane; k++) e = (xi0 + e) / 2.0;  // e_{lane+1}
+		ek1 = e;
+		double y = 1.0 - (chu2 * ek1 * exp(Rol * (1.0 - (1.0 / ek1))));
+		y = 1.0 / sqrt((y / s2) - (ek1 * ek1));
+		// interval k: [xi0, e_k] with midpoint e_{k+1}; y(e_k) is y_one for k = 0
+		// and the lower lane's value otherwise
+		// every lane takes part in each shuffle; lane 0 then substitutes e_0, y_one
+		const double y_up = __shfl_up_sync(0xffffffffu, y, 1);
+		const double e_up = __shfl_up_sync(0xffffffffu, ek1, 1);
+		const double y_ek = lane == 0 ? y_one : y_up;
+		const double e_k = lane == 0 ? 1.0 : e_up;
+		const bool linear = !(fabs(y_ek - y - (y - y0)) > 0.01);
+		const uint32_t pass = __ballot_sync(0xffffffffu, linear);
+		if (pass == 0) {
+			// more than 32 halvings needed at this xi0: continue from e_32
+			const double e32 = __shfl_sync(0xffffffffu, ek1, 31);
+			if (e32 <= xi0 || ++intervals > SIMPSON_CAP) {
+				ok = false;
+				return 0.0;
+			}
+			// the sequential loop would keep halving towards xi0 from e_32;
+			// restart the batch with e_32 playing the role of 1
+			double e2 = e32, y2 = __shfl_sync(0xffffffffu, y, 31);
+			bool done = false;
+			for (int guard = 0; guard < SIMPSON_CAP && !done; guard++) {
+				double xe = e2;
+				for (uint32_t k = 0; k <= lane; k++) xe = (xi0 + xe) / 2.0;
+				double yy = 1.0 - (chu2 * xe * exp(Rol * (1.0 - (1.0 / xe))));
+				yy = 1.0 / sqrt((yy / s2) - (xe * xe));
+				const double yy_up = __shfl_up_sync(0xffffffffu, yy, 1);
+				const double xe_up = __shfl_up_sync(0xffffffffu, xe, 1);
+				const double y_hi = lane == 0 ? y2 : yy_up;
+				const double x_hi = lane == 0 ? e2 : xe_up;
+				const bool lin = !(fabs(y_hi - yy - (yy - y0)) > 0.01);
+				const uint32_t pb = __ballot_sync(0xffffffffu, lin);
+				if (pb) {
+					const int k = __ffs(pb) - 1;
+					const double xk = __shfl_sync(0xffffffffu, x_hi, k);
+					const double yk = __shfl_sync(0xffffffffu, y_hi, k);
+					const double ym = __shfl_sync(0xffffffffu, yy, k);
+					alpha += (xk - xi0) * (y0 + (4.0 * ym) + yk) / 6.0;
+					xi0 = xk;
+					y0 = yk;
+					done = true;
+				} else {
+					e2 = __shfl_sync(0xffffffffu, xe, 31);
+					y2 = __shfl_sync(0xffffffffu, yy, 31);
+				}
+			}
+			if (!done) {
+				ok = false;
+				return 0.0;
+			}
+		} else {
+			const int k = __ffs(pass) - 1;
+			const double xk = __shfl_sync(0xffffffffu, e_k, k);
+			const double yk = __shfl_sync(0xffffffffu, y_ek, k);
+			const double ym = __shfl_sync(0xffffffffu, y, k);
+			alpha += (xk - xi0) * (y0 + (4.0 * ym) + yk) / 6.0;
+			xi0 = xk;
+			y0 = yk;
+		}
+		if (!(xi0 < 1.0)) break;
+		if (++intervals > SIMPSON_CAP) {
+			ok = false;
+			return 0.0;
+		}
+	}
+	return alpha;
+}
+
 // rotate_vec_about_xy_dir, coord.c:22-37
 __device__ __forceinline__ void rot_xy(double d0, double d1, double s, double c, double& x, double& y, double& z,
                                        double offset)
@@ -138,7 +228,10 @@ __device__ __forceinline__ void nrv_pair(Stream& st, double sd, double& a, doubl
 	b = sd * r * s;
 }
 
-// sceptically_reinject, pot.c:496-652
+// sceptically_reinject, pot.c:496-652.  WARP: every lane of a warp runs
+// this for the same particle with identical streams (identical results) and
+// the orbit integral is evaluated cooperatively.
+template <bool WARP>
 __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Params& P, double4& p, double4& v,
                                  bool& ok)
 {
@@ -177,7 +270,8 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 		sincos(psi, &sps, &cps);
 		rot_xy(1.0, 0.0, sps, cps, u[0], u[1], u[2], 0.0);
 		b = sqrt(st.rnd(1.0 - (chi_b / u2)));
-		alpha = d_integrate_for_alpha(b, chi_b, u2, P.Rol, ok);
+		alpha = WARP ? d_integrate_for_alpha_warp(b, chi_b, u2, P.Rol, ok)
+		             : d_integrate_for_alpha(b, chi_b, u2, P.Rol, ok);
 		if (!isnan(alpha) || attempt + 1 >= RETRY_CAP) break;
 	}
 	if (isnan(alpha)) {
@@ -206,6 +300,7 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 }
 
 // inject, pot.c:658-765 (spherical domain, grain enabled)
+template <bool WARP>
 __device__ void inject(Stream& st, int sp, bool reinjection, double chi_b, const Params& P, double4& p, double4& v,
                        bool& ok)
 {
@@ -223,7 +318,7 @@ __device__ void inject(Stream& st, int sp, bool reinjection, double chi_b, const
 		r = P.mpp * P.r_pix;
 	}
 	if (sceptic && reinjection) {
-		sceptic_reinject(st, sp, chi_b, P, p, v, ok);
+		sceptic_reinject<WARP>(st, sp, chi_b, P, p, v, ok);
 		return;
 	}
 	const double phi = st.rnd(2.0 * PI_REF);
@@ -263,7 +358,10 @@ __global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel,
 	const uint32_t n = rec->n_rein;
 	const uint32_t t = (uint32_t)rec->t_steps;
 	const double chi_b = rec->chi_b;
-	for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+	// one warp per reinjected particle
+	for (uint32_t e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < n; e += warps) {
 		const uint32_t w = list[e];
 		const uint32_t s = w & 0x3FFFFFFFu;
 		const uint32_t reason = w >> 30;
@@ -275,14 +373,16 @@ __global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel,
 		uint32_t attempt = 0;
 		Stream st;
 		st.init(P.seed, id, t, 0x10000u | attempt++);
-		inject(st, sp, true, chi_b, P, p, v, ok);
+		inject<true>(st, sp, true, chi_b, P, p, v, ok);
 		if ((reason & 1u) && outside_sphere(p, P)) {
 			st.init(P.seed, id, t, 0x10000u | attempt++);
-			inject(st, sp, true, chi_b, P, p, v, ok);
+			inject<true>(st, sp, true, chi_b, P, p, v, ok);
 		}
-		if (!ok) set_status(rec, POT_E_ITER);
-		pos[s] = p;
-		vel[s] = v;
+		if (lane == 0) {
+			if (!ok) set_status(rec, POT_E_ITER);
+			pos[s] = p;
+			vel[s] = v;
+		}
 	}
 }
 
@@ -304,7 +404,7 @@ __global__ void k_init(double4* __restrict__ pos, double4* __restrict__ vel, uin
 	bool ok = true;
 	Stream st;
 	st.init(P.seed, i, 0u, 0x20000u);
-	inject(st, sp, false, 0.0, P, p, v, ok);
+	inject<false>(st, sp, false, 0.0, P, p, v, ok);
 	if (!ok) set_status(rec, POT_E_ITER);
 	pos[i] = p;
 	vel[i] = v;
@@ -314,7 +414,7 @@ void launch_reinject(double4* pos, double4* vel, const uint32_t* pid, const uint
                      const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
 {
 	ScopedKernel k(tm, "reinject");
-	k_reinject<<<148, 64, 0, s>>>(pos, vel, pid, rein_list, P, rec);
+	k_reinject<<<148, 128, 0, s>>>(pos, vel, pid, rein_list, P, rec);
 }
 
 void launch_init(double4* pos, double4* vel, uint32_t* pid, const Params& P, RunRec* rec, cudaStream_t s,

@@ -506,14 +506,37 @@ __device__ Mom5 mom_block_excl(Mom5 v, Mom5* tot)
 	return excl;
 }
 
+// Each warp owns a contiguous chunk of MOM_ITEMS * 32 particles of the tile
+// and walks it 32 at a time (coalesced loads).
+__device__ __forceinline__ Mom5 mom_warp_incl(Mom5 v)
+{
+	const int lane = threadIdx.x & 31;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const Mom5 t = mom_shfl_up(v, o);
+		if (lane >= o) v = mom_add(v, t);
+	}
+	return v;
+}
+
+__device__ __forceinline__ Mom5 mom_shfl(const Mom5& m, int src)
+{
+	return Mom5 { __shfl_sync(0xffffffffu, m.q, src), __shfl_sync(0xffffffffu, m.a, src),
+	              __shfl_sync(0xffffffffu, m.x, src), __shfl_sync(0xffffffffu, m.y, src),
+	              __shfl_sync(0xffffffffu, m.z, src) };
+}
+
 __global__ void __launch_bounds__(MOM_THREADS) k_mom_reduce(const double4* __restrict__ src64, uint32_t n, double c,
                                                            Mom5* __restrict__ bsum)
 {
 	__shared__ Mom5 tot;
-	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)threadIdx.x * MOM_ITEMS;
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)w * (MOM_ITEMS * 32);
 	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
-	for (int k = 0; k < MOM_ITEMS; k++)
-		if (base + k < n) s = mom_add(s, mom_of(src64[base + k], c));
+	for (int k = 0; k < MOM_ITEMS; k++) {
+		const size_t i = base + (size_t)k * 32 + lane;
+		if (i < n) s = mom_add(s, mom_of(src64[i], c));
+	}
 	mom_block_excl(s, &tot);
 	if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
 }
@@ -540,17 +563,34 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restr
                                                          const Mom5* __restrict__ bsum, Mom5* __restrict__ pre)
 {
 	__shared__ Mom5 tot;
-	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)threadIdx.x * MOM_ITEMS;
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)w * (MOM_ITEMS * 32);
+	// this warp's chunk total, then its offset among the block's warps
 	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
-	for (int k = 0; k < MOM_ITEMS; k++)
-		if (base + k < n) s = mom_add(s, mom_of(src64[base + k], c));
-	Mom5 run = mom_add(bsum[blockIdx.x], mom_block_excl(s, &tot));
 	for (int k = 0; k < MOM_ITEMS; k++) {
-		if (base + k < n) {
-			pre[base + k] = run;
-			run = mom_add(run, mom_of(src64[base + k], c));
-			if (base + k + 1 == n) pre[n] = run;
+		const size_t i = base + (size_t)k * 32 + lane;
+		if (i < n) s = mom_add(s, mom_of(src64[i], c));
+	}
+	// reduce the per-lane partial sums to the warp total on lane 0
+	Mom5 wt = s;
+#pragma unroll
+	for (int o = 16; o; o >>= 1) {
+		wt = mom_add(wt, Mom5 { __shfl_xor_sync(0xffffffffu, wt.q, o), __shfl_xor_sync(0xffffffffu, wt.a, o),
+		                        __shfl_xor_sync(0xffffffffu, wt.x, o), __shfl_xor_sync(0xffffffffu, wt.y, o),
+		                        __shfl_xor_sync(0xffffffffu, wt.z, o) });
+	}
+	const Mom5 mine = lane == 0 ? wt : Mom5 { 0, 0, 0, 0, 0 };
+	Mom5 carry = mom_add(bsum[blockIdx.x], mom_block_excl(mine, &tot));  // valid on lane 0
+	carry = mom_shfl(carry, 0);
+	for (int k = 0; k < MOM_ITEMS; k++) {
+		const size_t i = base + (size_t)k * 32 + lane;
+		const Mom5 v = i < n ? mom_of(src64[i], c) : Mom5 { 0, 0, 0, 0, 0 };
+		const Mom5 inc = mom_warp_incl(v);
+		if (i < n) {
+			pre[i] = mom_add(carry, Mom5 { inc.q - v.q, inc.a - v.a, inc.x - v.x, inc.y - v.y, inc.z - v.z });
+			if (i + 1 == n) pre[n] = mom_add(carry, inc);
 		}
+		carry = mom_add(carry, mom_shfl(inc, 31));
 	}
 }
 

@@ -29,7 +29,7 @@ namespace pot {
 constexpr int FW_WARPS = 4;        // warps per block
 constexpr int FW_TPL_MAX = 2;      // targets per lane (1 or 2; groups of 32 or 64)
 constexpr int FW_STACK = 1536;     // cells awaiting a test, per warp
-constexpr int FW_CELLS = 96;       // staged monopoles (flush at >= 64)
+constexpr int FW_CELLS = 104;      // staged monopoles (flush at >= 64, padded to a multiple of 8)
 constexpr int FW_CELL_FLUSH = 64;
 constexpr int FW_LEAVES = 64;      // staged leaf ranges (flush at >= 32)
 constexpr int FW_LEAF_FLUSH = 32;
@@ -78,7 +78,24 @@ struct Field {
 	float x[TPL], y[TPL], z[TPL];
 };
 
-// monopole (eps2 = 0) or softened pair contribution of source q to every target
+// unsoftened monopole of an accepted cell (pot.c:1737-1749); a cell is never
+// the target itself, so there is no exclusion test
+template <int TPL>
+__device__ __forceinline__ void accumulate_cell(Field<TPL>& E, const Targets<TPL>& T, float4 q)
+{
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		const float dx = T.t[k].x - q.x, dy = T.t[k].y - q.y, dz = T.t[k].z - q.z;
+		const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+		const float ri = rsqrtf(r2);
+		const float w = q.w * (ri * ri) * ri;
+		E.x[k] = fmaf(w, dx, E.x[k]);
+		E.y[k] = fmaf(w, dy, E.y[k]);
+		E.z[k] = fmaf(w, dz, E.z[k]);
+	}
+}
+
+// softened pair contribution (pot.c:1789-1798) of particle q in slot qslot
 template <int TPL>
 __device__ __forceinline__ void accumulate(Field<TPL>& E, const Targets<TPL>& T, float4 q, float eps2, uint32_t qslot)
 {
@@ -184,10 +201,16 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			len += tot;
 			__syncwarp();
 		}
-		// flush staged monopoles
+		// flush staged monopoles, padded to a multiple of 8 with zero-charge
+		// cells far outside the domain so the loop needs no remainder
 		if (ncell >= FW_CELL_FLUSH || (done && ncell > 0)) {
-#pragma unroll 4
-			for (int j = 0; j < ncell; j++) accumulate(E, tg, sm.cells[j], 0.f, 0xFFFFFFFEu);
+			const int padded = (ncell + 7) & ~7;
+			if ((int)lane < padded - ncell) sm.cells[ncell + lane] = make_float4(64.f, 64.f, 64.f, 0.f);
+			__syncwarp();
+			for (int j = 0; j < padded; j += 8) {
+#pragma unroll
+				for (int u = 0; u < 8; u++) accumulate_cell(E, tg, sm.cells[j + u]);
+			}
 			n_cells_ev += ncell;
 			ncell = 0;
 			__syncwarp();
@@ -220,7 +243,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 				sm.pbuf[lane] = p;
 				sm.pidx[lane] = id;
 				__syncwarp();
-#pragma unroll 8
+#pragma unroll 16
 				for (int m = 0; m < 32; m++) accumulate(E, tg, sm.pbuf[m], eps2, sm.pidx[m]);
 				__syncwarp();
 			}
