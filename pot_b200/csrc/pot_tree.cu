@@ -47,6 +47,30 @@ __device__ __forceinline__ uint64_t morton_key(double x, double y, double z, dou
 	return key;
 }
 
+// spread the low 21 bits of v to every third bit
+__device__ __forceinline__ uint64_t spread3(uint64_t v)
+{
+	v &= 0x1FFFFFull;
+	v = (v | (v << 32)) & 0x1F00000000FFFFull;
+	v = (v | (v << 16)) & 0x1F0000FF0000FFull;
+	v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+	v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+	v = (v | (v << 2)) & 0x1249249249249249ull;
+	return v;
+}
+
+// Fast form: the same key layout from the scaled coordinate, cell j of level
+// 21 being [j, j + 1) * w / 2^21; it differs from the midpoint descent only
+// for points within rounding of a cell face, which the fast form tolerates.
+__device__ __forceinline__ uint64_t scaled_key(double x, double y, double z, double scale)
+{
+	const double m = 2097151.0;
+	const uint64_t ix = (uint64_t)fmin(fmax(x * scale, 0.0), m);
+	const uint64_t iy = (uint64_t)fmin(fmax(y * scale, 0.0), m);
+	const uint64_t iz = (uint64_t)fmin(fmax(z * scale, 0.0), m);
+	return (spread3(ix) << 2) | (spread3(iy) << 1) | spread3(iz);
+}
+
 __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ keys,
                        uint32_t* __restrict__ vals, Params P, RunRec* rec, int begin_step)
 {
@@ -75,7 +99,8 @@ __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ k
 	} else if (p.x < 0.0 || p.x > P.root_w || p.y < 0.0 || p.y > P.root_w || p.z < 0.0 || p.z > P.root_w) {
 		set_status(rec, POT_E_DOMAIN);  // build_tree returns NULL, pot.c:1491-1500
 	}
-	keys[s] = morton_key(p.x, p.y, p.z, P.root_w);
+	keys[s] = P.form == POT_FORM_FAST ? scaled_key(p.x, p.y, p.z, 2097152.0 / P.root_w)
+	                                  : morton_key(p.x, p.y, p.z, P.root_w);
 	vals[s] = s;
 }
 

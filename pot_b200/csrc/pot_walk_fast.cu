@@ -185,20 +185,24 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 					}
 				}
 			}
+			// one warp scan for the three appends: accepted cells in bits 0-9,
+			// leaf ranges in bits 10-19, children in bits 20-31 (totals <= 32,
+			// <= 32 and <= 256 fit)
 			int tot;
-			const int co = warp_excl(acc ? 1 : 0, tot);
+			const int packed = (acc ? 1 : 0) | ((leafr ? 1 : 0) << 10) | (nch << 20);
+			const int off = warp_excl(packed, tot);
+			const int co = off & 0x3FF, lo = (off >> 10) & 0x3FF, po = off >> 20;
+			const int tcell = tot & 0x3FF, tleaf = (tot >> 10) & 0x3FF, tch = tot >> 20;
 			if (acc) sm.cells[ncell + co] = cell;
-			ncell += tot;
-			const int lo = warp_excl(leafr ? 1 : 0, tot);
+			ncell += tcell;
 			if (leafr) sm.leaves[nleaf + lo] = range;
-			nleaf += tot;
-			const int po = warp_excl(nch, tot);
-			if (len + tot > FW_STACK) {
+			nleaf += tleaf;
+			if (len + tch > FW_STACK) {
 				err = POT_E_WALK;
 				break;
 			}
 			for (int j = 0; j < nch; j++) sm.stack[len + po + j] = ch[j];
-			len += tot;
+			len += tch;
 			__syncwarp();
 		}
 		// flush staged monopoles, padded to a multiple of 8 with zero-charge
@@ -294,10 +298,13 @@ __device__ __forceinline__ void emit_groups(RunRec* rec, uint2* groups, uint32_t
 }
 
 // Target groups aligned with tree cells.  dpre[s] = due particles in slots
-// [0, s).  A cell with more than GROUP_MAX due particles packs its children,
-// in key order, into runs of at most GROUP_MAX due particles (children with
-// more start their own packing); so every group lies inside one parent cell
-// and its bounding box stays compact.  A group is a range of the due list.
+// [0, s).  A cell with more than gmax due particles packs its children, in
+// key order, into runs of whole children holding at most gmax due particles
+// (children with more start their own packing); so every group lies inside
+// one parent cell and its bounding box stays compact.  (Cutting runs into
+// full groups across child boundaries fills warps but widens boxes: 18 %
+// more interactions and a slower walk at 1M particles.)  A group is a range
+// of the due list.
 __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __restrict__ groups, Params P,
                          RunRec* rec)
 {
