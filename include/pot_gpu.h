@@ -118,7 +118,12 @@ typedef struct pot_step_stats {
 	double chi_b;          /* edge potential in force after the step */
 	int32_t status;        /* POT_OK or the first device-side error */
 	uint32_t pad;
+	double epe[3];         /* POT_STEP_EPE: electrostatic potential energy (J) of the
+	                          grain, the ions, the electrons (Proc.epe, pot.c:2771-2864) */
 } pot_step_stats;
+
+/* pot_gpu_step flags */
+#define POT_STEP_EPE 0x1u  /* compute the potential energies (pot.c:2771-2804) */
 
 typedef struct pot_gpu_ctx pot_gpu_ctx;
 
@@ -142,14 +147,17 @@ int pot_gpu_upload(pot_gpu_ctx* ctx, const pot_particle* parts, uint64_t N,
    Maxwellian velocities, each particle drawing from its own Philox stream. */
 int pot_gpu_init_particles(pot_gpu_ctx* ctx);
 
-/* Run nsteps steps (each: t_steps++, build_tree, move_particles).  `flags`
-   is reserved (0).  `out` (may be NULL) receives the last step's stats. */
+/* Run nsteps steps (each: t_steps++, build_tree, move_particles).  `flags`:
+   POT_STEP_EPE also evaluates every particle's potential energy over the
+   step's tree (compute_epe of move_particles, pot.c:2771-2804, with each
+   particle at its step-start position).  `out` (may be NULL) receives the
+   last step's stats. */
 int pot_gpu_step(pot_gpu_ctx* ctx, uint32_t nsteps, uint32_t flags, pot_step_stats* out);
 
 /* Enqueue nsteps steps on the context's stream and return without waiting.
    Device-side errors surface at the next pot_gpu_sync / pot_gpu_step /
    pot_gpu_download, which return the first status recorded. */
-int pot_gpu_step_async(pot_gpu_ctx* ctx, uint32_t nsteps);
+int pot_gpu_step_async(pot_gpu_ctx* ctx, uint32_t nsteps, uint32_t flags);
 
 /* Copy particles back in reference order (index = original position), and
    the grain state.  Either pointer may be NULL. */

@@ -34,6 +34,8 @@ struct pot_gpu_ctx {
 	uint32_t* due_list = nullptr;
 	uint32_t* due_prefix = nullptr;  // n + 1
 	uint2* groups = nullptr;
+	uint2* groups_all = nullptr;     // fast form, potential energies
+	double* epe_partial = nullptr;   // per-block / per-group partial sums
 	uint32_t* rein_list = nullptr;
 	uint32_t* inv = nullptr;
 	pot_particle* aos = nullptr;
@@ -428,6 +430,8 @@ int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx
 	AL(c->due_list, n);
 	AL(c->due_prefix, (size_t)n + 1);
 	if (fast) AL(c->groups, n);
+	if (fast) AL(c->groups_all, n);
+	AL(c->epe_partial, 3 * (size_t)(n > (uint32_t)EPE_BLOCKS ? n : (uint32_t)EPE_BLOCKS));
 	AL(c->rein_list, 2 * (size_t)n);
 	AL(c->inv, n);
 	AL(c->rec, 1);
@@ -563,8 +567,9 @@ static void enqueue_tree(pot_gpu_ctx* c, int begin_step)
 	launch_build(c->keys[kb], c->T, c->src64, P, c->rec, c->block_sums, s, c->timer);
 }
 
-static void enqueue_step(pot_gpu_ctx* c)
+static void enqueue_step(pot_gpu_ctx* c, uint32_t flags)
 {
+	const int epe = (flags & POT_STEP_EPE) ? 1 : 0;
 	Params& P = c->P;
 	cudaStream_t s = c->stream;
 	enqueue_tree(c, 1);
@@ -574,18 +579,21 @@ static void enqueue_step(pot_gpu_ctx* c)
 	launch_push(c->pos[c->cur], c->vel[c->cur], c->T, c->src64, c->src32, c->due_list, c->groups, c->rein_list, P,
 	            c->rec, s, c->timer);
 	launch_absorb_late(c->pos[c->cur], c->vel[c->cur], c->src64, c->due_list, c->rein_list, P, c->rec, s, c->timer);
+	if (epe) {
+		launch_epe(c->pos[c->cur], c->T, c->src64, c->src32, c->groups_all, c->epe_partial, P, c->rec, s, c->timer);
+	}
 	launch_reinject(c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->rein_list, P, c->rec, s, c->timer);
-	launch_grain_end(c->pos[c->cur], c->vel[c->cur], c->hist, P, c->rec, s, c->timer);
+	launch_grain_end(c->pos[c->cur], c->vel[c->cur], c->hist, P, c->rec, epe, s, c->timer);
 }
 
 int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats* out)
 {
-	(void)flags;
 	if (!c) return POT_E_ARG;
+	if (flags & ~POT_STEP_EPE) return POT_E_ARG;
 	if (!c->uploaded) return POT_E_STATE;
 	if (c->sticky != POT_OK) return c->sticky;
 	CK(cudaSetDevice(c->device));
-	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c);
+	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c, flags);
 	CK(cudaGetLastError());
 	c->tree_valid = true;
 	const int st = sync_status(c);
@@ -606,17 +614,19 @@ int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats
 		out->n_nodes = h.n_nodes;
 		out->chi_b = r.chi_b;
 		out->status = r.status;
+		for (int k = 0; k < 3; k++) out->epe[k] = h.epe[k];
 	}
 	return st;
 }
 
-int pot_gpu_step_async(pot_gpu_ctx* c, uint32_t nsteps)
+int pot_gpu_step_async(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags)
 {
 	if (!c) return POT_E_ARG;
+	if (flags & ~POT_STEP_EPE) return POT_E_ARG;
 	if (!c->uploaded) return POT_E_STATE;
 	if (c->sticky != POT_OK) return c->sticky;
 	CK(cudaSetDevice(c->device));
-	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c);
+	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c, flags);
 	CK(cudaGetLastError());
 	c->tree_valid = true;
 	return POT_OK;

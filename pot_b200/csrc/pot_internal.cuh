@@ -76,10 +76,12 @@ struct RunRec {
 	unsigned int n_rein;
 	unsigned int n_nodes;
 	unsigned int work_ctr;   // dynamic work distribution counter
+	unsigned int work_ctr2;  // second counter (potential-energy walk)
 	unsigned int grain_due;
 	unsigned int warn;       // non-fatal conditions (bit 0: key collision at 21 levels)
 	unsigned int n_overflow; // deepest-level buckets of a leaf-size-1 tree this build
 	unsigned int n_groups;   // fast form: target groups this step
+	unsigned int n_groups_all;  // fast form: groups over every particle (potential energies)
 	long long dq;
 	unsigned long long de;
 	unsigned long long nabs_ion;
@@ -88,6 +90,10 @@ struct RunRec {
 	long long sumv_e[3];
 	unsigned long long interactions;
 	unsigned long long n_pushed;
+	double epe[3];           // potential energies of the last step that computed them (J)
+	double phi_grain;        // potential at the grain from every other particle (V)
+	unsigned int epe_step;   // 1 when this step computes them
+	unsigned int epe_pad;
 };
 
 constexpr double VFIX = 1048576.0;  // 2^20
@@ -106,8 +112,10 @@ struct StepHist {
 	double chi_b;
 	int status;
 	int pad;
+	double epe[3];
 };
 constexpr int HIST = 64;
+constexpr int EPE_BLOCKS = 592;  // per-block partial sums of the potential-energy walks (4 x 148)
 
 // Constant per-run parameters, passed by value to every kernel.
 struct Params {

@@ -55,8 +55,10 @@ void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const 
                    cudaStream_t s, Timer& tm);
 void launch_absorb_late(double4* pos, double4* vel, const double4* src64, const uint32_t* due_list,
                         uint32_t* rein_list, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
-void launch_grain_end(double4* pos, double4* vel, StepHist* hist, const Params& P, RunRec* rec, cudaStream_t s,
-                      Timer& tm);
+void launch_grain_end(double4* pos, double4* vel, StepHist* hist, const Params& P, RunRec* rec, int epe,
+                      cudaStream_t s, Timer& tm);
+void launch_epe(const double4* pos, const TreeDev& T, const double4* src64, const float4* src32, uint2* groups_all,
+                double* partial, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 void launch_field_query(const TreeDev& T, const double4* src64, const float4* src32, const double* xyz,
                         const uint32_t* self_slot, uint32_t nq, double* E, const Params& P, RunRec* rec,
                         cudaStream_t s, Timer& tm);

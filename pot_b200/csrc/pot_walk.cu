@@ -85,6 +85,117 @@ __device__ int field_plain(uint32_t self, double x, double y, double z, const Tr
 	return POT_OK;
 }
 
+// phi_particle_feels (pot.c:1934-2018): potential at (x, y, z) for the
+// particle in slot `self`, which is excluded; cells unsoftened, pairs
+// softened, the reference's visit order and expressions.
+__device__ double phi_plain(uint32_t self, double x, double y, double z, const TreeDev& T,
+                            const double4* __restrict__ src64, const Params& P, int& rc)
+{
+	int32_t stack[WALK_STACK];
+	int len = 1;
+	stack[0] = 0;
+	double phi = 0.0;
+	while (len) {
+		const int32_t code = stack[--len];
+		if (code >= 0) {
+			const double4 c = T.cq[code];
+			const double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
+			const double dist2 = dsq3(dx, dy, dz);
+			if (T.w2[code] < dmul(P.oap2, dist2)) {
+				if (c.w != 0.0) phi += ddiv(dmul(QE, c.w), dmul(P.k4, sqrt(dist2)));
+			} else {
+				if (len + 8 > WALK_STACK) {
+					rc = POT_E_WALK;
+					return 0.0;
+				}
+				const int32_t* ch = &T.child[8u * (uint32_t)code];
+#pragma unroll
+				for (int s = 0; s < 8; s++) {
+					const int32_t cc = ch[slot_digit(s)];
+					if (cc != CH_EMPTY) stack[len++] = cc;
+				}
+			}
+		} else {
+			const uint32_t e = leaf_payload(code);
+			uint32_t j0 = e, j1 = e + 1;
+			if (P.leaf_size > 1 || e >= P.n) {
+				const uint2 r = P.leaf_size > 1 ? T.lrange[e] : T.ovf[e - P.n];
+				j0 = r.x;
+				j1 = r.x + r.y;
+			}
+			for (uint32_t slot = j0; slot < j1; slot++) {
+				if (slot == self) continue;
+				const double4 p = src64[slot];
+				const double d2 = dsq3(dsub(x, p.x), dsub(y, p.y), dsub(z, p.z));
+				phi += ddiv(dmul(QE, p.w), dmul(P.k4, sqrt(dadd(d2, P.soft2))));
+			}
+		}
+	}
+	return phi;
+}
+
+// Deterministic block sum of three doubles (fixed shuffle and warp order).
+__device__ void block_sum3(double v[3], double* __restrict__ out)
+{
+	__shared__ double part[32][3];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+	for (int k = 0; k < 3; k++)
+		for (int o = 16; o; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+	if (lane == 0)
+		for (int k = 0; k < 3; k++) part[w][k] = v[k];
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t[3] = { 0.0, 0.0, 0.0 };
+		for (int j = 0; j < (int)(blockDim.x >> 5); j++)
+			for (int k = 0; k < 3; k++) t[k] += part[j][k];
+		for (int k = 0; k < 3; k++) out[k] = t[k];
+	}
+}
+
+// compute_epe of move_particles (pot.c:2771-2804), plain form: every
+// particle's potential at its step-start position; per-block partial sums
+// of q e phi per species (slots assigned to blocks statically).
+__global__ void __launch_bounds__(128) k_epe_plain(const double4* __restrict__ pos, TreeDev T,
+                                                   const double4* __restrict__ src64, double* __restrict__ partial,
+                                                   Params P, RunRec* rec)
+{
+	double acc[3] = { 0.0, 0.0, 0.0 };
+	if (rec->status == POT_OK) {
+		const uint32_t gs = rec->grain_slot;
+		for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P.n; s += gridDim.x * blockDim.x) {
+			const double4 p = src64[s];
+			int rc = POT_OK;
+			const double phi = phi_plain(s, p.x, p.y, p.z, T, src64, P, rc);
+			if (rc != POT_OK) set_status(rec, rc);
+			if (s == gs) {
+				rec->phi_grain = phi;
+				continue;
+			}
+			const int sp = (int)pos[s].w;
+			acc[sp] += (QE * p.w) * phi;
+		}
+	}
+	block_sum3(acc, &partial[3 * blockIdx.x]);
+}
+
+// Fixed-order sum of per-block (or per-group) partials into rec->epe.
+__global__ void __launch_bounds__(1024) k_epe_final(const double* __restrict__ partial, const unsigned int* count,
+                                                    uint32_t fixed, RunRec* rec)
+{
+	const uint32_t n = count ? *count : fixed;
+	double v[3] = { 0.0, 0.0, 0.0 };
+	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+		for (int k = 0; k < 3; k++) v[k] += partial[3 * i + k];
+	__shared__ double out[3];
+	block_sum3(v, out);
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		rec->epe[SP_ION] = out[SP_ION];
+		rec->epe[SP_E] = out[SP_E];
+	}
+}
+
 __device__ __forceinline__ void warp_add_u64(unsigned long long* dst, unsigned long long v)
 {
 #pragma unroll
@@ -164,7 +275,7 @@ __global__ void k_absorb_late(double4* __restrict__ pos, double4* __restrict__ v
 
 // Grain update of pot.c:2825-2848 and the step's statistics.
 __global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel, StepHist* hist, Params P,
-                            RunRec* rec)
+                            RunRec* rec, int epe)
 {
 	if (threadIdx.x != 0 || blockIdx.x != 0) return;
 	const double dm = (double)rec->nabs_ion * MASS_ION + (double)rec->nabs_e * MASS_E;
@@ -191,6 +302,10 @@ __global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel
 	rec->grain_m = m;
 	rec->grain_q += rec->dq;
 	rec->tot_absor_e += rec->de;
+	if (epe) {
+		// the grain's energy with its updated charge, pot.c:2859-2864
+		rec->epe[SP_DUST] = rec->grain_q ? (double)rec->grain_q * QE * rec->phi_grain : 0.0;
+	}
 	StepHist h;
 	h.t_steps = rec->t_steps;
 	h.grain_q = rec->grain_q;
@@ -204,6 +319,7 @@ __global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel
 	h.chi_b = rec->chi_b;
 	h.status = rec->status;
 	h.pad = (int)rec->warn;
+	for (int k = 0; k < 3; k++) h.epe[k] = epe ? rec->epe[k] : 0.0;
 	hist[rec->t_steps % HIST] = h;
 }
 
@@ -334,6 +450,8 @@ __global__ void k_field_query_plain(TreeDev T, const double4* __restrict__ src64
 void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,
                       const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P,
                       RunRec* rec, cudaStream_t s, Timer& tm);
+void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, uint2* groups_all, double* partial,
+                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 void launch_field_query_fast(const TreeDev& T, const float4* src32, const double* xyz, const uint32_t* self_slot,
                              uint32_t nq, double* E, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 
@@ -376,11 +494,25 @@ void launch_absorb_late(double4* pos, double4* vel, const double4* src64, const 
 	k_absorb_late<<<sm_count(), 256, 0, s>>>(pos, vel, src64, due_list, rein_list, P, rec);
 }
 
-void launch_grain_end(double4* pos, double4* vel, StepHist* hist, const Params& P, RunRec* rec, cudaStream_t s,
-                      Timer& tm)
+void launch_grain_end(double4* pos, double4* vel, StepHist* hist, const Params& P, RunRec* rec, int epe,
+                      cudaStream_t s, Timer& tm)
 {
 	ScopedKernel k(tm, "grain_end");
-	k_grain_end<<<1, 32, 0, s>>>(pos, vel, hist, P, rec);
+	k_grain_end<<<1, 32, 0, s>>>(pos, vel, hist, P, rec, epe);
+}
+
+void launch_epe(const double4* pos, const TreeDev& T, const double4* src64, const float4* src32, uint2* groups_all,
+                double* partial, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+{
+	if (P.form == POT_FORM_FAST) {
+		launch_epe_fast(pos, T, src32, groups_all, partial, P, rec, s, tm);
+		ScopedKernel k(tm, "epe_final");
+		k_epe_final<<<1, 1024, 0, s>>>(partial, &rec->n_groups_all, 0, rec);
+		return;
+	}
+	ScopedKernel k(tm, "epe_plain", 2);
+	k_epe_plain<<<EPE_BLOCKS, 128, 0, s>>>(pos, T, src64, partial, P, rec);
+	k_epe_final<<<1, 1024, 0, s>>>(partial, nullptr, EPE_BLOCKS, rec);
 }
 
 void launch_field_query(const TreeDev& T, const double4* src64, const float4* src32, const double* xyz,

@@ -80,7 +80,8 @@ struct Field {
 
 // unsoftened monopole of an accepted cell (pot.c:1737-1749); a cell is never
 // the target itself, so there is no exclusion test
-template <int TPL>
+// POT: accumulate the potential q / r in E.x instead (pot.c:1960-1973)
+template <int TPL, bool POT = false>
 __device__ __forceinline__ void accumulate_cell(Field<TPL>& E, const Targets<TPL>& T, float4 q)
 {
 #pragma unroll
@@ -88,15 +89,19 @@ __device__ __forceinline__ void accumulate_cell(Field<TPL>& E, const Targets<TPL
 		const float dx = T.t[k].x - q.x, dy = T.t[k].y - q.y, dz = T.t[k].z - q.z;
 		const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 		const float ri = rsqrtf(r2);
-		const float w = q.w * (ri * ri) * ri;
-		E.x[k] = fmaf(w, dx, E.x[k]);
-		E.y[k] = fmaf(w, dy, E.y[k]);
-		E.z[k] = fmaf(w, dz, E.z[k]);
+		if (POT) {
+			E.x[k] = fmaf(q.w, ri, E.x[k]);
+		} else {
+			const float w = q.w * (ri * ri) * ri;
+			E.x[k] = fmaf(w, dx, E.x[k]);
+			E.y[k] = fmaf(w, dy, E.y[k]);
+			E.z[k] = fmaf(w, dz, E.z[k]);
+		}
 	}
 }
 
 // softened pair contribution (pot.c:1789-1798) of particle q in slot qslot
-template <int TPL>
+template <int TPL, bool POT = false>
 __device__ __forceinline__ void accumulate(Field<TPL>& E, const Targets<TPL>& T, float4 q, float eps2, uint32_t qslot)
 {
 #pragma unroll
@@ -104,17 +109,21 @@ __device__ __forceinline__ void accumulate(Field<TPL>& E, const Targets<TPL>& T,
 		const float dx = T.t[k].x - q.x, dy = T.t[k].y - q.y, dz = T.t[k].z - q.z;
 		const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
 		const float ri = rsqrtf(r2);
-		const float w = (qslot == T.self[k]) ? 0.f : q.w * (ri * ri) * ri;
-		E.x[k] = fmaf(w, dx, E.x[k]);
-		E.y[k] = fmaf(w, dy, E.y[k]);
-		E.z[k] = fmaf(w, dz, E.z[k]);
+		if (POT) {
+			E.x[k] += (qslot == T.self[k]) ? 0.f : q.w * ri;
+		} else {
+			const float w = (qslot == T.self[k]) ? 0.f : q.w * (ri * ri) * ri;
+			E.x[k] = fmaf(w, dx, E.x[k]);
+			E.y[k] = fmaf(w, dy, E.y[k]);
+			E.z[k] = fmaf(w, dz, E.z[k]);
+		}
 	}
 }
 
 // Group walk.  Returns the fields in units of q / R^2 (multiply by
 // QE / (4 pi eps0 R^2) for V/m) and the number of entries evaluated per
 // target.
-template <int TPL>
+template <int TPL, bool POT = false>
 __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const float4* __restrict__ src32,
                                  const Params& P, FastSmem& sm, uint32_t& n_eval, int& err)
 {
@@ -213,7 +222,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			__syncwarp();
 			for (int j = 0; j < padded; j += 8) {
 #pragma unroll
-				for (int u = 0; u < 8; u++) accumulate_cell(E, tg, sm.cells[j + u]);
+				for (int u = 0; u < 8; u++) accumulate_cell<TPL, POT>(E, tg, sm.cells[j + u]);
 			}
 			n_cells_ev += ncell;
 			ncell = 0;
@@ -248,7 +257,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 				sm.pidx[lane] = id;
 				__syncwarp();
 #pragma unroll 16
-				for (int m = 0; m < 32; m++) accumulate(E, tg, sm.pbuf[m], eps2, sm.pidx[m]);
+				for (int m = 0; m < 32; m++) accumulate<TPL, POT>(E, tg, sm.pbuf[m], eps2, sm.pidx[m]);
 				__syncwarp();
 			}
 			n_parts_ev += total;
@@ -286,12 +295,12 @@ __device__ __forceinline__ void child_range(const TreeDev& T, int32_t code, cons
 	}
 }
 
-__device__ __forceinline__ void emit_groups(RunRec* rec, uint2* groups, uint32_t start, uint32_t count,
+__device__ __forceinline__ void emit_groups(unsigned int* ctr, uint2* groups, uint32_t start, uint32_t count,
                                             uint32_t gmax)
 {
 	while (count > 0) {
 		const uint32_t c = count < gmax ? count : gmax;
-		groups[atomicAdd(&rec->n_groups, 1u)] = make_uint2(start, c);
+		groups[atomicAdd(ctr, 1u)] = make_uint2(start, c);
 		start += c;
 		count -= c;
 	}
@@ -305,18 +314,23 @@ __device__ __forceinline__ void emit_groups(RunRec* rec, uint2* groups, uint32_t
 // full groups across child boundaries fills warps but widens boxes: 18 %
 // more interactions and a slower walk at 1M particles.)  A group is a range
 // of the due list.
-__global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __restrict__ groups, Params P,
-                         RunRec* rec)
+// dpre == nullptr groups every particle (dpre[s] = s).
+__device__ __forceinline__ uint32_t dpre_at(const uint32_t* __restrict__ dpre, uint32_t s)
+{
+	return dpre ? dpre[s] : s;
+}
+
+__global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __restrict__ groups,
+                         unsigned int* ctr, uint32_t gmax, Params P, RunRec* rec)
 {
 	if (rec->status != POT_OK) return;
 	const uint32_t M = rec->n_nodes;
-	const uint32_t gmax = P.group_max;
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
 		const uint32_t a = T.first[k], b = T.last[k] + 1;
-		const uint32_t d = dpre[b] - dpre[a];
+		const uint32_t d = dpre_at(dpre, b) - dpre_at(dpre, a);
 		if (d == 0) continue;
 		if (d <= gmax) {
-			if (k == 0) emit_groups(rec, groups, dpre[a], d, gmax);
+			if (k == 0) emit_groups(ctr, groups, dpre_at(dpre, a), d, gmax);
 			continue;
 		}
 		uint32_t run_start = 0, run = 0;
@@ -325,21 +339,21 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 			if (code == CH_EMPTY) continue;
 			uint32_t ca, cb;
 			child_range(T, code, P, ca, cb);
-			const uint32_t dc = dpre[cb] - dpre[ca];
+			const uint32_t dc = dpre_at(dpre, cb) - dpre_at(dpre, ca);
 			if (dc == 0) continue;
 			if (code >= 0 && dc > gmax) {
-				emit_groups(rec, groups, run_start, run, gmax);
+				emit_groups(ctr, groups, run_start, run, gmax);
 				run = 0;
 				continue;
 			}
 			if (run + dc > gmax) {
-				emit_groups(rec, groups, run_start, run, gmax);
+				emit_groups(ctr, groups, run_start, run, gmax);
 				run = 0;
 			}
-			if (run == 0) run_start = dpre[ca];
+			if (run == 0) run_start = dpre_at(dpre, ca);
 			run += dc;
 		}
-		emit_groups(rec, groups, run_start, run, gmax);
+		emit_groups(ctr, groups, run_start, run, gmax);
 	}
 }
 
@@ -490,7 +504,67 @@ void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const 
 {
 	cudaMemsetAsync(&rec->n_groups, 0, sizeof(unsigned int), s);
 	ScopedKernel k(tm, "groups");
-	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, dpre, groups, P, rec);
+	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, dpre, groups, &rec->n_groups, P.group_max, P, rec);
+}
+
+// compute_epe (pot.c:2771-2804), fast form: groups of 32 over every particle,
+// the group walk accumulating potentials; per-group partial sums of
+// q e phi per species, summed in group order by k_epe_final.
+__global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __restrict__ pos, TreeDev T,
+                                                           const float4* __restrict__ src32,
+                                                           const uint2* __restrict__ groups,
+                                                           double* __restrict__ partial, Params P, RunRec* rec)
+{
+	__shared__ FastSmem smem[FW_WARPS];
+	FastSmem& sm = smem[threadIdx.x >> 5];
+	if (rec->status != POT_OK) return;
+	const uint32_t n_groups = rec->n_groups_all;
+	const uint32_t gs = rec->grain_slot;
+	const double pscale = QE / (P.k4 * P.rad);
+	for (;;) {
+		uint32_t g = 0;
+		if (lane_f() == 0) g = atomicAdd(&rec->work_ctr2, 1u);
+		g = __shfl_sync(0xffffffffu, g, 0);
+		if (g >= n_groups) break;
+		const uint2 grp = groups[g];
+		Targets<1> tg;
+		const uint32_t slot = grp.x + lane_f();
+		tg.valid[0] = lane_f() < grp.y;
+		tg.self[0] = tg.valid[0] ? slot : 0xFFFFFFFFu;
+		const float4 me = tg.valid[0] ? src32[slot] : make_float4(0.f, 0.f, 0.f, 0.f);
+		tg.t[0] = make_float3(me.x, me.y, me.z);
+		uint32_t ne = 0;
+		int err = POT_OK;
+		const Field<1> f = group_walk<1, true>(tg, T, src32, P, sm, ne, err);
+		if (err != POT_OK) {
+			if (lane_f() == 0) set_status(rec, err);
+			break;
+		}
+		double acc[3] = { 0.0, 0.0, 0.0 };
+		if (tg.valid[0]) {
+			const double phi = (double)f.x[0] * pscale;
+			if (slot == gs) {
+				rec->phi_grain = phi;
+			} else {
+				acc[(int)pos[slot].w] = (QE * (double)me.w) * phi;
+			}
+		}
+#pragma unroll
+		for (int k = 0; k < 3; k++)
+			for (int o = 16; o; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+		if (lane_f() == 0)
+			for (int k = 0; k < 3; k++) partial[3 * g + k] = acc[k];
+	}
+}
+
+void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, uint2* groups_all, double* partial,
+                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+{
+	cudaMemsetAsync(&rec->n_groups_all, 0, sizeof(unsigned int), s);
+	cudaMemsetAsync(&rec->work_ctr2, 0, sizeof(unsigned int), s);
+	ScopedKernel k(tm, "epe_fast", 2);
+	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, nullptr, groups_all, &rec->n_groups_all, 32u, P, rec);
+	k_epe_fast<<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, groups_all, partial, P, rec);
 }
 
 void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,

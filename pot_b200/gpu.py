@@ -37,6 +37,7 @@ STATUS_NAMES = {0: "POT_OK", -1: "POT_E_ARG", -2: "POT_E_CUDA", -3: "POT_E_NOMEM
                 -9: "POT_E_CAPACITY", -10: "POT_E_STATE", -11: "POT_E_LIMIT"}
 NOALLOC_MAX_POINTS = 65536
 FORM_PLAIN, FORM_FAST = 0, 1
+STEP_EPE = 0x1
 CFG_SCEPTIC, CFG_DISABLE_GRAIN = 0x1, 0x2
 OPT_TIMING = 0x1
 
@@ -71,7 +72,7 @@ class _Stats(C.Structure):
     _fields_ = [("t_steps", C.c_uint64), ("grain_q", C.c_int64), ("dq", C.c_int64), ("de", C.c_uint64),
                 ("n_absorbed", C.c_uint64), ("n_reinjected", C.c_uint64), ("n_pushed", C.c_uint64),
                 ("interactions", C.c_uint64), ("n_nodes", C.c_uint64), ("chi_b", C.c_double),
-                ("status", C.c_int32), ("pad", C.c_uint32)]
+                ("status", C.c_int32), ("pad", C.c_uint32), ("epe", C.c_double * 3)]
 
 
 _LIB = None
@@ -110,7 +111,7 @@ def load_library(path: str = LIB_PATH, build_if_stale: bool = True):
     L.pot_gpu_upload.argtypes = [vp, vp, u64, C.POINTER(_Grain)]
     L.pot_gpu_init_particles.argtypes = [vp]
     L.pot_gpu_step.argtypes = [vp, u32, u32, C.POINTER(_Stats)]
-    L.pot_gpu_step_async.argtypes = [vp, u32]
+    L.pot_gpu_step_async.argtypes = [vp, u32, u32]
     L.pot_gpu_download.argtypes = [vp, vp, C.POINTER(_Grain)]
     L.pot_gpu_move_particles.argtypes = [vp, vp, u64, C.POINTER(_Grain), C.POINTER(_Stats)]
     L.pot_gpu_build_tree.argtypes = [vp, C.POINTER(u64)]
@@ -164,6 +165,12 @@ class RunConfig:
 
 def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def _stats_dict(st: "_Stats") -> dict:
+    d = {k: getattr(st, k) for k, _ in _Stats._fields_ if k not in ("pad", "epe")}
+    d["epe"] = np.array(list(st.epe))
+    return d
 
 
 def _grain_dict(g: _Grain) -> dict:
@@ -239,14 +246,15 @@ class Run:
     def init_particles(self):
         self._check(self.lib.pot_gpu_init_particles(self.h), "pot_gpu_init_particles")
 
-    def step(self, n: int = 1) -> dict:
+    def step(self, n: int = 1, epe: bool = False) -> dict:
+        """Run n steps; epe=True also computes the potential energies."""
         st = _Stats()
-        self._check(self.lib.pot_gpu_step(self.h, int(n), 0, C.byref(st)), "pot_gpu_step")
-        return {k: getattr(st, k) for k, _ in _Stats._fields_ if k != "pad"}
+        self._check(self.lib.pot_gpu_step(self.h, int(n), STEP_EPE if epe else 0, C.byref(st)), "pot_gpu_step")
+        return _stats_dict(st)
 
-    def step_async(self, n: int = 1):
+    def step_async(self, n: int = 1, epe: bool = False):
         """Enqueue n steps without waiting (errors surface at the next sync)."""
-        self._check(self.lib.pot_gpu_step_async(self.h, int(n)), "pot_gpu_step_async")
+        self._check(self.lib.pot_gpu_step_async(self.h, int(n), STEP_EPE if epe else 0), "pot_gpu_step_async")
 
     def download(self):
         out = np.zeros(self.cfg.N, PARTICLE_DTYPE)
@@ -261,7 +269,7 @@ class Run:
         st = _Stats()
         self._check(self.lib.pot_gpu_move_particles(self.h, _ptr(parts), len(parts), C.byref(g), C.byref(st)),
                     "pot_gpu_move_particles")
-        return _grain_dict(g), {k: getattr(st, k) for k, _ in _Stats._fields_ if k != "pad"}
+        return _grain_dict(g), _stats_dict(st)
 
     # -- inspection ---------------------------------------------------------------
     def build_tree(self) -> int:

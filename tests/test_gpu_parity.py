@@ -164,6 +164,55 @@ def test_one_step_plain_vs_oracle(d, sceptic, steps):
     assert abs(gg["m"] - go["m"]) <= 1e-15 * go["m"]
 
 
+@pytest.mark.parametrize("form", ["plain", "fast"])
+def test_potential_energies_match_oracle(form):
+    """compute_epe (pot.c:2771-2804): q e phi summed per species at the
+    step-start positions, the grain's from its end-of-step charge."""
+    d = dict(STRESS, N=20001)
+    o = oracle_snapshot(d, seed=13, mode="gpu", steps=2)
+    P0, g0 = o.particles().copy(), o.grain()
+    with gpu_from_oracle(d, o, form=form, leaf_size=1 if form == "plain" else 16) as r:
+        st = r.step(1, epe=True)
+        st_plain = r.step(1)
+    o.step(compute_epe=True)
+    ref = o.last_step_stats()["epe"]
+    assert st["status"] == 0
+    assert np.all(st_plain["epe"] == 0.0)
+    scale = np.abs(ref).max()
+    assert scale > 0
+    if form == "plain":
+        assert np.all(np.abs(st["epe"] - ref) <= 1e-10 * scale), (st["epe"], ref)
+        return
+    # The reference's monopole-at-centre-of-|q| cells leave tens of percent of
+    # error in these sums of a quasi-neutral plasma; the fast form's tree
+    # (leaves of 16, box criterion) must approximate no worse than that.
+    exact = _direct_epe(P0, g0["q"], o.grain()["q"], d["soft"])
+    ref_err = np.abs(ref - exact)
+    fast_err = np.abs(st["epe"] - exact)
+    assert np.all(fast_err <= 1.25 * ref_err + 2e-2 * scale), (st["epe"], ref, exact)
+    assert np.all(np.abs(st["epe"] - ref) <= 0.1 * scale), (st["epe"], ref)
+
+
+def _direct_epe(P, q_grain_start, q_grain_end, soft):
+    """Softened FP64 direct sum of compute_epe's sums (pot.c:2771-2804)."""
+    QE, EPS0, PI = 1.60217646e-19, 8.854187817e-12, 3.14159265358979
+    x = np.stack([P["x"], P["y"], P["z"]], 1)
+    sp = P["species"]
+    q = np.where(sp == ELECTRON, -1.0, np.where(sp == ION, 1.0, float(q_grain_start)))
+    phi = np.zeros(len(x))
+    for a in range(0, len(x), 1000):
+        b = min(a + 1000, len(x))
+        r = np.sqrt(((x[a:b, None, :] - x[None, :, :]) ** 2).sum(-1) + soft * soft)
+        w = QE * q[None, :] / (4 * PI * EPS0 * r)
+        w[np.arange(b - a), np.arange(a, b)] = 0.0
+        phi[a:b] = w.sum(1)
+    out = np.zeros(3)
+    for s in (ION, ELECTRON):
+        out[s] = (QE * q[sp == s] * phi[sp == s]).sum()
+    out[DUST] = q_grain_end * QE * phi[0]
+    return out
+
+
 def test_absorption_happens_and_matches():
     """Many steps of the stress case with a big grain: absorptions occur and
     the charge tally matches the oracle step by step while the states agree."""
