@@ -248,13 +248,14 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     assert stream.cuda_stream != 0
     cfgd = CONFIGS[args.config]
-    cfg = run_config(args.config)
+    cfg = run_config(args.config, N=args.particles or None)
     N = cfg.N
     n_plasma = N - 1
     hbm_peak, peak_kind = peaks()
 
-    run = Run(cfg, form=args.form, leaf_size=args.leaf or cfgd["leaf_size"], seed=1 + rank, device=local,
-              stream=stream.cuda_stream, timing=True)
+    group = args.group or cfgd.get("group_size", 32)
+    run = Run(cfg, form=args.form, leaf_size=args.leaf or cfgd["leaf_size"], group_size=group, seed=1 + rank,
+              device=local, stream=stream.cuda_stream, timing=True)
     run.init_particles()
     # warm-up
     for _ in range(args.warmup):
@@ -361,6 +362,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 force / f64 state", "data": "synthetic",
             "config": {"workload": WORKLOAD, "N": N, "form": args.form, "leaf_size": args.leaf or cfgd["leaf_size"],
+                       "group_size": group,
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
                        "parallelism": "replicas" if ws > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm_peak,
@@ -371,7 +373,7 @@ def run_ours(args):
             "interactions_per_s": (inter * ws / (t_ms / args.steps / 1e3)) if inter else None,
             "kernels_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
             "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
-            "status": st["status"]}
+            "walk_stack_max": st.get("stack_max"), "status": st["status"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     run.close()
@@ -390,6 +392,9 @@ def main(argv=None):
     ap.add_argument("--config", default="1m")
     ap.add_argument("--form", choices=("fast", "plain"), default="fast")
     ap.add_argument("--leaf", type=int, default=0)
+    ap.add_argument("--group", type=int, default=0, help="targets per warp group (32 or 64; default per config)")
+    ap.add_argument("--particles", type=int, default=0,
+                    help="override N (same domain and flags): a smaller case of the same kernels for profiling")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -117,10 +117,15 @@ typedef struct pot_step_stats {
 	uint64_t n_nodes;      /* internal tree nodes this step */
 	double chi_b;          /* edge potential in force after the step */
 	int32_t status;        /* POT_OK or the first device-side error */
-	uint32_t pad;
+	uint32_t stack_max;    /* fast form: deepest per-warp walk stack this step
+	                          (POT_WALK_STACK entries at most; 0 in the plain form) */
 	double epe[3];         /* POT_STEP_EPE: electrostatic potential energy (J) of the
 	                          grain, the ions, the electrons (Proc.epe, pot.c:2771-2864) */
 } pot_step_stats;
+
+/* capacity of the fast form's per-warp stack of cells awaiting a test;
+   a walk that needs more fails with POT_E_WALK */
+#define POT_WALK_STACK 1536
 
 /* pot_gpu_step flags */
 #define POT_STEP_EPE 0x1u  /* compute the potential energies (pot.c:2771-2804) */

@@ -29,6 +29,7 @@ def run_config(name: str, N: int | None = None, **over) -> RunConfig:
     c = dict(CONFIGS[name])
     c.pop("steps")
     c.pop("leaf_size")
+    c.pop("group_size", None)
     if N is not None:
         c["N"] = int(N)
     c.update(over)

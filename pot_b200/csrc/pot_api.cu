@@ -614,6 +614,7 @@ int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats
 		out->n_nodes = h.n_nodes;
 		out->chi_b = r.chi_b;
 		out->status = r.status;
+		out->stack_max = r.stack_max;
 		for (int k = 0; k < 3; k++) out->epe[k] = h.epe[k];
 	}
 	return st;

@@ -77,6 +77,7 @@ struct RunRec {
 	unsigned int n_nodes;
 	unsigned int work_ctr;   // dynamic work distribution counter
 	unsigned int work_ctr2;  // second counter (potential-energy walk)
+	unsigned int stack_max;  // deepest fast-walk stack this step
 	unsigned int grain_due;
 	unsigned int warn;       // non-fatal conditions (bit 0: key collision at 21 levels)
 	unsigned int n_overflow; // deepest-level buckets of a leaf-size-1 tree this build

@@ -82,6 +82,7 @@ __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ k
 		rec->n_nodes = 0;
 		rec->work_ctr = 0;
 		rec->work_ctr2 = 0;
+		rec->stack_max = 0;
 		rec->grain_due = (t % P.tss[SP_DUST]) == 0 ? 1u : 0u;
 		rec->dq = 0;
 		rec->de = 0;

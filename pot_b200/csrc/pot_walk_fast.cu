@@ -28,20 +28,25 @@ namespace pot {
 
 constexpr int FW_WARPS = 4;        // warps per block
 constexpr int FW_TPL_MAX = 2;      // targets per lane (1 or 2; groups of 32 or 64)
-constexpr int FW_STACK = 1536;     // cells awaiting a test, per warp
+constexpr int FW_STACK = POT_WALK_STACK;  // cells awaiting a test, per warp
 constexpr int FW_CELLS = 104;      // staged monopoles (flush at >= 64, padded to a multiple of 8)
 constexpr int FW_CELL_FLUSH = 64;
 constexpr int FW_LEAVES = 64;      // staged leaf ranges (flush at >= 32)
 constexpr int FW_LEAF_FLUSH = 32;
 static_assert(GROUP_MAX == 32 * FW_TPL_MAX, "one group per warp, at most FW_TPL_MAX targets per lane");
 
+// Per-warp shared memory.  A staged source (accepted cell or gathered
+// particle) takes TPL float4s: with one target per lane it is (x, y, z, q);
+// with two it is stored duplicated and negated as (-x, -x, -y, -y),
+// (-z, -z, q, q) so that each half is a ready operand of the packed FP32x2
+// instructions that evaluate both targets of a lane at once.
+template <int TPL>
 struct FastSmem {
 	int32_t stack[FW_STACK];
-	float4 cells[FW_CELLS];
+	float4 cells[FW_CELLS * TPL];
 	uint2 leaves[FW_LEAVES];
 	uint32_t loff[FW_LEAVES];  // exclusive prefix of the staged leaves' particle counts
-	float4 pbuf[32];           // one 32-particle chunk of opened leaves
-	uint32_t pidx[32];         // their slots (self exclusion)
+	float4 pbuf[32 * TPL];     // one 32-particle chunk of opened leaves
 };
 
 __device__ __forceinline__ uint32_t lane_f() { return threadIdx.x & 31u; }
@@ -78,56 +83,135 @@ struct Field {
 	float x[TPL], y[TPL], z[TPL];
 };
 
-// unsoftened monopole of an accepted cell (pot.c:1737-1749); a cell is never
-// the target itself, so there is no exclusion test
-// POT: accumulate the potential q / r in E.x instead (pot.c:1960-1973)
-template <int TPL, bool POT = false>
-__device__ __forceinline__ void accumulate_cell(Field<TPL>& E, const Targets<TPL>& T, float4 q)
+// Field sums in evaluation form: scalars for one target per lane; for two,
+// FP32x2 pairs (target 0 in .x, target 1 in .y).
+template <int TPL> struct Acc;
+template <> struct Acc<1> { float x, y, z; };
+template <> struct Acc<2> { float2 x, y, z; };
+
+template <int TPL> struct TgtE;
+template <> struct TgtE<1> { float x, y, z; };
+template <> struct TgtE<2> { float2 x, y, z; };
+
+__device__ __forceinline__ void stage_src(float4* buf, int i, float4 c, Acc<1>*) { buf[i] = c; }
+__device__ __forceinline__ void stage_src(float4* buf, int i, float4 c, Acc<2>*)
 {
-#pragma unroll
-	for (int k = 0; k < TPL; k++) {
-		const float dx = T.t[k].x - q.x, dy = T.t[k].y - q.y, dz = T.t[k].z - q.z;
-		const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-		const float ri = rsqrtf(r2);
-		if (POT) {
-			E.x[k] = fmaf(q.w, ri, E.x[k]);
-		} else {
-			const float w = q.w * (ri * ri) * ri;
-			E.x[k] = fmaf(w, dx, E.x[k]);
-			E.y[k] = fmaf(w, dy, E.y[k]);
-			E.z[k] = fmaf(w, dz, E.z[k]);
-		}
+	buf[2 * i] = make_float4(-c.x, -c.x, -c.y, -c.y);
+	buf[2 * i + 1] = make_float4(-c.z, -c.z, c.w, c.w);
+}
+
+// One source against the lane's target(s).  SOFT: Plummer-softened pair
+// (pot.c:1789-1798); else an unsoftened monopole (pot.c:1737-1749).  POT:
+// accumulate q / r in .x (pot.c:1960-1973).  The operation order is the same
+// in both forms: r2 = dx dx + (dy dy + (dz dz [+ eps2])), w = (q ri^2) ri.
+template <bool SOFT, bool POT>
+__device__ __forceinline__ void eval_src(Acc<1>& E, const TgtE<1>& t, const float4* buf, int i, float eps2)
+{
+	const float4 q = buf[i];
+	const float dx = t.x - q.x, dy = t.y - q.y, dz = t.z - q.z;
+	const float r2 = fmaf(dx, dx, fmaf(dy, dy, SOFT ? fmaf(dz, dz, eps2) : dz * dz));
+	const float ri = rsqrtf(r2);
+	if (POT) {
+		E.x = fmaf(q.w, ri, E.x);
+	} else {
+		const float w = q.w * (ri * ri) * ri;
+		E.x = fmaf(w, dx, E.x);
+		E.y = fmaf(w, dy, E.y);
+		E.z = fmaf(w, dz, E.z);
 	}
 }
 
-// softened pair contribution (pot.c:1789-1798) of particle q in slot qslot
-template <int TPL, bool POT = false>
-__device__ __forceinline__ void accumulate(Field<TPL>& E, const Targets<TPL>& T, float4 q, float eps2, uint32_t qslot)
+template <bool SOFT, bool POT>
+__device__ __forceinline__ void eval_src(Acc<2>& E, const TgtE<2>& t, const float4* buf, int i, float eps2)
 {
-#pragma unroll
-	for (int k = 0; k < TPL; k++) {
-		const float dx = T.t[k].x - q.x, dy = T.t[k].y - q.y, dz = T.t[k].z - q.z;
-		const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-		const float ri = rsqrtf(r2);
-		if (POT) {
-			E.x[k] += (qslot == T.self[k]) ? 0.f : q.w * ri;
-		} else {
-			const float w = (qslot == T.self[k]) ? 0.f : q.w * (ri * ri) * ri;
-			E.x[k] = fmaf(w, dx, E.x[k]);
-			E.y[k] = fmaf(w, dy, E.y[k]);
-			E.z[k] = fmaf(w, dz, E.z[k]);
-		}
+	const float4 a = buf[2 * i], b = buf[2 * i + 1];
+	const float2 dx = __fadd2_rn(t.x, make_float2(a.x, a.y));
+	const float2 dy = __fadd2_rn(t.y, make_float2(a.z, a.w));
+	const float2 dz = __fadd2_rn(t.z, make_float2(b.x, b.y));
+	const float2 q = make_float2(b.z, b.w);
+	float2 r2 = SOFT ? __ffma2_rn(dz, dz, make_float2(eps2, eps2)) : __fmul2_rn(dz, dz);
+	r2 = __ffma2_rn(dy, dy, r2);
+	r2 = __ffma2_rn(dx, dx, r2);
+	const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+	if (POT) {
+		E.x = __ffma2_rn(q, ri, E.x);
+	} else {
+		const float2 w = __fmul2_rn(__fmul2_rn(q, __fmul2_rn(ri, ri)), ri);
+		E.x = __ffma2_rn(w, dx, E.x);
+		E.y = __ffma2_rn(w, dy, E.y);
+		E.z = __ffma2_rn(w, dz, E.z);
 	}
+}
+
+__device__ __forceinline__ void to_eval(const Targets<1>& tg, TgtE<1>& t, Acc<1>& E)
+{
+	t.x = tg.t[0].x;
+	t.y = tg.t[0].y;
+	t.z = tg.t[0].z;
+	E.x = E.y = E.z = 0.f;
+}
+__device__ __forceinline__ void to_eval(const Targets<2>& tg, TgtE<2>& t, Acc<2>& E)
+{
+	t.x = make_float2(tg.t[0].x, tg.t[1].x);
+	t.y = make_float2(tg.t[0].y, tg.t[1].y);
+	t.z = make_float2(tg.t[0].z, tg.t[1].z);
+	E.x = E.y = E.z = make_float2(0.f, 0.f);
+}
+__device__ __forceinline__ Field<1> from_eval(const Acc<1>& E)
+{
+	Field<1> f;
+	f.x[0] = E.x;
+	f.y[0] = E.y;
+	f.z[0] = E.z;
+	return f;
+}
+__device__ __forceinline__ Field<2> from_eval(const Acc<2>& E)
+{
+	Field<2> f;
+	f.x[0] = E.x.x;
+	f.x[1] = E.x.y;
+	f.y[0] = E.y.x;
+	f.y[1] = E.y.y;
+	f.z[0] = E.z.x;
+	f.z[1] = E.z.y;
+	return f;
 }
 
 // Group walk.  Returns the fields in units of q / R^2 (multiply by
 // QE / (4 pi eps0 R^2) for V/m) and the number of entries evaluated per
 // target.
+//
+// Self exclusion (pot.c:1789, node->part != part).  A target's own particle
+// can only be evaluated as a particle of an opened leaf.  Opened leaves
+// whose slot range meets the group's [min, max] self slots are few (the
+// group lies inside one cell); for those the lanes test membership, and a
+// target whose own particle was evaluated gets that same FP32 term
+// subtracted at the end.  The softening is floored at 1e-20 R^2 (far below
+// FP32 resolution of positions) so that the term is finite when a target sits
+// exactly on its own particle.
 template <int TPL, bool POT = false>
 __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const float4* __restrict__ src32,
-                                 const Params& P, FastSmem& sm, uint32_t& n_eval, int& err)
+                                 const Params& P, FastSmem<TPL>& sm, uint32_t& n_eval, uint32_t& stack_max,
+                                 int& err)
 {
 	const uint32_t lane = lane_f();
+	uint32_t smin = 0xFFFFFFFFu, smax = 0u;
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		if (tg.valid[k] && tg.self[k] != 0xFFFFFFFFu) {
+			smin = min(smin, tg.self[k]);
+			smax = max(smax, tg.self[k]);
+		}
+	}
+#pragma unroll
+	for (int o = 16; o; o >>= 1) {
+		smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+		smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+	}
+	bool seen[TPL];
+#pragma unroll
+	for (int k = 0; k < TPL; k++) seen[k] = false;
+	int maxlen = 1;
 	// bounding box of the valid targets
 	float3 bmin = make_float3(3.0e38f, 3.0e38f, 3.0e38f), bmax = make_float3(-3.0e38f, -3.0e38f, -3.0e38f);
 #pragma unroll
@@ -146,11 +230,12 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		bmax.y = fmaxf(bmax.y, __shfl_xor_sync(0xffffffffu, bmax.y, o));
 		bmax.z = fmaxf(bmax.z, __shfl_xor_sync(0xffffffffu, bmax.z, o));
 	}
-	const float eps2 = P.soft2_f;
+	const float eps2 = fmaxf(P.soft2_f, 1e-20f);
 	const bool single_leaves = P.leaf_size == 1;
-	Field<TPL> E;
-#pragma unroll
-	for (int k = 0; k < TPL; k++) E.x[k] = E.y[k] = E.z[k] = 0.f;
+	TgtE<TPL> te;
+	Acc<TPL> E;
+	to_eval(tg, te, E);
+	Acc<TPL>* tag = nullptr;  // selects the staging layout
 	int len = 1, ncell = 0, nleaf = 0;
 	uint32_t n_cells_ev = 0, n_parts_ev = 0;
 	if (lane == 0) sm.stack[0] = 0;
@@ -166,7 +251,9 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
 			uint2 range = make_uint2(0u, 0u);
 			int nch = 0;
-			int32_t ch[8];
+			int32_t cc[8];
+#pragma unroll
+			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
 			if (code >= 0) {
 				cell = T.f[code];
 				if (box_d2(bmin, bmax, cell) > T.r2[code]) {
@@ -174,10 +261,10 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 				} else {
 					const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * (uint32_t)code]);
 					const int4 c0 = cp[0], c1 = cp[1];
-					const int32_t cc[8] = { c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w };
+					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
+					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
 #pragma unroll
-					for (int d = 0; d < 8; d++)
-						if (cc[d] != CH_EMPTY) ch[nch++] = cc[d];
+					for (int d = 0; d < 8; d++) nch += cc[d] != CH_EMPTY;
 				}
 			} else if (code != CH_EMPTY) {
 				const uint32_t e = leaf_payload(code);
@@ -202,27 +289,41 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			const int off = warp_excl(packed, tot);
 			const int co = off & 0x3FF, lo = (off >> 10) & 0x3FF, po = off >> 20;
 			const int tcell = tot & 0x3FF, tleaf = (tot >> 10) & 0x3FF, tch = tot >> 20;
-			if (acc) sm.cells[ncell + co] = cell;
+			if (acc) stage_src(sm.cells, ncell + co, cell, tag);
 			ncell += tcell;
 			if (leafr) sm.leaves[nleaf + lo] = range;
 			nleaf += tleaf;
+			// opened leaves that may hold members' own particles
+			unsigned int hits = __ballot_sync(0xffffffffu, leafr && range.x <= smax && range.x + range.y > smin);
+			while (hits) {
+				const int b = __ffs(hits) - 1;
+				hits &= hits - 1;
+				const uint32_t rx = __shfl_sync(0xffffffffu, range.x, b);
+				const uint32_t ry = __shfl_sync(0xffffffffu, range.y, b);
+#pragma unroll
+				for (int k = 0; k < TPL; k++) seen[k] = seen[k] || (tg.self[k] - rx < ry);
+			}
 			if (len + tch > FW_STACK) {
 				err = POT_E_WALK;
 				break;
 			}
-			for (int j = 0; j < nch; j++) sm.stack[len + po + j] = ch[j];
+			int w = len + po;
+#pragma unroll
+			for (int d = 0; d < 8; d++)
+				if (cc[d] != CH_EMPTY) sm.stack[w++] = cc[d];
 			len += tch;
+			maxlen = max(maxlen, len);
 			__syncwarp();
 		}
 		// flush staged monopoles, padded to a multiple of 8 with zero-charge
 		// cells far outside the domain so the loop needs no remainder
 		if (ncell >= FW_CELL_FLUSH || (done && ncell > 0)) {
 			const int padded = (ncell + 7) & ~7;
-			if ((int)lane < padded - ncell) sm.cells[ncell + lane] = make_float4(64.f, 64.f, 64.f, 0.f);
+			if ((int)lane < padded - ncell) stage_src(sm.cells, ncell + lane, make_float4(64.f, 64.f, 64.f, 0.f), tag);
 			__syncwarp();
 			for (int j = 0; j < padded; j += 8) {
 #pragma unroll
-				for (int u = 0; u < 8; u++) accumulate_cell<TPL, POT>(E, tg, sm.cells[j + u]);
+				for (int u = 0; u < 8; u++) eval_src<false, POT>(E, te, sm.cells, j + u, eps2);
 			}
 			n_cells_ev += ncell;
 			ncell = 0;
@@ -242,22 +343,20 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			__syncwarp();
 			for (uint32_t base = 0; base < total; base += 32) {
 				const uint32_t g = base + lane;
-				float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-				uint32_t id = 0xFFFFFFFFu;
+				// padding: zero charge far outside the domain
+				float4 p = make_float4(64.f, 64.f, 64.f, 0.f);
 				if (g < total) {
 					int a = 0, b = nleaf - 1;
 					while (a < b) {  // last staged leaf whose offset <= g
 						const int mid = (a + b + 1) >> 1;
 						if (sm.loff[mid] <= g) a = mid; else b = mid - 1;
 					}
-					id = sm.leaves[a].x + (g - sm.loff[a]);
-					p = __ldg(&src32[id]);
+					p = __ldg(&src32[sm.leaves[a].x + (g - sm.loff[a])]);
 				}
-				sm.pbuf[lane] = p;
-				sm.pidx[lane] = id;
+				stage_src(sm.pbuf, (int)lane, p, tag);
 				__syncwarp();
 #pragma unroll 16
-				for (int m = 0; m < 32; m++) accumulate<TPL, POT>(E, tg, sm.pbuf[m], eps2, sm.pidx[m]);
+				for (int m = 0; m < 32; m++) eval_src<true, POT>(E, te, sm.pbuf, m, eps2);
 				__syncwarp();
 			}
 			n_parts_ev += total;
@@ -266,8 +365,27 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		}
 		if (done) break;
 	}
+	Field<TPL> F = from_eval(E);
+	// take back the members' own terms
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		if (seen[k]) {
+			Acc<1> s1;
+			TgtE<1> t1;
+			t1.x = tg.t[k].x;
+			t1.y = tg.t[k].y;
+			t1.z = tg.t[k].z;
+			s1.x = s1.y = s1.z = 0.f;
+			const float4 own = __ldg(&src32[tg.self[k]]);
+			eval_src<true, POT>(s1, t1, &own, 0, eps2);
+			F.x[k] -= s1.x;
+			F.y[k] -= s1.y;
+			F.z[k] -= s1.z;
+		}
+	}
 	n_eval = n_cells_ev + n_parts_ev;
-	return E;
+	stack_max = (uint32_t)maxlen;
+	return F;
 }
 
 // Slot range [a, b) of a child code.
@@ -365,8 +483,8 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict
                                                             uint32_t* __restrict__ rein_list, Params P,
                                                             RunRec* rec)
 {
-	__shared__ FastSmem smem[FW_WARPS];
-	FastSmem& sm = smem[threadIdx.x >> 5];
+	__shared__ FastSmem<TPL> smem[FW_WARPS];
+	FastSmem<TPL>& sm = smem[threadIdx.x >> 5];
 	if (rec->status != POT_OK) return;
 	const uint32_t n_groups = rec->n_groups;
 	const unsigned long long t_step = rec->t_steps;
@@ -376,6 +494,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict
 	const double qg = (double)rec->grain_q;
 	const double escale = QE / (P.k4 * P.rad * P.rad);
 	unsigned long long n_inter = 0, n_push = 0;
+	uint32_t stack_max = 0;
 	for (;;) {
 		uint32_t g = 0;
 		if (lane_f() == 0) g = atomicAdd(&rec->work_ctr, 1u);
@@ -402,9 +521,10 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict
 			tg.t[k] = make_float3((float)((h[k].x - P.rad) * P.inv_rad), (float)((h[k].y - P.rad) * P.inv_rad),
 			                      (float)((h[k].z - P.rad) * P.inv_rad));
 		}
-		uint32_t ne = 0;
+		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, err);
+		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, depth, err);
+		stack_max = max(stack_max, depth);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
 			break;
@@ -440,6 +560,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict
 	if (lane_f() == 0) {
 		if (a) atomicAdd(&rec->interactions, a);
 		if (b) atomicAdd(&rec->n_pushed, b);
+		if (stack_max) atomicMax(&rec->stack_max, stack_max);
 	}
 }
 
@@ -450,8 +571,8 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_field_query_fast(TreeDev T, c
                                                                    uint32_t nq, double* __restrict__ E, Params P,
                                                                    RunRec* rec)
 {
-	__shared__ FastSmem smem[FW_WARPS];
-	FastSmem& sm = smem[threadIdx.x >> 5];
+	__shared__ FastSmem<TPL> smem[FW_WARPS];
+	FastSmem<TPL>& sm = smem[threadIdx.x >> 5];
 	const uint32_t gsize = 32u * TPL;
 	const uint32_t n_groups = (nq + gsize - 1) / gsize;
 	const double escale = QE / (P.k4 * P.rad * P.rad);
@@ -472,9 +593,9 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_field_query_fast(TreeDev T, c
 				tg.self[k] = self_slot[j];
 			}
 		}
-		uint32_t ne = 0;
+		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, err);
+		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, depth, err);
 		if (err != POT_OK && lane_f() == 0) set_status(rec, err);
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
@@ -507,16 +628,17 @@ void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const 
 	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, dpre, groups, &rec->n_groups, P.group_max, P, rec);
 }
 
-// compute_epe (pot.c:2771-2804), fast form: groups of 32 over every particle,
-// the group walk accumulating potentials; per-group partial sums of
-// q e phi per species, summed in group order by k_epe_final.
+// compute_epe (pot.c:2771-2804), fast form: groups of up to 32 TPL over
+// every particle, the group walk accumulating potentials; per-group partial
+// sums of q e phi per species, summed in group order by k_epe_final.
+template <int TPL>
 __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __restrict__ pos, TreeDev T,
                                                            const float4* __restrict__ src32,
                                                            const uint2* __restrict__ groups,
                                                            double* __restrict__ partial, Params P, RunRec* rec)
 {
-	__shared__ FastSmem smem[FW_WARPS];
-	FastSmem& sm = smem[threadIdx.x >> 5];
+	__shared__ FastSmem<TPL> smem[FW_WARPS];
+	FastSmem<TPL>& sm = smem[threadIdx.x >> 5];
 	if (rec->status != POT_OK) return;
 	const uint32_t n_groups = rec->n_groups_all;
 	const uint32_t gs = rec->grain_slot;
@@ -527,26 +649,34 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 		g = __shfl_sync(0xffffffffu, g, 0);
 		if (g >= n_groups) break;
 		const uint2 grp = groups[g];
-		Targets<1> tg;
-		const uint32_t slot = grp.x + lane_f();
-		tg.valid[0] = lane_f() < grp.y;
-		tg.self[0] = tg.valid[0] ? slot : 0xFFFFFFFFu;
-		const float4 me = tg.valid[0] ? src32[slot] : make_float4(0.f, 0.f, 0.f, 0.f);
-		tg.t[0] = make_float3(me.x, me.y, me.z);
-		uint32_t ne = 0;
+		Targets<TPL> tg;
+		float qme[TPL];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			const uint32_t m = lane_f() + 32u * k;
+			tg.valid[k] = m < grp.y;
+			tg.self[k] = tg.valid[k] ? grp.x + m : 0xFFFFFFFFu;
+			const float4 me = tg.valid[k] ? src32[grp.x + m] : make_float4(0.f, 0.f, 0.f, 0.f);
+			tg.t[k] = make_float3(me.x, me.y, me.z);
+			qme[k] = me.w;
+		}
+		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<1> f = group_walk<1, true>(tg, T, src32, P, sm, ne, err);
+		const Field<TPL> f = group_walk<TPL, true>(tg, T, src32, P, sm, ne, depth, err);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
 			break;
 		}
 		double acc[3] = { 0.0, 0.0, 0.0 };
-		if (tg.valid[0]) {
-			const double phi = (double)f.x[0] * pscale;
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			if (!tg.valid[k]) continue;
+			const uint32_t slot = tg.self[k];
+			const double phi = (double)f.x[k] * pscale;
 			if (slot == gs) {
 				rec->phi_grain = phi;
 			} else {
-				acc[(int)pos[slot].w] = (QE * (double)me.w) * phi;
+				acc[(int)pos[slot].w] += (QE * (double)qme[k]) * phi;
 			}
 		}
 #pragma unroll
@@ -563,8 +693,14 @@ void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, 
 	cudaMemsetAsync(&rec->n_groups_all, 0, sizeof(unsigned int), s);
 	cudaMemsetAsync(&rec->work_ctr2, 0, sizeof(unsigned int), s);
 	ScopedKernel k(tm, "epe_fast", 2);
-	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, nullptr, groups_all, &rec->n_groups_all, 32u, P, rec);
-	k_epe_fast<<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, groups_all, partial, P, rec);
+	const bool two = P.group_max > 32;
+	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, nullptr, groups_all, &rec->n_groups_all, two ? 64u : 32u, P,
+	                                              rec);
+	if (two) {
+		k_epe_fast<2><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, groups_all, partial, P, rec);
+	} else {
+		k_epe_fast<1><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, groups_all, partial, P, rec);
+	}
 }
 
 void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,

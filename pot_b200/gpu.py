@@ -72,7 +72,7 @@ class _Stats(C.Structure):
     _fields_ = [("t_steps", C.c_uint64), ("grain_q", C.c_int64), ("dq", C.c_int64), ("de", C.c_uint64),
                 ("n_absorbed", C.c_uint64), ("n_reinjected", C.c_uint64), ("n_pushed", C.c_uint64),
                 ("interactions", C.c_uint64), ("n_nodes", C.c_uint64), ("chi_b", C.c_double),
-                ("status", C.c_int32), ("pad", C.c_uint32), ("epe", C.c_double * 3)]
+                ("status", C.c_int32), ("stack_max", C.c_uint32), ("epe", C.c_double * 3)]
 
 
 _LIB = None

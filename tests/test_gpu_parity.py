@@ -164,14 +164,14 @@ def test_one_step_plain_vs_oracle(d, sceptic, steps):
     assert abs(gg["m"] - go["m"]) <= 1e-15 * go["m"]
 
 
-@pytest.mark.parametrize("form", ["plain", "fast"])
-def test_potential_energies_match_oracle(form):
+@pytest.mark.parametrize("form,group", [("plain", 0), ("fast", 32), ("fast", 64)])
+def test_potential_energies_match_oracle(form, group):
     """compute_epe (pot.c:2771-2804): q e phi summed per species at the
     step-start positions, the grain's from its end-of-step charge."""
     d = dict(STRESS, N=20001)
     o = oracle_snapshot(d, seed=13, mode="gpu", steps=2)
     P0, g0 = o.particles().copy(), o.grain()
-    with gpu_from_oracle(d, o, form=form, leaf_size=1 if form == "plain" else 16) as r:
+    with gpu_from_oracle(d, o, form=form, leaf_size=1 if form == "plain" else 16, group_size=group) as r:
         st = r.step(1, epe=True)
         st_plain = r.step(1)
     o.step(compute_epe=True)
@@ -244,12 +244,15 @@ def test_init_particles_distribution():
         assert np.abs(Pg[k] - Po[k]).max() < 1e-9 * np.abs(Po[k]).max()
 
 
-@pytest.mark.parametrize("leaf", [1, 8, 16])
-def test_fast_field_accuracy_vs_direct_sum(leaf):
+@pytest.mark.parametrize("leaf,group,shift", [(1, 32, 0.0), (8, 32, 0.0), (16, 32, 0.0), (16, 64, 0.0),
+                                              (16, 32, 0.3), (16, 64, 0.3), (1, 64, 0.3)])
+def test_fast_field_accuracy_vs_direct_sum(leaf, group, shift):
     """FP32 grouped walk: per-particle relative error against an FP64
     (long double) direct sum on sampled particles, as pot.c:2197-2238 checks
     its own tree.  Bar: no worse than the reference's own FP64 tree at the
-    same opening angle (plus 1e-3 for FP32), and RMS below 2 %."""
+    same opening angle (plus 1e-3 for FP32), and RMS below 2 %.  shift moves
+    each target off its own particle by that many softening lengths (as the
+    half drift does), so its own term must be excluded."""
     d = dict(SMALL, N=40001)
     o = oracle_snapshot(d, seed=4, mode="gpu", steps=1)
     o.set_grain(q=-600)
@@ -257,13 +260,15 @@ def test_fast_field_accuracy_vs_direct_sum(leaf):
     idx = np.sort(rng.choice(np.arange(1, d["N"]), size=2048, replace=False)).astype(np.uint32)
     P = o.particles()
     xyz = np.stack([P["x"][idx], P["y"][idx], P["z"][idx]], 1)
+    u = rng.normal(size=xyz.shape)
+    xyz = xyz + shift * d["soft"] * u / np.linalg.norm(u, axis=1, keepdims=True)
     # every pair softened, as the tree's near field is
     hi, lo = o.field_direct_many(idx, xyz, soften_all=True)
     E_dir = ld(hi, lo).astype(np.float64)
     o.build_tree()
     hi, lo = o.field_many(idx, xyz)
     E_tree = ld(hi, lo).astype(np.float64)
-    with gpu_from_oracle(d, o, form="fast", leaf_size=leaf) as r:
+    with gpu_from_oracle(d, o, form="fast", leaf_size=leaf, group_size=group) as r:
         r.build_tree()
         E = r.field_at(idx, xyz)
 
@@ -276,10 +281,11 @@ def test_fast_field_accuracy_vs_direct_sum(leaf):
     assert fast_err < 2e-2
 
 
-def test_fast_step_runs_and_conserves():
+@pytest.mark.parametrize("group", [32, 64])
+def test_fast_step_runs_and_conserves(group):
     d = dict(STRESS, N=20001, theta=0.5)
     o = oracle_snapshot(d, seed=8, mode="gpu", steps=1)
-    with gpu_from_oracle(d, o, form="fast", leaf_size=16) as r:
+    with gpu_from_oracle(d, o, form="fast", leaf_size=16, group_size=group) as r:
         q0 = r.download()[1]["q"]
         tot_dq = 0
         for _ in range(10):
