@@ -48,11 +48,27 @@ def splitmix64_words(seed: int, n: int = 16):
     return np.array(out[:n], dtype=np.uint32)
 
 
+def shape_of(A: float) -> int:
+    """Grain shape code: 0 sphere (pot.c), 1 prolate (A > 1), 2 oblate
+    (0 < A < 1) -- pot-spheroid.c's PROLATE / OBLATE programs."""
+    if not A:
+        return 0
+    if A > 1.0:
+        return 1
+    if 0.0 < A < 1.0:
+        return 2
+    raise ValueError("aspect ratio must be 0 (sphere), > 1 (prolate) or in (0, 1) (oblate)")
+
+
 class RunParams:
-    """The reference's Run settings (pot.c:335-358) for a spherical domain."""
+    """The reference's Run settings (pot.c:335-358) for a spherical domain.
+    ``A`` is pot-spheroid.c's aspect ratio (Run.A, pot-spheroid.c:376-378;
+    0 = the spherical grain of pot.c) and ``axis`` the spheroid's symmetry
+    axis (x in the reference; any other unit vector is this project's
+    extension, unpinned)."""
 
     def __init__(self, N, r, dt, mpp, soft, Te, Ti, x_drift=0.0, a=2.5e-6, settle=0.0,
-                 theta=0.5, B=(0.0, 0.0, 0.0)):
+                 theta=0.5, B=(0.0, 0.0, 0.0), A=0.0, axis=(1.0, 0.0, 0.0)):
         self.N = int(N)
         self.r = int(r)
         self.dt = float(dt)
@@ -65,11 +81,14 @@ class RunParams:
         self.settle = float(settle)
         self.theta = float(theta)
         self.B = tuple(float(b) for b in B)
+        self.A = float(A)
+        self.axis = tuple(float(u) for u in axis)
+        self.shape = shape_of(self.A)
 
     def as_dict(self):
         return dict(N=self.N, r=self.r, dt=self.dt, mpp=self.mpp, soft=self.soft, Te=self.Te,
                     Ti=self.Ti, x_drift=self.x_drift, a=self.a, settle=self.settle,
-                    theta=self.theta, B=list(self.B))
+                    theta=self.theta, B=list(self.B), A=self.A, axis=list(self.axis))
 
 
 def _ptr(a, t=C.c_void_p):
@@ -121,13 +140,19 @@ class RefLib:
                                        C.POINTER(C.c_ulong), C.c_void_p, C.c_void_p, C.c_void_p]
         L.potref_tree_dump.restype = C.c_int
         L.potref_field_many.argtypes = [C.c_ulong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-        L.potref_phi_at.argtypes = [C.c_double, C.c_double, C.c_double]
-        L.potref_phi_at.restype = C.c_double
+        self.has_phi_at = bool(L.potref_has_phi_at())
+        if self.has_phi_at:
+            L.potref_phi_at.argtypes = [C.c_double, C.c_double, C.c_double]
+            L.potref_phi_at.restype = C.c_double
         L.potref_phi_particle_feels.argtypes = [C.c_uint, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.potref_cross_grain.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
         L.potref_cross_grain.restype = C.c_int
         L.potref_inject.argtypes = [C.c_void_p, C.c_int]
         L.potref_get_epe.argtypes = [C.c_void_p]
+        L.potref_set_aspect.argtypes = [C.c_double]
+        L.potref_set_aspect.restype = None
+        self.shape = int(L.potref_shape())
+        self.grain_enabled = bool(L.potref_grain_enabled())
         self.sceptic = bool(L.potref_has_sceptic())
         if self.sceptic:
             L.potref_measure_chi_b.restype = C.c_double
@@ -146,6 +171,12 @@ class RefLib:
         """Set up a run; with nprocs > 1 this process plays MPI rank `rank`
         (it builds the whole tree and steps only its own block)."""
         words = splitmix64_words(seed)
+        if p.shape != self.shape:
+            raise ValueError("run shape %d does not match the %s program" % (p.shape, self.variant))
+        if self.shape:
+            if p.axis != (1.0, 0.0, 0.0):
+                raise ValueError("the reference's spheroid axis is x")
+            self.lib.potref_set_aspect(p.A)
         rc = self.lib.potref_setup(p.N, p.r, p.dt, p.mpp, p.soft, p.Te, p.Ti, p.x_drift, p.a,
                                    p.settle, p.theta, p.B[0], p.B[1], p.B[2], _ptr(words),
                                    1 if init else 0, int(nprocs), int(rank))
@@ -265,7 +296,8 @@ class _PtoCfg(C.Structure):
                 ("soft", C.c_double), ("Te", C.c_double), ("Ti", C.c_double),
                 ("x_drift", C.c_double), ("a", C.c_double), ("settle", C.c_double),
                 ("theta", C.c_double), ("B", C.c_double * 3), ("sceptic", C.c_int32),
-                ("quirk", C.c_int32), ("rng", C.c_int32), ("pad", C.c_int32), ("seed", C.c_uint64)]
+                ("quirk", C.c_int32), ("rng", C.c_int32), ("pad", C.c_int32), ("seed", C.c_uint64),
+                ("shape", C.c_int32), ("pad2", C.c_int32), ("A", C.c_double), ("axis", C.c_double * 3)]
 
 
 WELL_DTYPE = np.dtype([("abcd", "<u4", 4), ("index", "<u4"), ("state", "<u4", 16)])
@@ -308,6 +340,13 @@ class Oracle:
             L.pto_phi_particle_feels.argtypes = [vp, u32]
             L.pto_phi_particle_feels.restype = d
             L.pto_cross_grain.argtypes = [vp, vp, vp, d]
+            L.pto_cross_grain_run.argtypes = [vp, vp, vp, vp]
+            L.pto_grain_field.argtypes = [vp, d, d, d, vp]
+            L.pto_grain_field.restype = None
+            L.pto_grain_phi.argtypes = [vp, d, d, d]
+            L.pto_grain_phi.restype = d
+            L.pto_integrate_for_alpha_dev.argtypes = [d, d, d, d, d]
+            L.pto_integrate_for_alpha_dev.restype = d
             L.pto_measure_chi_b.argtypes = [vp]
             L.pto_measure_chi_b.restype = d
             L.pto_step.argtypes = [vp, i32]
@@ -337,6 +376,10 @@ class Oracle:
         cfg.quirk = 1 if mode == "reference" else 0
         cfg.rng = 0 if mode == "reference" else 1
         cfg.seed = seed & ((1 << 64) - 1)
+        cfg.shape = p.shape
+        cfg.A = p.A
+        for k in range(3):
+            cfg.axis[k] = p.axis[k]
         self.cfg = cfg
         self.params = p
         self.mode = mode
@@ -449,6 +492,21 @@ class Oracle:
         gr = np.ascontiguousarray(gr, PARTICLE_DTYPE).reshape(1)
         d = np.ascontiguousarray(d_pos, np.float64)
         return bool(self.lib().pto_cross_grain(_ptr(p), _ptr(d), _ptr(gr), float(a)))
+
+    def cross_grain_run(self, p, d_pos, gr):
+        """The run's absorption test (sphere or spheroid)."""
+        p = np.ascontiguousarray(p, PARTICLE_DTYPE).reshape(1)
+        gr = np.ascontiguousarray(gr, PARTICLE_DTYPE).reshape(1)
+        d = np.ascontiguousarray(d_pos, np.float64)
+        return bool(self.lib().pto_cross_grain_run(self.h, _ptr(p), _ptr(d), _ptr(gr)))
+
+    def grain_field(self, x, y, z):
+        out = np.zeros(3)
+        self.lib().pto_grain_field(self.h, x, y, z, _ptr(out))
+        return out
+
+    def grain_phi(self, x, y, z):
+        return self.lib().pto_grain_phi(self.h, x, y, z)
 
     def step(self, compute_epe=False):
         rc = self.lib().pto_step(self.h, 1 if compute_epe else 0)

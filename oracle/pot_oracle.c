@@ -31,6 +31,7 @@
 #define O_QE 1.6021766e-19
 #define O_ME 9.109383e-31
 #define O_MIME 1836.15
+#define O_MIME_SPHEROID 1836.153  /* pot-spheroid.c:61 */
 #define O_PI 3.14159265358979
 #define O_SQRT_PI 1.77245385090552
 #define O_MAX_PATH 400   /* pot.c:196 */
@@ -38,7 +39,8 @@
 
 enum { O_DUST = 0, O_ION = 1, O_ELECTRON = 2 };
 static const int O_CHARGE[3] = { 0, 1, -1 };                               /* pot.c:291 */
-static const long double O_MASS[3] = { 1.67e-12, O_MIME * O_ME, O_ME };    /* pot.c:292 */
+/* MASS of pot.c:292 is { 1.67e-12, MIME * 9.109383e-31, 9.109383e-31 };
+   per run here, since pot-spheroid.c's MIME differs */
 
 /* Octree node.  Child slots are kept in the reference's member order
    (pot.c:323-330): gxlylz, gxlygz, lxlylz, lxlygz, lxgylz, lxgygz, gxgylz,
@@ -73,6 +75,10 @@ struct pto_ctx {
 	uint64_t t_steps;
 	double chi_b;
 	uint32_t tss[3];
+	long double mass[3];     /* MASS, pot.c:292 / pot-spheroid.c:61 */
+	double max_lin_dev;      /* integrate_for_alpha tolerance, pot.c:436 / pot-spheroid.c:457 */
+	int tilted;              /* spheroid axis other than x */
+	double ax[3], e1[3], e2[3];  /* spheroid frame */
 	/* Philox stream currently feeding rnd() (rng = 1) */
 	uint32_t ph_ctr[4];
 	uint32_t ph_buf[4];
@@ -277,10 +283,9 @@ static void o_rot(const double* d, double s, double cs, double* x, double* y, do
 
 /* Orbit-angle integral of Hutchinson's SCEPTIC by crude adaptive Simpson,
    pot.c:433-492.  A cap on the interval halvings keeps the loop finite. */
-double pto_integrate_for_alpha(double s, double chi_b, double u2, double Rol)
+double pto_integrate_for_alpha_dev(double s, double chi_b, double u2, double Rol, double max_lin_dev)
 {
 	const double chu2 = chi_b / u2;
-	const double max_lin_dev = 0.01;
 	const double s2 = s * s;
 	const double y_one = s / sqrt(1.0 - chu2 - s2);
 	double alpha = 0.0;
@@ -311,6 +316,11 @@ double pto_integrate_for_alpha(double s, double chi_b, double u2, double Rol)
 	return alpha;
 }
 
+double pto_integrate_for_alpha(double s, double chi_b, double u2, double Rol)
+{
+	return pto_integrate_for_alpha_dev(s, chi_b, u2, Rol, 0.01);
+}
+
 /* SCEPTIC-like reinjection at the domain edge, pot.c:496-652.  The
    reference retries by recursion when alpha is NaN; this is the same retry
    as a loop, including the reference's undo of the electron rescaling of
@@ -322,7 +332,7 @@ static void o_sceptic(pto_ctx* c, pto_particle* part, double chi_b)
 	int tries = 0;
 
 	for (;;) {
-		v_n = 2.0 * O_KB / O_MASS[part->species];
+		v_n = 2.0 * O_KB / c->mass[part->species];
 		if (part->species == O_ELECTRON) {
 			v_n *= ru->Te;
 			chi_b *= -ru->Ti / ru->Te;
@@ -364,7 +374,7 @@ static void o_sceptic(pto_ctx* c, pto_particle* part, double chi_b)
 		Rol = O_QE * O_QE * (ru->N - 1) / 2.0;
 		Rol /= (4.0 * O_PI / 3.0) * ru->mpp * ru->r * O_EPSILON0 * O_KB * ru->Te;
 		Rol = sqrt(Rol);
-		alpha = pto_integrate_for_alpha(b, chi_b, u2, Rol);
+		alpha = pto_integrate_for_alpha_dev(b, chi_b, u2, Rol, c->max_lin_dev);
 		if (isnan(alpha) && ++tries < 100000) {
 			if (part->species == O_ELECTRON) {
 				chi_b /= -ru->Ti / ru->Te;
@@ -406,9 +416,9 @@ static void o_inject(pto_ctx* c, pto_particle* part, int reinjection)
 	double sigma, phi, r, theta, v[3];
 
 	if (part->species == O_ION) {
-		sigma = sqrt(O_KB * ru->Ti / O_MASS[O_ION]);
+		sigma = sqrt(O_KB * ru->Ti / c->mass[O_ION]);
 	} else {
-		sigma = sqrt(O_KB * ru->Te / O_MASS[O_ELECTRON]);
+		sigma = sqrt(O_KB * ru->Te / c->mass[O_ELECTRON]);
 	}
 	if (!ru->sceptic && !reinjection) {
 		sigma *= 0.85;  /* pot.c:684-690 */
@@ -466,12 +476,42 @@ pto_ctx* pto_create(const pto_cfg* cfg)
 		pto_destroy(c);
 		return NULL;
 	}
+	{
+		const double mime = cfg->shape ? O_MIME_SPHEROID : O_MIME;
+		c->mass[O_DUST] = 1.67e-12;
+		c->mass[O_ION] = mime * O_ME;
+		c->mass[O_ELECTRON] = O_ME;
+		c->max_lin_dev = cfg->shape ? 0.1 : 0.01;
+	}
+	if (cfg->shape) {
+		/* spheroid frame: axis, then e1 = y (or z) made orthogonal, e2 = axis x e1 */
+		double n = sqrt(cfg->axis[0] * cfg->axis[0] + cfg->axis[1] * cfg->axis[1] + cfg->axis[2] * cfg->axis[2]);
+		if (!(n > 0.0)) {
+			c->ax[0] = 1.0;
+			c->ax[1] = c->ax[2] = 0.0;
+		} else {
+			for (int k = 0; k < 3; k++) c->ax[k] = cfg->axis[k] / n;
+		}
+		c->tilted = !(c->ax[0] == 1.0 && c->ax[1] == 0.0 && c->ax[2] == 0.0);
+		double ref[3] = { 0.0, 1.0, 0.0 };
+		if (fabs(c->ax[1]) > 0.9) {
+			ref[1] = 0.0;
+			ref[2] = 1.0;
+		}
+		double d = ref[0] * c->ax[0] + ref[1] * c->ax[1] + ref[2] * c->ax[2];
+		for (int k = 0; k < 3; k++) c->e1[k] = ref[k] - d * c->ax[k];
+		n = sqrt(c->e1[0] * c->e1[0] + c->e1[1] * c->e1[1] + c->e1[2] * c->e1[2]);
+		for (int k = 0; k < 3; k++) c->e1[k] /= n;
+		c->e2[0] = c->ax[1] * c->e1[2] - c->ax[2] * c->e1[1];
+		c->e2[1] = c->ax[2] * c->e1[0] - c->ax[0] * c->e1[2];
+		c->e2[2] = c->ax[0] * c->e1[1] - c->ax[1] * c->e1[0];
+	}
 	c->grain_q = O_CHARGE[O_DUST];
-	c->grain_m = O_MASS[O_DUST];
+	c->grain_m = c->mass[O_DUST];
 	/* species time-step multiples, pot.c:4157-4159 */
 	c->tss[O_ELECTRON] = 1;
-	c->tss[O_ION] = (int) sqrt(cfg->Te * O_MASS[O_ION] / (cfg->Ti * O_MASS[O_ELECTRON]));
-	c->tss[O_DUST] = c->tss[O_ION] * (int) sqrt(0.1 * O_MASS[O_DUST] / O_MASS[O_ION]);
+	c->tss[O_ION] = (int) sqrt(cfg->Te * c->mass[O_ION] / (cfg->Ti * c->mass[O_ELECTRON]));
+	c->tss[O_DUST] = c->tss[O_ION] * (int) sqrt(0.1 * c->mass[O_DUST] / c->mass[O_ION]);
 	return c;
 }
 
@@ -617,7 +657,8 @@ int pto_build_tree(pto_ctx* c)
 	root->z2 = root->y2;
 	root->part = O_NONE;
 
-	uint64_t pn = 0;
+	/* pot-spheroid.c:1516-1518: the spheroidal grain is not in the tree */
+	uint64_t pn = ru->shape ? 1 : 0;
 	while (pn < ru->N) {
 		const pto_particle* part = &c->parts[pn];
 		if ((part->x < 0.0) || (part->x > root->x2) || (part->y < 0.0) || (part->y > root->y2)
@@ -712,6 +753,133 @@ int pto_tree_dump(const pto_ctx* c, uint64_t max_nodes,
 /* Field and potential walks                                                */
 /* ------------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------------ */
+/* Spheroidal grain (pot-spheroid.c, PROLATE / OBLATE)                      */
+/* ------------------------------------------------------------------------ */
+
+/* Components of a grain-relative vector along the spheroid's axis and two
+   perpendicular directions; the identity (bit for bit) for the reference's
+   x axis. */
+static void o_to_frame(const pto_ctx* c, double dx, double dy, double dz, double* u, double* v, double* w)
+{
+	if (!c->tilted) {
+		*u = dx;
+		*v = dy;
+		*w = dz;
+		return;
+	}
+	*u = dx * c->ax[0] + dy * c->ax[1] + dz * c->ax[2];
+	*v = dx * c->e1[0] + dy * c->e1[1] + dz * c->e1[2];
+	*w = dx * c->e2[0] + dy * c->e2[1] + dz * c->e2[2];
+}
+
+static void o_from_frame(const pto_ctx* c, double u, double v, double w, double* out)
+{
+	if (!c->tilted) {
+		out[0] = u;
+		out[1] = v;
+		out[2] = w;
+		return;
+	}
+	for (int k = 0; k < 3; k++) out[k] = u * c->ax[k] + v * c->e1[k] + w * c->e2[k];
+}
+
+/* field_particle_feels_from_grain, pot-spheroid.c:1689-1779: the analytic
+   field of the charged conducting spheroid at (x, y, z); zero for the grain
+   itself.  Expressions in the reference's order (double arithmetic). */
+static void o_spheroid_field(const pto_ctx* c, uint32_t part, double x, double y, double z, double* Eo)
+{
+	const double A = c->cfg.A;
+	const double a = c->cfg.a;
+	double fc, phi_const, rho2, rt, e2, E_n, beta, theta, dx, dy, dz;
+	if (c->cfg.shape == 1) {
+		fc = (a * sqrt(A * A - 1.0)) * pow(A, -1.0 / 3.0);
+		phi_const = (O_QE * c->grain_q * acosh(A)) / (4.0 * O_PI * O_EPSILON0 * fc * log(A - sqrt(A * A - 1.0)));
+	} else {
+		fc = (a * sqrt(1.0 - A * A)) * pow(A, -1.0 / 3.0);
+		phi_const = (O_QE * c->grain_q * acos(A))
+		            / (8.0 * O_PI * O_EPSILON0 * fc * (atan((1.0 - sqrt(1.0 - A * A)) / A) - 0.25 * O_PI));
+	}
+	if (!part) {
+		Eo[0] = Eo[1] = Eo[2] = 0.0;
+		return;
+	}
+	const pto_particle* g = &c->parts[0];
+	o_to_frame(c, x - g->x, y - g->y, z - g->z, &dx, &dy, &dz);
+	rho2 = (dy * dy) + (dz * dz);
+	if (c->cfg.shape == 1) {
+		rt = sqrt(rho2 * rho2 + dx * dx * dx * dx + fc * fc * fc * fc + 2.0 * rho2 * dx * dx
+		          + 2.0 * rho2 * fc * fc - 2.0 * dx * dx * fc * fc);
+		e2 = (rho2 + dx * dx - fc * fc + rt) / (2.0 * fc * fc);   /* sinh^2 */
+		E_n = -phi_const / sqrt(e2 * rt);
+		beta = atan((-e2 * dx) / ((e2 + 1.0) * sqrt(rho2)));
+	} else {
+		rt = sqrt(rho2 * rho2 + dx * dx * dx * dx + fc * fc * fc * fc + 2.0 * rho2 * dx * dx
+		          - 2.0 * rho2 * fc * fc + 2.0 * dx * dx * fc * fc);
+		e2 = (rho2 + dx * dx + fc * fc + rt) / (2.0 * fc * fc);   /* cosh^2 */
+		E_n = -phi_const / sqrt(e2 * rt);
+		beta = atan((-e2 * dx) / ((e2 - 1.0) * sqrt(rho2)));
+	}
+	theta = atan(fabs(dz) / fabs(dy));
+	o_from_frame(c, -E_n * sin(beta), E_n * cos(beta) * cos(theta) * fabs(dy) / dy,
+	             E_n * cos(beta) * sin(theta) * fabs(dz) / dz, Eo);
+}
+
+/* the spheroid's potential at grain-relative (dx, dy, dz) in its frame:
+   phi_particle_feels_from_grain, pot-spheroid.c:2054-2078 */
+static double o_spheroid_phi_rel(const pto_ctx* c, double dx, double dy, double dz)
+{
+	const double A = c->cfg.A;
+	const double a = c->cfg.a;
+	const double rho2 = (dy * dy) + (dz * dz);
+	if (c->cfg.shape == 1) {
+		const double fc = a * sqrt(A * A - 1.0) / pow(A, 1.0 / 3.0);
+		const double phi_const = (O_QE * c->grain_q * acosh(A))
+		                         / (4.0 * O_PI * O_EPSILON0 * fc * log(A - sqrt(A * A - 1.0)));
+		const double rt = sqrt(rho2 * rho2 + dx * dx * dx * dx + fc * fc * fc * fc + 2.0 * rho2 * dx * dx
+		                       + 2.0 * rho2 * fc * fc - 2.0 * dx * dx * fc * fc);
+		return phi_const * log((sqrt(rho2 + dx * dx + fc * fc + rt) - fc * sqrt(2.0))
+		                       / sqrt(rho2 + dx * dx - fc * fc + rt));
+	}
+	const double fc = (a * sqrt(1.0 - A * A)) * pow(A, -1.0 / 3.0);
+	const double phi_const = (O_QE * c->grain_q * acos(A))
+	                         / (4.0 * O_PI * O_EPSILON0 * fc * (atan((1.0 - sqrt(1.0 - A * A)) / A) - 0.25 * O_PI));
+	const double rt = sqrt(rho2 * rho2 + dx * dx * dx * dx + fc * fc * fc * fc + 2.0 * rho2 * dx * dx
+	                       - 2.0 * rho2 * fc * fc + 2.0 * dx * dx * fc * fc);
+	return phi_const * (atan((sqrt(rho2 + dx * dx + fc * fc + rt) - fc * sqrt(2.0))
+	                         / sqrt(rho2 + dx * dx - fc * fc + rt)) - 0.25 * O_PI);
+}
+
+/* potential of the spheroid felt by particle `part` at its stored position
+   (pot-spheroid.c:2037-2085); zero for the grain */
+static double o_spheroid_phi_particle(const pto_ctx* c, uint32_t part)
+{
+	double u, v, w;
+	if (!part) return 0.0;
+	const pto_particle* g = &c->parts[0];
+	const pto_particle* p = &c->parts[part];
+	o_to_frame(c, p->x - g->x, p->y - g->y, p->z - g->z, &u, &v, &w);
+	return o_spheroid_phi_rel(c, u, v, w);
+}
+
+void pto_grain_field(const pto_ctx* c, double x, double y, double z, double* E3)
+{
+	if (!c->cfg.shape) {
+		E3[0] = E3[1] = E3[2] = 0.0;
+		return;
+	}
+	o_spheroid_field(c, 1, x, y, z, E3);
+}
+
+double pto_grain_phi(const pto_ctx* c, double x, double y, double z)
+{
+	double u, v, w;
+	if (!c->cfg.shape) return 0.0;
+	const pto_particle* g = &c->parts[0];
+	o_to_frame(c, x - g->x, y - g->y, z - g->z, &u, &v, &w);
+	return o_spheroid_phi_rel(c, u, v, w);
+}
+
 /* Barnes-Hut E at (x, y, z) for target `part`, pot.c:1696-1808 (monopole):
    accepted cells add an unsoftened monopole, leaves add a Plummer-softened
    pair term, the target itself is skipped by index.  Returns -1 when the
@@ -726,6 +894,14 @@ static int o_field(const pto_ctx* c, uint32_t part, double x, double y, double z
 	double dist, dist2, dx, dy, dz;
 	long double E_scale;
 	E[0] = E[1] = E[2] = 0.0;
+	if (c->cfg.shape) {
+		/* pot-spheroid.c:1815-1819: E starts as the spheroid's own field */
+		double Eg[3];
+		o_spheroid_field(c, part, x, y, z, Eg);
+		E[0] = Eg[0];
+		E[1] = Eg[1];
+		E[2] = Eg[2];
+	}
 	path[0] = 0;
 	do {
 		const onode* node = &nodes[path[len - 1]];
@@ -827,6 +1003,13 @@ double pto_phi_at(const pto_ctx* c, double x, double y, double z)
 	uint32_t path[O_MAX_PATH];
 	unsigned int len = 1;
 	double phi = 0.0, dist, dist2, dx, dy, dz;
+	if (c->cfg.shape) {
+		/* pot-spheroid.c:1924-1953 evaluates the spheroid's potential at the
+		   point's coordinates themselves, not relative to the grain */
+		double u, v, w;
+		o_to_frame(c, x, y, z, &u, &v, &w);
+		phi = o_spheroid_phi_rel(c, u, v, w);
+	}
 	path[0] = 0;
 	do {
 		const onode* node = &c->nodes[path[len - 1]];
@@ -871,6 +1054,7 @@ static long double o_phi_particle(const pto_ctx* c, uint32_t part)
 	unsigned int len = 1;
 	long double phi = 0.0;
 	double dist, dist2, dx, dy, dz;
+	if (c->cfg.shape) phi = o_spheroid_phi_particle(c, part);  /* pot-spheroid.c:2107-2109 */
 	path[0] = 0;
 	do {
 		const onode* node = &c->nodes[path[len - 1]];
@@ -940,6 +1124,33 @@ int pto_cross_grain(const pto_particle* p, const double* d_pos, const pto_partic
 	return dist2 <= (a * a);
 }
 
+/* spheroid absorption test, pot-spheroid.c:2448-2537: (1) the new position
+   inside x^2 + A^2 rho^2 <= a^2 A^(4/3); (2) the closest approach of the
+   step's line, found in the x-rho plane, between the old and new x and
+   inside the surface.  s and d_pos are taken into the spheroid's frame
+   first (the identity for the reference's x axis). */
+static int o_cross_spheroid(const pto_ctx* c, const pto_particle* p, const double* d_pos, const pto_particle* gr)
+{
+	const double a = c->cfg.a, A = c->cfg.A;
+	double s[3], d[3], x_min, x_prev, y_min, z_min;
+	o_to_frame(c, gr->x - p->x, gr->y - p->y, gr->z - p->z, &s[0], &s[1], &s[2]);
+	o_to_frame(c, d_pos[0], d_pos[1], d_pos[2], &d[0], &d[1], &d[2]);
+	if ((s[0] * s[0] + (s[1] * s[1] + s[2] * s[2]) * A * A) <= (a * a * pow(A, 4.0 / 3.0))) return 1;
+	x_min = (d[1] * (d[1] * s[0] - d[0] * s[1]) + d[2] * (d[2] * s[0] - d[0] * s[2]))
+	        / ((d[0] * d[0] / (A * A)) + d[1] * d[1] + d[2] * d[2]);
+	x_prev = s[0] - d[0];
+	if (((x_min > s[0]) && (x_min > x_prev)) || ((x_min < s[0]) && (x_min < x_prev))) return 0;
+	y_min = d[1] * (x_min - s[0]) / d[0] + s[1];
+	z_min = d[2] * (x_min - s[0]) / d[0] + s[2];
+	return ((x_min * x_min) + (y_min * y_min + z_min * z_min) * A * A) <= (a * a * pow(A, 4.0 / 3.0));
+}
+
+int pto_cross_grain_run(const pto_ctx* c, const pto_particle* p, const double* d_pos, const pto_particle* gr)
+{
+	if (c->cfg.shape) return o_cross_spheroid(c, p, d_pos, gr);
+	return pto_cross_grain(p, d_pos, gr, c->cfg.a);
+}
+
 /* One rank's move_particles with the Boris integrator, pot.c:2330-2934,
    without MPI: memcpy, chi_b refresh, due range, half-drift, field, kick,
    rotate, kick, half-drift, absorption + reinjection, boundary reinjection,
@@ -997,7 +1208,7 @@ static int o_move(pto_ctx* c, int compute_epe, uint64_t time_steps)
 		} else {
 			qom = O_QE * O_CHARGE[p->species];
 		}
-		qom /= O_MASS[p->species];
+		qom /= c->mass[p->species];
 		ax = 0.5 * qom * E[0];
 		ay = 0.5 * qom * E[1];
 		az = 0.5 * qom * E[2];
@@ -1023,13 +1234,13 @@ static int o_move(pto_ctx* c, int compute_epe, uint64_t time_steps)
 		uint32_t attempt = 0;
 		if ((i > 0) && ((time_steps * c->dt) > ru->settle)) {
 			double d[3] = { pn->x - c->prev[3 * ims], pn->y - c->prev[3 * ims + 1], pn->z - c->prev[3 * ims + 2] };
-			if (pto_cross_grain(pn, d, &np[0], ru->a)) {
+			if (pto_cross_grain_run(c, pn, d, &np[0])) {
 				if (pn->species == O_ELECTRON) absorbed_e++;
-				absorbed_m += O_MASS[pn->species];
+				absorbed_m += c->mass[pn->species];
 				absorbed_q += O_CHARGE[pn->species];
-				dpx += O_MASS[pn->species] * pn->vx;
-				dpy += O_MASS[pn->species] * pn->vy;
-				dpz += O_MASS[pn->species] * pn->vz;
+				dpx += c->mass[pn->species] * pn->vx;
+				dpy += c->mass[pn->species] * pn->vy;
+				dpz += c->mass[pn->species] * pn->vz;
 				if (ru->rng) ph_stream(c, (uint32_t) i, time_steps, 0x10000u | attempt);
 				attempt++;
 				o_inject(c, pn, 1);

@@ -60,6 +60,15 @@ typedef struct pto_cfg {
 	int32_t rng;      /* 0: WELL512 stream, 1: Philox counter stream */
 	int32_t pad;
 	uint64_t seed;    /* Philox key (rng = 1) */
+	/* grain shape: 0 the sphere of pot.c; 1 prolate, 2 oblate spheroid of
+	   pot-spheroid.c (PROLATE / OBLATE), which also bring that program's
+	   constants (m_i/m_e = 1836.153, SCEPTIC max_lin_dev = 0.1) and keep the
+	   grain out of the tree */
+	int32_t shape;
+	int32_t pad2;
+	double A;         /* aspect ratio (pot-spheroid.c -A) */
+	double axis[3];   /* symmetry axis, unit vector; (1, 0, 0) in the reference,
+	                     anything else is an extension (unpinned) */
 } pto_cfg;
 
 typedef struct pto_ctx pto_ctx;
@@ -91,6 +100,12 @@ void pto_field_direct_many(const pto_ctx* c, uint64_t n, const uint32_t* idx, co
 double pto_phi_at(const pto_ctx* c, double x, double y, double z);
 double pto_phi_particle_feels(const pto_ctx* c, uint32_t part);
 int pto_cross_grain(const pto_particle* p, const double* d_pos, const pto_particle* gr, double a);
+/* the run's absorption test (sphere, or the spheroid of its shape) */
+int pto_cross_grain_run(const pto_ctx* c, const pto_particle* p, const double* d_pos, const pto_particle* gr);
+/* the spheroid's own field and potential at a point (grain charge and
+   position of the run), pot-spheroid.c:1689-1779 and 2037-2085 */
+void pto_grain_field(const pto_ctx* c, double x, double y, double z, double* E3);
+double pto_grain_phi(const pto_ctx* c, double x, double y, double z);
 double pto_measure_chi_b(const pto_ctx* c);
 
 /* One step: t_steps++, build the tree, move the particles (pot.c:4261-4386).
@@ -106,6 +121,7 @@ void pto_sample_reinject(pto_ctx* c, uint64_t n, int32_t species, pto_particle* 
 double pto_u_icdf(double U, double chi, double q);
 double pto_u_no_flow_icdf(double chi, double q);
 double pto_integrate_for_alpha(double s, double chi_b, double u2, double Rol);
+double pto_integrate_for_alpha_dev(double s, double chi_b, double u2, double Rol, double max_lin_dev);
 
 /* Philox4x32-10 block function (Salmon et al., SC'11), for RNG tests. */
 void pto_philox4x32(const uint32_t* ctr4, const uint32_t* key2, uint32_t* out4);

@@ -13,6 +13,8 @@
  *   move_particles        pot.c:2330-2934
  *   inject / init_particles pot.c:658-846 / 887-996
  *   measure_chi_b         pot.c:2251-2279 (SCEPTIC variant)
+ * The spheroid variants include pot-spheroid.c instead (same entry points;
+ * grain field pot-spheroid.c:1689-1779, absorption 2448-2537).
  * Process set-up mirrors what main() and run() do for a single rank
  * (pot.c:4998-5190 and pot.c:4115-4159), without the output writers.
  */
@@ -22,6 +24,38 @@ double pot_ref_oap = 0.5;
 double pot_ref_bx = 0.0;
 double pot_ref_by = 0.0;
 double pot_ref_bz = 0.0;
+static double pot_ref_aspect = 3.0;  /* Run.A of pot-spheroid.c (pot-spheroid.c:376-378) */
+
+#if defined(PROLATE) || defined(OBLATE)
+#define H_SPHEROID 1
+#else
+#define H_SPHEROID 0
+#endif
+
+/* 0 sphere (pot.c), 1 prolate, 2 oblate (pot-spheroid.c) */
+int potref_shape(void)
+{
+#if defined(PROLATE)
+	return 1;
+#elif defined(OBLATE)
+	return 2;
+#else
+	return 0;
+#endif
+}
+
+/* 1 when the grain absorbs (DISABLE_GRAIN off), 0 otherwise */
+int potref_grain_enabled(void)
+{
+#ifdef DISABLE_GRAIN
+	return 0;
+#else
+	return 1;
+#endif
+}
+
+/* aspect ratio for the next potref_setup (spheroid variants) */
+void potref_set_aspect(double A) { pot_ref_aspect = A; }
 
 static Proc H;
 static Run R;
@@ -77,7 +111,11 @@ int potref_setup(unsigned long N, unsigned int r, double dt, double mpp, double 
 	R.tim_lim = 0.0;
 	R.Te = Te;
 	R.Ti = Ti;
+#if H_SPHEROID
+	R.A = pot_ref_aspect;
+#else
 	R.read_out = false;
+#endif
 	pot_ref_oap = oap;
 	pot_ref_bx = bx;
 	pot_ref_by = by;
@@ -245,7 +283,12 @@ void potref_field_many(unsigned long n, const unsigned int* idx, const double* x
 		potref_field_at(idx[k], xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2], &hi[3 * k], &lo[3 * k]);
 }
 
+#ifdef USING_PHI_AT
 double potref_phi_at(double x, double y, double z) { return phi_at(x, y, z, &H, &R, H.root); }
+int potref_has_phi_at(void) { return 1; }
+#else
+int potref_has_phi_at(void) { return 0; }
+#endif
 
 void potref_phi_particle_feels(unsigned int part, double* hi, double* lo)
 {
@@ -254,7 +297,11 @@ void potref_phi_particle_feels(unsigned int part, double* hi, double* lo)
 
 int potref_cross_grain(const Particle* p, const double* d_pos, const Particle* gr, double a)
 {
+#if H_SPHEROID
+	return does_particle_cross_grain(p, d_pos, gr, a, R.A) ? 1 : 0;
+#else
 	return does_particle_cross_grain(p, d_pos, gr, a) ? 1 : 0;
+#endif
 }
 
 /* inject() on a caller-supplied particle with the harness PRNG (pot.c:658). */

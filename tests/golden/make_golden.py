@@ -9,8 +9,11 @@ as double-double pairs of the reference's long double accumulators, edge
 potentials, absorption decisions on crafted segments, the inverse CDFs and
 orbit integral of the SCEPTIC sampler on a grid.
 
+The spheroid fixtures (spheroid.json, spheroid.npz) come from the
+reference's pot-spheroid.c compiled the same way.
+
 Usage (where the reference tree is present):
-    python tests/golden/make_golden.py [--ref-root /path/to/reference]
+    python tests/golden/make_golden.py [--ref-root /path/to/reference] [--spheroid-only]
 """
 from __future__ import annotations
 
@@ -128,10 +131,74 @@ def sampler_grid(ref_root: str):
     return dict(icdf_q=qs, icdf_U=Us, icdf_chi=chis, icdf=icdf, icdf_noflow=nf, alpha_cases=np.array(ia))
 
 
+SPHEROID = dict(STRESS, a=3.0e-7)
+SPHEROID_RUNS = (("prolate_sceptic", 3.0, 11, 120), ("prolate", 5.0, 12, 80),
+                 ("oblate_sceptic", 0.4, 13, 120))
+
+
+def spheroid(ref_root: str):
+    """pot-spheroid.c (PROLATE / OBLATE programs): run digests with a
+    charged grain, and for prolate A = 3 the grain-free tree, fields,
+    potentials and absorption decisions on one snapshot."""
+    obuild.build_ref(ref_root, variants=obuild.SPHEROID_VARIANTS)
+    meta = {}
+    for variant, A, seed, steps in SPHEROID_RUNS:
+        ref = RefLib(variant, build=False).setup(RunParams(**SPHEROID, A=A), seed=seed)
+        ref.set_grain(q=-400)
+        rec = {"variant": variant, "params": dict(SPHEROID, A=A), "seed": seed, "grain_q0": -400,
+               "init_sha256": digest(ref.particles())}
+        ref.run_steps(steps, compute_epe=True)
+        rec["steps"] = steps
+        rec["final_sha256"] = digest(ref.particles())
+        rec["final_grain"] = grain_json(ref.grain())
+        rec["final_epe"] = [float(v) for v in ref.epe()]
+        meta[variant] = rec
+    ref = RefLib("prolate_sceptic", build=False).setup(RunParams(**SPHEROID, A=3.0), seed=21)
+    ref.set_grain(q=-250)
+    ref.build_tree()
+    t = ref.tree_dump()
+    P = ref.particles()
+    rng = np.random.default_rng(4321)
+    idx = np.concatenate([[0], rng.choice(np.arange(1, SPHEROID["N"]), 255, replace=False)]).astype(np.uint32)
+    xyz = np.stack([P["x"][idx], P["y"][idx], P["z"][idx]], 1) + rng.normal(0, 1e-9, (len(idx), 3))
+    hi, lo = ref.field_many(idx, xyz)
+    R = SPHEROID["r"] * SPHEROID["mpp"]
+    pts = R + rng.uniform(-0.95 * R, 0.95 * R, (32, 3))
+    phi = np.array([ref.phi_at(*p) for p in pts])
+    pp = np.array([ref.phi_particle_feels(int(i)) for i in idx[:64]])
+    chi_b = ref.measure_chi_b()
+    a = SPHEROID["a"]
+    a_ax = a * 3.0 ** (2.0 / 3.0)
+    g = P[0:1].copy()
+    n = 2000
+    cpts = np.zeros(n, PARTICLE_DTYPE)
+    cd = np.zeros((n, 3))
+    cres = np.zeros(n, np.int8)
+    for k in range(n):
+        end = np.array([g["x"][0], g["y"][0], g["z"][0]]) + rng.uniform(-2.0, 2.0, 3) * a_ax
+        cpts[k]["x"], cpts[k]["y"], cpts[k]["z"] = end
+        cd[k] = rng.normal(0, a_ax, 3)
+        cres[k] = ref.cross_grain(cpts[k], cd[k], g[0], a)
+    arrays = dict(int_level=t["int_level"], int_path=t["int_path"], int_q=t["int_q"], int_aq=t["int_aq"],
+                  int_c=t["int_c"], int_w=t["int_w"], leaf_part=t["leaf_part"], leaf_level=t["leaf_level"],
+                  leaf_path=t["leaf_path"], field_idx=idx, field_xyz=xyz, field_hi=hi, field_lo=lo,
+                  phi_pts=pts, phi=phi, phi_part=pp, chi_b=np.array([chi_b]), cross_pts=cpts, cross_dpos=cd,
+                  cross_res=cres, snapshot_sha256=np.array([digest(P)]))
+    return meta, arrays
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=obuild.DEFAULT_REF_ROOT)
+    ap.add_argument("--spheroid-only", action="store_true", help="write only spheroid.json / spheroid.npz")
     a = ap.parse_args(argv)
+    meta_s, arrays_s = spheroid(a.ref_root)
+    with open(os.path.join(HERE, "spheroid.json"), "w") as f:
+        json.dump(meta_s, f, indent=1, sort_keys=True)
+    np.savez_compressed(os.path.join(HERE, "spheroid.npz"), **arrays_s)
+    if a.spheroid_only:
+        print("wrote spheroid.json, spheroid.npz")
+        return
     meta = runs(a.ref_root)
     with open(os.path.join(HERE, "runs.json"), "w") as f:
         json.dump(meta, f, indent=1, sort_keys=True)

@@ -100,3 +100,68 @@ def test_sceptic_sampler_matches_reference(snap):
             assert np.isnan(got)
         else:
             assert got == pytest.approx(alpha, rel=1e-13, abs=0)
+
+
+# ---- spheroidal grain (pot-spheroid.c) -------------------------------------
+
+def spheroid_runs():
+    with open(os.path.join(GOLD, "spheroid.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def sph():
+    return np.load(os.path.join(GOLD, "spheroid.npz"))
+
+
+@pytest.mark.parametrize("key", ["prolate_sceptic", "prolate", "oblate_sceptic"])
+def test_oracle_reproduces_spheroid_runs(key):
+    rec = spheroid_runs()[key]
+    p = dict(rec["params"])
+    p["B"] = tuple(p["B"])
+    o = Oracle(RunParams(**p), mode="reference", sceptic=key.endswith("_sceptic"), seed=rec["seed"])
+    o.set_grain(q=rec["grain_q0"])
+    assert digest(o.particles()) == rec["init_sha256"]
+    for _ in range(rec["steps"]):
+        o.step(compute_epe=True)
+    assert digest(o.particles()) == rec["final_sha256"]
+    g = o.grain()
+    for k, v in rec["final_grain"].items():
+        assert g[k] == v, k
+    assert o.last_step_stats()["epe"].tolist() == rec["final_epe"]
+
+
+def _spheroid_oracle():
+    rec = spheroid_runs()["prolate_sceptic"]
+    p = dict(rec["params"])
+    p["B"] = tuple(p["B"])
+    o = Oracle(RunParams(**p), mode="reference", sceptic=True, seed=21)
+    o.set_grain(q=-250)
+    o.build_tree()
+    return o
+
+
+def test_spheroid_tree_fields_potentials_match_reference(sph):
+    o = _spheroid_oracle()
+    assert digest(o.particles()) == str(sph["snapshot_sha256"][0])
+    d = o.tree_dump()
+    for k in ("int_level", "int_path", "int_q", "int_aq", "int_c", "int_w", "leaf_part", "leaf_level",
+              "leaf_path"):
+        assert np.array_equal(d[k], sph[k]), k
+    assert 0 not in set(d["leaf_part"].tolist())
+    hi, lo = o.field_many(sph["field_idx"], sph["field_xyz"])
+    assert np.array_equal(hi, sph["field_hi"])
+    assert np.array_equal(lo, sph["field_lo"])
+    phi = np.array([o.phi_at(*p) for p in sph["phi_pts"]])
+    assert np.array_equal(phi, sph["phi"])
+    pp = np.array([o.phi_particle_feels(int(i)) for i in sph["field_idx"][:64]])
+    assert np.array_equal(pp, sph["phi_part"][:, 0])
+    assert o.measure_chi_b() == sph["chi_b"][0]
+
+
+def test_spheroid_absorption_decisions_match_reference(sph):
+    o = _spheroid_oracle()
+    g = o.particles()[0:1]
+    res = np.array([o.cross_grain_run(p, dp, g[0]) for p, dp in zip(sph["cross_pts"], sph["cross_dpos"])])
+    assert np.array_equal(res.astype(np.int8), sph["cross_res"])
+    assert 0 < res.sum() < len(res)

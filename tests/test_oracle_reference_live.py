@@ -47,3 +47,84 @@ def test_gpu_semantics_close_to_reference():
     # electrons: same push except the sources' half-drift; reinjected ones differ (RNG)
     dx = np.sqrt((a["x"] - b["x"]) ** 2 + (a["y"] - b["y"]) ** 2 + (a["z"] - b["z"]) ** 2)[moved]
     assert np.median(dx) < 1e-7 * R
+
+
+SPHEROID = dict(STRESS, a=3.0e-7)
+
+
+@pytest.mark.parametrize("variant,A,sceptic,seed,steps", [("prolate_sceptic", 3.0, True, 3, 40),
+                                                          ("prolate", 5.0, False, 4, 40),
+                                                          ("oblate_sceptic", 0.4, True, 5, 40),
+                                                          ("oblate", 0.5, False, 6, 30)])
+def test_spheroid_reference_mode_bit_identical(variant, A, sceptic, seed, steps):
+    """pot-spheroid.c (grain out of the tree, analytic spheroid field and
+    potential, spheroid absorption, m_i/m_e = 1836.153, SCEPTIC tolerance
+    0.1) against the oracle's spheroid mode, bit for bit."""
+    ref = _ref(variant).setup(params(SPHEROID, A=A), seed=seed)
+    ref.set_grain(q=-400)
+    o = Oracle(params(SPHEROID, A=A), mode="reference", sceptic=sceptic, seed=seed)
+    o.set_grain(q=-400)
+    assert list(ref.tss()) == list(o.tss())
+    absorbed = 0
+    for _ in range(steps):
+        ref.step(compute_epe=True)
+        o.step(compute_epe=True)
+        absorbed += abs(o.last_step_stats()["dq"])
+    a, b = ref.particles(), o.particles()
+    a["_pad"] = 0
+    b["_pad"] = 0
+    assert a.tobytes() == b.tobytes()
+    ga, gb = ref.grain(), o.grain()
+    for k in ("q", "m", "tot_absor_e", "t_steps", "chi_b"):
+        assert ga[k] == gb[k], k
+    assert absorbed > 0
+    assert np.array_equal(ref.epe(), o.last_step_stats()["epe"])
+    # the tree holds no grain (pot-spheroid.c:1516-1518) and matches node for node
+    ref.build_tree()
+    o.build_tree()
+    dr, do = ref.tree_dump(), o.tree_dump()
+    assert 0 not in set(dr["leaf_part"].tolist())
+    for k in dr:
+        assert np.array_equal(dr[k], do[k]), k
+
+
+@pytest.mark.parametrize("variant,A", [("prolate_sceptic", 3.0), ("oblate_sceptic", 0.4)])
+def test_spheroid_field_phi_and_absorption_functions(variant, A):
+    """The reference's field_particle_feels_at / phi_at / phi_particle_feels /
+    does_particle_cross_grain on one snapshot, against the oracle's."""
+    d = SPHEROID
+    ref = _ref(variant).setup(params(d, A=A), seed=9)
+    ref.set_grain(q=-250)
+    o = Oracle(params(d, A=A), mode="reference", sceptic=False, seed=9, init=False)
+    o.set_particles(ref.particles())
+    o.set_grain(q=-250)
+    ref.build_tree()
+    o.build_tree()
+    rng = np.random.default_rng(1)
+    idx = rng.choice(np.arange(0, d["N"]), size=256, replace=False).astype(np.uint32)
+    P = ref.particles()
+    xyz = np.stack([P["x"][idx], P["y"][idx], P["z"][idx]], 1) * (1 + 1e-6 * rng.normal(size=(256, 3)))
+    hr, lr = ref.field_many(idx, xyz)
+    ho, lo = o.field_many(idx, xyz)
+    assert np.array_equal(hr, ho) and np.array_equal(lr, lo)
+    R = d["r"] * d["mpp"]
+    for x, y, z in rng.uniform(0.2 * R, 1.8 * R, size=(16, 3)):
+        assert ref.phi_at(x, y, z) == o.phi_at(x, y, z)
+    for i in idx[:64]:
+        hr, lr = ref.phi_particle_feels(int(i))
+        assert hr == o.phi_particle_feels(int(i))
+    # absorption: segments aimed at and past the grain
+    g = P[0:1].copy()
+    a_ax = d["a"] * A ** (2.0 / 3.0)
+    hits = 0
+    for k in range(400):
+        p = P[1:2].copy()
+        end = np.array([g["x"][0], g["y"][0], g["z"][0]]) + rng.uniform(-2.5, 2.5, 3) * a_ax
+        start = end + rng.normal(size=3) * a_ax
+        p["x"], p["y"], p["z"] = end
+        dpos = end - start
+        r1 = ref.cross_grain(p, dpos, g, d["a"])
+        r2 = o.cross_grain_run(p, dpos, g)
+        assert r1 == r2
+        hits += r1
+    assert 0 < hits < 400
