@@ -69,7 +69,11 @@ typedef struct pot_run_cfg {
 	double settle;    /* settling time before absorption starts, s (-e) */
 	double theta;     /* opening angle OAP (pot.c:97) */
 	double B[3];      /* EXTERNAL_B_X/Y/Z, tesla (pot.c:55-57) */
-	double A;         /* spheroid aspect ratio (-A of pot-spheroid.c); 0 = sphere */
+	double A;         /* spheroid aspect ratio (-A of pot-spheroid.c): 0 = the sphere of
+	                     pot.c; > 1 prolate, in (0, 1) oblate (PROLATE / OBLATE programs,
+	                     whose grain stays out of the tree and whose m_i/m_e is 1836.153) */
+	double axis[3];   /* spheroid symmetry axis; zero = x, the reference's.  Any other
+	                     direction tilts the grain (no counterpart in the reference) */
 } pot_run_cfg;
 
 #define POT_CFG_SCEPTIC 0x1u        /* SCEPTIC_REINJECTION (pot.c:181): flux-weighted reinjection */

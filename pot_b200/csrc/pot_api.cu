@@ -234,7 +234,65 @@ static int fill_params(pot_gpu_ctx* c)
 	P.key_bits = c->opts.form == POT_FORM_FAST ? 63u - 3u * P.max_level : 0u;
 	P.group_max = c->opts.group_size == 64 ? 64u : 32u;
 	P.seed = c->opts.seed;
-	const long double m_ion = (long double)MASS_ION, m_e = (long double)MASS_E, m_d = (long double)MASS_DUST;
+	// grain shape: 0 sphere, A > 1 prolate, 0 < A < 1 oblate (pot-spheroid.c:4797-4827)
+	if (r.A == 0.0) {
+		P.shape = 0;
+	} else if (r.A > 1.0) {
+		P.shape = 1;
+	} else if (r.A > 0.0 && r.A < 1.0) {
+		P.shape = 2;
+	} else {
+		return POT_E_ARG;
+	}
+	P.n_tree = P.shape ? P.n - 1 : P.n;
+	P.m_ion = (P.shape ? 1836.153 : MIME) * ME;
+	P.max_lin_dev = P.shape ? 0.1 : 0.01;
+	if (P.shape) {
+		const double A = r.A, a = r.a;
+		P.s_A = A;
+		P.s_thr = a * a * std::pow(A, 4.0 / 3.0);
+		if (P.shape == 1) {
+			P.s_fc_f = (a * std::sqrt(A * A - 1.0)) * std::pow(A, -1.0 / 3.0);
+			P.s_fc_p = a * std::sqrt(A * A - 1.0) / std::pow(A, 1.0 / 3.0);
+			P.s_num = std::acosh(A);
+			P.s_den_f = 4.0 * PI_REF * EPSILON0 * P.s_fc_f * std::log(A - std::sqrt(A * A - 1.0));
+			P.s_den_p = 4.0 * PI_REF * EPSILON0 * P.s_fc_p * std::log(A - std::sqrt(A * A - 1.0));
+		} else {
+			P.s_fc_f = (a * std::sqrt(1.0 - A * A)) * std::pow(A, -1.0 / 3.0);
+			P.s_fc_p = P.s_fc_f;
+			P.s_num = std::acos(A);
+			const double at = std::atan((1.0 - std::sqrt(1.0 - A * A)) / A) - 0.25 * PI_REF;
+			P.s_den_f = 8.0 * PI_REF * EPSILON0 * P.s_fc_f * at;
+			P.s_den_p = 4.0 * PI_REF * EPSILON0 * P.s_fc_p * at;
+		}
+		double ax[3] = { r.axis[0], r.axis[1], r.axis[2] };
+		double nrm = std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
+		if (!(nrm > 0.0)) {
+			ax[0] = 1.0;
+			ax[1] = ax[2] = 0.0;
+		} else {
+			for (int k = 0; k < 3; k++) ax[k] /= nrm;
+		}
+		P.s_tilted = !(ax[0] == 1.0 && ax[1] == 0.0 && ax[2] == 0.0);
+		double ref[3] = { 0.0, 1.0, 0.0 };
+		if (std::fabs(ax[1]) > 0.9) {
+			ref[1] = 0.0;
+			ref[2] = 1.0;
+		}
+		const double d = ref[0] * ax[0] + ref[1] * ax[1] + ref[2] * ax[2];
+		double e1[3];
+		for (int k = 0; k < 3; k++) e1[k] = ref[k] - d * ax[k];
+		nrm = std::sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+		for (int k = 0; k < 3; k++) e1[k] /= nrm;
+		const double e2[3] = { ax[1] * e1[2] - ax[2] * e1[1], ax[2] * e1[0] - ax[0] * e1[2],
+		                       ax[0] * e1[1] - ax[1] * e1[0] };
+		for (int k = 0; k < 3; k++) {
+			P.s_ax[k] = ax[k];
+			P.s_e1[k] = e1[k];
+			P.s_e2[k] = e2[k];
+		}
+	}
+	const long double m_ion = (long double)P.m_ion, m_e = (long double)MASS_E, m_d = (long double)MASS_DUST;
 	// species time-step multiples, pot.c:4157-4159
 	P.tss[SP_E] = 1;
 	P.tss[SP_ION] = (uint32_t)(int)std::sqrt((double)(r.Te * m_ion / (r.Ti * m_e)));
@@ -369,11 +427,13 @@ int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx
 	if (o.form == POT_FORM_PLAIN && o.leaf_size != 1) return POT_E_ARG;
 	if (o.leaf_size > 64) return POT_E_ARG;
 	if (o.group_size != 0 && o.group_size != 32 && o.group_size != 64) return POT_E_ARG;
-	if (cfg->N < 2 || cfg->N > (1ull << 24) || cfg->N <= o.leaf_size) return POT_E_ARG;  // scans cover 2^24
+	// aspect ratio: 0 (sphere), > 1 (prolate) or in (0, 1) (oblate)
+	if (!(cfg->A == 0.0 || cfg->A > 1.0 || (cfg->A > 0.0 && cfg->A < 1.0))) return POT_E_ARG;
+	// scans cover 2^24; the tree needs more sources than a leaf holds
+	if (cfg->N < 2 || cfg->N > (1ull << 24) || cfg->N <= o.leaf_size + (cfg->A != 0.0 ? 1u : 0u)) return POT_E_ARG;
 	if (cfg->r == 0 || !(cfg->mpp > 0.0) || !(cfg->dt > 0.0) || !(cfg->a > 0.0) || cfg->soft < 0.0 ||
 	    !(cfg->theta > 0.0) || cfg->Te < 0.0 || cfg->Ti <= 0.0)
 		return POT_E_ARG;
-	if (cfg->A != 0.0 && cfg->A != 1.0) return POT_E_ARG;  // spheroidal grains are not in this build
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return POT_E_CUDA;
 	if (o.device < 0 || o.device >= ndev) return POT_E_ARG;
@@ -741,9 +801,9 @@ int pot_gpu_tree_dump(pot_gpu_ctx* c, uint64_t max_nodes, uint64_t* n_int, int32
 			if (c->P.leaf_size > 1) {
 				s0 = lrange[e].x;
 				cnt = lrange[e].y;
-			} else if (e >= c->n) {
-				s0 = ovf[e - c->n].x;
-				cnt = ovf[e - c->n].y;
+			} else if (e >= c->P.n_tree) {
+				s0 = ovf[e - c->P.n_tree].x;
+				cnt = ovf[e - c->P.n_tree].y;
 			}
 			for (uint32_t j = 0; j < cnt; j++) {
 				if (nl >= max_nodes) return POT_E_ARG;

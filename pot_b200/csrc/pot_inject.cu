@@ -62,7 +62,8 @@ __device__ double d_u_icdf(double U, double chi, double q, bool& ok)
 	return u;
 }
 
-__device__ double d_integrate_for_alpha(double s, double chi_b, double u2, double Rol, bool& ok)
+// mld: max_lin_dev, 0.01 in pot.c:436 and 0.1 in pot-spheroid.c:457
+__device__ double d_integrate_for_alpha(double s, double chi_b, double u2, double Rol, double mld, bool& ok)
 {
 	const double chu2 = chi_b / u2;
 	const double s2 = s * s;
@@ -77,7 +78,7 @@ __device__ double d_integrate_for_alpha(double s, double chi_b, double u2, doubl
 		xi1 = (xi0 + xi2) / 2.0;
 		y1 = 1.0 - (chu2 * xi1 * exp(Rol * (1.0 - (1.0 / xi1))));
 		y1 = 1.0 / sqrt((y1 / s2) - (xi1 * xi1));
-		while (fabs(y2 - y1 - (y1 - y0)) > 0.01) {
+		while (fabs(y2 - y1 - (y1 - y0)) > mld) {
 			xi2 = xi1;
 			y2 = y1;
 			xi1 = (xi0 + xi2) / 2.0;
@@ -100,7 +101,7 @@ __device__ double d_integrate_for_alpha(double s, double chi_b, double u2, doubl
 // once, and a ballot picks the first k that passes the linearity test -- the
 // interval the sequential loop stops at, with the same values.  All lanes
 // return the same alpha.
-__device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, double Rol, bool& ok)
+__device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, double Rol, double mld, bool& ok)
 {
 	const uint32_t lane = threadIdx.x & 31u;
 	const double chu2 = chi_b / u2;
@@ -123,7 +124,7 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 		const double e_up = __shfl_up_sync(0xffffffffu, ek1, 1);
 		const double y_ek = lane == 0 ? y_one : y_up;
 		const double e_k = lane == 0 ? 1.0 : e_up;
-		const bool linear = !(fabs(y_ek - y - (y - y0)) > 0.01);
+		const bool linear = !(fabs(y_ek - y - (y - y0)) > mld);
 		const uint32_t pass = __ballot_sync(0xffffffffu, linear);
 		if (pass == 0) {
 			// more than 32 halvings needed at this xi0: continue from e_32
@@ -145,7 +146,7 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 				const double xe_up = __shfl_up_sync(0xffffffffu, xe, 1);
 				const double y_hi = lane == 0 ? y2 : yy_up;
 				const double x_hi = lane == 0 ? e2 : xe_up;
-				const bool lin = !(fabs(y_hi - yy - (yy - y0)) > 0.01);
+				const bool lin = !(fabs(y_hi - yy - (yy - y0)) > mld);
 				const uint32_t pb = __ballot_sync(0xffffffffu, lin);
 				if (pb) {
 					const int k = __ffs(pb) - 1;
@@ -270,8 +271,8 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 		sincos(psi, &sps, &cps);
 		rot_xy(1.0, 0.0, sps, cps, u[0], u[1], u[2], 0.0);
 		b = sqrt(st.rnd(1.0 - (chi_b / u2)));
-		alpha = WARP ? d_integrate_for_alpha_warp(b, chi_b, u2, P.Rol, ok)
-		             : d_integrate_for_alpha(b, chi_b, u2, P.Rol, ok);
+		alpha = WARP ? d_integrate_for_alpha_warp(b, chi_b, u2, P.Rol, P.max_lin_dev, ok)
+		             : d_integrate_for_alpha(b, chi_b, u2, P.Rol, P.max_lin_dev, ok);
 		if (!isnan(alpha) || attempt + 1 >= RETRY_CAP) break;
 	}
 	if (isnan(alpha)) {

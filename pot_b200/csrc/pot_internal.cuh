@@ -147,7 +147,18 @@ struct Params {
 	double Rol;               // R / Debye length of pot.c:577-579
 	float oap2_f;
 	float soft2_f;        // (soft / rad)^2: FP32 walk works in units of the domain radius
-	float pad[2];
+	uint32_t n_tree;      // tree sources: slots [0, n_tree); n - 1 with a spheroidal grain (kept last, outside)
+	uint32_t shape;       // grain: 0 sphere (pot.c), 1 prolate, 2 oblate spheroid (pot-spheroid.c)
+	double m_ion;         // MASS[ION] = MIME * ME; MIME 1836.15, or 1836.153 in pot-spheroid.c:61
+	double max_lin_dev;   // integrate_for_alpha tolerance: 0.01, or 0.1 in pot-spheroid.c:457
+	// spheroid constants (host libm, in the reference's operation order):
+	// phi_const = ((QE q) s_num) / s_den_*, s_fc_* the focal distances of the
+	// field (pot-spheroid.c:1702-1715) and potential (1926-1946, 2056-2069) forms
+	double s_A, s_fc_f, s_fc_p, s_num, s_den_f, s_den_p;
+	double s_thr;         // a^2 A^(4/3): surface x^2 + A^2 rho^2 = a^2 A^(4/3)
+	uint32_t s_tilted;    // symmetry axis other than x (an extension of the reference)
+	uint32_t s_pad;
+	double s_ax[3], s_e1[3], s_e2[3];  // spheroid frame
 };
 
 // ---- exactly rounded double helpers (no FMA contraction) ---------------

@@ -21,13 +21,128 @@ __device__ __forceinline__ bool cross_grain(double px, double py, double pz, dou
 	return dsub(ss, dmul(alpha, ds)) <= a2;
 }
 
+// ---- spheroidal grain (pot-spheroid.c, PROLATE / OBLATE programs) -------
+// Grain-relative vectors are taken into the spheroid's frame (axis, e1, e2);
+// for the reference's x axis that is the identity, bit for bit.  Products
+// and sums are unfused and in the reference's order; the transcendental
+// functions are CUDA's (within a few ulp of the host libm).
+
+__device__ __forceinline__ void sph_to_frame(const Params& P, double dx, double dy, double dz, double& u, double& v,
+                                             double& w)
+{
+	if (!P.s_tilted) {
+		u = dx;
+		v = dy;
+		w = dz;
+		return;
+	}
+	u = dadd(dadd(dmul(dx, P.s_ax[0]), dmul(dy, P.s_ax[1])), dmul(dz, P.s_ax[2]));
+	v = dadd(dadd(dmul(dx, P.s_e1[0]), dmul(dy, P.s_e1[1])), dmul(dz, P.s_e1[2]));
+	w = dadd(dadd(dmul(dx, P.s_e2[0]), dmul(dy, P.s_e2[1])), dmul(dz, P.s_e2[2]));
+}
+
+__device__ __forceinline__ void sph_from_frame(const Params& P, double u, double v, double w, double out[3])
+{
+	if (!P.s_tilted) {
+		out[0] = u;
+		out[1] = v;
+		out[2] = w;
+		return;
+	}
+#pragma unroll
+	for (int k = 0; k < 3; k++) out[k] = dadd(dadd(dmul(u, P.s_ax[k]), dmul(v, P.s_e1[k])), dmul(w, P.s_e2[k]));
+}
+
+// rt of the prolate / oblate forms (pot-spheroid.c:1740-1752):
+// rho2^2 + x^4 + c^4 + 2 rho2 x^2 -/+ 2 rho2 c^2 +/- 2 x^2 c^2, left to right
+__device__ __forceinline__ double sph_rt(int shape, double rho2, double x, double fc)
+{
+	const double x4 = dmul(dmul(dmul(x, x), x), x);
+	const double c4 = dmul(dmul(dmul(fc, fc), fc), fc);
+	const double t4 = dmul(dmul(dmul(2.0, rho2), x), x);
+	const double t5 = dmul(dmul(dmul(2.0, rho2), fc), fc);
+	const double t6 = dmul(dmul(dmul(2.0, x), x), fc);
+	const double t6c = dmul(t6, fc);
+	const double head = dadd(dadd(dadd(dmul(rho2, rho2), x4), c4), t4);
+	return shape == 1 ? sqrt(dsub(dadd(head, t5), t6c)) : sqrt(dadd(dsub(head, t5), t6c));
+}
+
+// field_particle_feels_from_grain (pot-spheroid.c:1689-1779) at
+// grain-relative (dx, dy, dz) for grain charge q (elementary charges), V/m.
+__device__ __forceinline__ void spheroid_field(const Params& P, double q, double dx, double dy, double dz,
+                                               double E[3])
+{
+	double x, y, z;
+	sph_to_frame(P, dx, dy, dz, x, y, z);
+	const double fc = P.s_fc_f;
+	const double phi_const = ddiv(dmul(dmul(QE, q), P.s_num), P.s_den_f);
+	const double rho2 = dadd(dmul(y, y), dmul(z, z));
+	const double rt = sph_rt((int)P.shape, rho2, x, fc);
+	const double c2 = dmul(fc, fc);
+	const double num = P.shape == 1 ? dadd(dsub(dadd(rho2, dmul(x, x)), c2), rt)
+	                                : dadd(dadd(dadd(rho2, dmul(x, x)), c2), rt);
+	const double e2 = ddiv(num, dmul(dmul(2.0, fc), fc));  // sinh^2 (prolate), cosh^2 (oblate)
+	const double En = ddiv(-phi_const, sqrt(dmul(e2, rt)));
+	const double beta = atan(ddiv(dmul(-e2, x), dmul(P.shape == 1 ? dadd(e2, 1.0) : dsub(e2, 1.0), sqrt(rho2))));
+	const double theta = atan(ddiv(fabs(z), fabs(y)));
+	const double cb = cos(beta);
+	const double u = dmul(-En, sin(beta));
+	const double v = ddiv(dmul(dmul(dmul(En, cb), cos(theta)), fabs(y)), y);
+	const double w = ddiv(dmul(dmul(dmul(En, cb), sin(theta)), fabs(z)), z);
+	sph_from_frame(P, u, v, w, E);
+}
+
+// the spheroid's potential at (x, y, z) already in its frame, V
+// (pot-spheroid.c:2054-2078; the same forms at 1924-1953)
+__device__ __forceinline__ double spheroid_phi_frame(const Params& P, double q, double x, double y, double z)
+{
+	const double fc = P.s_fc_p;
+	const double phi_const = ddiv(dmul(dmul(QE, q), P.s_num), P.s_den_p);
+	const double rho2 = dadd(dmul(y, y), dmul(z, z));
+	const double rt = sph_rt((int)P.shape, rho2, x, fc);
+	const double c2 = dmul(fc, fc);
+	const double rx = dadd(rho2, dmul(x, x));
+	const double ratio = ddiv(dsub(sqrt(dadd(dadd(rx, c2), rt)), dmul(fc, sqrt(2.0))), sqrt(dadd(dsub(rx, c2), rt)));
+	return P.shape == 1 ? dmul(phi_const, log(ratio)) : dmul(phi_const, dsub(atan(ratio), dmul(0.25, PI_REF)));
+}
+
+// phi_particle_feels_from_grain: grain-relative (dx, dy, dz)
+__device__ __forceinline__ double spheroid_phi(const Params& P, double q, double dx, double dy, double dz)
+{
+	double x, y, z;
+	sph_to_frame(P, dx, dy, dz, x, y, z);
+	return spheroid_phi_frame(P, q, x, y, z);
+}
+
+// does_particle_cross_grain of pot-spheroid.c:2448-2537, p the new position,
+// d the step's displacement, g the grain.
+__device__ __forceinline__ bool cross_spheroid(const Params& P, double px, double py, double pz, double ddx,
+                                               double ddy, double ddz, double gx, double gy, double gz)
+{
+	double s0, s1, s2, d0, d1, d2;
+	sph_to_frame(P, dsub(gx, px), dsub(gy, py), dsub(gz, pz), s0, s1, s2);
+	sph_to_frame(P, ddx, ddy, ddz, d0, d1, d2);
+	const double A = P.s_A;
+	if (dadd(dmul(s0, s0), dmul(dmul(dadd(dmul(s1, s1), dmul(s2, s2)), A), A)) <= P.s_thr) return true;
+	const double xm = ddiv(dadd(dmul(d1, dsub(dmul(d1, s0), dmul(d0, s1))), dmul(d2, dsub(dmul(d2, s0), dmul(d0, s2)))),
+	                       dadd(dadd(ddiv(dmul(d0, d0), dmul(A, A)), dmul(d1, d1)), dmul(d2, d2)));
+	const double xp = dsub(s0, d0);
+	if (((xm > s0) && (xm > xp)) || ((xm < s0) && (xm < xp))) return false;
+	const double ym = dadd(ddiv(dmul(d1, dsub(xm, s0)), d0), s1);
+	const double zm = dadd(ddiv(dmul(d2, dsub(xm, s0)), d0), s2);
+	return dadd(dmul(xm, xm), dmul(dmul(dadd(dmul(ym, ym), dmul(zm, zm)), A), A)) <= P.s_thr;
+}
+
 // check_particle_in_sim_area, pot.c:2071-2076 (spherical domain)
 __device__ __forceinline__ bool outside_domain(double x, double y, double z, const Params& P)
 {
 	return sqrt(dsq3(dsub(x, P.rad), dsub(y, P.rad), dsub(z, P.rad))) > P.rad;
 }
 
-__device__ __forceinline__ double mass_of(int sp) { return sp == SP_DUST ? MASS_DUST : (sp == SP_ION ? MASS_ION : MASS_E); }
+__device__ __forceinline__ double mass_of(int sp, const Params& P)
+{
+	return sp == SP_DUST ? MASS_DUST : (sp == SP_ION ? P.m_ion : MASS_E);
+}
 
 // Boris step of pot.c:2475-2532 given E at the half-drifted position h:
 // v += dt a; rotate about b by 2 atan(dt qom |B| / 2); v += dt a;
@@ -84,9 +199,13 @@ __device__ __forceinline__ uint32_t after_push(int sp, const double4& p_old, con
                                                double gy, double gz)
 {
 	uint32_t reason = 0;
-	if (absorb_on && sp != SP_DUST &&
-	    cross_grain(xn.x, xn.y, xn.z, dsub(xn.x, p_old.x), dsub(xn.y, p_old.y), dsub(xn.z, p_old.z), gx, gy, gz,
-	                P.a)) {
+	bool hit = false;
+	if (absorb_on && sp != SP_DUST) {
+		const double ddx = dsub(xn.x, p_old.x), ddy = dsub(xn.y, p_old.y), ddz = dsub(xn.z, p_old.z);
+		hit = P.shape ? cross_spheroid(P, xn.x, xn.y, xn.z, ddx, ddy, ddz, gx, gy, gz)
+		              : cross_grain(xn.x, xn.y, xn.z, ddx, ddy, ddz, gx, gy, gz, P.a);
+	}
+	if (hit) {
 		tally_absorbed(rec, sp, vn);
 		reason = 1;
 	} else if (outside_domain(xn.x, xn.y, xn.z, P)) {

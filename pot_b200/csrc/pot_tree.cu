@@ -101,8 +101,12 @@ __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ k
 	} else if (p.x < 0.0 || p.x > P.root_w || p.y < 0.0 || p.y > P.root_w || p.z < 0.0 || p.z > P.root_w) {
 		set_status(rec, POT_E_DOMAIN);  // build_tree returns NULL, pot.c:1491-1500
 	}
-	keys[s] = P.form == POT_FORM_FAST ? scaled_key(p.x, p.y, p.z, 2097152.0 / P.root_w)
-	                                  : morton_key(p.x, p.y, p.z, P.root_w);
+	// A spheroidal grain is not a tree source (pot-spheroid.c:1516-1518): the
+	// largest key sorts it to the last slot, outside [0, n_tree).  No
+	// particle of the spherical domain lies in that corner cell.
+	keys[s] = (P.shape && (int)p.w == SP_DUST) ? 0x7FFFFFFFFFFFFFFFull
+	          : P.form == POT_FORM_FAST       ? scaled_key(p.x, p.y, p.z, 2097152.0 / P.root_w)
+	                                          : morton_key(p.x, p.y, p.z, P.root_w);
 	vals[s] = s;
 }
 
@@ -328,7 +332,7 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 				const double2 c01 = __ldcg(cp2), c23 = __ldcg(cp2 + 1);
 				const double4 c = make_double4(c01.x, c01.y, c23.x, c23.y);
 				ccx = c.x; ccy = c.y; ccz = c.z;
-			} else if (L == 1 && leaf_payload(code) < P.n) {
+			} else if (L == 1 && leaf_payload(code) < P.n_tree) {
 				const double4 sp = src64[leaf_payload(code)];
 				cq = (int)sp.w;
 				caq = (uint32_t)abs(cq);
@@ -336,7 +340,7 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 			} else {
 				// bucket leaf: its own running moments over its particles
 				const uint32_t e = leaf_payload(code);
-				const uint2 r = L == 1 ? T.ovf[e - P.n] : T.lrange[e];
+				const uint2 r = L == 1 ? T.ovf[e - P.n_tree] : T.lrange[e];
 				cq = 0;
 				caq = 0;
 				ccx = ccy = ccz = 0.0;
@@ -417,8 +421,8 @@ __global__ void k_moments_fast(TreeDev T, const double4* __restrict__ src64, Par
 					const uint2 r = T.lrange[e];
 					j0 = r.x;
 					j1 = r.x + r.y;
-				} else if (e >= P.n) {
-					const uint2 r = T.ovf[e - P.n];
+				} else if (e >= P.n_tree) {
+					const uint2 r = T.ovf[e - P.n_tree];
 					j0 = r.x;
 					j1 = r.x + r.y;
 				}
@@ -686,8 +690,8 @@ void launch_reorder(const uint32_t* perm, const double4* pos_in, const double4* 
 void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const Params& P, RunRec* rec,
                   uint32_t* block_sums, cudaStream_t s, Timer& tm)
 {
-	const uint32_t n = P.n, L = P.leaf_size;
-	const uint32_t n_pairs = n - L;  // n > L is checked at creation
+	const uint32_t n = P.n_tree, L = P.leaf_size;
+	const uint32_t n_pairs = n - L;  // n_tree > L is checked at creation
 	cudaMemsetAsync(&rec->n_overflow, 0, sizeof(unsigned int), s);
 	{
 		ScopedKernel k(tm, "tree_pairs");

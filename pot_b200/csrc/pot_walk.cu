@@ -17,6 +17,8 @@ __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
 // E (V/m) at (x, y, z) for the particle in Morton slot `self`:
 // field_particle_feels_at, pot.c:1696-1808 (monopole cells).
+// E[] holds the starting field on entry: zero, or a spheroidal grain's own
+// field (pot-spheroid.c:1815-1819).
 __device__ int field_plain(uint32_t self, double x, double y, double z, const TreeDev& T,
                            const double4* __restrict__ src64, const Params& P, double E[3],
                            uint32_t& n_inter)
@@ -24,7 +26,7 @@ __device__ int field_plain(uint32_t self, double x, double y, double z, const Tr
 	int32_t stack[WALK_STACK];
 	int len = 1;
 	stack[0] = 0;
-	double ex = 0.0, ey = 0.0, ez = 0.0;
+	double ex = E[0], ey = E[1], ez = E[2];
 	while (len) {
 		const int32_t code = stack[--len];
 		if (code >= 0) {
@@ -55,8 +57,8 @@ __device__ int field_plain(uint32_t self, double x, double y, double z, const Tr
 		} else {
 			const uint32_t e = leaf_payload(code);
 			uint32_t j0 = e, j1 = e + 1;
-			if (e >= P.n) {  // overflow bucket (see OVF_CAP)
-				const uint2 r = T.ovf[e - P.n];
+			if (e >= P.n_tree) {  // overflow bucket (see OVF_CAP)
+				const uint2 r = T.ovf[e - P.n_tree];
 				j0 = r.x;
 				j1 = r.x + r.y;
 			}
@@ -118,8 +120,8 @@ __device__ double phi_plain(uint32_t self, double x, double y, double z, const T
 		} else {
 			const uint32_t e = leaf_payload(code);
 			uint32_t j0 = e, j1 = e + 1;
-			if (P.leaf_size > 1 || e >= P.n) {
-				const uint2 r = P.leaf_size > 1 ? T.lrange[e] : T.ovf[e - P.n];
+			if (P.leaf_size > 1 || e >= P.n_tree) {
+				const uint2 r = P.leaf_size > 1 ? T.lrange[e] : T.ovf[e - P.n_tree];
 				j0 = r.x;
 				j1 = r.x + r.y;
 			}
@@ -166,11 +168,15 @@ __global__ void __launch_bounds__(128) k_epe_plain(const double4* __restrict__ p
 		for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P.n; s += gridDim.x * blockDim.x) {
 			const double4 p = src64[s];
 			int rc = POT_OK;
-			const double phi = phi_plain(s, p.x, p.y, p.z, T, src64, P, rc);
+			double phi = phi_plain(s, p.x, p.y, p.z, T, src64, P, rc);
 			if (rc != POT_OK) set_status(rec, rc);
 			if (s == gs) {
 				rec->phi_grain = phi;
 				continue;
+			}
+			if (P.shape) {  // pot-spheroid.c:2107-2109: the grain's own potential first
+				phi = spheroid_phi(P, (double)rec->grain_q, dsub(p.x, rec->grain_pos[0]), dsub(p.y, rec->grain_pos[1]),
+				                   dsub(p.z, rec->grain_pos[2])) + phi;
 			}
 			const int sp = (int)pos[s].w;
 			acc[sp] += (QE * p.w) * phi;
@@ -230,14 +236,15 @@ __global__ void __launch_bounds__(128) k_push_plain(double4* __restrict__ pos, d
 		const double dt = P.dt * (double)P.tss[sp];
 		const double half = 0.5 * dt;
 		const double3 h = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
-		double E[3];
+		double E[3] = { 0.0, 0.0, 0.0 };
+		if (P.shape && sp != SP_DUST) spheroid_field(P, qg, dsub(h.x, gx), dsub(h.y, gy), dsub(h.z, gz), E);
 		uint32_t ni = 0;
 		const int rc = field_plain(s, h.x, h.y, h.z, T, src64, P, E, ni);
 		if (rc != POT_OK) set_status(rec, rc);
 		n_inter += ni;
 		n_push++;
 		const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
-		const double qom = (QE * charge) / mass_of(sp);
+		const double qom = (QE * charge) / mass_of(sp, P);
 		double3 xn;
 		boris(v, h, E, qom, dt, P, xn);
 		uint32_t reason = 0;
@@ -278,11 +285,11 @@ __global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel
                             RunRec* rec, int epe)
 {
 	if (threadIdx.x != 0 || blockIdx.x != 0) return;
-	const double dm = (double)rec->nabs_ion * MASS_ION + (double)rec->nabs_e * MASS_E;
+	const double dm = (double)rec->nabs_ion * P.m_ion + (double)rec->nabs_e * MASS_E;
 	const double m = rec->grain_m + dm;
 	double dp[3];
 	for (int k = 0; k < 3; k++) {
-		dp[k] = MASS_E * ((double)rec->sumv_e[k] / VFIX) + MASS_ION * ((double)rec->sumv_ion[k] / VFIX);
+		dp[k] = MASS_E * ((double)rec->sumv_e[k] / VFIX) + P.m_ion * ((double)rec->sumv_ion[k] / VFIX);
 	}
 	const uint32_t gs = rec->grain_slot;
 	double gv[3] = { rec->grain_vel[0], rec->grain_vel[1], rec->grain_vel[2] };
@@ -364,8 +371,8 @@ __device__ double warp_phi(double x, double y, double z, const TreeDev& T, const
 		} else if (code != CH_EMPTY) {
 			const uint32_t e = leaf_payload(code);
 			uint32_t j0 = e, j1 = e + 1;
-			if (P.leaf_size > 1 || e >= P.n) {
-				const uint2 r = P.leaf_size > 1 ? T.lrange[e] : T.ovf[e - P.n];
+			if (P.leaf_size > 1 || e >= P.n_tree) {
+				const uint2 r = P.leaf_size > 1 ? T.lrange[e] : T.ovf[e - P.n_tree];
 				j0 = r.x;
 				j1 = r.x + r.y;
 			}
@@ -396,6 +403,18 @@ __device__ double warp_phi(double x, double y, double z, const TreeDev& T, const
 	return overflow ? __longlong_as_double(0x7ff8000000000000ll) : acc;
 }
 
+// The spheroid's term of phi_at (pot-spheroid.c:1924-1953), which the
+// reference evaluates at the point's own coordinates rather than relative
+// to the grain; reproduced as written.  Zero for a spherical grain, whose
+// charge is a tree source.
+__device__ __forceinline__ double spheroid_phi_at(const Params& P, const RunRec* rec, double x, double y, double z)
+{
+	if (!P.shape) return 0.0;
+	double u, v, w;
+	sph_to_frame(P, x, y, z, u, v, w);
+	return spheroid_phi_frame(P, (double)rec->grain_q, u, v, w);
+}
+
 // measure_chi_b (pot.c:2251-2279) for one rank: azimuth 0 in the x-y plane
 // through the grain, every 20 steps (pot.c:2409).
 __global__ void k_chi_b(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec, int force)
@@ -408,7 +427,7 @@ __global__ void k_chi_b(TreeDev T, const double4* __restrict__ src64, Params P, 
 	const double x = rec->grain_pos[0] + (r * cos(0.0) * sin(zen));
 	const double y = rec->grain_pos[1] + (r * sin(0.0) * sin(zen));
 	const double z = rec->grain_pos[2] + (r * cos(zen));
-	const double phi = warp_phi(x, y, z, T, src64, P, stack);
+	const double phi = spheroid_phi_at(P, rec, x, y, z) + warp_phi(x, y, z, T, src64, P, stack);
 	if (lane_id() == 0) {
 		if (isnan(phi)) set_status(rec, POT_E_WALK);
 		else rec->chi_b = phi / (KB * P.Ti / (1 * QE));
@@ -421,7 +440,8 @@ __global__ void k_phi_query(TreeDev T, const double4* __restrict__ src64, const 
 	__shared__ int32_t stack[4][PHI_STACK];
 	const uint32_t w = threadIdx.x >> 5;
 	for (uint32_t q = blockIdx.x * 4 + w; q < nq; q += gridDim.x * 4) {
-		const double v = warp_phi(xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2], T, src64, P, stack[w]);
+		const double v = spheroid_phi_at(P, rec, xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]) +
+		                 warp_phi(xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2], T, src64, P, stack[w]);
 		if (lane_id() == 0) {
 			phi[q] = v;
 			if (isnan(v)) set_status(rec, POT_E_WALK);
@@ -435,7 +455,11 @@ __global__ void k_field_query_plain(TreeDev T, const double4* __restrict__ src64
 {
 	const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
 	if (q >= nq) return;
-	double e[3];
+	double e[3] = { 0.0, 0.0, 0.0 };
+	if (P.shape && self_slot[q] != rec->grain_slot) {
+		spheroid_field(P, (double)rec->grain_q, dsub(xyz[3 * q], rec->grain_pos[0]), dsub(xyz[3 * q + 1], rec->grain_pos[1]),
+		               dsub(xyz[3 * q + 2], rec->grain_pos[2]), e);
+	}
 	uint32_t ni = 0;
 	const int rc = field_plain(self_slot[q], xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2], T, src64, P, e, ni);
 	if (rc != POT_OK) set_status(rec, rc);
@@ -450,8 +474,8 @@ __global__ void k_field_query_plain(TreeDev T, const double4* __restrict__ src64
 void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,
                       const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P,
                       RunRec* rec, cudaStream_t s, Timer& tm);
-void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, uint2* groups_all, double* partial,
-                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, const double4* src64,
+                     uint2* groups_all, double* partial, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 void launch_field_query_fast(const TreeDev& T, const float4* src32, const double* xyz, const uint32_t* self_slot,
                              uint32_t nq, double* E, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 
@@ -505,7 +529,7 @@ void launch_epe(const double4* pos, const TreeDev& T, const double4* src64, cons
                 double* partial, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
 {
 	if (P.form == POT_FORM_FAST) {
-		launch_epe_fast(pos, T, src32, groups_all, partial, P, rec, s, tm);
+		launch_epe_fast(pos, T, src32, src64, groups_all, partial, P, rec, s, tm);
 		ScopedKernel k(tm, "epe_final");
 		k_epe_final<<<1, 1024, 0, s>>>(partial, &rec->n_groups_all, 0, rec);
 		return;

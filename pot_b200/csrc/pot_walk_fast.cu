@@ -270,7 +270,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 				const uint32_t e = leaf_payload(code);
 				if (single_leaves) {
 					leafr = true;
-					range = e < P.n ? make_uint2(e, 1u) : T.ovf[e - P.n];
+					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
 				} else {
 					cell = T.lf[e];
 					if (box_d2(bmin, bmax, cell) > T.lr2[e]) {
@@ -398,11 +398,11 @@ __device__ __forceinline__ void child_range(const TreeDev& T, int32_t code, cons
 	}
 	const uint32_t e = leaf_payload(code);
 	if (P.leaf_size == 1) {
-		if (e < P.n) {
+		if (e < P.n_tree) {
 			a = e;
 			b = e + 1;
 		} else {
-			const uint2 r = T.ovf[e - P.n];
+			const uint2 r = T.ovf[e - P.n_tree];
 			a = r.x;
 			b = r.x + r.y;
 		}
@@ -473,6 +473,11 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 		}
 		emit_groups(ctr, groups, run_start, run, gmax);
 	}
+	// slots after the tree's (a spheroidal grain) are a group of their own
+	if (blockIdx.x == 0 && threadIdx.x == 0 && P.n_tree < P.n) {
+		const uint32_t a = dpre_at(dpre, P.n_tree), b = dpre_at(dpre, P.n);
+		if (b > a) emit_groups(ctr, groups, a, b - a, gmax);
+	}
 }
 
 template <int TPL>
@@ -539,9 +544,17 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict
 			const double dt = P.dt * (double)P.tss[sp];
 			n_inter += ne;
 			n_push++;
-			const double E[3] = { (double)ef.x[k] * escale, (double)ef.y[k] * escale, (double)ef.z[k] * escale };
+			double E[3] = { (double)ef.x[k] * escale, (double)ef.y[k] * escale, (double)ef.z[k] * escale };
+			if (P.shape && sp != SP_DUST) {
+				// the spheroid's own field in FP64 (pot-spheroid.c:1815-1819)
+				double Eg[3];
+				spheroid_field(P, qg, dsub(h[k].x, gx), dsub(h[k].y, gy), dsub(h[k].z, gz), Eg);
+				E[0] += Eg[0];
+				E[1] += Eg[1];
+				E[2] += Eg[2];
+			}
 			const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
-			const double qom = (QE * charge) / mass_of(sp);
+			const double qom = (QE * charge) / mass_of(sp, P);
 			double3 xn;
 			boris(v, h[k], E, qom, dt, P, xn);
 			uint32_t reason = 0;
@@ -601,9 +614,14 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_field_query_fast(TreeDev T, c
 		for (int k = 0; k < TPL; k++) {
 			if (!tg.valid[k]) continue;
 			const uint32_t j = q[k];
-			E[3 * j] = (double)ef.x[k] * escale;
-			E[3 * j + 1] = (double)ef.y[k] * escale;
-			E[3 * j + 2] = (double)ef.z[k] * escale;
+			double Eg[3] = { 0.0, 0.0, 0.0 };
+			if (P.shape && self_slot[j] != rec->grain_slot) {
+				spheroid_field(P, (double)rec->grain_q, dsub(xyz[3 * j], rec->grain_pos[0]),
+				               dsub(xyz[3 * j + 1], rec->grain_pos[1]), dsub(xyz[3 * j + 2], rec->grain_pos[2]), Eg);
+			}
+			E[3 * j] = (double)ef.x[k] * escale + Eg[0];
+			E[3 * j + 1] = (double)ef.y[k] * escale + Eg[1];
+			E[3 * j + 2] = (double)ef.z[k] * escale + Eg[2];
 		}
 	}
 }
@@ -634,6 +652,7 @@ void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const 
 template <int TPL>
 __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __restrict__ pos, TreeDev T,
                                                            const float4* __restrict__ src32,
+                                                           const double4* __restrict__ src64,
                                                            const uint2* __restrict__ groups,
                                                            double* __restrict__ partial, Params P, RunRec* rec)
 {
@@ -672,10 +691,15 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 		for (int k = 0; k < TPL; k++) {
 			if (!tg.valid[k]) continue;
 			const uint32_t slot = tg.self[k];
-			const double phi = (double)f.x[k] * pscale;
+			double phi = (double)f.x[k] * pscale;
 			if (slot == gs) {
 				rec->phi_grain = phi;
 			} else {
+				if (P.shape) {  // the spheroid's own potential, FP64 (pot-spheroid.c:2107-2109)
+					const double4 p = src64[slot];
+					phi += spheroid_phi(P, (double)rec->grain_q, dsub(p.x, rec->grain_pos[0]),
+					                    dsub(p.y, rec->grain_pos[1]), dsub(p.z, rec->grain_pos[2]));
+				}
 				acc[(int)pos[slot].w] += (QE * (double)qme[k]) * phi;
 			}
 		}
@@ -687,8 +711,8 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 	}
 }
 
-void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, uint2* groups_all, double* partial,
-                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, const double4* src64,
+                     uint2* groups_all, double* partial, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
 {
 	cudaMemsetAsync(&rec->n_groups_all, 0, sizeof(unsigned int), s);
 	cudaMemsetAsync(&rec->work_ctr2, 0, sizeof(unsigned int), s);
@@ -697,9 +721,11 @@ void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, 
 	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, nullptr, groups_all, &rec->n_groups_all, two ? 64u : 32u, P,
 	                                              rec);
 	if (two) {
-		k_epe_fast<2><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, groups_all, partial, P, rec);
+		k_epe_fast<2><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, src64, groups_all, partial, P,
+		                                                            rec);
 	} else {
-		k_epe_fast<1><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, groups_all, partial, P, rec);
+		k_epe_fast<1><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, src64, groups_all, partial, P,
+		                                                            rec);
 	}
 }
 

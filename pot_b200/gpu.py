@@ -53,7 +53,7 @@ class _RunCfg(C.Structure):
     _fields_ = [("N", C.c_uint64), ("r", C.c_uint32), ("flags", C.c_uint32), ("dt", C.c_double),
                 ("mpp", C.c_double), ("soft", C.c_double), ("Te", C.c_double), ("Ti", C.c_double),
                 ("x_drift", C.c_double), ("a", C.c_double), ("settle", C.c_double), ("theta", C.c_double),
-                ("B", C.c_double * 3), ("A", C.c_double)]
+                ("B", C.c_double * 3), ("A", C.c_double), ("axis", C.c_double * 3)]
 
 
 class _Opts(C.Structure):
@@ -151,6 +151,7 @@ class RunConfig:
     A: float = 0.0
     sceptic: bool = True
     disable_grain: bool = False
+    axis: Sequence[float] = field(default_factory=lambda: (0.0, 0.0, 0.0))
 
     def to_c(self) -> _RunCfg:
         c = _RunCfg()
@@ -160,6 +161,7 @@ class RunConfig:
         c.x_drift, c.a, c.settle, c.theta, c.A = self.x_drift, self.a, self.settle, self.theta, self.A
         for k in range(3):
             c.B[k] = float(self.B[k])
+            c.axis[k] = float(self.axis[k])
         return c
 
 

@@ -24,7 +24,7 @@ def test_particle_record_is_the_reference_layout():
 
 
 def test_struct_sizes():
-    assert C.sizeof(gpu._RunCfg) == 8 + 4 + 4 + 8 * 9 + 24 + 8
+    assert C.sizeof(gpu._RunCfg) == 8 + 4 + 4 + 8 * 9 + 24 + 8 + 24
     assert C.sizeof(gpu._Opts) == 40
     assert C.sizeof(gpu._Grain) == 88
     assert C.sizeof(gpu._Stats) == 88 + 24
@@ -43,8 +43,9 @@ def test_create_rejects_bad_arguments_before_touching_a_device():
     cfg = gpu.RunConfig(N=1, r=1000, dt=1e-15, mpp=1e-9, soft=1e-9, Te=1e4, Ti=1e4).to_c()
     opts = gpu._Opts()
     assert L.pot_gpu_create(C.byref(cfg), C.byref(opts), C.byref(h)) == -1  # N < 2
-    cfg = gpu.RunConfig(N=100, r=1000, dt=1e-15, mpp=1e-9, soft=1e-9, Te=1e4, Ti=1e4, A=3.0).to_c()
-    assert L.pot_gpu_create(C.byref(cfg), C.byref(opts), C.byref(h)) == -1  # spheroid not in this build
+    for A in (1.0, -2.0, float("nan")):  # neither sphere (0), prolate (> 1) nor oblate (0, 1)
+        cfg = gpu.RunConfig(N=100, r=1000, dt=1e-15, mpp=1e-9, soft=1e-9, Te=1e4, Ti=1e4, A=A).to_c()
+        assert L.pot_gpu_create(C.byref(cfg), C.byref(opts), C.byref(h)) == -1
     opts.form = 0
     opts.leaf_size = 8  # plain form is leaf size 1
     cfg = gpu.RunConfig(N=100, r=1000, dt=1e-15, mpp=1e-9, soft=1e-9, Te=1e4, Ti=1e4).to_c()
