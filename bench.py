@@ -44,9 +44,17 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200 vs plain GPU & CPU; batch p99 latency @1% charge err"
 UNIT = "particle-steps/s"
-WORKLOAD = ("1m plasma: 1,000,001 particles (grain + 500,000 ions + 500,000 electrons), Te/Ti = 10, "
-            "Mach-1 ion drift along x, R = 10 lambda_De, a = 0.2 lambda_De, theta = 0.5, "
-            "SCEPTIC reinjection, dt = 0.005/omega_pe")
+WORKLOADS = {
+    "1m": ("1m plasma: 1,000,001 particles (grain + 500,000 ions + 500,000 electrons), Te/Ti = 10, "
+           "Mach-1 ion drift along x, R = 10 lambda_De, a = 0.2 lambda_De, theta = 0.5, "
+           "SCEPTIC reinjection, dt = 0.005/omega_pe"),
+    "4m": ("4m spheroid plasma (pot-spheroid.c): 4,000,001 particles, prolate grain 0.3/0.1/0.1 lambda_De "
+           "tilted 30 deg to the flow, Te/Ti = 10, Mach-0.5 drift, B = 0.9533 T (electron gyroradius "
+           "0.5 lambda_De), R = 12 lambda_De, theta = 0.4, SCEPTIC reinjection"),
+    "small": ("small plasma: 8,193 particles, Te = Ti, no flow, R = 5 lambda_De, a = 0.1 lambda_De, "
+              "theta = 0.5"),
+}
+WORKLOAD = WORKLOADS["1m"]
 
 
 def peaks():
@@ -93,7 +101,7 @@ class Clocks:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -134,13 +142,11 @@ def cpu_baseline_reference(cfg_name: str):
     """One step of the reference program (compiled from its own sources,
     one MPI rank on one core) on the same configuration."""
     from oracle.oracle import RefLib, RunParams
-    from pot_b200.configs import CONFIGS
-    c = dict(CONFIGS[cfg_name])
-    steps, leaf = c.pop("steps"), c.pop("leaf_size")
-    p = RunParams(**c)
+    from pot_b200.configs import run_params, variant
+    p = RunParams(**run_params(cfg_name, untilted=True))
     kind = "reference"
     try:
-        ref = RefLib("sceptic", build=False)
+        ref = RefLib(variant(cfg_name), build=False)
     except Exception:
         ref = None
     if ref is not None:
@@ -157,7 +163,7 @@ def cpu_baseline_reference(cfg_name: str):
                           "init_particles (%.1f s); step took %.1f s" % (p.N, n_plasma // 2, cfg_name, t_init,
                                                                          t_step)}
     from oracle.oracle import Oracle
-    o = Oracle(p, mode="reference", seed=1)
+    o = Oracle(p, mode="reference", seed=1, sceptic=variant(cfg_name).endswith("sceptic"))
     t0 = time.perf_counter()
     o.step()
     t_step = time.perf_counter() - t0
@@ -168,12 +174,9 @@ def cpu_baseline_reference(cfg_name: str):
 def _ref_rank_worker(args):
     cfg_name, nprocs, rank, n_steps, q = args
     from oracle.oracle import RefLib, RunParams
-    from pot_b200.configs import CONFIGS
-    c = dict(CONFIGS[cfg_name])
-    c.pop("steps")
-    c.pop("leaf_size")
-    p = RunParams(**c)
-    ref = RefLib("sceptic", build=False)
+    from pot_b200.configs import run_params, variant
+    p = RunParams(**run_params(cfg_name, untilted=True))
+    ref = RefLib(variant(cfg_name), build=False)
     ref.setup(p, seed=1, nprocs=nprocs, rank=rank)
     times = []
     for _ in range(n_steps):
@@ -217,7 +220,9 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/x87",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "N": N},
+            "data": "synthetic", "config": {"workload": WORKLOADS.get(args.config, args.config), "N": N,
+                                            "reference_axis": "x (the reference cannot tilt its grain)"
+                                            if "axis" in CONFIGS[args.config] else None},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": "reference",
                              "sample": "%d processes, each one MPI rank of a %d-rank run of the reference pot.c "
                                        "(gcc -O2, single-rank MPI stand-in): full tree build plus its own block "
@@ -226,6 +231,63 @@ def run_reference_arm(args):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def walk_compute(interactions, kernel, launch_s, clk):
+    """FP32 rate of the fast walk, the kernel's real bound (it is issue- and
+    FP32-pipe-limited, not HBM-bound): 17 FP32 flops and one rsqrt per
+    target-source interaction, against 148 SMs x 128 FP32 lanes x 2 flops x
+    the median SM clock sampled during the timed region (nominal peak; no
+    measured FP32 figure exists)."""
+    if not interactions or not kernel.startswith("walk_push") or not launch_s:
+        return None
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    achieved = interactions * 17.0 / launch_s / 1e12
+    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_kind": "nominal at the sampled SM clock", "flop_per_interaction": 17,
+            "interactions_per_launch": interactions}
+
+
+def time_config(name, stream, dev, flush, steps=10, warmup=3, plain_steps=3):
+    """Device-timed steps of another configuration, fast form and plain
+    FP64 form, with the same event / L2-flush discipline as the main line."""
+    import torch
+
+    from pot_b200.configs import CONFIGS, run_config
+    from pot_b200.gpu import Run
+
+    cfgd = CONFIGS[name]
+    cfg = run_config(name)
+    out = {"workload": WORKLOADS.get(name, name), "N": cfg.N, "steps": steps}
+
+    def timed(run, k):
+        run.init_particles()
+        for _ in range(warmup):
+            run.step_async(1)
+        run.sync()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        torch.cuda.synchronize(dev)
+        for a, b in ev:
+            a.record(stream)
+            run.step_async(1)
+            b.record(stream)
+            flush.zero_()
+        torch.cuda.synchronize(dev)
+        st = run.step(0)
+        return sum(a.elapsed_time(b) for a, b in ev) / k, st
+
+    with Run(cfg, form="fast", leaf_size=cfgd["leaf_size"], seed=cfgd.get("seed", 1), stream=stream.cuda_stream,
+             device=dev.index) as run:
+        ms, st = timed(run, steps)
+    out["fast"] = {"value": (cfg.N - 1) / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+                   "form": "fast FP32 walk / FP64 state, leaf %d" % cfgd["leaf_size"], "status": st["status"]}
+    with Run(cfg, form="plain", seed=cfgd.get("seed", 1), stream=stream.cuda_stream, device=dev.index) as run:
+        msp, stp = timed(run, plain_steps)
+    out["plain_fp64"] = {"value": (cfg.N - 1) / (msp / 1e3), "unit": UNIT, "ms_per_step": msp,
+                         "steps": plain_steps, "form": "plain FP64, leaf 1", "status": stp["status"]}
+    out["fast_over_plain"] = msp / ms
+    return out
 
 
 def run_ours(args):
@@ -254,7 +316,8 @@ def run_ours(args):
     hbm_peak, peak_kind = peaks()
 
     group = args.group or cfgd.get("group_size", 32)
-    run = Run(cfg, form=args.form, leaf_size=args.leaf or cfgd["leaf_size"], group_size=group, seed=1 + rank,
+    seed0 = cfgd.get("seed", 1)
+    run = Run(cfg, form=args.form, leaf_size=args.leaf or cfgd["leaf_size"], group_size=group, seed=seed0 + rank,
               device=local, stream=stream.cuda_stream, timing=True)
     run.init_particles()
     # warm-up
@@ -315,7 +378,7 @@ def run_ours(args):
     # plain FP64 form on the same workload (fewer steps: it is the slow form)
     plain = None
     if args.plain_steps > 0:
-        runp = Run(cfg, form="plain", seed=1 + rank, device=local, stream=stream.cuda_stream, timing=False)
+        runp = Run(cfg, form="plain", seed=seed0 + rank, device=local, stream=stream.cuda_stream, timing=False)
         runp.init_particles()
         runp.step_async(1)
         runp.sync()
@@ -358,10 +421,16 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference(args.config)
 
+    extra = {}
+    if ws == 1 and args.extra_config not in ("none", "", args.config):
+        extra[args.extra_config] = time_config(args.extra_config, stream, dev, flush, steps=min(args.steps, 10),
+                                               warmup=3, plain_steps=min(args.plain_steps, 3) or 2)
+
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 force / f64 state", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "N": N, "form": args.form, "leaf_size": args.leaf or cfgd["leaf_size"],
+            "config": {"workload": WORKLOADS.get(args.config, args.config), "N": N, "form": args.form,
+                       "leaf_size": args.leaf or cfgd["leaf_size"],
                        "group_size": group,
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
                        "parallelism": "replicas" if ws > 1 else "1 GPU"},
@@ -371,9 +440,10 @@ def run_ours(args):
                          "ms_per_launch": per_launch_s * 1e3,
                          "share_of_step": dom_ms / t_ms if t_ms else None},
             "interactions_per_s": (inter * ws / (t_ms / args.steps / 1e3)) if inter else None,
+            "walk_compute": walk_compute(inter, dom_name, per_launch_s, clk),
             "kernels_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
             "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
-            "walk_stack_max": st.get("stack_max"), "status": st["status"]}
+            "walk_stack_max": st.get("stack_max"), "extra_configs": extra or None, "status": st["status"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     run.close()
@@ -386,7 +456,7 @@ def run_ours(args):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", default="1m")
@@ -398,6 +468,9 @@ def main(argv=None):
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--extra-config", default="4m",
+                    help="also time this configuration (fast and plain FP64 form, N=1 only) into the line's "
+                         "extra_configs; 'none' to skip")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

@@ -12,6 +12,18 @@ domain radius R = r * mpp.
   0.2 lambda, domain 10 lambda, Te/Ti = 10, ions drifting at Mach 1 (the ion
   sound speed sqrt(k Te / m_i)) along the reference's flow axis x,
   dt = 0.005 / omega_pe, 10,000 steps, theta 0.5, leaf size 16.
+* ``4m``     the spheroidal-grain program (pot-spheroid.c, PROLATE):
+  4,000,001 particles, a prolate spheroid of semi-axes 0.3 / 0.1 / 0.1
+  lambda (-a 7.21387e-07 -A 3: a is the volume-equivalent radius, the
+  semi-axes a A^(2/3) and a A^(-1/3)) tilted 30 degrees from the flow axis x
+  towards y, Te/Ti = 10, Mach 0.5 drift, B = 0.9533 T along z (electron
+  gyroradius sqrt(k Te / m_e) / omega_ce = 0.5 lambda), domain 12 lambda,
+  theta 0.4, 20,000 steps, seed 3.  The reference cannot tilt its grain;
+  its runs of this plasma use the untilted spheroid (axis x).
+
+Keys beyond the run's flags: ``steps`` (run length), ``leaf_size`` (fast
+form), ``seed`` and ``variant`` (the reference program that realises it:
+pot.c with SCEPTIC reinjection, or pot-spheroid.c's prolate program).
 """
 from __future__ import annotations
 
@@ -22,16 +34,32 @@ CONFIGS = {
                   Te=11600.0, Ti=11600.0, x_drift=0.0, settle=0.0, theta=0.5, steps=2000, leaf_size=8),
     "1m": dict(N=1000001, r=1000, mpp=2.16079e-08, a=4.32157e-07, soft=2.16079e-08, dt=2.57665e-14,
                Te=11600.0, Ti=1160.0, x_drift=9785.26, settle=0.0, theta=0.5, steps=10000, leaf_size=16),
+    "4m": dict(N=4000001, r=1000, mpp=6.00218e-08, a=7.21387e-07, A=3.0, soft=5.00182e-08, dt=5.96447e-14,
+               Te=11600.0, Ti=1160.0, x_drift=4892.63, settle=0.0, theta=0.4, B=(0.0, 0.0, 0.9533),
+               axis=(0.8660254037844387, 0.5, 0.0), steps=20000, leaf_size=16, seed=3,
+               variant="prolate_sceptic"),
 }
+
+EXTRA_KEYS = ("steps", "leaf_size", "group_size", "seed", "variant")
+
+
+def run_params(name: str, N: int | None = None, untilted: bool = False) -> dict:
+    """The run's flags only (RunParams / RunConfig keywords); ``untilted``
+    puts a spheroid's axis back on x, as the reference has it."""
+    c = {k: v for k, v in CONFIGS[name].items() if k not in EXTRA_KEYS}
+    if N is not None:
+        c["N"] = int(N)
+    if untilted and "axis" in c:
+        c["axis"] = (1.0, 0.0, 0.0)
+    return c
+
+
+def variant(name: str) -> str:
+    return CONFIGS[name].get("variant", "sceptic")
 
 
 def run_config(name: str, N: int | None = None, **over) -> RunConfig:
-    c = dict(CONFIGS[name])
-    c.pop("steps")
-    c.pop("leaf_size")
-    c.pop("group_size", None)
-    if N is not None:
-        c["N"] = int(N)
+    c = run_params(name, N)
     c.update(over)
     return RunConfig(**c)
 
@@ -39,6 +67,9 @@ def run_config(name: str, N: int | None = None, **over) -> RunConfig:
 def flags(name: str) -> str:
     """The reference command line for a configuration."""
     c = CONFIGS[name]
-    return ("-N %d -r %d -m %g -a %g -s %g -d %g -E %g -I %g -x %g -e %g -i %d"
-            % (c["N"], c["r"], c["mpp"], c["a"], c["soft"], c["dt"], c["Te"], c["Ti"], c["x_drift"],
-               c["settle"], c["steps"]))
+    s = ("-N %d -r %d -m %g -a %g -s %g -d %g -E %g -I %g -x %g -e %g -i %d"
+         % (c["N"], c["r"], c["mpp"], c["a"], c["soft"], c["dt"], c["Te"], c["Ti"], c["x_drift"],
+            c["settle"], c["steps"]))
+    if c.get("A"):
+        s += " -A %g" % c["A"]
+    return s

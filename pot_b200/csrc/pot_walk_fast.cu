@@ -481,7 +481,7 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 }
 
 template <int TPL>
-__global__ void __launch_bounds__(FW_WARPS * 32) k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel,
+__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel,
                                                             TreeDev T, const float4* __restrict__ src32,
                                                             const uint32_t* __restrict__ due_list,
                                                             const uint2* __restrict__ groups,
