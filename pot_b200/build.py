@@ -77,6 +77,28 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     return LIB
 
 
+HOST_SRC = os.path.join(PKG, "host", "potgpu.c")
+HOST_BIN = os.path.join(PKG, "potgpu")
+
+
+def build_host(force: bool = False) -> str:
+    """The C host program (pot's command line and output files) linked to
+    libpotgpu.so with an $ORIGIN run path."""
+    lib = build()
+    if not force and os.path.exists(HOST_BIN) and \
+            os.path.getmtime(HOST_BIN) >= max(os.path.getmtime(HOST_SRC), os.path.getmtime(lib)):
+        return HOST_BIN
+    cc = shutil.which("gcc") or "gcc"
+    tmp = HOST_BIN + ".tmp%d" % os.getpid()
+    cmd = [cc, "-O2", "-std=c99", "-Wall", "-Wextra", "-Wno-unused-parameter", "-I", INCLUDE, HOST_SRC, "-o", tmp,
+           "-L", PKG, "-lpotgpu", "-Wl,-rpath,$ORIGIN", "-lm"]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError("gcc failed for %s:\n%s%s" % (HOST_SRC, p.stdout, p.stderr))
+    os.replace(tmp, HOST_BIN)
+    return HOST_BIN
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description="build libpotgpu.so for sm_100a")
     ap.add_argument("--force", action="store_true")
@@ -84,6 +106,7 @@ def main(argv=None):
     ap.add_argument("--ptxas-info", action="store_true", help="print registers/spills per kernel")
     a = ap.parse_args(argv)
     print(build(force=a.force, verbose=a.verbose, ptxas_info=a.ptxas_info))
+    print(build_host(force=a.force))
     return 0
 
 

@@ -1,0 +1,955 @@
+/*
+ * potgpu -- pot's command line and output files, stepping on one B200.
+ *
+ * The host program of the reference (pot.c main() and run(), pot.c:4998-5311
+ * and 4066-4555; pot-spheroid.c the same) with its MPI ranks replaced by one
+ * GPU through the C ABI of include/pot_gpu.h.  Kept from the reference:
+ *   - the flags of set_run_params_from_args (pot.c:4557-4850): -a -d -E -e -f
+ *     -g -I -i -l -m -N -R -r -s -t -w -x, and -A of pot-spheroid.c, with the
+ *     same defaults (pot.c:199-217, pot-spheroid.c:205-228) and messages;
+ *   - the output files under ./output/: pot-run-init-info.txt and
+ *     pot-run-descrip.txt at start (pot.c:3512-3812), pot-macroscopic.dat on
+ *     the reference's record steps (pot.c:4364-4373, 3261-3508),
+ *     pot-phi.dat every 20,000 steps (pot.c:3001-3042, 4397-4403), and the
+ *     format C state file of -f every 50,000 steps and at the end
+ *     (pot.c:3816-3900), read back by -g / -R (pot.c:3903-4019, 4948-4961);
+ *   - the stopping rules: -i steps, -w minutes of wall time.
+ * The reference selects its physics with compile-time switches; here they
+ * are options (defaults = the configuration its benchmarks use):
+ *   --oap X (OAP, pot.c:97), --bx/--by/--bz T (EXTERNAL_B_*, pot.c:55-57),
+ *   --no-sceptic (SCEPTIC_REINJECTION, pot.c:181), --disable-grain
+ *   (DISABLE_GRAIN, pot.c:30), --prolate / --oblate (pot-spheroid.c's
+ *   PROLATE / OBLATE programs, with that program's defaults), and for the
+ *   GPU: --form fast|plain, --leaf N, --group 32|64, --seed S, --axis x,y,z
+ *   (spheroid axis; x in the reference), --output-dir DIR.
+ * Random numbers: the device draws from Philox4x32-10 streams keyed by a
+ * 64-bit seed (--seed, else 8 bytes of /dev/urandom), not from the
+ * reference's WELL512 state.  State files carry the seed in the WELL512
+ * slot (see prng_block_from_seed); a reference-written state seeds Philox
+ * from a hash of its WELL512 words.
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <errno.h>
+#include <inttypes.h>
+#include <math.h>
+#include <stdbool.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <time.h>
+
+#include "pot_gpu.h"
+
+/* Physical constants of pot.c:278-282 and PI of prng.h. */
+#define KB (1.38065e-23)
+#define EPSILON0 (8.85419e-12)
+#define QE (1.6021766e-19)
+#define ME (9.109383e-31)
+#define PI 3.14159265358979
+#define MAX_PATH_LEN 400
+#define CELLS_R 50
+#define CELLS_AZI 4
+#define CELLS_ZEN 10
+
+enum { DUST = 0, ION = 1, ELECTRON = 2 };
+static const int CHARGE[3] = { 0, 1, -1 };
+
+typedef struct {
+	unsigned long N;
+	unsigned int r;
+	long double dt;
+	double mpp;
+	unsigned long run_for;
+	double soft, Te, Ti, x_drift, a, settle;
+	double tim_lim;
+	unsigned short track;
+	char* sw_path;
+	const char* sr_path;
+	bool read_out;
+	/* compile-time switches of the reference, as options */
+	double oap;
+	double B[3];
+	bool sceptic, disable_grain;
+	int shape; /* 0 sphere, 1 prolate, 2 oblate */
+	double A;
+	double axis[3];
+	/* GPU execution */
+	unsigned int form, leaf, group;
+	uint64_t seed;
+	bool have_seed;
+	char out_dir[4096];
+} Run;
+
+typedef struct {
+	unsigned long N, r, run_for;
+	double dt, mpp, soft, Te, Ti, x_drift, a, settle, tim_lim, A;
+} Defaults;
+
+/* pot.c:199-217 */
+static const Defaults SPHERE_DEFAULTS = { 150001, 1000, 0, 1e-12, 4e-7, 2e-8, 220, 220, 0.0, 2.5e-6, 5e-7, 0.0, 0.0 };
+/* pot-spheroid.c:203-228 */
+static const Defaults PROLATE_DEFAULTS = { 150001, 654, 0, 1e-12, 4e-7, 4e-10, 11600, 11600, 0.0, 2.5e-6, 0.0, 0.0, 5.0 };
+static const Defaults OBLATE_DEFAULTS = { 150001, 654, 0, 1e-12, 4e-7, 4e-10, 11600, 11600, 0.0, 2.5e-6, 0.0, 0.0, 0.5 };
+
+static double mime_of(const Run* ru) { return ru->shape ? 1836.153 : 1836.15; }
+static long double mass_of(const Run* ru, int sp)
+{
+	if (sp == DUST) return 1.67e-12;
+	if (sp == ION) return (long double)(mime_of(ru) * ME);
+	return ME;
+}
+
+static void e_puts(const char* s) { fprintf(stderr, "%s\n", s); }
+
+static const Defaults* defaults_of(const Run* ru)
+{
+	return ru->shape == 1 ? &PROLATE_DEFAULTS : (ru->shape == 2 ? &OBLATE_DEFAULTS : &SPHERE_DEFAULTS);
+}
+
+static void set_defaults(Run* ru)
+{
+	const Defaults* d = defaults_of(ru);
+	ru->N = d->N;
+	ru->r = (unsigned int)d->r;
+	ru->dt = d->dt;
+	ru->mpp = d->mpp;
+	ru->run_for = d->run_for;
+	ru->soft = d->soft;
+	ru->Te = d->Te;
+	ru->Ti = d->Ti;
+	ru->x_drift = d->x_drift;
+	ru->a = d->a;
+	ru->settle = d->settle;
+	ru->tim_lim = d->tim_lim;
+	ru->A = d->A;
+	ru->track = 0;
+}
+
+static void usage(const char* prog)
+{
+	fprintf(stderr, "Usage: %s [OPTIONS]\n", prog);
+	e_puts("  -a [SIZE]     grain radius in metres");
+	e_puts("  -A [NUMBER]   aspect ratio of a spheroidal grain (with --prolate / --oblate)");
+	e_puts("  -d [NUMBER]   time step in seconds");
+	e_puts("  -E [NUMBER]   initial electron temperature in Kelvin");
+	e_puts("  -e [NUMBER]   initial settling/equilibration time");
+	e_puts("  -f [PATH]     write final simulation state to [PATH]");
+	e_puts("  -g [PATH]     read initial simulation state from [PATH]");
+	e_puts("  -I [NUMBER]   initial ion temperature in Kelvin");
+	e_puts("  -i [INTEGER]  number of time steps to run for");
+	e_puts("  -l            show runtime settings as command-line arguments");
+	e_puts("  -m [SIZE]     pixel length in metres");
+	e_puts("  -N [INTEGER]  number of particles to simulate");
+	e_puts("  -R [PATH]     read out the simulation state at [PATH]");
+	e_puts("  -r [INTEGER]  simulation radius in pixels");
+	e_puts("  -s [NUMBER]   softening parameter in metres");
+	e_puts("  -t [NUMBER]   number of particle trajectories to display (no display here)");
+	e_puts("  -w [NUMBER]   limit on wall-time spent running in minutes");
+	e_puts("  -x [NUMBER]   drift velocity in x-direction");
+	e_puts("The reference's compile-time switches:");
+	e_puts("  --oap X  --bx T --by T --bz T  --no-sceptic  --disable-grain  --prolate  --oblate");
+	e_puts("GPU execution:");
+	e_puts("  --form fast|plain  --leaf N  --group 32|64  --seed S  --axis X,Y,Z  --output-dir DIR");
+}
+
+static int want(int* n, int argc) { return ++(*n) < argc; }
+
+/* 0 OK, 1 usage, 2 message shown, 3 list settings (pot.c:4557-4850) */
+static int parse_args(int argc, char** argv, Run* ru)
+{
+	bool just_output_args = false;
+	/* the program variant first: it sets the defaults */
+	for (int n = 1; n < argc; n++) {
+		if (!strcmp(argv[n], "--prolate")) ru->shape = 1;
+		if (!strcmp(argv[n], "--oblate")) ru->shape = 2;
+	}
+	set_defaults(ru);
+	for (int n = 1; n < argc; n++) {
+		const char* f = argv[n];
+		if (f[0] != '-') return 1;
+		if (f[1] == '-') {
+			if (!strcmp(f, "--prolate") || !strcmp(f, "--oblate")) continue;
+			if (!strcmp(f, "--no-sceptic")) { ru->sceptic = false; continue; }
+			if (!strcmp(f, "--disable-grain")) { ru->disable_grain = true; continue; }
+			if (!want(&n, argc)) return 1;
+			const char* v = argv[n];
+			if (!strcmp(f, "--oap")) ru->oap = strtod(v, NULL);
+			else if (!strcmp(f, "--bx")) ru->B[0] = strtod(v, NULL);
+			else if (!strcmp(f, "--by")) ru->B[1] = strtod(v, NULL);
+			else if (!strcmp(f, "--bz")) ru->B[2] = strtod(v, NULL);
+			else if (!strcmp(f, "--form")) {
+				if (!strcmp(v, "fast")) ru->form = POT_FORM_FAST;
+				else if (!strcmp(v, "plain")) ru->form = POT_FORM_PLAIN;
+				else return 1;
+			} else if (!strcmp(f, "--leaf")) ru->leaf = (unsigned int)strtoul(v, NULL, 10);
+			else if (!strcmp(f, "--group")) ru->group = (unsigned int)strtoul(v, NULL, 10);
+			else if (!strcmp(f, "--seed")) {
+				ru->seed = strtoull(v, NULL, 10);
+				ru->have_seed = true;
+			} else if (!strcmp(f, "--axis")) {
+				if (sscanf(v, "%lf,%lf,%lf", &ru->axis[0], &ru->axis[1], &ru->axis[2]) != 3) return 1;
+			} else if (!strcmp(f, "--output-dir")) {
+				snprintf(ru->out_dir, sizeof(ru->out_dir), "%s/", v);
+			} else return 1;
+			continue;
+		}
+		switch (f[1]) {
+		case 'a':
+			if (!want(&n, argc)) return 1;
+			ru->a = strtod(argv[n], NULL);
+			if (ru->a <= 0.0) { e_puts("Grain radius must be positive."); return 2; }
+			if (ru->a == HUGE_VAL) { e_puts("Given grain radius is too huge!"); return 2; }
+			break;
+		case 'A':
+			if (!want(&n, argc)) return 1;
+			ru->A = strtod(argv[n], NULL);
+			if (ru->shape == 1 && ru->A <= 1.0) { e_puts("Prolate aspect ratio must be greater than 1."); return 2; }
+			if (ru->shape == 2 && ru->A >= 1.0) { e_puts("Oblate aspect ratio must be less than 1."); return 2; }
+			if (ru->shape == 0) { e_puts("Aspect ratio is not a parameter for a sphere."); return 2; }
+			break;
+		case 'd':
+			if (!want(&n, argc)) return 1;
+			ru->dt = strtold(argv[n], NULL);
+			if (ru->dt <= 0.0) { e_puts("Time step must be positive."); return 2; }
+			if (ru->dt == HUGE_VALL) { e_puts("Given time step is too huge!"); return 2; }
+			break;
+		case 'E':
+			if (!want(&n, argc)) return 1;
+			ru->Te = (double)strtold(argv[n], NULL);
+			if (ru->Te < 0.0) { e_puts("Electron temperature must be non-negative."); return 2; }
+			break;
+		case 'e':
+			if (!want(&n, argc)) return 1;
+			ru->settle = (double)strtold(argv[n], NULL);
+			if (ru->settle < 0.0) { e_puts("Settling time must be non-negative."); return 2; }
+			break;
+		case 'f':
+			if (!want(&n, argc)) return 1;
+			free(ru->sw_path);
+			ru->sw_path = strdup(argv[n]);
+			if (!ru->sw_path) { e_puts("Can't allocate memory for -f's argument."); return 2; }
+			break;
+		case 'g':
+			if (!want(&n, argc)) return 1;
+			ru->sr_path = argv[n];
+			break;
+		case 'I':
+			if (!want(&n, argc)) return 1;
+			ru->Ti = (double)strtold(argv[n], NULL);
+			if (ru->Ti < 0.0) { e_puts("Ion temperature must be non-negative."); return 2; }
+			break;
+		case 'i':
+			if (!want(&n, argc)) return 1;
+			if ((ru->run_for = strtoul(argv[n], NULL, 10)) == 0) {
+				e_puts("Number of time steps to run for must be a valid nonzero integer.");
+				return 2;
+			}
+			break;
+		case 'l':
+			just_output_args = true;
+			break;
+		case 'm':
+			if (!want(&n, argc)) return 1;
+			ru->mpp = strtod(argv[n], NULL);
+			if (ru->mpp <= 0.0) { e_puts("Pixel size must be positive."); return 2; }
+			break;
+		case 'N':
+			if (!want(&n, argc)) return 1;
+			if ((ru->N = strtoul(argv[n], NULL, 10)) == 0) {
+				e_puts("Number of particles must be a valid nonzero integer.");
+				return 2;
+			}
+			break;
+		case 'R':
+			if (!want(&n, argc)) return 1;
+			ru->read_out = true;
+			ru->sr_path = argv[n];
+			break;
+		case 'r':
+			if (!want(&n, argc)) return 1;
+			if ((ru->r = (unsigned int)strtoul(argv[n], NULL, 10)) == 0) {
+				e_puts("Simulation radius in pixels must be a valid nonzero integer.");
+				return 2;
+			}
+			break;
+		case 's':
+			if (!want(&n, argc)) return 1;
+			ru->soft = strtod(argv[n], NULL);
+			if (ru->soft < 0.0) { e_puts("Softening parameter must be non-negative."); return 2; }
+			break;
+		case 't':
+			if (!want(&n, argc)) return 1;
+			ru->track = (unsigned short)strtoul(argv[n], NULL, 10);
+			break;
+		case 'w':
+			if (!want(&n, argc)) return 1;
+			ru->tim_lim = strtod(argv[n], NULL);
+			if (ru->tim_lim < 0.0) { e_puts("Wall-time limit must be non-negative."); return 2; }
+			break;
+		case 'x':
+			if (!want(&n, argc)) return 1;
+			ru->x_drift = strtod(argv[n], NULL);
+			break;
+		default:
+			return 1;
+		}
+	}
+	return just_output_args ? 3 : 0;
+}
+
+/* output_args_for_run, pot.c:4879-4917 */
+static void output_args_for_run(const char* prog, const Run* ru)
+{
+	printf("Settings: %s -N %lu -r %u", prog, ru->N, ru->r);
+	printf(" -d %Lg -m %g -s %g -E %g -I %g -x %g -a %g -e %g", ru->dt, ru->mpp, ru->soft, ru->Te, ru->Ti,
+	       ru->x_drift, ru->a, ru->settle);
+	if (ru->shape) printf(" -A %g", ru->A);
+	if (ru->run_for) printf(" -i %lu", ru->run_for);
+	if (ru->tim_lim > 0.0) printf(" -w %g", ru->tim_lim);
+	if (ru->sw_path) printf(" -f %s", ru->sw_path);
+	if (ru->sr_path) printf(ru->read_out ? " -R %s" : " -g %s", ru->sr_path);
+	printf(" --oap %g", ru->oap);
+	if (ru->B[0] != 0.0 || ru->B[1] != 0.0 || ru->B[2] != 0.0) printf(" --bx %g --by %g --bz %g", ru->B[0], ru->B[1], ru->B[2]);
+	if (!ru->sceptic) printf(" --no-sceptic");
+	if (ru->disable_grain) printf(" --disable-grain");
+	if (ru->shape == 1) printf(" --prolate");
+	if (ru->shape == 2) printf(" --oblate");
+	printf(" --form %s", ru->form == POT_FORM_PLAIN ? "plain" : "fast");
+	putchar('\n');
+}
+
+static FILE* open_out(const Run* ru, const char* name, const char* mode)
+{
+	char path[4200];
+	snprintf(path, sizeof(path), "%s%s", ru->out_dir, name);
+	return fopen(path, mode);
+}
+
+/* ---- run descriptions (pot.c:3512-3812) --------------------------------- */
+
+static long double total_number_density(const Run* ru)
+{
+	return (ru->N - 1) / ((4.0 / 3.0) * PI * powl(ru->r * ru->mpp, 3.0));
+}
+
+static double early_oml_charge_time(const Run* ru, double n_total)
+{
+	const double mi = (double)mass_of(ru, ION), me = (double)mass_of(ru, ELECTRON);
+	const double nu = sqrt(mi * ru->Te / (me * ru->Ti));
+	double tim = EPSILON0 * sqrt(2.0 * PI * mi * KB * ru->Te * ru->Te / ru->Ti);
+	tim /= (QE * QE * ru->a * n_total / 2.0);
+	tim *= log((1.0 - nu) / (pow(nu, 1.0 - exp(-1.0)) - nu));
+	return tim;
+}
+
+static void write_run_info(const Run* ru)
+{
+	FILE* fp = open_out(ru, "pot-run-init-info.txt", "ab");
+	char date_time[50];
+	time_t t = time(NULL);
+	struct tm* tm = localtime(&t);
+	if (!fp) {
+		fprintf(stderr, "Can't open %spot-run-init-info.txt to write information about this run.\n", ru->out_dir);
+		return;
+	}
+	if (!tm || !strftime(date_time, sizeof(date_time), "%Y-%m-%d %H:%M:%S", tm)) snprintf(date_time, sizeof(date_time), "?");
+	fprintf(fp, "%s\t%lu\t%Lg\t%g\t%g\t%g\t%g\t%g\t%s\t%s\t%u\t%g\t%u\t%g\n", date_time, ru->N, ru->dt, ru->soft,
+	        ru->mpp, ru->Ti, ru->Te, ru->x_drift, __DATE__, __TIME__, ru->r, ru->a, 1u, ru->oap);
+	fclose(fp);
+}
+
+static void write_run_description(const Run* ru)
+{
+	const Defaults* d = defaults_of(ru);
+	FILE* fp = open_out(ru, "pot-run-descrip.txt", "ab");
+	if (!fp) {
+		fprintf(stderr, "Can't open %spot-run-descrip.txt to write this run's initial description.\n", ru->out_dir);
+		return;
+	}
+	fprintf(fp,
+	        "%c total particle count:          %lu\n"
+	        "%c time step (s):                 %Lg\n"
+	        "%c nominal elec. temperature (K): %g\n"
+	        "%c nominal ion temperature (K):   %g\n"
+	        "%c softening parameter (m):       %g\n"
+	        "%c drift velocity (m*s^-1):       %g\n"
+	        "%c pixel size (m):                %g\n"
+	        "%c simulation radius (px.):       %u\n"
+	        "%c tracked particles:             %hu\n"
+	        "%c number of time steps:          %lu\n"
+	        "%c grain radius (m):              %g\n"
+	        "%c settling time (s):             %g\n",
+	        (ru->N != d->N) ? '*' : ' ', ru->N, (ru->dt != d->dt) ? '*' : ' ', ru->dt,
+	        (ru->Te != d->Te) ? '*' : ' ', ru->Te, (ru->Ti != d->Ti) ? '*' : ' ', ru->Ti,
+	        (ru->soft != d->soft) ? '*' : ' ', ru->soft, (ru->x_drift != d->x_drift) ? '*' : ' ', ru->x_drift,
+	        (ru->mpp != d->mpp) ? '*' : ' ', ru->mpp, (ru->r != d->r) ? '*' : ' ', ru->r, ' ', (unsigned short)0,
+	        (ru->run_for != d->run_for) ? '*' : ' ', ru->run_for, (ru->a != d->a) ? '*' : ' ', ru->a,
+	        (ru->settle != d->settle) ? '*' : ' ', ru->settle);
+	if (ru->shape) fprintf(fp, "%c aspect ratio:                  %g\n", (ru->A != d->A) ? '*' : ' ', ru->A);
+	fputc('\n', fp);
+
+	const long double n = total_number_density(ru);
+	const long double size = 2.0 * ru->r * ru->mpp;
+	const long double mi = mass_of(ru, ION), me = mass_of(ru, ELECTRON);
+	const long double debye_len = sqrtl(EPSILON0 * KB * ru->Te / ((n / 2.0) * QE * QE));
+	const double debye_number = (4.0 / 3.0) * PI * powl(debye_len, 3.0) * n / 2.0;
+	const long double wsr = powl(4.0 * PI * n / 3.0, -1.0 / 3.0);
+	double ccp = QE * CHARGE[ION] * QE * CHARGE[ION];
+	ccp /= (4.0 * PI * EPSILON0 * wsr * KB * ru->Te);
+	const double coulomb_log = log(9.0 * debye_number);
+	const long double e_colll = 16.0 * PI * (n / 2.0) * powl(debye_len, 4.0) / coulomb_log;
+	const long double edct = ru->a / sqrtl(3.0 * KB * ru->Te / me);
+	const long double eop = 2.0 * PI * sqrtl(ME * EPSILON0 / (n * QE * QE / 2.0));
+	const double charge_osc_rat = early_oml_charge_time(ru, (double)n) / eop;
+	long double htcd = QE * QE / (12 * PI * EPSILON0 * KB);
+	htcd /= (ru->Te > ru->Ti) ? ru->Te : ru->Ti;
+	fprintf(fp,
+	        "  particle density (m^-3):    %Lg\n"
+	        "  Debye length (m):           %Lg\n"
+	        "  grain radius/DL:            %Lg\n"
+	        "  elec. oscil. period (s):    %Lg\n"
+	        "  early OML chg. time (s):    %g\n"
+	        "  Wigner-Seitz radius (m):    %Lg\n"
+	        "  normalized drift speed:     %Lg\n"
+	        "  ion traversal time (s):     %Lg\n"
+	        "  Coulomb logarithm:          %g\n"
+	        "  electron coll. len. (m):    %Lg\n"
+	        "%c electron Knudsen number:    %Lg\n"
+	        "%c Debye number:               %g\n"
+	        "%c Coulomb coupling param.:    %g\n"
+	        "%c softening parameter/WSR:    %Lg\n"
+	        "%c t. step/elec. cross time:   %Lg\n"
+	        "%c DL/characteristic size:     %Lg\n"
+	        "%c OML time/elec. osc. period: %g\n"
+	        "%c soft. par./head coll. dist: %Lg\n"
+	        "%c soft. par./grain radius:    %g\n\n",
+	        n, debye_len, ru->a / debye_len, eop, early_oml_charge_time(ru, (double)n), wsr,
+	        ru->x_drift / sqrtl(KB * ru->Ti / mi), size / sqrtl(3.0 * KB * ru->Ti / mi), coulomb_log, e_colll,
+	        ((e_colll / size) > 0.5) ? '!' : ' ', e_colll / size, (debye_number < 2.0) ? '!' : ' ', debye_number,
+	        (ccp > 1.0) ? '!' : ' ', ccp, ((ru->soft / wsr) > 1.0) ? '!' : ' ', ru->soft / wsr,
+	        ((ru->dt / edct) > 0.5) ? '!' : ' ', ru->dt / edct, ((debye_len / size) > 0.1) ? '!' : ' ',
+	        debye_len / size, (charge_osc_rat < 100.0) ? '!' : ' ', charge_osc_rat,
+	        ((ru->soft / htcd) > 0.5) ? '!' : ' ', ru->soft / htcd, ((ru->soft / ru->a) > 0.1) ? '!' : ' ',
+	        ru->soft / ru->a);
+	fprintf(fp,
+	        "opening angle parameter: %g\n"
+	        "ion/electron mass ratio: %Lg\n"
+	        "external B field (T):    (%g, %g, %g)\n"
+	        "spatial bin counts:      (%i, %i, %i)\n"
+	        "max. tree walk length:   %i\n"
+	        "grain mass (kg):         %Lg\n\n",
+	        ru->oap, mi / me, ru->B[0], ru->B[1], ru->B[2], CELLS_R, CELLS_AZI, CELLS_ZEN, MAX_PATH_LEN,
+	        mass_of(ru, DUST));
+	fputs(ru->disable_grain ? "grain:                disabled\n" : "grain:                enabled\n", fp);
+	fputs("OpenGL interface:     no\n", fp);
+	fputs("trajectory length:    N/A\n", fp);
+	fputs(ru->sceptic ? "containment:          reinjection (SCEPTIC-style)\n"
+	                  : "containment:          reinjection (old-style)\n", fp);
+	fputs("FP exceptions:        no\n", fp);
+	fputs("multipole expansion:  monopole\n", fp);
+	fputs("simulation shape:     spherical\n", fp);
+	fputs("numerical integrator: Boris\n", fp);
+	fputs("pos. Pois. collec'n:  no\n", fp);
+	fputs("Langmuir test wave:   no\n", fp);
+	fputs("P-P interactions:     yes\n", fp);
+	fputs(ru->shape == 1 ? "Grain shape:          prolate spheroid\n\n"
+	      : ru->shape == 2 ? "Grain shape:          oblate spheroid\n\n" : "Grain shape:          sphere\n\n", fp);
+	fprintf(fp, "output file dir.:     %s\ncompiled on:          %s %s\n",
+	        ru->out_dir[0] ? ru->out_dir : "./output/", __DATE__, __TIME__);
+	fprintf(fp, "stepped on:           one GPU (%s form)\n",
+	        ru->form == POT_FORM_PLAIN ? "plain FP64" : "fast FP32-walk");
+	fclose(fp);
+}
+
+/* ---- macroscopic summary (pot.c:3249-3508) ------------------------------ */
+
+#define isnt_weird(x) (isnormal(x) || (fpclassify(x) == FP_ZERO))
+#define pythag(x, y, z) sqrt((x) * (x) + (y) * (y) + (z) * (z))
+
+static void central_moments(long double* cms, unsigned int N)
+{
+	cms[1] /= N;
+	cms[2] /= N * powl(cms[1], 1.5);
+	cms[3] /= N * cms[1] * cms[1];
+	cms[3] -= 3.0;
+}
+
+static void write_macro(FILE* fp, const Run* ru, const pot_particle* P, const pot_grain_state* g,
+                        const long double epe[3], unsigned long step)
+{
+	long double K_e[4] = { 0 }, s_e[4] = { 0 }, s_i[4] = { 0 };
+	long double v_e[3] = { 0 }, v_i[3] = { 0 }, am_e[3] = { 0 }, am_i[3] = { 0 }, lm_e[3], lm_i[3];
+	long double sum_K_ions = 0, sum_sq_K_elec = 0, sum_sq_K_ions = 0, sum_x_elec = 0, sum_sq_x_elec = 0;
+	double temp_e = 0, temp_i = 0;
+	unsigned int N_e = 0, N_i = 0;
+	const double cent = ru->r * ru->mpp;
+	const long double volume = (4.0 / 3.0) * PI * powl(ru->r * ru->mpp, 3.0);
+	const long double me = mass_of(ru, ELECTRON), mi = mass_of(ru, ION);
+	if (ru->N < 6 || !fp) return;
+	for (unsigned long k = 1; k < ru->N; k++) {
+		const pot_particle* p = &P[k];
+		const long double v = pythag(p->vx, p->vy, p->vz);
+		long double *vm, *am;
+		if (isnan(v)) {
+			fprintf(stderr, "Particle %lu (%g, %g, %g) has velocity (%g, %g, %g) at time step %lu.\n", k, p->x,
+			        p->y, p->z, p->vx, p->vy, p->vz, step);
+		}
+		if (p->species == ELECTRON) {
+			K_e[0] += 0.5 * me * v * v;
+			s_e[0] += v;
+			vm = v_e;
+			am = am_e;
+			N_e++;
+		} else {
+			s_i[0] += v;
+			vm = v_i;
+			am = am_i;
+			N_i++;
+		}
+		vm[0] += p->vx;
+		vm[1] += p->vy;
+		vm[2] += p->vz;
+		am[0] += ((p->y - cent) * p->vz) - ((p->z - cent) * p->vy);
+		am[1] -= ((p->x - cent) * p->vz) - ((p->z - cent) * p->vx);
+		am[2] += ((p->x - cent) * p->vy) - ((p->y - cent) * p->vx);
+	}
+	K_e[0] /= N_e;
+	s_e[0] /= N_e;
+	s_i[0] /= N_i;
+	for (int k = 0; k < 3; k++) {
+		v_e[k] /= N_e;
+		v_i[k] /= N_i;
+		am_e[k] *= me;
+		am_i[k] *= mi;
+		lm_e[k] = me * v_e[k];
+		lm_i[k] = mi * v_i[k];
+	}
+	for (unsigned long k = 1; k < ru->N; k++) {
+		const pot_particle* p = &P[k];
+		const long double v = pythag(p->vx, p->vy, p->vz);
+		const long double K = 0.5 * mass_of(ru, p->species) * v * v;
+		if (p->species == ELECTRON) {
+			sum_sq_K_elec += K * K;
+			sum_x_elec += p->x;
+			sum_sq_x_elec += p->x * p->x;
+			const long double Ks = K - K_e[0];
+			K_e[1] += Ks * Ks;
+			K_e[2] += Ks * Ks * Ks;
+			K_e[3] += Ks * Ks * Ks * Ks;
+			const long double vs = v - s_e[0];
+			s_e[1] += vs * vs;
+			s_e[2] += vs * vs * vs;
+			s_e[3] += vs * vs * vs * vs;
+			temp_e += (p->vx - v_e[0]) * (p->vx - v_e[0]);
+			temp_e += (p->vy - v_e[1]) * (p->vy - v_e[1]);
+			temp_e += (p->vz - v_e[2]) * (p->vz - v_e[2]);
+		} else {
+			sum_K_ions += K;
+			sum_sq_K_ions += K * K;
+			const long double vs = v - s_i[0];
+			s_i[1] += vs * vs;
+			s_i[2] += vs * vs * vs;
+			s_i[3] += vs * vs * vs * vs;
+			temp_i += (p->vx - v_i[0]) * (p->vx - v_i[0]);
+			temp_i += (p->vy - v_i[1]) * (p->vy - v_i[1]);
+			temp_i += (p->vz - v_i[2]) * (p->vz - v_i[2]);
+		}
+	}
+	central_moments(K_e, N_e);
+	central_moments(s_e, N_e);
+	central_moments(s_i, N_i);
+	temp_e *= (me / (3.0 * KB)) / N_e;
+	temp_i *= (mi / (3.0 * KB)) / N_i;
+	const long double debye = sqrtl(EPSILON0 * KB * temp_e / ((N_e / volume) * QE * QE));
+	fprintf(fp, "%.7Lg %Lg ", step * ru->dt, K_e[0]);
+	if (isnt_weird(epe[ELECTRON])) fprintf(fp, "%Lg ", epe[ELECTRON] / N_e); else fputs("NA ", fp);
+	fprintf(fp, "%Lg ", sum_K_ions / N_i);
+	if (isnt_weird(epe[ION])) fprintf(fp, "%Lg ", epe[ION] / N_i); else fputs("NA ", fp);
+	fprintf(fp, "%Lg ", 0.5 * (long double)g->m * hypot(g->vx, hypot(g->vy, g->vz)));
+	if (isnt_weird(epe[DUST])) fprintf(fp, "%Lg ", epe[DUST]); else fputs("NA ", fp);
+	fprintf(fp,
+	        "%.7Lg %.7Lg %i %Lg %Lg"
+	        " %Lg %Lg %Lg %Lg %Lg %Lg %Lg %Lg %g %g %Lg %Lg %Lg"
+	        " %Lg %Lg %Lg %Lg %Lg %Lg %Lg %Lg %Lg %u\n",
+	        sum_x_elec / N_e, sqrtl(sum_sq_x_elec / N_e - (sum_x_elec / N_e) * sum_x_elec / N_e), (int)g->q, debye,
+	        (4.0 * PI / 3.0) * debye * debye * debye * N_e / volume, s_e[0], s_e[1], s_e[2], s_e[3], s_i[0], s_i[1],
+	        s_i[2], s_i[3], temp_e, temp_i, lm_e[0], lm_e[1], lm_e[2], lm_i[0], lm_i[1], lm_i[2], am_e[0], am_e[1],
+	        am_e[2], am_i[0], am_i[1], am_i[2], (unsigned int)g->tot_absor_e);
+	if (fflush(fp)) e_puts("Can't force write of macroscopic summary data to disk.");
+}
+
+/* ---- pot-phi.dat (pot.c:3001-3042) -------------------------------------- */
+
+static int write_phi(const Run* ru, pot_gpu_ctx* ctx, const pot_grain_state* g, unsigned long step)
+{
+	enum { NP = CELLS_R * CELLS_AZI * (CELLS_ZEN + 1) };
+	static double xyz[3 * NP], phi[NP], rr[NP], az[NP], ze[NP];
+	const double r_step = ru->r * ru->mpp / CELLS_R;
+	int k = 0;
+	for (unsigned int ri = 1; ri <= CELLS_R; ri++) {
+		for (unsigned int ai = 0; ai < CELLS_AZI; ai++) {
+			for (unsigned int zi = 0; zi <= CELLS_ZEN; zi++) {
+				const double r = r_step * ri, azi = 2.0 * PI * ai / CELLS_AZI, zen = PI * zi / CELLS_ZEN;
+				rr[k] = r;
+				az[k] = azi;
+				ze[k] = zen;
+				xyz[3 * k] = g->x + (r * cos(azi) * sin(zen));
+				xyz[3 * k + 1] = g->y + (r * sin(azi) * sin(zen));
+				xyz[3 * k + 2] = g->z + (r * cos(zen));
+				k++;
+			}
+		}
+	}
+	const int rc = pot_gpu_phi_at(ctx, NP, xyz, phi);
+	if (rc != POT_OK) return rc;
+	FILE* fp = open_out(ru, "pot-phi.dat", "ab");
+	if (!fp) {
+		fprintf(stderr, "Can't open %spot-phi.dat to write electric potential data.\n", ru->out_dir);
+		return POT_OK;
+	}
+	for (int j = 0; j < NP; j++) fprintf(fp, "%Lg %g %g %g %g\n", step * ru->dt, rr[j], az[j], ze[j], phi[j]);
+	fclose(fp);
+	return POT_OK;
+}
+
+/* ---- state files (pot.c:3816-4019) -------------------------------------- */
+
+/* WELL512 record of prng.h:17-24 (84 bytes) */
+typedef struct {
+	uint32_t a, b, c, d, index;
+	uint32_t state[16];
+} PrngBlock;
+
+static uint64_t splitmix64(uint64_t* x)
+{
+	uint64_t z = (*x += 0x9E3779B97F4A7C15ull);
+	z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+	z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+	return z ^ (z >> 31);
+}
+
+#define SEED_MARK 0x506F7447u /* "GtoP" */
+
+/* The Philox seed in the WELL512 slot: words 0-1 the seed, word 2 a mark,
+   words 3-15 a splitmix64 stream of the seed (a valid WELL512 state should
+   the reference read it). */
+static void prng_block_from_seed(uint64_t seed, PrngBlock* b)
+{
+	memset(b, 0, sizeof(*b));
+	b->state[0] = (uint32_t)seed;
+	b->state[1] = (uint32_t)(seed >> 32);
+	b->state[2] = SEED_MARK;
+	uint64_t x = seed;
+	for (int k = 3; k < 16; k++) b->state[k] = (uint32_t)splitmix64(&x);
+}
+
+static uint64_t seed_from_prng_block(const PrngBlock* b)
+{
+	PrngBlock mine;
+	const uint64_t s = (uint64_t)b->state[0] | ((uint64_t)b->state[1] << 32);
+	prng_block_from_seed(s, &mine);
+	if (!memcmp(mine.state, b->state, sizeof(mine.state))) return s;
+	uint64_t h = 0x243F6A8885A308D3ull;
+	for (int k = 0; k < 16; k++) {
+		h ^= b->state[k];
+		h = splitmix64(&h);
+	}
+	return h;
+}
+
+static int write_state(const Run* ru, const char* path, const pot_particle* P, const pot_grain_state* g,
+                       const long double epe[3], uint64_t seed)
+{
+	FILE* fp = fopen(path, "wb");
+	PrngBlock b;
+	if (!fp) {
+		fprintf(stderr, "Failed to open simulation state file %s for writing.\n", path);
+		return -1;
+	}
+	fprintf(fp, "C %u %i %Lg %lu %Lg %Lg %Lg %u %g\n", 1u, (int)g->q, (long double)g->m,
+	        (unsigned long)g->t_steps, epe[0], epe[1], epe[2], (unsigned int)g->tot_absor_e,
+	        ru->sceptic ? g->chi_b : 9999.99);
+	prng_block_from_seed(seed, &b);
+	if (fwrite(&b, sizeof(b), 1, fp) != 1) fprintf(stderr, "Failed to write proc. 0's PRNG state to %s.\n", path);
+	if (fwrite(P, sizeof(pot_particle), ru->N, fp) != ru->N) fprintf(stderr, "Failed to write particle states to %s.\n", path);
+	if (fclose(fp)) fprintf(stderr, "Failed to close simulation state output file %s.\n", path);
+	return 0;
+}
+
+/* formats A, B and C; any worker count (one GPU replaces them all; the
+   first rank's PRNG record seeds the run) */
+static int read_state(const Run* ru, const char* path, pot_particle* P, pot_grain_state* g, long double epe[3],
+                      uint64_t* seed)
+{
+	FILE* fp = fopen(path, "rb");
+	unsigned int workers = 0, tae = 0;
+	int q = 0;
+	unsigned long t = 0;
+	long double m = 1.67e-12;
+	double chi_b = 0.0;
+	if (!fp) {
+		fprintf(stderr, "0: failed to open simulation state file %s to read.\n", path);
+		return -1;
+	}
+	const int c = getc(fp);
+	int ok;
+	if (c == 'C') {
+		ok = fscanf(fp, " %u %i %Lg %lu %Lg %Lg %Lg %u %lg\n", &workers, &q, &m, &t, &epe[0], &epe[1], &epe[2], &tae,
+		            &chi_b) == 9;
+	} else if (c == 'B') {
+		ok = fscanf(fp, " %u %i %lu %Lg %Lg %Lg %u\n", &workers, &q, &t, &epe[0], &epe[1], &epe[2], &tae) == 7;
+	} else if (c >= '0' && c <= '9') {
+		rewind(fp);
+		ok = fscanf(fp, "%u %i %lu %Lg %Lg %Lg\n", &workers, &q, &t, &epe[0], &epe[1], &epe[2]) == 6;
+	} else {
+		fprintf(stderr, "0: alleged state file %s isn't.\n", path);
+		fclose(fp);
+		return -1;
+	}
+	if (!ok || workers == 0) {
+		fprintf(stderr, "0: failed to read the assorted data values from %s.\n", path);
+		fclose(fp);
+		return -1;
+	}
+	for (unsigned int w = 0; w < workers; w++) {
+		PrngBlock b;
+		if (fread(&b, sizeof(b), 1, fp) != 1) {
+			fprintf(stderr, "0: failed to read proc. %u's PRNG state from %s.\n", w, path);
+			fclose(fp);
+			return -1;
+		}
+		if (w == 0) *seed = seed_from_prng_block(&b);
+	}
+	if (fread(P, sizeof(pot_particle), ru->N, fp) != ru->N) {
+		fprintf(stderr, "0: failed to read particle states from %s.\n", path);
+		fclose(fp);
+		return -1;
+	}
+	fclose(fp);
+	memset(g, 0, sizeof(*g));
+	g->q = q;
+	g->m = (double)m;
+	g->x = P[0].x;
+	g->y = P[0].y;
+	g->z = P[0].z;
+	g->vx = P[0].vx;
+	g->vy = P[0].vy;
+	g->vz = P[0].vz;
+	g->tot_absor_e = tae;
+	g->t_steps = t;
+	g->chi_b = chi_b;
+	return 0;
+}
+
+static void read_out_state(const Run* ru, const pot_particle* P)
+{
+	const char letters[] = "die";
+	puts("NO S X Y Z VX VY VZ");
+	for (unsigned long k = 0; k < ru->N; k++) {
+		const pot_particle* p = &P[k];
+		printf("%lu \"%c\" %g %g %g %g %g %g\n", k, letters[p->species], p->x, p->y, p->z, p->vx, p->vy, p->vz);
+	}
+}
+
+/* ---- main (pot.c:4998-5311, run() 4066-4555) ---------------------------- */
+
+static bool record_macro(const Run* ru, unsigned long t)
+{
+	bool rec = t <= 200;
+	if ((t * ru->dt) > (2.0 * ru->settle)) rec |= !(t % 2000);
+	else rec |= !(t % 200);
+	return rec;
+}
+
+static int fail(pot_gpu_ctx* ctx, unsigned long t, int rc)
+{
+	fprintf(stderr, "0:%lu: %s\n", t, pot_gpu_strerror(rc));
+	(void)ctx;
+	return rc;
+}
+
+int main(int argc, char** argv)
+{
+	Run ru;
+	memset(&ru, 0, sizeof(ru));
+	ru.oap = 0.5;
+	ru.sceptic = true;
+	ru.form = POT_FORM_FAST;
+	snprintf(ru.out_dir, sizeof(ru.out_dir), "./output/");
+	if (argc < 2) e_puts("Run without arguments; attempting to use default settings.");
+	switch (parse_args(argc, argv, &ru)) {
+	case 1:
+		usage(argv[0]);
+		free(ru.sw_path);
+		return EXIT_FAILURE;
+	case 2:
+		free(ru.sw_path);
+		return EXIT_FAILURE;
+	case 3:
+		output_args_for_run(argv[0], &ru);
+		free(ru.sw_path);
+		return EXIT_SUCCESS;
+	default:
+		break;
+	}
+	if (ru.a >= (ru.r * ru.mpp)) {
+		fprintf(stderr, "Grain radius (%g m) must be less than simulation region radius (%g m).\n", ru.a,
+		        ru.r * ru.mpp);
+		free(ru.sw_path);
+		return EXIT_FAILURE;
+	}
+	pot_particle* P = malloc(sizeof(pot_particle) * ru.N);
+	if (!P) {
+		fprintf(stderr, "0: can't allocate %.1f MiB for %lu particles' data.\n",
+		        sizeof(pot_particle) * ru.N / 1048576.0, ru.N);
+		free(ru.sw_path);
+		return EXIT_FAILURE;
+	}
+	pot_grain_state g;
+	long double epe[3] = { 0.0L, 0.0L, 0.0L };
+	memset(&g, 0, sizeof(g));
+	uint64_t seed = ru.seed;
+	if (ru.sr_path) {
+		uint64_t file_seed = 0;
+		if (read_state(&ru, ru.sr_path, P, &g, epe, &file_seed)) {
+			free(P);
+			free(ru.sw_path);
+			return EXIT_FAILURE;
+		}
+		if (ru.read_out) {
+			read_out_state(&ru, P);
+			free(P);
+			free(ru.sw_path);
+			return EXIT_SUCCESS;
+		}
+		if (!ru.have_seed) seed = file_seed;
+		if (ru.run_for && g.t_steps >= ru.run_for) {
+			printf("0: simulation's already run for %lu steps, exiting.\n", ru.run_for);
+			free(P);
+			free(ru.sw_path);
+			return EXIT_SUCCESS;
+		}
+	} else if (!ru.have_seed) {
+		FILE* ur = fopen("/dev/urandom", "rb");
+		if (!ur || fread(&seed, sizeof(seed), 1, ur) != 1) {
+			fprintf(stderr, "0: can't read PRNG seed from /dev/urandom, PRNG may behave inadequately.\n");
+			seed = 0;
+		}
+		if (ur) fclose(ur);
+	}
+
+	pot_run_cfg cfg;
+	pot_gpu_opts opt;
+	memset(&cfg, 0, sizeof(cfg));
+	memset(&opt, 0, sizeof(opt));
+	cfg.N = ru.N;
+	cfg.r = ru.r;
+	cfg.flags = (ru.sceptic ? POT_CFG_SCEPTIC : 0u) | (ru.disable_grain ? POT_CFG_DISABLE_GRAIN : 0u);
+	cfg.dt = (double)ru.dt;
+	cfg.mpp = ru.mpp;
+	cfg.soft = ru.soft;
+	cfg.Te = ru.Te;
+	cfg.Ti = ru.Ti;
+	cfg.x_drift = ru.x_drift;
+	cfg.a = ru.a;
+	cfg.settle = ru.settle;
+	cfg.theta = ru.oap;
+	for (int k = 0; k < 3; k++) {
+		cfg.B[k] = ru.B[k];
+		cfg.axis[k] = ru.axis[k];
+	}
+	cfg.A = ru.shape ? ru.A : 0.0;
+	opt.form = ru.form;
+	opt.leaf_size = ru.leaf;
+	opt.group_size = ru.group;
+	opt.seed = seed;
+	pot_gpu_ctx* ctx = NULL;
+	int rc = pot_gpu_create(&cfg, &opt, &ctx);
+	if (rc != POT_OK) {
+		fprintf(stderr, "0: can't set up the GPU run: %s\n", pot_gpu_strerror(rc));
+		free(P);
+		free(ru.sw_path);
+		return EXIT_FAILURE;
+	}
+	rc = ru.sr_path ? pot_gpu_upload(ctx, P, ru.N, &g) : pot_gpu_init_particles(ctx);
+	if (rc != POT_OK) {
+		fail(ctx, 0, rc);
+		pot_gpu_destroy(ctx);
+		free(P);
+		free(ru.sw_path);
+		return EXIT_FAILURE;
+	}
+	FILE* fp_macro = NULL;
+	if (ru.N >= 6) {
+		if (!(fp_macro = open_out(&ru, "pot-macroscopic.dat", "ab"))) {
+			fprintf(stderr, "Can't open %spot-macroscopic.dat to write macroscopic data.\n", ru.out_dir);
+		} else if (!ftell(fp_macro)) {
+			fputs("TIME KE PE KI PI KG PG XE XESD DGQ DL DN "
+			      "SE1 SE2 SE3 SE4 SI1 SI2 SI3 SI4 TE TI LMEX LMEY LMEZ "
+			      "LMIX LMIY LMIZ AMEX AMEY AMEZ AMIX AMIY AMIZ TOTE\n", fp_macro);
+		}
+	}
+	write_run_info(&ru);
+	write_run_description(&ru);
+
+	const time_t start = time(NULL);
+	unsigned long t = g.t_steps;  /* steps completed */
+	bool recorded_last = false;
+	int status = EXIT_SUCCESS;
+	pot_step_stats st;
+	for (;;) {
+		const unsigned long next = t + 1;
+		if (ru.run_for && next > ru.run_for) break;
+		if (ru.tim_lim > 0.0 && (time(NULL) - start) > (60 * ru.tim_lim)) break;
+		/* state file every 50,000 steps, before the step (pot.c:4353-4356) */
+		if (ru.sw_path && !(next % 50000)) {
+			if ((rc = pot_gpu_download(ctx, P, &g)) != POT_OK) { status = fail(ctx, t, rc); break; }
+			write_state(&ru, ru.sw_path, P, &g, epe, seed);
+		}
+		/* steps that record nothing run straight through, up to the next
+		   event (at most 1,000 per call, so the wall-time limit is seen) */
+		if (!record_macro(&ru, next) && (next % 20000)) {
+			unsigned long run_to = next;
+			while (true) {
+				const unsigned long u = run_to + 1;
+				if ((ru.run_for && u > ru.run_for) || record_macro(&ru, u) || !(u % 20000) ||
+				    (ru.sw_path && !(u % 50000)) || u - next >= 1000)
+					break;
+				run_to = u;
+			}
+			if ((rc = pot_gpu_step(ctx, (uint32_t)(run_to - next + 1), 0, &st)) != POT_OK) {
+				status = fail(ctx, t, rc);
+				break;
+			}
+			t = run_to;
+			recorded_last = false;
+			continue;
+		}
+		const bool rec = record_macro(&ru, next);
+		if ((rc = pot_gpu_step(ctx, 1, rec ? POT_STEP_EPE : 0u, &st)) != POT_OK) { status = fail(ctx, next, rc); break; }
+		t = next;
+		if (rec)
+			for (int k = 0; k < 3; k++) epe[k] = st.epe[k];
+		if (!(t % 20000)) {
+			if ((rc = pot_gpu_download(ctx, P, &g)) != POT_OK) { status = fail(ctx, t, rc); break; }
+			if ((rc = write_phi(&ru, ctx, &g, t)) != POT_OK) { status = fail(ctx, t, rc); break; }
+		}
+		if (rec) {
+			if ((rc = pot_gpu_download(ctx, P, &g)) != POT_OK) { status = fail(ctx, t, rc); break; }
+			write_macro(fp_macro, &ru, P, &g, epe, t);
+		}
+		recorded_last = rec;
+		if (ru.tim_lim > 0.0 && (time(NULL) - start) > (60 * ru.tim_lim)) break;
+	}
+	if (status == EXIT_SUCCESS && (pot_gpu_download(ctx, P, &g) == POT_OK)) {
+		if (ru.sw_path) write_state(&ru, ru.sw_path, P, &g, epe, seed);
+		if (!recorded_last) write_macro(fp_macro, &ru, P, &g, epe, t);
+	}
+	if (fp_macro) fclose(fp_macro);
+	pot_gpu_destroy(ctx);
+	free(P);
+	free(ru.sw_path);
+	return status == EXIT_SUCCESS ? EXIT_SUCCESS : EXIT_FAILURE;
+}
