@@ -125,6 +125,16 @@ typedef struct pot_step_stats {
 	                          (POT_WALK_STACK entries at most; 0 in the plain form) */
 	double epe[3];         /* POT_STEP_EPE: electrostatic potential energy (J) of the
 	                          grain, the ions, the electrons (Proc.epe, pot.c:2771-2864) */
+	int64_t q_sum;         /* sum of the grain charge after each step since upload / init
+	                          (moving means of the charge; no counterpart in the reference) */
+	uint32_t warn;         /* non-fatal conditions and causes: bit 0 a leaf-size-1 key
+	                          collision at 21 levels (an overflow bucket); with POT_E_ITER,
+	                          the sampler cap reached: 2 inverse-CDF Newton, 4 the u^2 <
+	                          chi_b rejection, 8 NaN-alpha retries, 16 orbit-integral
+	                          halvings, 32 the initial shell radius, 64 no speed
+	                          distribution for the edge potential (the reference's inverse
+	                          CDF is NaN there and it retries without end) */
+	uint32_t pad2;
 } pot_step_stats;
 
 /* capacity of the fast form's per-warp stack of cells awaiting a test;
@@ -232,6 +242,60 @@ int pot_gpu_launch_count(pot_gpu_ctx* ctx, uint64_t* n);
 /* Block the calling thread until all work queued on the context's stream
    has finished; returns the first device-side status seen. */
 int pot_gpu_sync(pot_gpu_ctx* ctx);
+
+/* Device bytes a context with these settings allocates (no device work). */
+int pot_gpu_bytes_needed(const pot_run_cfg* cfg, const pot_gpu_opts* opts, uint64_t* bytes);
+
+/* ---- batches of independent runs ---------------------------------------
+   No counterpart in the reference, which runs one grain per MPI job.  A
+   batch holds many runs (each its own context and stream) and advances all
+   of them with one CUDA-graph launch per `steps_per_launch` steps; runs are
+   admitted while free HBM allows and evicted when done.  Runs share no
+   state: each result is bit-identical to the same run stepped alone. */
+typedef struct pot_batch pot_batch;
+
+typedef struct pot_batch_opts {
+	int32_t device;
+	uint32_t steps_per_launch;  /* steps per graph launch, even; 0 = 2 */
+	uint64_t reserve_bytes;     /* HBM left free when admitting */
+} pot_batch_opts;
+
+/* One member's state, gathered on the device for the whole batch. */
+typedef struct pot_batch_row {
+	int32_t slot;
+	int32_t status;
+	uint64_t t_steps;
+	int64_t grain_q;
+	int64_t q_sum;        /* sum of the grain charge after each step since upload/init */
+	uint64_t tot_absor_e;
+	uint64_t particles;
+	uint32_t warn;        /* as pot_step_stats.warn */
+	uint32_t pad;
+} pot_batch_row;
+
+int pot_batch_create(const pot_batch_opts* opts, pot_batch** out);
+void pot_batch_destroy(pot_batch* b);
+/* Admit a run: POT_E_NOMEM (nothing allocated) when its device state would
+   leave less than reserve_bytes of HBM free.  parts == NULL initialises
+   the particles as pot_gpu_init_particles does; else they are uploaded
+   with `grain`.  Writes the run's slot id. */
+int pot_batch_admit(pot_batch* b, const pot_run_cfg* cfg, const pot_gpu_opts* opts, const pot_particle* parts,
+                    const pot_grain_state* grain, int32_t* slot);
+int pot_batch_evict(pot_batch* b, int32_t slot);
+/* Enqueue nsteps (a multiple of steps_per_launch) for every member. */
+int pot_batch_step(pot_batch* b, uint32_t nsteps);
+int pot_batch_sync(pot_batch* b);
+/* Members' current state (synchronises). */
+int pot_batch_summary(pot_batch* b, uint32_t max, pot_batch_row* rows, uint32_t* n_rows);
+int pot_batch_count(pot_batch* b, uint32_t* runs, uint64_t* particles, uint64_t* bytes);
+/* A member's own context (after the batch's queued work), for downloads
+   and queries; stepping it directly is allowed (the batch re-captures). */
+int pot_batch_ctx(pot_batch* b, int32_t slot, pot_gpu_ctx** ctx);
+
+/* Autotuner: time `steps` steps of each candidate (leaf size, group size)
+   of the fast form on a fresh run of cfg and write the fastest into opts
+   (its ms per step into *ms_per_step). */
+int pot_gpu_tune(const pot_run_cfg* cfg, pot_gpu_opts* opts, uint32_t steps, double* ms_per_step);
 
 #ifdef __cplusplus
 }

@@ -77,25 +77,29 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     return LIB
 
 
-HOST_SRC = os.path.join(PKG, "host", "potgpu.c")
+HOST_PROGRAMS = {"potgpu": os.path.join(PKG, "host", "potgpu.c"),      # pot's command line and files
+                 "potserve": os.path.join(PKG, "host", "potserve.c")}  # batched sweep and serving loop
 HOST_BIN = os.path.join(PKG, "potgpu")
+SERVE_BIN = os.path.join(PKG, "potserve")
 
 
 def build_host(force: bool = False) -> str:
-    """The C host program (pot's command line and output files) linked to
-    libpotgpu.so with an $ORIGIN run path."""
+    """The C host programs, linked to libpotgpu.so with an $ORIGIN run path;
+    returns the path of potgpu."""
     lib = build()
-    if not force and os.path.exists(HOST_BIN) and \
-            os.path.getmtime(HOST_BIN) >= max(os.path.getmtime(HOST_SRC), os.path.getmtime(lib)):
-        return HOST_BIN
     cc = shutil.which("gcc") or "gcc"
-    tmp = HOST_BIN + ".tmp%d" % os.getpid()
-    cmd = [cc, "-O2", "-std=c99", "-Wall", "-Wextra", "-Wno-unused-parameter", "-I", INCLUDE, HOST_SRC, "-o", tmp,
-           "-L", PKG, "-lpotgpu", "-Wl,-rpath,$ORIGIN", "-lm"]
-    p = subprocess.run(cmd, capture_output=True, text=True)
-    if p.returncode != 0:
-        raise RuntimeError("gcc failed for %s:\n%s%s" % (HOST_SRC, p.stdout, p.stderr))
-    os.replace(tmp, HOST_BIN)
+    for name, src in HOST_PROGRAMS.items():
+        out = os.path.join(PKG, name)
+        deps = [src, lib, os.path.join(INCLUDE, "pot_gpu.h")]
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+            continue
+        tmp = out + ".tmp%d" % os.getpid()
+        cmd = [cc, "-O2", "-std=c99", "-Wall", "-Wextra", "-Wno-unused-parameter", "-I", INCLUDE, src, "-o", tmp,
+               "-L", PKG, "-lpotgpu", "-Wl,-rpath,$ORIGIN", "-lm"]
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError("gcc failed for %s:\n%s%s" % (src, p.stdout, p.stderr))
+        os.replace(tmp, out)
     return HOST_BIN
 
 

@@ -51,6 +51,8 @@ struct pot_gpu_ctx {
 	bool uploaded = false;
 	bool tree_valid = false;
 	int sticky = POT_OK;
+	bool dry = false;       // count bytes, allocate nothing (pot_gpu_bytes_needed)
+	uint64_t bytes = 0;     // device bytes held (or needed, when dry)
 	Timer timer;
 	std::vector<void*> allocs;
 };
@@ -207,6 +209,8 @@ static int dalloc(pot_gpu_ctx* c, T** p, size_t count)
 {
 	*p = nullptr;
 	if (count == 0) count = 1;
+	c->bytes += (sizeof(T) * count + 255) & ~(size_t)255;
+	if (c->dry) return POT_OK;
 	cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
 	if (e != cudaSuccess) {
 		*p = nullptr;
@@ -386,6 +390,31 @@ static int fetch(std::vector<T>& v, const T* d, size_t n)
 }
 
 extern "C" {
+static void enqueue_step(pot_gpu_ctx* c, uint32_t flags);
+}
+
+// ---- internal interface of the batch runtime (pot_batch.cu) --------------
+namespace pot {
+cudaStream_t ctx_stream(pot_gpu_ctx* c) { return c->stream; }
+int ctx_parity(const pot_gpu_ctx* c) { return c->cur; }
+RunRec* ctx_rec(pot_gpu_ctx* c) { return c->rec; }
+uint64_t ctx_bytes(const pot_gpu_ctx* c) { return c->bytes; }
+uint64_t ctx_particles(const pot_gpu_ctx* c) { return c->n; }
+int ctx_ready(const pot_gpu_ctx* c) { return !c->uploaded ? POT_E_STATE : c->sticky; }
+// Enqueue steps without synchronising (stream capture safe: no host sync,
+// no allocation; the timer must be off).
+int ctx_enqueue(pot_gpu_ctx* c, uint32_t nsteps)
+{
+	const int rc = ctx_ready(c);
+	if (rc != POT_OK) return rc;
+	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c, 0);
+	c->tree_valid = true;
+	return POT_OK;
+}
+void ctx_mark_error(pot_gpu_ctx* c, int rc) { if (c->sticky == POT_OK) c->sticky = rc; }
+}  // namespace pot
+
+extern "C" {
 
 const char* pot_gpu_strerror(int s)
 {
@@ -416,7 +445,23 @@ void pot_gpu_destroy(pot_gpu_ctx* c)
 	delete c;
 }
 
+static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx** out, bool dry,
+                       uint64_t* bytes);
+
 int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx** out)
+{
+	return create_impl(cfg, opts, out, false, nullptr);
+}
+
+int pot_gpu_bytes_needed(const pot_run_cfg* cfg, const pot_gpu_opts* opts, uint64_t* bytes)
+{
+	pot_gpu_ctx* c = nullptr;
+	if (!bytes) return POT_E_ARG;
+	return create_impl(cfg, opts, &c, true, bytes);
+}
+
+static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx** out, bool dry,
+                       uint64_t* bytes)
 {
 	if (!cfg || !out) return POT_E_ARG;
 	*out = nullptr;
@@ -434,15 +479,18 @@ int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx
 	if (cfg->r == 0 || !(cfg->mpp > 0.0) || !(cfg->dt > 0.0) || !(cfg->a > 0.0) || cfg->soft < 0.0 ||
 	    !(cfg->theta > 0.0) || cfg->Te < 0.0 || cfg->Ti <= 0.0)
 		return POT_E_ARG;
-	int ndev = 0;
-	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return POT_E_CUDA;
-	if (o.device < 0 || o.device >= ndev) return POT_E_ARG;
+	if (!dry) {
+		int ndev = 0;
+		if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return POT_E_CUDA;
+		if (o.device < 0 || o.device >= ndev) return POT_E_ARG;
+	}
 	pot_gpu_ctx* c = new (std::nothrow) pot_gpu_ctx();
 	if (!c) return POT_E_NOMEM;
 	c->cfg = *cfg;
 	c->opts = o;
 	c->device = o.device;
-	if (cudaSetDevice(c->device) != cudaSuccess) {
+	c->dry = dry;
+	if (!dry && cudaSetDevice(c->device) != cudaSuccess) {
 		delete c;
 		return POT_E_CUDA;
 	}
@@ -451,7 +499,9 @@ int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx
 		delete c;
 		return rc;
 	}
-	if (o.stream) {
+	if (dry) {
+		// the allocation plan below only counts
+	} else if (o.stream) {
 		c->stream = (cudaStream_t)o.stream;
 	} else {
 		if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -531,6 +581,11 @@ int pot_gpu_create(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu_ctx
 	}
 	tree_ptrs_fast(c, fast);
 #undef AL
+	if (dry) {
+		*bytes = c->bytes;
+		delete c;
+		return POT_OK;
+	}
 	RunRec r0;
 	std::memset(&r0, 0, sizeof(r0));
 	r0.grain_m = MASS_DUST;
@@ -646,6 +701,7 @@ static void enqueue_step(pot_gpu_ctx* c, uint32_t flags)
 	launch_grain_end(c->pos[c->cur], c->vel[c->cur], c->hist, P, c->rec, epe, s, c->timer);
 }
 
+
 int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats* out)
 {
 	if (!c) return POT_E_ARG;
@@ -676,6 +732,8 @@ int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats
 		out->status = r.status;
 		out->stack_max = r.stack_max;
 		for (int k = 0; k < 3; k++) out->epe[k] = h.epe[k];
+		out->q_sum = r.q_sum;
+		out->warn = r.warn;
 	}
 	return st;
 }

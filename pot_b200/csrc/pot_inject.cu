@@ -19,12 +19,24 @@
 
 namespace pot {
 
+// Which cap stopped a sampler: bits recorded in RunRec::warn beside POT_E_ITER.
+constexpr uint32_t FAIL_NEWTON = 2u;   // inverse-CDF Newton iteration (prng.c:138-214)
+constexpr uint32_t FAIL_REJECT = 4u;   // u^2 < chi_b rejection (pot.c:530-546)
+constexpr uint32_t FAIL_RETRY = 8u;    // NaN alpha retries (pot.c:584-598)
+constexpr uint32_t FAIL_SIMPSON = 16u; // orbit-integral halvings (pot.c:433-492)
+constexpr uint32_t FAIL_SHELL = 32u;   // initial radius outside the grain (pot.c:703-708)
+constexpr uint32_t FAIL_SPEED = 64u;   // no speed distribution for this chi_b: the inverse CDF is NaN
+                                       // (u_icdf for chi_b above about U^2 + 1/2, prng.c:171-214)
 constexpr int NEWTON_CAP = 200;
 constexpr int REJECT_CAP = 10000;
-constexpr int RETRY_CAP = 1000;
+// NaN alpha means the sampled orbit meets a potential barrier; with cold ions
+// (Te/Ti >> 1) and a noisy single-point edge potential, most samples can be
+// rejected for a while, so this cap is generous (the reference recurses
+// without bound).
+constexpr int RETRY_CAP = 100000;
 constexpr int SIMPSON_CAP = 100000;
 
-__device__ double d_u_no_flow_icdf(double chi, double q, bool& ok)
+__device__ double d_u_no_flow_icdf(double chi, double q, uint32_t& fail)
 {
 	const double omc = 1.0 - chi;
 	double u = 1.29951, p;
@@ -34,11 +46,11 @@ __device__ double d_u_no_flow_icdf(double chi, double q, bool& ok)
 		p = 1.0 - ((usq + omc) * exp(-usq) / omc) - q;
 		u -= p / (2.0 * u * exp(-usq) * (chi - usq) / -omc);
 	} while ((p * p) > 1e-16 && ++it < NEWTON_CAP);
-	if (it >= NEWTON_CAP) ok = false;
+	if (it >= NEWTON_CAP) fail |= FAIL_NEWTON;
 	return u;
 }
 
-__device__ double d_u_icdf(double U, double chi, double q, bool& ok)
+__device__ double d_u_icdf(double U, double chi, double q, uint32_t& fail)
 {
 	const double Usq = U * U;
 	const double psi = SQRT_PI_REF * (1.0 + (2.0 * (Usq - chi))) / 2.0;
@@ -58,12 +70,12 @@ __device__ double d_u_icdf(double U, double chi, double q, bool& ok)
 		dp_num *= exp(-u * ((2.0 * U) + u)) - exp((2.0 * U * u) - usq);
 		u -= p / (dp_num / dp_den);
 	} while ((p * p) > 1e-16 && ++it < NEWTON_CAP);
-	if (it >= NEWTON_CAP) ok = false;
+	if (it >= NEWTON_CAP) fail |= FAIL_NEWTON;
 	return u;
 }
 
 // mld: max_lin_dev, 0.01 in pot.c:436 and 0.1 in pot-spheroid.c:457
-__device__ double d_integrate_for_alpha(double s, double chi_b, double u2, double Rol, double mld, bool& ok)
+__device__ double d_integrate_for_alpha(double s, double chi_b, double u2, double Rol, double mld, uint32_t& fail)
 {
 	const double chu2 = chi_b / u2;
 	const double s2 = s * s;
@@ -84,12 +96,12 @@ __device__ double d_integrate_for_alpha(double s, double chi_b, double u2, doubl
 			xi1 = (xi0 + xi2) / 2.0;
 			y1 = 1.0 - (chu2 * xi1 * exp(Rol * (1.0 - (1.0 / xi1))));
 			y1 = 1.0 / sqrt((y1 / s2) - (xi1 * xi1));
-			if (++guard > SIMPSON_CAP) { ok = false; return 0.0; }
+			if (++guard > SIMPSON_CAP) { fail |= FAIL_SIMPSON; return 0.0; }
 		}
 		alpha += (xi2 - xi0) * (y0 + (4.0 * y1) + y2) / 6.0;
 		xi0 = xi2;
 		y0 = y2;
-		if (++guard > SIMPSON_CAP) { ok = false; return 0.0; }
+		if (++guard > SIMPSON_CAP) { fail |= FAIL_SIMPSON; return 0.0; }
 	} while (xi2 < 1.0);
 	return alpha;
 }
@@ -101,7 +113,7 @@ __device__ double d_integrate_for_alpha(double s, double chi_b, double u2, doubl
 // once, and a ballot picks the first k that passes the linearity test -- the
 // interval the sequential loop stops at, with the same values.  All lanes
 // return the same alpha.
-__device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, double Rol, double mld, bool& ok)
+__device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, double Rol, double mld, uint32_t& fail)
 {
 	const uint32_t lane = threadIdx.x & 31u;
 	const double chu2 = chi_b / u2;
@@ -130,7 +142,7 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 			// more than 32 halvings needed at this xi0: continue from e_32
 			const double e32 = __shfl_sync(0xffffffffu, ek1, 31);
 			if (e32 <= xi0 || ++intervals > SIMPSON_CAP) {
-				ok = false;
+				fail |= FAIL_SIMPSON;
 				return 0.0;
 			}
 			// the sequential loop would keep halving towards xi0 from e_32;
@@ -163,7 +175,7 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 				}
 			}
 			if (!done) {
-				ok = false;
+				fail |= FAIL_SIMPSON;
 				return 0.0;
 			}
 		} else {
@@ -177,7 +189,7 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 		}
 		if (!(xi0 < 1.0)) break;
 		if (++intervals > SIMPSON_CAP) {
-			ok = false;
+			fail |= FAIL_SIMPSON;
 			return 0.0;
 		}
 	}
@@ -234,7 +246,7 @@ __device__ __forceinline__ void nrv_pair(Stream& st, double sd, double& a, doubl
 // the orbit integral is evaluated cooperatively.
 template <bool WARP>
 __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Params& P, double4& p, double4& v,
-                                 bool& ok)
+                                 uint32_t& fail)
 {
 	const double v_n = sp == SP_E ? P.vn_e : P.vn_i;
 	double chi_b = chi_b_in;
@@ -246,21 +258,27 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 			const double U = P.x_drift / v_n;
 			int k = 0;
 			do {
-				u_mag = d_u_icdf(U, chi_b, st.rnd(1.0), ok);
+				u_mag = d_u_icdf(U, chi_b, st.rnd(1.0), fail);
 				u2 = u_mag * u_mag;
 			} while (u2 < chi_b && ++k < REJECT_CAP);
-			if (k >= REJECT_CAP) ok = false;
+			if (k >= REJECT_CAP) fail |= FAIL_REJECT;
 			const double q = st.rnd(1.0);
 			cz = log(q + (1.0 - q) * exp(-4.0 * u_mag * U)) / (2.0 * u_mag * U);
 			cz += 1.0;
 		} else {
 			int k = 0;
 			do {
-				u_mag = d_u_no_flow_icdf(chi_b, st.rnd(1.0), ok);
+				u_mag = d_u_no_flow_icdf(chi_b, st.rnd(1.0), fail);
 				u2 = u_mag * u_mag;
 			} while (u2 < chi_b && ++k < REJECT_CAP);
-			if (k >= REJECT_CAP) ok = false;
+			if (k >= REJECT_CAP) fail |= FAIL_REJECT;
 			cz = st.rnd(2.0) - 1.0;
+		}
+		if (isnan(u2)) {
+			// the reference would retry forever: every speed it can draw is NaN
+			fail |= FAIL_SPEED;
+			alpha = 0.0;
+			break;
 		}
 		u[0] = 0.0;
 		u[1] = 0.0;
@@ -271,12 +289,12 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 		sincos(psi, &sps, &cps);
 		rot_xy(1.0, 0.0, sps, cps, u[0], u[1], u[2], 0.0);
 		b = sqrt(st.rnd(1.0 - (chi_b / u2)));
-		alpha = WARP ? d_integrate_for_alpha_warp(b, chi_b, u2, P.Rol, P.max_lin_dev, ok)
-		             : d_integrate_for_alpha(b, chi_b, u2, P.Rol, P.max_lin_dev, ok);
+		alpha = WARP ? d_integrate_for_alpha_warp(b, chi_b, u2, P.Rol, P.max_lin_dev, fail)
+		             : d_integrate_for_alpha(b, chi_b, u2, P.Rol, P.max_lin_dev, fail);
 		if (!isnan(alpha) || attempt + 1 >= RETRY_CAP) break;
 	}
 	if (isnan(alpha)) {
-		ok = false;
+		fail |= FAIL_RETRY;
 		alpha = 0.0;
 	}
 	const double phi = st.rnd(2.0 * PI_REF);
@@ -303,7 +321,7 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 // inject, pot.c:658-765 (spherical domain, grain enabled)
 template <bool WARP>
 __device__ void inject(Stream& st, int sp, bool reinjection, double chi_b, const Params& P, double4& p, double4& v,
-                       bool& ok)
+                       uint32_t& fail)
 {
 	double sigma = sp == SP_ION ? P.sigma_i : P.sigma_e;
 	const bool sceptic = (P.flags & FLAG_SCEPTIC) != 0;
@@ -314,12 +332,12 @@ __device__ void inject(Stream& st, int sp, bool reinjection, double chi_b, const
 		r = P.mpp * cbrt(st.rnd(rmax3));
 		int guard = 0;
 		while (r <= P.a && ++guard < REJECT_CAP) r = P.mpp * cbrt(st.rnd(rmax3));
-		if (guard >= REJECT_CAP) ok = false;
+		if (guard >= REJECT_CAP) fail |= FAIL_SHELL;
 	} else {
 		r = P.mpp * P.r_pix;
 	}
 	if (sceptic && reinjection) {
-		sceptic_reinject<WARP>(st, sp, chi_b, P, p, v, ok);
+		sceptic_reinject<WARP>(st, sp, chi_b, P, p, v, fail);
 		return;
 	}
 	const double phi = st.rnd(2.0 * PI_REF);
@@ -370,17 +388,17 @@ __global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel,
 		double4 p = pos[s];
 		double4 v = vel[s];
 		const int sp = (int)p.w;
-		bool ok = true;
+		uint32_t fail = 0;
 		uint32_t attempt = 0;
 		Stream st;
 		st.init(P.seed, id, t, 0x10000u | attempt++);
-		inject<true>(st, sp, true, chi_b, P, p, v, ok);
+		inject<true>(st, sp, true, chi_b, P, p, v, fail);
 		if ((reason & 1u) && outside_sphere(p, P)) {
 			st.init(P.seed, id, t, 0x10000u | attempt++);
-			inject<true>(st, sp, true, chi_b, P, p, v, ok);
+			inject<true>(st, sp, true, chi_b, P, p, v, fail);
 		}
 		if (lane == 0) {
-			if (!ok) set_status(rec, POT_E_ITER);
+			if (fail) { atomicOr(&rec->warn, fail); set_status(rec, POT_E_ITER); }
 			pos[s] = p;
 			vel[s] = v;
 		}
@@ -402,11 +420,11 @@ __global__ void k_init(double4* __restrict__ pos, double4* __restrict__ vel, uin
 	}
 	const int sp = species_of_id(i, P.n_ions);
 	double4 p = make_double4(0.0, 0.0, 0.0, (double)sp), v;
-	bool ok = true;
+	uint32_t fail = 0;
 	Stream st;
 	st.init(P.seed, i, 0u, 0x20000u);
-	inject<false>(st, sp, false, 0.0, P, p, v, ok);
-	if (!ok) set_status(rec, POT_E_ITER);
+	inject<false>(st, sp, false, 0.0, P, p, v, fail);
+	if (fail) { atomicOr(&rec->warn, fail); set_status(rec, POT_E_ITER); }
 	pos[i] = p;
 	vel[i] = v;
 }

@@ -95,6 +95,7 @@ struct RunRec {
 	double phi_grain;        // potential at the grain from every other particle (V)
 	unsigned int epe_step;   // 1 when this step computes them
 	unsigned int epe_pad;
+	long long q_sum;         // sum over completed steps of the grain charge after each step (moving means)
 };
 
 constexpr double VFIX = 1048576.0;  // 2^20
@@ -177,7 +178,9 @@ __device__ __forceinline__ double dsq3(double x, double y, double z)
 // ---- Philox4x32-10 (Salmon et al., SC'11) -------------------------------
 __host__ __device__ inline void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1)
 {
+#ifdef __CUDA_ARCH__
 #pragma unroll
+#endif
 	for (int r = 0; r < 10; r++) {
 		const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
 		const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];

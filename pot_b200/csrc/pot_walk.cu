@@ -308,6 +308,7 @@ __global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel
 	for (int k = 0; k < 3; k++) rec->grain_vel[k] = gv[k];
 	rec->grain_m = m;
 	rec->grain_q += rec->dq;
+	rec->q_sum += rec->grain_q;
 	rec->tot_absor_e += rec->de;
 	if (epe) {
 		// the grain's energy with its updated charge, pot.c:2859-2864

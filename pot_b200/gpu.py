@@ -72,7 +72,8 @@ class _Stats(C.Structure):
     _fields_ = [("t_steps", C.c_uint64), ("grain_q", C.c_int64), ("dq", C.c_int64), ("de", C.c_uint64),
                 ("n_absorbed", C.c_uint64), ("n_reinjected", C.c_uint64), ("n_pushed", C.c_uint64),
                 ("interactions", C.c_uint64), ("n_nodes", C.c_uint64), ("chi_b", C.c_double),
-                ("status", C.c_int32), ("stack_max", C.c_uint32), ("epe", C.c_double * 3)]
+                ("status", C.c_int32), ("stack_max", C.c_uint32), ("epe", C.c_double * 3),
+                ("q_sum", C.c_int64), ("warn", C.c_uint32), ("pad2", C.c_uint32)]
 
 
 _LIB = None
@@ -124,6 +125,22 @@ def load_library(path: str = LIB_PATH, build_if_stale: bool = True):
     L.pot_gpu_reset_kernel_times.argtypes = [vp]
     L.pot_gpu_sync.argtypes = [vp]
     L.pot_gpu_launch_count.argtypes = [vp, C.POINTER(u64)]
+    L.pot_gpu_bytes_needed.argtypes = [C.POINTER(_RunCfg), C.POINTER(_Opts), C.POINTER(u64)]
+    L.pot_gpu_tune.argtypes = [C.POINTER(_RunCfg), C.POINTER(_Opts), u32, C.POINTER(C.c_double)]
+    L.pot_batch_create.argtypes = [C.POINTER(_BatchOpts), C.POINTER(vp)]
+    L.pot_batch_destroy.argtypes = [vp]
+    L.pot_batch_destroy.restype = None
+    L.pot_batch_admit.argtypes = [vp, C.POINTER(_RunCfg), C.POINTER(_Opts), vp, C.POINTER(_Grain),
+                                  C.POINTER(C.c_int32)]
+    L.pot_batch_evict.argtypes = [vp, C.c_int32]
+    L.pot_batch_step.argtypes = [vp, u32]
+    L.pot_batch_sync.argtypes = [vp]
+    L.pot_batch_summary.argtypes = [vp, u32, vp, C.POINTER(u32)]
+    L.pot_batch_count.argtypes = [vp, C.POINTER(u32), C.POINTER(u64), C.POINTER(u64)]
+    L.pot_batch_ctx.argtypes = [vp, C.c_int32, C.POINTER(vp)]
+    for name in ("pot_batch_create", "pot_batch_admit", "pot_batch_evict", "pot_batch_step", "pot_batch_sync",
+                 "pot_batch_summary", "pot_batch_count", "pot_batch_ctx"):
+        getattr(L, name).restype = C.c_int
     for name in header_symbols():
         fn = getattr(L, name)
         if fn.restype is C.c_int or name not in ("pot_gpu_destroy", "pot_gpu_strerror"):
@@ -131,6 +148,15 @@ def load_library(path: str = LIB_PATH, build_if_stale: bool = True):
                 fn.restype = C.c_int
     _LIB = L
     return L
+
+
+class _BatchOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("steps_per_launch", C.c_uint32), ("reserve_bytes", C.c_uint64)]
+
+
+BATCH_ROW_DTYPE = np.dtype([("slot", "<i4"), ("status", "<i4"), ("t_steps", "<u8"), ("grain_q", "<i8"),
+                            ("q_sum", "<i8"), ("tot_absor_e", "<u8"), ("particles", "<u8"), ("warn", "<u4"),
+                            ("pad", "<u4")])
 
 
 @dataclass
@@ -170,7 +196,7 @@ def _ptr(a):
 
 
 def _stats_dict(st: "_Stats") -> dict:
-    d = {k: getattr(st, k) for k, _ in _Stats._fields_ if k not in ("pad", "epe")}
+    d = {k: getattr(st, k) for k, _ in _Stats._fields_ if k not in ("pad", "pad2", "epe")}
     d["epe"] = np.array(list(st.epe))
     return d
 
@@ -340,3 +366,123 @@ class Run:
 
     def sync(self):
         self._check(self.lib.pot_gpu_sync(self.h), "pot_gpu_sync")
+
+
+def _opts(form="fast", leaf_size=0, group_size=0, seed=1, device=0) -> _Opts:
+    o = _Opts()
+    o.form = FORM_PLAIN if form == "plain" else FORM_FAST
+    o.leaf_size = int(leaf_size)
+    o.group_size = int(group_size)
+    o.device = int(device)
+    o.seed = int(seed) & ((1 << 64) - 1)
+    return o
+
+
+def bytes_needed(cfg: RunConfig, form="fast", leaf_size=0, group_size=0) -> int:
+    """Device bytes a run with these settings allocates."""
+    L = load_library()
+    b = C.c_uint64()
+    rc = L.pot_gpu_bytes_needed(C.byref(cfg.to_c()), C.byref(_opts(form, leaf_size, group_size)), C.byref(b))
+    if rc != POT_OK:
+        raise PotError(rc, "pot_gpu_bytes_needed", L.pot_gpu_strerror(rc).decode())
+    return b.value
+
+
+def tune(cfg: RunConfig, steps: int = 6, seed: int = 1, device: int = 0):
+    """Autotuner: the fastest (leaf size, group size) of the fast form for
+    this run, and its ms per step."""
+    L = load_library()
+    o = _opts("fast", seed=seed, device=device)
+    ms = C.c_double()
+    rc = L.pot_gpu_tune(C.byref(cfg.to_c()), C.byref(o), int(steps), C.byref(ms))
+    if rc != POT_OK:
+        raise PotError(rc, "pot_gpu_tune", L.pot_gpu_strerror(rc).decode())
+    return dict(leaf_size=o.leaf_size, group_size=o.group_size, ms_per_step=ms.value)
+
+
+class Batch:
+    """Many independent runs stepped by one CUDA-graph launch
+    (``pot_batch``)."""
+
+    def __init__(self, device: int = 0, steps_per_launch: int = 2, reserve_bytes: int = 0):
+        self.lib = load_library()
+        o = _BatchOpts()
+        o.device, o.steps_per_launch, o.reserve_bytes = int(device), int(steps_per_launch), int(reserve_bytes)
+        self.h = C.c_void_p()
+        self.cfgs = {}
+        self._check(self.lib.pot_batch_create(C.byref(o), C.byref(self.h)), "pot_batch_create")
+
+    def _check(self, rc, where):
+        if rc != POT_OK:
+            raise PotError(rc, where, self.lib.pot_gpu_strerror(rc).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.pot_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def admit(self, cfg: RunConfig, form="fast", leaf_size=0, group_size=0, seed=1, parts=None, grain=None) -> int:
+        slot = C.c_int32(-1)
+        o = _opts(form, leaf_size, group_size, seed)
+        pp = None
+        if parts is not None:
+            parts = np.ascontiguousarray(parts, dtype=PARTICLE_DTYPE)
+            pp = _ptr(parts)
+        g = _grain_c(grain)
+        self._check(self.lib.pot_batch_admit(self.h, C.byref(cfg.to_c()), C.byref(o), pp, C.byref(g) if g else None,
+                                             C.byref(slot)), "pot_batch_admit")
+        self.cfgs[slot.value] = cfg
+        return slot.value
+
+    def try_admit(self, *a, **k):
+        """admit, or None when the run does not fit in free HBM."""
+        try:
+            return self.admit(*a, **k)
+        except PotError as e:
+            if e.status == -3:
+                return None
+            raise
+
+    def evict(self, slot: int):
+        self._check(self.lib.pot_batch_evict(self.h, int(slot)), "pot_batch_evict")
+        self.cfgs.pop(slot, None)
+
+    def step(self, n: int = 2):
+        self._check(self.lib.pot_batch_step(self.h, int(n)), "pot_batch_step")
+
+    def sync(self):
+        self._check(self.lib.pot_batch_sync(self.h), "pot_batch_sync")
+
+    def summary(self) -> np.ndarray:
+        cap = max(1, len(self.cfgs))
+        rows = np.zeros(cap, BATCH_ROW_DTYPE)
+        n = C.c_uint32()
+        self._check(self.lib.pot_batch_summary(self.h, cap, _ptr(rows), C.byref(n)), "pot_batch_summary")
+        return rows[:n.value]
+
+    def count(self):
+        r, p, b = C.c_uint32(), C.c_uint64(), C.c_uint64()
+        self._check(self.lib.pot_batch_count(self.h, C.byref(r), C.byref(p), C.byref(b)), "pot_batch_count")
+        return dict(runs=r.value, particles=p.value, bytes=b.value)
+
+    def download(self, slot: int):
+        h = C.c_void_p()
+        self._check(self.lib.pot_batch_ctx(self.h, int(slot), C.byref(h)), "pot_batch_ctx")
+        cfg = self.cfgs[slot]
+        out = np.zeros(cfg.N, PARTICLE_DTYPE)
+        g = _Grain()
+        self._check(self.lib.pot_gpu_download(h, _ptr(out), C.byref(g)), "pot_gpu_download")
+        return out, _grain_dict(g)
