@@ -233,6 +233,32 @@ def run_reference_arm(args):
     return 0
 
 
+def run_batches(args, device):
+    """The batched sweep and the serving loop (pot_b200/potserve), short
+    versions: a sweep of --batch-runs runs (16k-256k particles) and a serving
+    window of Poisson arrivals (8k-1M particles), each run capped at
+    --batch-steps steps.  The full-length runs are separate invocations."""
+    from pot_b200 import build as gpu_build
+    try:
+        exe = os.path.join(os.path.dirname(gpu_build.HOST_BIN), "potserve")
+        if not os.path.exists(exe):
+            gpu_build.build_host()
+    except Exception as e:  # no compiler and no binary
+        return {"unavailable": str(e)}
+    out = {}
+    common = ["--max-steps", str(args.batch_steps), "--tune", "--device", str(device)]
+    runs = [("sweep", ["--mode", "sweep", "--runs", str(args.batch_runs), "--nmin", "16000", "--nmax", "256000"]),
+            ("serve", ["--mode", "serve", "--rate", "20", "--duration", str(args.serve_seconds), "--nmin", "8000",
+                       "--nmax", "1000000", "--bmax", "1.0"])]
+    for name, extra in runs:
+        try:
+            p = subprocess.run([exe] + extra + common, capture_output=True, text=True, timeout=600)
+            out[name] = json.loads(p.stdout) if p.returncode == 0 else {"error": p.stderr[-400:]}
+        except Exception as e:
+            out[name] = {"error": str(e)}
+    return out
+
+
 def walk_compute(interactions, kernel, launch_s, clk):
     """FP32 rate of the fast walk, the kernel's real bound (it is issue- and
     FP32-pipe-limited, not HBM-bound): 17 FP32 flops and one rsqrt per
@@ -421,6 +447,10 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference(args.config)
 
+    batch = None
+    if ws == 1 and args.batch_runs > 0:
+        batch = run_batches(args, local)
+
     extra = {}
     if ws == 1 and args.extra_config not in ("none", "", args.config):
         extra[args.extra_config] = time_config(args.extra_config, stream, dev, flush, steps=min(args.steps, 10),
@@ -443,7 +473,8 @@ def run_ours(args):
             "walk_compute": walk_compute(inter, dom_name, per_launch_s, clk),
             "kernels_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
             "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
-            "walk_stack_max": st.get("stack_max"), "extra_configs": extra or None, "status": st["status"]}
+            "walk_stack_max": st.get("stack_max"), "extra_configs": extra or None, "batch": batch,
+            "status": st["status"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     run.close()
@@ -468,6 +499,10 @@ def main(argv=None):
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-runs", type=int, default=64,
+                    help="runs in the short batched sweep (0 to skip the batch and serving measurements)")
+    ap.add_argument("--batch-steps", type=int, default=400, help="step cap per run in the short batch measurements")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window of the short serving run")
     ap.add_argument("--extra-config", default="4m",
                     help="also time this configuration (fast and plain FP64 form, N=1 only) into the line's "
                          "extra_configs; 'none' to skip")

@@ -86,7 +86,9 @@ typedef struct pot_gpu_opts {
 	uint32_t group_size;  /* POT_FORM_FAST: largest target group per warp, 32 (default) or 64 */
 	uint32_t flags;       /* POT_OPT_* */
 	int32_t device;       /* CUDA device ordinal */
-	uint32_t pad;
+	uint32_t chi_b_ranks; /* SCEPTIC edge potential: the mean over this many equally spaced
+	                         azimuths, as a run of that many MPI ranks measures it
+	                         (pot.c:2251-2279, 2409-2418); 0 or 1 = one rank, at most 64 */
 	uint64_t seed;        /* key of the Philox streams used for (re)injection */
 	void* stream;         /* cudaStream_t to launch on; NULL = a private stream */
 } pot_gpu_opts;

@@ -297,7 +297,7 @@ class _PtoCfg(C.Structure):
                 ("x_drift", C.c_double), ("a", C.c_double), ("settle", C.c_double),
                 ("theta", C.c_double), ("B", C.c_double * 3), ("sceptic", C.c_int32),
                 ("quirk", C.c_int32), ("rng", C.c_int32), ("pad", C.c_int32), ("seed", C.c_uint64),
-                ("shape", C.c_int32), ("pad2", C.c_int32), ("A", C.c_double), ("axis", C.c_double * 3)]
+                ("shape", C.c_int32), ("chi_ranks", C.c_int32), ("A", C.c_double), ("axis", C.c_double * 3)]
 
 
 WELL_DTYPE = np.dtype([("abcd", "<u4", 4), ("index", "<u4"), ("state", "<u4", 16)])
@@ -349,6 +349,8 @@ class Oracle:
             L.pto_integrate_for_alpha_dev.restype = d
             L.pto_measure_chi_b.argtypes = [vp]
             L.pto_measure_chi_b.restype = d
+            L.pto_measure_chi_b_ranks.argtypes = [vp, i32]
+            L.pto_measure_chi_b_ranks.restype = d
             L.pto_step.argtypes = [vp, i32]
             L.pto_run_steps.argtypes = [vp, u64, i32]
             L.pto_last_step_stats.argtypes = [vp, vp, vp, vp, vp, vp, vp]
@@ -365,7 +367,7 @@ class Oracle:
         return cls._lib
 
     def __init__(self, p: RunParams, mode: str = "reference", sceptic: bool = True, seed: int = 1,
-                 init: bool = True):
+                 init: bool = True, chi_ranks: int = 0):
         L = self.lib()
         cfg = _PtoCfg()
         cfg.N, cfg.r, cfg.dt, cfg.mpp, cfg.soft = p.N, p.r, p.dt, p.mpp, p.soft
@@ -377,6 +379,7 @@ class Oracle:
         cfg.rng = 0 if mode == "reference" else 1
         cfg.seed = seed & ((1 << 64) - 1)
         cfg.shape = p.shape
+        cfg.chi_ranks = int(chi_ranks)
         cfg.A = p.A
         for k in range(3):
             cfg.axis[k] = p.axis[k]

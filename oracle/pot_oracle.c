@@ -1091,6 +1091,27 @@ static long double o_phi_particle(const pto_ctx* c, uint32_t part)
 
 double pto_phi_particle_feels(const pto_ctx* c, uint32_t part) { return (double) o_phi_particle(c, part); }
 
+/* normalised edge potential seen by rank k of P, pot.c:2251-2279 */
+static double o_chi_b_rank(const pto_ctx* c, int32_t k, int32_t P)
+{
+	const double azi = 2.0 * O_PI * k / P;
+	const double zen = O_PI / 2.0;
+	const double r = c->cfg.r * c->cfg.mpp;
+	const pto_particle* g = &c->parts[0];
+	double phi = pto_phi_at(c, g->x + (r * cos(azi) * sin(zen)), g->y + (r * sin(azi) * sin(zen)),
+	                        g->z + (r * cos(zen)));
+	return phi / (O_KB * c->cfg.Ti / (O_CHARGE[O_ION] * O_QE));
+}
+
+/* MPI_Allreduce(SUM) of the ranks' samples, then / num_workers (pot.c:2409-2418) */
+double pto_measure_chi_b_ranks(const pto_ctx* c, int32_t P)
+{
+	if (P < 1) P = 1;
+	double sum = 0.0;
+	for (int32_t k = 0; k < P; k++) sum += o_chi_b_rank(c, k, P);
+	return sum / P;
+}
+
 /* normalised edge potential at azimuth 0 (one rank), pot.c:2251-2279 */
 double pto_measure_chi_b(const pto_ctx* c)
 {
@@ -1173,8 +1194,12 @@ static int o_move(pto_ctx* c, int compute_epe, uint64_t time_steps)
 	memcpy(np, parts, sizeof(pto_particle) * N);
 
 	if (ru->sceptic && !(c->t_steps % 20)) {
-		c->chi_b = pto_measure_chi_b(c);
-		c->chi_b /= 1;  /* averaged over one rank */
+		if (ru->chi_ranks > 1) {
+			c->chi_b = pto_measure_chi_b_ranks(c, ru->chi_ranks);
+		} else {
+			c->chi_b = pto_measure_chi_b(c);
+			c->chi_b /= 1;  /* averaged over one rank */
+		}
 	}
 
 	for (start = 0; start < N; start++) {

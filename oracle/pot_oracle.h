@@ -65,7 +65,7 @@ typedef struct pto_cfg {
 	   constants (m_i/m_e = 1836.153, SCEPTIC max_lin_dev = 0.1) and keep the
 	   grain out of the tree */
 	int32_t shape;
-	int32_t pad2;
+	int32_t chi_ranks; /* chi_b as the mean over this many ranks' azimuths (0/1 = one) */
 	double A;         /* aspect ratio (pot-spheroid.c -A) */
 	double axis[3];   /* symmetry axis, unit vector; (1, 0, 0) in the reference,
 	                     anything else is an extension (unpinned) */
@@ -107,6 +107,8 @@ int pto_cross_grain_run(const pto_ctx* c, const pto_particle* p, const double* d
 void pto_grain_field(const pto_ctx* c, double x, double y, double z, double* E3);
 double pto_grain_phi(const pto_ctx* c, double x, double y, double z);
 double pto_measure_chi_b(const pto_ctx* c);
+/* the mean of measure_chi_b over P ranks' azimuths 2 pi k / P (pot.c:2268, 2409-2418) */
+double pto_measure_chi_b_ranks(const pto_ctx* c, int32_t P);
 
 /* One step: t_steps++, build the tree, move the particles (pot.c:4261-4386).
    Returns 0, or a negative status (tree build failure). */

@@ -237,6 +237,8 @@ static int fill_params(pot_gpu_ctx* c)
 	P.max_level = c->opts.form == POT_FORM_FAST ? 16u : (uint32_t)MAX_LEVELS;
 	P.key_bits = c->opts.form == POT_FORM_FAST ? 63u - 3u * P.max_level : 0u;
 	P.group_max = c->opts.group_size == 64 ? 64u : 32u;
+	P.chi_ranks = c->opts.chi_b_ranks ? c->opts.chi_b_ranks : 1u;
+	if (P.chi_ranks > 64) return POT_E_ARG;
 	P.seed = c->opts.seed;
 	// grain shape: 0 sphere, A > 1 prolate, 0 < A < 1 oblate (pot-spheroid.c:4797-4827)
 	if (r.A == 0.0) {

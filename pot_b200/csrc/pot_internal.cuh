@@ -158,7 +158,7 @@ struct Params {
 	double s_A, s_fc_f, s_fc_p, s_num, s_den_f, s_den_p;
 	double s_thr;         // a^2 A^(4/3): surface x^2 + A^2 rho^2 = a^2 A^(4/3)
 	uint32_t s_tilted;    // symmetry axis other than x (an extension of the reference)
-	uint32_t s_pad;
+	uint32_t chi_ranks;   // azimuths averaged for chi_b (ranks of an MPI run), >= 1
 	double s_ax[3], s_e1[3], s_e2[3];  // spheroid frame
 };
 

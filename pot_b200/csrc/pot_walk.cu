@@ -416,22 +416,43 @@ __device__ __forceinline__ double spheroid_phi_at(const Params& P, const RunRec*
 	return spheroid_phi_frame(P, (double)rec->grain_q, u, v, w);
 }
 
-// measure_chi_b (pot.c:2251-2279) for one rank: azimuth 0 in the x-y plane
-// through the grain, every 20 steps (pot.c:2409).
-__global__ void k_chi_b(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec, int force)
+// measure_chi_b (pot.c:2251-2279) as a run of P = chi_ranks MPI ranks does
+// it (pot.c:2409-2418): rank k samples phi at azimuth 2 pi k / P in the x-y
+// plane through the grain, the samples are summed and divided by P; every 20
+// steps.  Four warps share the samples; the sum is taken in rank order.
+__global__ void __launch_bounds__(128) k_chi_b(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec,
+                                              int force)
 {
-	__shared__ int32_t stack[PHI_STACK];
+	__shared__ int32_t stack[4][PHI_STACK];
+	__shared__ double sample[64];
+	__shared__ int bad;
 	if (!(P.flags & FLAG_SCEPTIC) || rec->status != POT_OK) return;
 	if (!force && (rec->t_steps % 20) != 0) return;
+	const uint32_t w = threadIdx.x >> 5;
+	if (threadIdx.x == 0) bad = 0;
+	__syncthreads();
 	const double zen = PI_REF / 2.0;
 	const double r = P.rad;
-	const double x = rec->grain_pos[0] + (r * cos(0.0) * sin(zen));
-	const double y = rec->grain_pos[1] + (r * sin(0.0) * sin(zen));
-	const double z = rec->grain_pos[2] + (r * cos(zen));
-	const double phi = spheroid_phi_at(P, rec, x, y, z) + warp_phi(x, y, z, T, src64, P, stack);
-	if (lane_id() == 0) {
-		if (isnan(phi)) set_status(rec, POT_E_WALK);
-		else rec->chi_b = phi / (KB * P.Ti / (1 * QE));
+	for (uint32_t k = w; k < P.chi_ranks; k += 4) {
+		const double azi = 2.0 * PI_REF * k / P.chi_ranks;
+		const double x = rec->grain_pos[0] + (r * cos(azi) * sin(zen));
+		const double y = rec->grain_pos[1] + (r * sin(azi) * sin(zen));
+		const double z = rec->grain_pos[2] + (r * cos(zen));
+		const double phi = spheroid_phi_at(P, rec, x, y, z) + warp_phi(x, y, z, T, src64, P, stack[w]);
+		if (lane_id() == 0) {
+			sample[k] = phi / (KB * P.Ti / (1 * QE));
+			if (isnan(phi)) bad = 1;
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		if (bad) {
+			set_status(rec, POT_E_WALK);
+		} else {
+			double sum = 0.0;
+			for (uint32_t k = 0; k < P.chi_ranks; k++) sum += sample[k];
+			rec->chi_b = sum / P.chi_ranks;
+		}
 	}
 }
 
@@ -497,7 +518,7 @@ void launch_chi_b(const TreeDev& T, const double4* src64, const Params& P, RunRe
 {
 	if (!(P.flags & FLAG_SCEPTIC)) return;
 	ScopedKernel k(tm, "chi_b");
-	k_chi_b<<<1, 32, 0, s>>>(T, src64, P, rec, force);
+	k_chi_b<<<1, 128, 0, s>>>(T, src64, P, rec, force);
 }
 
 void launch_push(double4* pos, double4* vel, const TreeDev& T, const double4* src64, const float4* src32,

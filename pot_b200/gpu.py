@@ -58,7 +58,7 @@ class _RunCfg(C.Structure):
 
 class _Opts(C.Structure):
     _fields_ = [("form", C.c_uint32), ("leaf_size", C.c_uint32), ("group_size", C.c_uint32),
-                ("flags", C.c_uint32), ("device", C.c_int32), ("pad", C.c_uint32), ("seed", C.c_uint64),
+                ("flags", C.c_uint32), ("device", C.c_int32), ("chi_b_ranks", C.c_uint32), ("seed", C.c_uint64),
                 ("stream", C.c_void_p)]
 
 
@@ -226,7 +226,8 @@ class Run:
     """One simulation run on one GPU (a ``pot_gpu_ctx``)."""
 
     def __init__(self, cfg: RunConfig, form: str = "plain", leaf_size: int = 0, group_size: int = 0,
-                 seed: int = 1, device: int = 0, stream: Optional[int] = None, timing: bool = False):
+                 seed: int = 1, device: int = 0, stream: Optional[int] = None, timing: bool = False,
+                 chi_b_ranks: int = 0):
         self.lib = load_library()
         self.cfg = cfg
         o = _Opts()
@@ -237,6 +238,7 @@ class Run:
         o.device = int(device)
         o.seed = int(seed) & ((1 << 64) - 1)
         o.stream = stream
+        o.chi_b_ranks = int(chi_b_ranks)
         self.form = form
         self.h = C.c_void_p()
         self._check(self.lib.pot_gpu_create(C.byref(cfg.to_c()), C.byref(o), C.byref(self.h)), "pot_gpu_create")

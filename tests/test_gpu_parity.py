@@ -325,3 +325,20 @@ def test_coincident_error_status():
         with pytest.raises(PotError) as e:
             r.step(1)
         assert e.value.status == -5
+
+
+@pytest.mark.parametrize("ranks", [2, 8, 64])
+def test_chi_b_over_ranks(ranks):
+    """chi_b as a run of `ranks` MPI ranks measures it: the mean over the
+    ranks' azimuths, refreshed on steps that are multiples of 20."""
+    o = oracle_snapshot(SMALL, seed=2, mode="gpu", steps=2)
+    g = o.grain()
+    o2 = Oracle(params(SMALL), mode="gpu", seed=2, init=False, chi_ranks=ranks)
+    o2.set_particles(o.particles())
+    o2.set_grain(q=-400, m=g["m"], tot_absor_e=g["tot_absor_e"], t_steps=19, chi_b=0.0)
+    o2.build_tree()
+    chi_ref = o2.lib().pto_measure_chi_b_ranks(o2.h, ranks)
+    with gpu_from_oracle(SMALL, o2, chi_b_ranks=ranks) as r:
+        st = r.step(1)
+    assert st["t_steps"] == 20
+    assert abs(st["chi_b"] - chi_ref) <= 1e-12 * abs(chi_ref)

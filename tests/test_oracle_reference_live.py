@@ -128,3 +128,27 @@ def test_spheroid_field_phi_and_absorption_functions(variant, A):
         assert r1 == r2
         hits += r1
     assert 0 < hits < 400
+
+
+def test_chi_b_over_ranks_matches_reference():
+    """measure_chi_b of each rank of a P-rank run (azimuth 2 pi rank / P,
+    pot.c:2268), summed and divided by P as pot.c:2409-2418 does, against
+    the oracle's restatement."""
+    d = dict(SMALL, N=2049)
+    P = 4
+    base = _ref("sceptic").setup(params(d), seed=12)
+    base.set_grain(q=-150)
+    parts = base.particles()
+    samples = []
+    for k in range(P):
+        ref = RefLib("sceptic", build=False).setup(params(d), seed=12, init=False, nprocs=P, rank=k)
+        ref.set_particles(parts)
+        ref.set_grain(q=-150)
+        ref.build_tree()
+        samples.append(ref.measure_chi_b())
+    o = Oracle(params(d), mode="reference", seed=12, init=False)
+    o.set_particles(parts)
+    o.set_grain(q=-150)
+    o.build_tree()
+    assert o.lib().pto_measure_chi_b_ranks(o.h, P) == sum(samples) / P
+    assert o.lib().pto_measure_chi_b_ranks(o.h, 1) == o.measure_chi_b()
