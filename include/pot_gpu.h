@@ -245,6 +245,35 @@ int pot_gpu_launch_count(pot_gpu_ctx* ctx, uint64_t* n);
    has finished; returns the first device-side status seen. */
 int pot_gpu_sync(pot_gpu_ctx* ctx);
 
+/* Sums behind the macroscopic summary (write_macroscopic_data_to_file,
+   pot.c:3261-3508) over the plasma particles of the current state, in two
+   passes like the reference's, without downloading the particles.  FP64
+   with a fixed summation order (the reference uses long double). */
+typedef struct pot_macro_sums {
+	/* pass 1 */
+	double n_e, n_i;          /* electrons, ions */
+	double K_e;               /* sum 0.5 m_e |v|^2, electrons */
+	double s_e, s_i;          /* sum |v| */
+	double v_e[3], v_i[3];    /* sum v */
+	double am_e[3], am_i[3];  /* sum (r - c) x v, c the domain centre (times the mass gives the
+	                             angular momentum) */
+	double pad1[3];
+	/* pass 2, about the pass-1 means */
+	double sumsq_K_e, sum_x_e, sumsq_x_e;
+	double K_e_c[3];          /* sum (K - <K>)^k, k = 2, 3, 4, electrons */
+	double s_e_c[3];          /* sum (|v| - <|v|>)^k, k = 2, 3, 4, electrons */
+	double T_e;               /* sum |v - <v>|^2, electrons */
+	double sum_K_i, sumsq_K_i;
+	double s_i_c[3];          /* sum (|v| - <|v|>)^k, k = 2, 3, 4, ions */
+	double T_i;               /* sum |v - <v>|^2, ions */
+	double pad2[2];
+} pot_macro_sums;
+
+int pot_gpu_macro(pot_gpu_ctx* ctx, pot_macro_sums* out);
+
+/* The grain's state alone (pot_gpu_download without the particles). */
+int pot_gpu_grain(pot_gpu_ctx* ctx, pot_grain_state* grain);
+
 /* Device bytes a context with these settings allocates (no device work). */
 int pot_gpu_bytes_needed(const pot_run_cfg* cfg, const pot_gpu_opts* opts, uint64_t* bytes);
 

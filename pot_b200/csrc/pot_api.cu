@@ -36,6 +36,7 @@ struct pot_gpu_ctx {
 	uint2* groups = nullptr;
 	uint2* groups_all = nullptr;     // fast form, potential energies
 	double* epe_partial = nullptr;   // per-block / per-group partial sums
+	double* macro = nullptr;         // macroscopic-summary partials and sums
 	uint32_t* rein_list = nullptr;
 	uint32_t* inv = nullptr;
 	pot_particle* aos = nullptr;
@@ -545,6 +546,7 @@ static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu
 	if (fast) AL(c->groups_all, n);
 	AL(c->epe_partial, 3 * (size_t)(n > (uint32_t)EPE_BLOCKS ? n : (uint32_t)EPE_BLOCKS));
 	AL(c->rein_list, 2 * (size_t)n);
+	AL(c->macro, macro_scratch_doubles());
 	AL(c->inv, n);
 	AL(c->rec, 1);
 	AL(c->hist, HIST);
@@ -1002,6 +1004,38 @@ int pot_gpu_phi_at(pot_gpu_ctx* c, uint64_t n, const double* xyz, double* phi)
 	CK(cudaGetLastError());
 	CK(cudaMemcpyAsync(phi, c->q_out, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
 	return sync_status(c);
+}
+
+int pot_gpu_macro(pot_gpu_ctx* c, pot_macro_sums* out)
+{
+	static_assert(sizeof(pot_macro_sums) == 38 * sizeof(double), "two passes of 20 and 18 sums");
+	if (!c || !out) return POT_E_ARG;
+	if (!c->uploaded) return POT_E_STATE;
+	CK(cudaSetDevice(c->device));
+	launch_macro(c->pos[c->cur], c->vel[c->cur], c->P, c->macro, c->stream, c->timer);
+	CK(cudaGetLastError());
+	CK(cudaMemcpyAsync(out, c->macro + (macro_scratch_doubles() - 80), sizeof(pot_macro_sums),
+	                   cudaMemcpyDeviceToHost, c->stream));
+	return sync_status(c);
+}
+
+int pot_gpu_grain(pot_gpu_ctx* c, pot_grain_state* g)
+{
+	if (!c || !g) return POT_E_ARG;
+	if (!c->uploaded) return POT_E_STATE;
+	CK(cudaSetDevice(c->device));
+	const int st = sync_status(c);
+	RunRec r;
+	CK(cudaMemcpy(&r, c->rec, sizeof(r), cudaMemcpyDeviceToHost));
+	std::memset(g, 0, sizeof(*g));
+	g->q = r.grain_q;
+	g->m = r.grain_m;
+	g->x = r.grain_pos[0]; g->y = r.grain_pos[1]; g->z = r.grain_pos[2];
+	g->vx = r.grain_vel[0]; g->vy = r.grain_vel[1]; g->vz = r.grain_vel[2];
+	g->tot_absor_e = r.tot_absor_e;
+	g->t_steps = r.t_steps;
+	g->chi_b = r.chi_b;
+	return st;
 }
 
 int pot_gpu_kernel_times(pot_gpu_ctx* c, int max, const char** names, double* ms, uint64_t* launches)

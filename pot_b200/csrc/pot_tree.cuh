@@ -46,6 +46,9 @@ void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const 
                   uint32_t* block_sums, cudaStream_t s, Timer& tm);
 
 // walk.cu
+size_t macro_scratch_doubles();
+void launch_macro(const double4* pos, const double4* vel, const Params& P, double* scratch, cudaStream_t s,
+                  Timer& tm);
 void launch_chi_b(const TreeDev& T, const double4* src64, const Params& P, RunRec* rec, int force,
                   cudaStream_t s, Timer& tm);
 void launch_push(double4* pos, double4* vel, const TreeDev& T, const double4* src64, const float4* src32,

@@ -125,6 +125,8 @@ def load_library(path: str = LIB_PATH, build_if_stale: bool = True):
     L.pot_gpu_reset_kernel_times.argtypes = [vp]
     L.pot_gpu_sync.argtypes = [vp]
     L.pot_gpu_launch_count.argtypes = [vp, C.POINTER(u64)]
+    L.pot_gpu_macro.argtypes = [vp, C.POINTER(_MacroSums)]
+    L.pot_gpu_grain.argtypes = [vp, C.POINTER(_Grain)]
     L.pot_gpu_bytes_needed.argtypes = [C.POINTER(_RunCfg), C.POINTER(_Opts), C.POINTER(u64)]
     L.pot_gpu_tune.argtypes = [C.POINTER(_RunCfg), C.POINTER(_Opts), u32, C.POINTER(C.c_double)]
     L.pot_batch_create.argtypes = [C.POINTER(_BatchOpts), C.POINTER(vp)]
@@ -148,6 +150,15 @@ def load_library(path: str = LIB_PATH, build_if_stale: bool = True):
                 fn.restype = C.c_int
     _LIB = L
     return L
+
+
+class _MacroSums(C.Structure):
+    _fields_ = [("n_e", C.c_double), ("n_i", C.c_double), ("K_e", C.c_double), ("s_e", C.c_double),
+                ("s_i", C.c_double), ("v_e", C.c_double * 3), ("v_i", C.c_double * 3), ("am_e", C.c_double * 3),
+                ("am_i", C.c_double * 3), ("pad1", C.c_double * 3), ("sumsq_K_e", C.c_double),
+                ("sum_x_e", C.c_double), ("sumsq_x_e", C.c_double), ("K_e_c", C.c_double * 3),
+                ("s_e_c", C.c_double * 3), ("T_e", C.c_double), ("sum_K_i", C.c_double), ("sumsq_K_i", C.c_double),
+                ("s_i_c", C.c_double * 3), ("T_i", C.c_double), ("pad2", C.c_double * 2)]
 
 
 class _BatchOpts(C.Structure):
@@ -300,6 +311,23 @@ class Run:
         self._check(self.lib.pot_gpu_move_particles(self.h, _ptr(parts), len(parts), C.byref(g), C.byref(st)),
                     "pot_gpu_move_particles")
         return _grain_dict(g), _stats_dict(st)
+
+    def macro(self) -> dict:
+        """The macroscopic-summary sums of the current state, on the device."""
+        m = _MacroSums()
+        self._check(self.lib.pot_gpu_macro(self.h, C.byref(m)), "pot_gpu_macro")
+        out = {}
+        for k, t in _MacroSums._fields_:
+            if k.startswith("pad"):
+                continue
+            v = getattr(m, k)
+            out[k] = np.array(list(v)) if hasattr(v, "__len__") else v
+        return out
+
+    def grain(self) -> dict:
+        g = _Grain()
+        self._check(self.lib.pot_gpu_grain(self.h, C.byref(g)), "pot_gpu_grain")
+        return _grain_dict(g)
 
     # -- inspection ---------------------------------------------------------------
     def build_tree(self) -> int:

@@ -79,6 +79,7 @@ typedef struct {
 	unsigned int form, leaf, group;
 	uint64_t seed;
 	bool have_seed;
+	bool host_macro;  /* summary sums from downloaded particles instead of on the device */
 	char out_dir[4096];
 } Run;
 
@@ -152,6 +153,7 @@ static void usage(const char* prog)
 	e_puts("  --oap X  --bx T --by T --bz T  --no-sceptic  --disable-grain  --prolate  --oblate");
 	e_puts("GPU execution:");
 	e_puts("  --form fast|plain  --leaf N  --group 32|64  --seed S  --axis X,Y,Z  --output-dir DIR");
+	e_puts("  --host-macro  compute the summary from downloaded particles (default: on the device)");
 }
 
 static int want(int* n, int argc) { return ++(*n) < argc; }
@@ -173,6 +175,7 @@ static int parse_args(int argc, char** argv, Run* ru)
 			if (!strcmp(f, "--prolate") || !strcmp(f, "--oblate")) continue;
 			if (!strcmp(f, "--no-sceptic")) { ru->sceptic = false; continue; }
 			if (!strcmp(f, "--disable-grain")) { ru->disable_grain = true; continue; }
+			if (!strcmp(f, "--host-macro")) { ru->host_macro = true; continue; }
 			if (!want(&n, argc)) return 1;
 			const char* v = argv[n];
 			if (!strcmp(f, "--oap")) ru->oap = strtod(v, NULL);
@@ -476,96 +479,93 @@ static void central_moments(long double* cms, unsigned int N)
 	cms[3] -= 3.0;
 }
 
-static void write_macro(FILE* fp, const Run* ru, const pot_particle* P, const pot_grain_state* g,
-                        const long double epe[3], unsigned long step)
+/* The sums of both passes from downloaded particles, accumulated in long
+   double as pot.c:3354-3461 does (the --host-macro path). */
+static void host_macro_sums(const Run* ru, const pot_particle* P, pot_macro_sums* m)
 {
-	long double K_e[4] = { 0 }, s_e[4] = { 0 }, s_i[4] = { 0 };
-	long double v_e[3] = { 0 }, v_i[3] = { 0 }, am_e[3] = { 0 }, am_i[3] = { 0 }, lm_e[3], lm_i[3];
-	long double sum_K_ions = 0, sum_sq_K_elec = 0, sum_sq_K_ions = 0, sum_x_elec = 0, sum_sq_x_elec = 0;
-	double temp_e = 0, temp_i = 0;
-	unsigned int N_e = 0, N_i = 0;
+	long double a1[20] = { 0 }, a2[18] = { 0 };
 	const double cent = ru->r * ru->mpp;
-	const long double volume = (4.0 / 3.0) * PI * powl(ru->r * ru->mpp, 3.0);
 	const long double me = mass_of(ru, ELECTRON), mi = mass_of(ru, ION);
-	if (ru->N < 6 || !fp) return;
 	for (unsigned long k = 1; k < ru->N; k++) {
 		const pot_particle* p = &P[k];
 		const long double v = pythag(p->vx, p->vy, p->vz);
-		long double *vm, *am;
-		if (isnan(v)) {
-			fprintf(stderr, "Particle %lu (%g, %g, %g) has velocity (%g, %g, %g) at time step %lu.\n", k, p->x,
-			        p->y, p->z, p->vx, p->vy, p->vz, step);
-		}
-		if (p->species == ELECTRON) {
-			K_e[0] += 0.5 * me * v * v;
-			s_e[0] += v;
-			vm = v_e;
-			am = am_e;
-			N_e++;
+		const int e = p->species == ELECTRON;
+		const long double amx = ((p->y - cent) * p->vz) - ((p->z - cent) * p->vy);
+		const long double amy = -(((p->x - cent) * p->vz) - ((p->z - cent) * p->vx));
+		const long double amz = ((p->x - cent) * p->vy) - ((p->y - cent) * p->vx);
+		if (e) {
+			a1[0] += 1;
+			a1[2] += 0.5 * me * v * v;
+			a1[3] += v;
+			a1[5] += p->vx; a1[6] += p->vy; a1[7] += p->vz;
+			a1[11] += amx; a1[12] += amy; a1[13] += amz;
 		} else {
-			s_i[0] += v;
-			vm = v_i;
-			am = am_i;
-			N_i++;
+			a1[1] += 1;
+			a1[4] += v;
+			a1[8] += p->vx; a1[9] += p->vy; a1[10] += p->vz;
+			a1[14] += amx; a1[15] += amy; a1[16] += amz;
 		}
-		vm[0] += p->vx;
-		vm[1] += p->vy;
-		vm[2] += p->vz;
-		am[0] += ((p->y - cent) * p->vz) - ((p->z - cent) * p->vy);
-		am[1] -= ((p->x - cent) * p->vz) - ((p->z - cent) * p->vx);
-		am[2] += ((p->x - cent) * p->vy) - ((p->y - cent) * p->vx);
 	}
+	const long double Km = a1[2] / a1[0], sme = a1[3] / a1[0], smi = a1[4] / a1[1];
+	const long double ve[3] = { a1[5] / a1[0], a1[6] / a1[0], a1[7] / a1[0] };
+	const long double vi[3] = { a1[8] / a1[1], a1[9] / a1[1], a1[10] / a1[1] };
+	for (unsigned long k = 1; k < ru->N; k++) {
+		const pot_particle* p = &P[k];
+		const long double v = pythag(p->vx, p->vy, p->vz);
+		if (p->species == ELECTRON) {
+			const long double K = 0.5 * me * v * v, Ks = K - Km, vs = v - sme;
+			a2[0] += K * K;
+			a2[1] += p->x;
+			a2[2] += p->x * p->x;
+			a2[3] += Ks * Ks; a2[4] += Ks * Ks * Ks; a2[5] += Ks * Ks * Ks * Ks;
+			a2[6] += vs * vs; a2[7] += vs * vs * vs; a2[8] += vs * vs * vs * vs;
+			a2[9] += (p->vx - ve[0]) * (p->vx - ve[0]) + (p->vy - ve[1]) * (p->vy - ve[1]) +
+			         (p->vz - ve[2]) * (p->vz - ve[2]);
+		} else {
+			const long double K = 0.5 * mi * v * v, vs = v - smi;
+			a2[10] += K;
+			a2[11] += K * K;
+			a2[12] += vs * vs; a2[13] += vs * vs * vs; a2[14] += vs * vs * vs * vs;
+			a2[15] += (p->vx - vi[0]) * (p->vx - vi[0]) + (p->vy - vi[1]) * (p->vy - vi[1]) +
+			          (p->vz - vi[2]) * (p->vz - vi[2]);
+		}
+	}
+	double* out = (double*)m;
+	for (int k = 0; k < 20; k++) out[k] = (double)a1[k];
+	for (int k = 0; k < 18; k++) out[20 + k] = (double)a2[k];
+}
+
+/* One row of pot-macroscopic.dat from the sums (pot.c:3398-3508). */
+static void write_macro(FILE* fp, const Run* ru, const pot_macro_sums* m, const pot_grain_state* g,
+                        const long double epe[3], unsigned long step)
+{
+	if (ru->N < 6 || !fp) return;
+	const long double me = mass_of(ru, ELECTRON), mi = mass_of(ru, ION);
+	const unsigned int N_e = (unsigned int)m->n_e, N_i = (unsigned int)m->n_i;
+	const long double volume = (4.0 / 3.0) * PI * powl(ru->r * ru->mpp, 3.0);
+	long double K_e[4] = { m->K_e, m->K_e_c[0], m->K_e_c[1], m->K_e_c[2] };
+	long double s_e[4] = { m->s_e, m->s_e_c[0], m->s_e_c[1], m->s_e_c[2] };
+	long double s_i[4] = { m->s_i, m->s_i_c[0], m->s_i_c[1], m->s_i_c[2] };
+	long double lm_e[3], lm_i[3], am_e[3], am_i[3];
 	K_e[0] /= N_e;
 	s_e[0] /= N_e;
 	s_i[0] /= N_i;
 	for (int k = 0; k < 3; k++) {
-		v_e[k] /= N_e;
-		v_i[k] /= N_i;
-		am_e[k] *= me;
-		am_i[k] *= mi;
-		lm_e[k] = me * v_e[k];
-		lm_i[k] = mi * v_i[k];
-	}
-	for (unsigned long k = 1; k < ru->N; k++) {
-		const pot_particle* p = &P[k];
-		const long double v = pythag(p->vx, p->vy, p->vz);
-		const long double K = 0.5 * mass_of(ru, p->species) * v * v;
-		if (p->species == ELECTRON) {
-			sum_sq_K_elec += K * K;
-			sum_x_elec += p->x;
-			sum_sq_x_elec += p->x * p->x;
-			const long double Ks = K - K_e[0];
-			K_e[1] += Ks * Ks;
-			K_e[2] += Ks * Ks * Ks;
-			K_e[3] += Ks * Ks * Ks * Ks;
-			const long double vs = v - s_e[0];
-			s_e[1] += vs * vs;
-			s_e[2] += vs * vs * vs;
-			s_e[3] += vs * vs * vs * vs;
-			temp_e += (p->vx - v_e[0]) * (p->vx - v_e[0]);
-			temp_e += (p->vy - v_e[1]) * (p->vy - v_e[1]);
-			temp_e += (p->vz - v_e[2]) * (p->vz - v_e[2]);
-		} else {
-			sum_K_ions += K;
-			sum_sq_K_ions += K * K;
-			const long double vs = v - s_i[0];
-			s_i[1] += vs * vs;
-			s_i[2] += vs * vs * vs;
-			s_i[3] += vs * vs * vs * vs;
-			temp_i += (p->vx - v_i[0]) * (p->vx - v_i[0]);
-			temp_i += (p->vy - v_i[1]) * (p->vy - v_i[1]);
-			temp_i += (p->vz - v_i[2]) * (p->vz - v_i[2]);
-		}
+		lm_e[k] = me * ((long double)m->v_e[k] / N_e);
+		lm_i[k] = mi * ((long double)m->v_i[k] / N_i);
+		am_e[k] = (long double)m->am_e[k] * me;
+		am_i[k] = (long double)m->am_i[k] * mi;
 	}
 	central_moments(K_e, N_e);
 	central_moments(s_e, N_e);
 	central_moments(s_i, N_i);
-	temp_e *= (me / (3.0 * KB)) / N_e;
-	temp_i *= (mi / (3.0 * KB)) / N_i;
+	const double temp_e = m->T_e * (me / (3.0 * KB)) / N_e;
+	const double temp_i = m->T_i * (mi / (3.0 * KB)) / N_i;
+	const long double sum_x_elec = m->sum_x_e, sum_sq_x_elec = m->sumsq_x_e;
 	const long double debye = sqrtl(EPSILON0 * KB * temp_e / ((N_e / volume) * QE * QE));
 	fprintf(fp, "%.7Lg %Lg ", step * ru->dt, K_e[0]);
 	if (isnt_weird(epe[ELECTRON])) fprintf(fp, "%Lg ", epe[ELECTRON] / N_e); else fputs("NA ", fp);
-	fprintf(fp, "%Lg ", sum_K_ions / N_i);
+	fprintf(fp, "%Lg ", (long double)m->sum_K_i / N_i);
 	if (isnt_weird(epe[ION])) fprintf(fp, "%Lg ", epe[ION] / N_i); else fputs("NA ", fp);
 	fprintf(fp, "%Lg ", 0.5 * (long double)g->m * hypot(g->vx, hypot(g->vy, g->vz)));
 	if (isnt_weird(epe[DUST])) fprintf(fp, "%Lg ", epe[DUST]); else fputs("NA ", fp);
@@ -578,6 +578,23 @@ static void write_macro(FILE* fp, const Run* ru, const pot_particle* P, const po
 	        s_i[2], s_i[3], temp_e, temp_i, lm_e[0], lm_e[1], lm_e[2], lm_i[0], lm_i[1], lm_i[2], am_e[0], am_e[1],
 	        am_e[2], am_i[0], am_i[1], am_i[2], (unsigned int)g->tot_absor_e);
 	if (fflush(fp)) e_puts("Can't force write of macroscopic summary data to disk.");
+}
+
+/* a record step's row: on-device sums (default) or from downloaded particles */
+static int record_row(FILE* fp, const Run* ru, pot_gpu_ctx* ctx, pot_particle* P, pot_grain_state* g,
+                      const long double epe[3], unsigned long step)
+{
+	pot_macro_sums m;
+	int rc;
+	if (ru->host_macro) {
+		if ((rc = pot_gpu_download(ctx, P, g)) != POT_OK) return rc;
+		host_macro_sums(ru, P, &m);
+	} else {
+		if ((rc = pot_gpu_macro(ctx, &m)) != POT_OK) return rc;
+		if ((rc = pot_gpu_grain(ctx, g)) != POT_OK) return rc;
+	}
+	write_macro(fp, ru, &m, g, epe, step);
+	return POT_OK;
 }
 
 /* ---- pot-phi.dat (pot.c:3001-3042) -------------------------------------- */
@@ -936,16 +953,16 @@ int main(int argc, char** argv)
 			if ((rc = pot_gpu_download(ctx, P, &g)) != POT_OK) { status = fail(ctx, t, rc); break; }
 			if ((rc = write_phi(&ru, ctx, &g, t)) != POT_OK) { status = fail(ctx, t, rc); break; }
 		}
-		if (rec) {
-			if ((rc = pot_gpu_download(ctx, P, &g)) != POT_OK) { status = fail(ctx, t, rc); break; }
-			write_macro(fp_macro, &ru, P, &g, epe, t);
+		if (rec && (rc = record_row(fp_macro, &ru, ctx, P, &g, epe, t)) != POT_OK) {
+			status = fail(ctx, t, rc);
+			break;
 		}
 		recorded_last = rec;
 		if (ru.tim_lim > 0.0 && (time(NULL) - start) > (60 * ru.tim_lim)) break;
 	}
-	if (status == EXIT_SUCCESS && (pot_gpu_download(ctx, P, &g) == POT_OK)) {
-		if (ru.sw_path) write_state(&ru, ru.sw_path, P, &g, epe, seed);
-		if (!recorded_last) write_macro(fp_macro, &ru, P, &g, epe, t);
+	if (status == EXIT_SUCCESS) {
+		if (ru.sw_path && pot_gpu_download(ctx, P, &g) == POT_OK) write_state(&ru, ru.sw_path, P, &g, epe, seed);
+		if (!recorded_last) record_row(fp_macro, &ru, ctx, P, &g, epe, t);
 	}
 	if (fp_macro) fclose(fp_macro);
 	pot_gpu_destroy(ctx);
