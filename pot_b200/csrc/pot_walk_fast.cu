@@ -143,6 +143,22 @@ __device__ __forceinline__ void eval_src(Acc<2>& E, const TgtE<2>& t, const floa
 	}
 }
 
+__device__ __forceinline__ void add_xor(Acc<1>& E, int o)
+{
+	E.x += __shfl_xor_sync(0xffffffffu, E.x, o);
+	E.y += __shfl_xor_sync(0xffffffffu, E.y, o);
+	E.z += __shfl_xor_sync(0xffffffffu, E.z, o);
+}
+__device__ __forceinline__ void add_xor(Acc<2>& E, int o)
+{
+	E.x.x += __shfl_xor_sync(0xffffffffu, E.x.x, o);
+	E.x.y += __shfl_xor_sync(0xffffffffu, E.x.y, o);
+	E.y.x += __shfl_xor_sync(0xffffffffu, E.y.x, o);
+	E.y.y += __shfl_xor_sync(0xffffffffu, E.y.y, o);
+	E.z.x += __shfl_xor_sync(0xffffffffu, E.z.x, o);
+	E.z.y += __shfl_xor_sync(0xffffffffu, E.z.y, o);
+}
+
 __device__ __forceinline__ void to_eval(const Targets<1>& tg, TgtE<1>& t, Acc<1>& E)
 {
 	t.x = tg.t[0].x;
@@ -189,10 +205,16 @@ __device__ __forceinline__ Field<2> from_eval(const Acc<2>& E)
 // subtracted at the end.  The softening is floored at 1e-20 R^2 (far below
 // FP32 resolution of positions) so that the term is finite when a target sits
 // exactly on its own particle.
+//
+// Split lists (one target per lane).  A group of at most 16 (8) targets
+// would leave half (three quarters) of the warp idle during evaluation, so
+// the lanes are split instead: lane l holds member l mod 32/split and
+// evaluates the staged entries with index = sub (mod split), sub = l div
+// 32/split; the split partial fields are added across lanes at the end.
 template <int TPL, bool POT = false>
 __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const float4* __restrict__ src32,
                                  const Params& P, FastSmem<TPL>& sm, uint32_t& n_eval, uint32_t& stack_max,
-                                 int& err)
+                                 int& err, int split = 1)
 {
 	const uint32_t lane = lane_f();
 	uint32_t smin = 0xFFFFFFFFu, smax = 0u;
@@ -232,6 +254,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 	}
 	const float eps2 = fmaxf(P.soft2_f, 1e-20f);
 	const bool single_leaves = P.leaf_size == 1;
+	const int sub = (int)lane / (32 / split);  // this lane's share of each staged list
 	TgtE<TPL> te;
 	Acc<TPL> E;
 	to_eval(tg, te, E);
@@ -318,12 +341,21 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		// flush staged monopoles, padded to a multiple of 8 with zero-charge
 		// cells far outside the domain so the loop needs no remainder
 		if (ncell >= FW_CELL_FLUSH || (done && ncell > 0)) {
-			const int padded = (ncell + 7) & ~7;
+			const int unit = 8 * split;
+			const int padded = (ncell + unit - 1) / unit * unit;
 			if ((int)lane < padded - ncell) stage_src(sm.cells, ncell + lane, make_float4(64.f, 64.f, 64.f, 0.f), tag);
 			__syncwarp();
-			for (int j = 0; j < padded; j += 8) {
+			if (split == 1) {
+				for (int j = 0; j < padded; j += 8) {
 #pragma unroll
-				for (int u = 0; u < 8; u++) eval_src<false, POT>(E, te, sm.cells, j + u, eps2);
+					for (int u = 0; u < 8; u++) eval_src<false, POT>(E, te, sm.cells, j + u, eps2);
+				}
+			} else {
+				const int per = padded / split;
+				for (int j = 0; j < per; j += 8) {
+#pragma unroll
+					for (int u = 0; u < 8; u++) eval_src<false, POT>(E, te, sm.cells, (j + u) * split + sub, eps2);
+				}
 			}
 			n_cells_ev += ncell;
 			ncell = 0;
@@ -355,8 +387,14 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 				}
 				stage_src(sm.pbuf, (int)lane, p, tag);
 				__syncwarp();
+				if (split == 1) {
 #pragma unroll 16
-				for (int m = 0; m < 32; m++) eval_src<true, POT>(E, te, sm.pbuf, m, eps2);
+					for (int m = 0; m < 32; m++) eval_src<true, POT>(E, te, sm.pbuf, m, eps2);
+				} else {
+					const int per = 32 / split;
+#pragma unroll 8
+					for (int m = 0; m < per; m++) eval_src<true, POT>(E, te, sm.pbuf, m * split + sub, eps2);
+				}
 				__syncwarp();
 			}
 			n_parts_ev += total;
@@ -364,6 +402,9 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			__syncwarp();
 		}
 		if (done) break;
+	}
+	if (split > 1) {  // add the split partial fields (lanes l, l ^ 16, l ^ 8, ... share a member)
+		for (int o = 16; o >= 32 / split; o >>= 1) add_xor(E, o);
 	}
 	Field<TPL> F = from_eval(E);
 	// take back the members' own terms
@@ -509,9 +550,14 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 		Targets<TPL> tg;
 		uint32_t slot[TPL];
 		double3 h[TPL];
+		// small groups split the warp (see group_walk): lanes past the
+		// first 32 / split hold copies of members and push nothing
+		const int split = TPL == 1 ? (grp.y <= 8 ? 4 : (grp.y <= 16 ? 2 : 1)) : 1;
+		const uint32_t width = 32u / (uint32_t)split;
+		const bool owner = lane_f() < width;
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
-			const uint32_t m = lane_f() + 32u * k;
+			const uint32_t m = (lane_f() & (width - 1u)) + 32u * k;
 			tg.valid[k] = m < grp.y;
 			slot[k] = 0xFFFFFFFFu;
 			h[k] = make_double3(P.rad, P.rad, P.rad);
@@ -528,7 +574,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 		}
 		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, depth, err);
+		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, depth, err, split);
 		stack_max = max(stack_max, depth);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
@@ -536,7 +582,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 		}
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
-			if (!tg.valid[k]) continue;
+			if (!tg.valid[k] || !owner) continue;
 			const uint32_t s = slot[k];
 			const double4 p = pos[s];
 			double4 v = vel[s];
@@ -670,9 +716,12 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 		const uint2 grp = groups[g];
 		Targets<TPL> tg;
 		float qme[TPL];
+		const int split = TPL == 1 ? (grp.y <= 8 ? 4 : (grp.y <= 16 ? 2 : 1)) : 1;
+		const uint32_t width = 32u / (uint32_t)split;
+		const bool owner = lane_f() < width;
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
-			const uint32_t m = lane_f() + 32u * k;
+			const uint32_t m = (lane_f() & (width - 1u)) + 32u * k;
 			tg.valid[k] = m < grp.y;
 			tg.self[k] = tg.valid[k] ? grp.x + m : 0xFFFFFFFFu;
 			const float4 me = tg.valid[k] ? src32[grp.x + m] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -681,7 +730,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 		}
 		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> f = group_walk<TPL, true>(tg, T, src32, P, sm, ne, depth, err);
+		const Field<TPL> f = group_walk<TPL, true>(tg, T, src32, P, sm, ne, depth, err, split);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
 			break;
@@ -689,7 +738,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 		double acc[3] = { 0.0, 0.0, 0.0 };
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
-			if (!tg.valid[k]) continue;
+			if (!tg.valid[k] || !owner) continue;
 			const uint32_t slot = tg.self[k];
 			double phi = (double)f.x[k] * pscale;
 			if (slot == gs) {

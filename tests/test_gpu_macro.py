@@ -80,3 +80,26 @@ def test_host_program_rows_agree_between_paths(tmp_path):
     # skewness cancel: compare each column against its own scale
     scale = np.abs(B).max(0)
     assert np.all(np.abs(A - B) <= 1e-5 * scale + 1e-300), np.abs(A - B).max(0) / (scale + 1e-300)
+
+
+def test_grain_charging_fast_matches_plain():
+    """The FP32-walk fast form charges the grain like the plain FP64 form:
+    over four seeds, the grain charge averaged over steps 1001-3000 (from the
+    device-side charge sums) agrees within three standard errors of the
+    seed-to-seed spread, or 1 %."""
+    from pot_b200.configs import run_config as cfg_of
+    cfg = cfg_of("1m", N=20001)
+    means = {}
+    for form in ("fast", "plain"):
+        vals = []
+        for seed in (11, 12, 13, 14):
+            with Run(cfg, form=form, seed=seed) as r:
+                r.init_particles()
+                a = r.step(1000)["q_sum"]
+                b = r.step(2000)["q_sum"]
+            vals.append((b - a) / 2000.0)
+        means[form] = np.array(vals)
+    f, p = means["fast"], means["plain"]
+    assert np.all(f < 0) and np.all(p < 0)
+    se = np.sqrt(f.var(ddof=1) / len(f) + p.var(ddof=1) / len(p))
+    assert abs(f.mean() - p.mean()) <= max(3 * se, 0.01 * abs(p.mean())), (f, p)
