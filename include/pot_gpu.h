@@ -83,7 +83,9 @@ typedef struct pot_run_cfg {
 typedef struct pot_gpu_opts {
 	uint32_t form;        /* POT_FORM_PLAIN or POT_FORM_FAST */
 	uint32_t leaf_size;   /* particles per leaf; 1 in POT_FORM_PLAIN (the reference's tree) */
-	uint32_t group_size;  /* POT_FORM_FAST: largest target group per warp, 32 (default) or 64 */
+	uint32_t group_size;  /* POT_FORM_FAST: largest target group per warp: 8, 16, 32 (default) or 64;
+	                         groups of at most 16 (8) share each warp between 2 (4) lanes per
+	                         target, 64 puts two targets on each lane */
 	uint32_t flags;       /* POT_OPT_* */
 	int32_t device;       /* CUDA device ordinal */
 	uint32_t chi_b_ranks; /* SCEPTIC edge potential: the mean over this many equally spaced

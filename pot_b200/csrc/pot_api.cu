@@ -235,9 +235,13 @@ static int fill_params(pot_gpu_ctx* c)
 	P.leaf_size = c->opts.leaf_size;
 	P.flags = r.flags;
 	P.form = c->opts.form;
-	P.max_level = c->opts.form == POT_FORM_FAST ? 16u : (uint32_t)MAX_LEVELS;
+	// Fast form: bucket leaves of 8 or more need few levels (a level-10 cell holds on
+	// average N / 5.6e8 particles, 0.03 at the largest N), and 30 key bits sort in
+	// four passes; smaller leaves keep 16 levels.  A cell at the deepest level is a
+	// leaf whatever its count.
+	P.max_level = c->opts.form == POT_FORM_FAST ? (c->opts.leaf_size >= 8 ? 10u : 16u) : (uint32_t)MAX_LEVELS;
 	P.key_bits = c->opts.form == POT_FORM_FAST ? 63u - 3u * P.max_level : 0u;
-	P.group_max = c->opts.group_size == 64 ? 64u : 32u;
+	P.group_max = c->opts.group_size ? c->opts.group_size : 32u;
 	P.chi_ranks = c->opts.chi_b_ranks ? c->opts.chi_b_ranks : 1u;
 	if (P.chi_ranks > 64) return POT_E_ARG;
 	P.seed = c->opts.seed;
@@ -474,7 +478,8 @@ static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu
 	if (o.leaf_size == 0) o.leaf_size = o.form == POT_FORM_PLAIN ? 1 : 16;
 	if (o.form == POT_FORM_PLAIN && o.leaf_size != 1) return POT_E_ARG;
 	if (o.leaf_size > 64) return POT_E_ARG;
-	if (o.group_size != 0 && o.group_size != 32 && o.group_size != 64) return POT_E_ARG;
+	if (o.group_size != 0 && o.group_size != 8 && o.group_size != 16 && o.group_size != 32 && o.group_size != 64)
+		return POT_E_ARG;
 	// aspect ratio: 0 (sphere), > 1 (prolate) or in (0, 1) (oblate)
 	if (!(cfg->A == 0.0 || cfg->A > 1.0 || (cfg->A > 0.0 && cfg->A < 1.0))) return POT_E_ARG;
 	// scans cover 2^24; the tree needs more sources than a leaf holds
