@@ -74,10 +74,26 @@ typedef struct pot_run_cfg {
 	                     whose grain stays out of the tree and whose m_i/m_e is 1836.153) */
 	double axis[3];   /* spheroid symmetry axis; zero = x, the reference's.  Any other
 	                     direction tilts the grain (no counterpart in the reference) */
+	double bounce;    /* OUT_BOUNCE (pot.c:113-119, 2036-2069): the domain wall's coefficient of
+	                     restitution, in (0, 1]; 0 = particles that leave are reinjected (the
+	                     default program) */
+	uint32_t integrator;  /* POT_INT_*: the particle integrator (pot.c:121-133) */
+	uint32_t pad;
 } pot_run_cfg;
 
 #define POT_CFG_SCEPTIC 0x1u        /* SCEPTIC_REINJECTION (pot.c:181): flux-weighted reinjection */
 #define POT_CFG_DISABLE_GRAIN 0x2u  /* DISABLE_GRAIN (pot.c:30): no absorption */
+#define POT_CFG_DIPOLES 0x4u        /* DIPOLES (pot.c:99-104): cells carry dipole moments about their
+                                       centre of charge, used in fields and potentials; plain form */
+#define POT_CFG_POIS_IONS 0x8u      /* POIS_POS_COLLECTION (pot.c:165-173, 2837-2854): absorbed ions
+                                       add no charge; each step after the settling time the grain
+                                       gains a Poisson number of elementary charges at the OML ion
+                                       flux of the cached ion temperature (pot_gpu_set_ion_temp) */
+
+#define POT_INT_BORIS 0u             /* BORIS (pot.c:132, 2472-2532), the default program */
+#define POT_INT_VERLET 1u            /* BORIS off: velocity Verlet, two field evaluations per step
+                                        (pot.c:2533-2639) */
+#define POT_INT_EULER_RICHARDSON 2u  /* EULER_RICHARDSON (pot.c:127): midpoint (RK2) form */
 
 /* Execution options (no counterpart in the reference). */
 typedef struct pot_gpu_opts {
@@ -137,8 +153,12 @@ typedef struct pot_step_stats {
 	                          chi_b rejection, 8 NaN-alpha retries, 16 orbit-integral
 	                          halvings, 32 the initial shell radius, 64 no speed
 	                          distribution for the edge potential (the reference's inverse
-	                          CDF is NaN there and it retries without end) */
-	uint32_t pad2;
+	                          CDF is NaN there and it retries without end); 128 a particle in
+	                          the domain wall moving inwards (OUT_BOUNCE, the reference's
+	                          warning at pot.c:2719-2722); 256 the Poisson variate's cap */
+	uint32_t n_collected;  /* POT_CFG_POIS_IONS: charges the Poisson ion collection added */
+	uint32_t n_wall;       /* OUT_BOUNCE: particles found outside moving inwards, left in place */
+	uint32_t n_bounced;    /* OUT_BOUNCE: particles bounced off the wall */
 } pot_step_stats;
 
 /* capacity of the fast form's per-warp stack of cells awaiting a test;
@@ -275,6 +295,14 @@ int pot_gpu_macro(pot_gpu_ctx* ctx, pot_macro_sums* out);
 
 /* The grain's state alone (pot_gpu_download without the particles). */
 int pot_gpu_grain(pot_gpu_ctx* ctx, pot_grain_state* grain);
+
+/* POT_CFG_POIS_IONS: the cached ion temperature (Proc.Ti, K) that sets the
+   collection rate.  It starts at cfg->Ti (pot.c:4252); pot_gpu_macro
+   replaces it with the ions' measured temperature, as the reference's
+   macroscopic summary does (pot.c:3442-3448); a caller that computes the
+   summary itself sets it here. */
+int pot_gpu_set_ion_temp(pot_gpu_ctx* ctx, double Ti);
+int pot_gpu_ion_temp(pot_gpu_ctx* ctx, double* Ti);
 
 /* Device bytes a context with these settings allocates (no device work). */
 int pot_gpu_bytes_needed(const pot_run_cfg* cfg, const pot_gpu_opts* opts, uint64_t* bytes);

@@ -27,6 +27,10 @@ Two things are built here, both with gcc, both outside the GPU product path:
                   ``#define GL`` taken out -- no graphics stack is needed or
                   used -- PROLATE or OBLATE selected, SCEPTIC_REINJECTION on
                   or off); the aspect ratio A is set at run time.
+   Feature suffixes switch on the reference's other variants, on either
+   program: ``_dip`` DIPOLES, ``_bounce`` OUT_BOUNCE 0.95, ``_pois``
+   POIS_POS_COLLECTION, ``_verlet`` BORIS off (velocity Verlet), ``_er``
+   BORIS off and EULER_RICHARDSON on -- e.g. ``sceptic_dip``.
    In all, OAP and EXTERNAL_B_{X,Y,Z} become run-time globals
    (``pot_ref_oap``, ``pot_ref_b{x,y,z}``) so one library serves every
    opening angle and field; C evaluates ``OAP * OAP * dist2`` identically for
@@ -49,6 +53,34 @@ DEFAULT_REF_ROOT = os.environ.get("POT_REFERENCE_ROOT", "/root/reference")
 
 VARIANTS = ("sphere", "sceptic")
 SPHEROID_VARIANTS = ("prolate", "prolate_sceptic", "oblate", "oblate_sceptic")
+FEATURES = ("dip", "bounce", "pois", "verlet", "er")
+FEATURE_VARIANTS = tuple("sceptic_" + f for f in FEATURES)
+
+
+def split_variant(variant: str):
+    """(program variant, feature list): 'sceptic_dip' -> ('sceptic', ['dip'])."""
+    parts = variant.split("_")
+    feats = []
+    while parts and parts[-1] in FEATURES:
+        feats.insert(0, parts.pop())
+    return "_".join(parts), feats
+
+
+def _patch_features(t: str, feats, sub1) -> str:
+    """Switch on the commented-out variant defines (pot.c:99-133, 165-173;
+    pot-spheroid.c:97-180 has the same lines)."""
+    for f in feats:
+        if f == "dip":
+            t = sub1(r"^(/\*\n#define DIPOLES\n\*/)$", r"\1\n#define DIPOLES", t)
+        elif f == "bounce":
+            t = sub1(r"^(/\*\n#define OUT_BOUNCE 0\.95\n\*/)$", r"\1\n#define OUT_BOUNCE 0.95", t)
+        elif f == "pois":
+            t = sub1(r"^(/\*\n#define POIS_POS_COLLECTION\n\*/)$", r"\1\n#define POIS_POS_COLLECTION", t)
+        elif f in ("verlet", "er"):
+            t = sub1(r"^#define BORIS\s*$", "/* BORIS switched off by the oracle recipe */", t)
+            if f == "er":
+                t = sub1(r"^(/\*\n#define EULER_RICHARDSON\n\*/)$", r"\1\n#define EULER_RICHARDSON", t)
+    return t
 
 CFLAGS = ["-O2", "-std=c99", "-fPIC", "-shared", "-Wall", "-Wno-unused-function",
           "-Wno-unused-variable", "-Wno-unused-but-set-variable", "-Wno-format",
@@ -106,8 +138,10 @@ def _patch_pot_c(text: str, variant: str) -> str:
     t = sub1(r"^#define EXTERNAL_B_Z 0\.0\s*$", "#define EXTERNAL_B_Z pot_ref_bz", t)
     # SPHERICAL sits commented out (pot.c:109-111); define it right after.
     t = sub1(r"^(/\*\n#define SPHERICAL\n\*/)$", r"\1\n#define SPHERICAL", t)
-    if variant == "sceptic":
+    base, feats = split_variant(variant)
+    if base == "sceptic":
         t = sub1(r"^(/\*\n#define SCEPTIC_REINJECTION\n\*/)$", r"\1\n#define SCEPTIC_REINJECTION", t)
+    t = _patch_features(t, feats, sub1)
     header = ("/* Generated by oracle/build.py from the reference pot.c; variant %s. */\n"
               "extern double pot_ref_oap, pot_ref_bx, pot_ref_by, pot_ref_bz;\n" % variant)
     return header + t
@@ -130,8 +164,10 @@ def _patch_spheroid_c(text: str, variant: str) -> str:
     t = sub1(r"^#define EXTERNAL_B_X 0\.0\s*$", "#define EXTERNAL_B_X pot_ref_bx", t)
     t = sub1(r"^#define EXTERNAL_B_Y 0\.0\s*$", "#define EXTERNAL_B_Y pot_ref_by", t)
     t = sub1(r"^#define EXTERNAL_B_Z 0\.0\s*$", "#define EXTERNAL_B_Z pot_ref_bz", t)
-    if not variant.endswith("_sceptic"):
+    base, feats = split_variant(variant)
+    if not base.endswith("_sceptic"):
         t = sub1(r"^#define SCEPTIC_REINJECTION\s*$", "/* SCEPTIC_REINJECTION switched off by the oracle recipe */", t)
+    t = _patch_features(t, feats, sub1)
     if variant.startswith("oblate"):
         t = sub1(r"^#define PROLATE\s*$", "/* PROLATE switched off by the oracle recipe */\n#define OBLATE", t)
     header = ("/* Generated by oracle/build.py from the reference pot-spheroid.c; variant %s. */\n"
@@ -156,7 +192,7 @@ def build_ref(ref_root: str = DEFAULT_REF_ROOT, force: bool = False, variants=VA
         os.makedirs(srcdir, exist_ok=True)
         patched = os.path.join(srcdir, "pot.c")
         lib = ref_lib_path(v)
-        spheroid = v in SPHEROID_VARIANTS
+        spheroid = split_variant(v)[0] in SPHEROID_VARIANTS
         pot_c = os.path.join(ref_root, "pot-spheroid.c" if spheroid else "pot.c")
         deps = [pot_c, prng_c, harness, stub, __file__]
         if force or _stale(lib, deps) or not os.path.exists(patched):

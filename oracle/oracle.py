@@ -65,10 +65,15 @@ class RunParams:
     ``A`` is pot-spheroid.c's aspect ratio (Run.A, pot-spheroid.c:376-378;
     0 = the spherical grain of pot.c) and ``axis`` the spheroid's symmetry
     axis (x in the reference; any other unit vector is this project's
-    extension, unpinned)."""
+    extension, unpinned).  The reference's other compile-time variants:
+    ``bounce`` (OUT_BOUNCE, the wall's coefficient of restitution; 0 =
+    reinjection), ``integrator`` (0 Boris, 1 velocity Verlet, 2
+    Euler-Richardson), ``dipoles`` (DIPOLES) and ``pois_ions``
+    (POIS_POS_COLLECTION)."""
 
     def __init__(self, N, r, dt, mpp, soft, Te, Ti, x_drift=0.0, a=2.5e-6, settle=0.0,
-                 theta=0.5, B=(0.0, 0.0, 0.0), A=0.0, axis=(1.0, 0.0, 0.0)):
+                 theta=0.5, B=(0.0, 0.0, 0.0), A=0.0, axis=(1.0, 0.0, 0.0), bounce=0.0, integrator=0,
+                 dipoles=False, pois_ions=False):
         self.N = int(N)
         self.r = int(r)
         self.dt = float(dt)
@@ -84,11 +89,21 @@ class RunParams:
         self.A = float(A)
         self.axis = tuple(float(u) for u in axis)
         self.shape = shape_of(self.A)
+        self.bounce = float(bounce)
+        self.integrator = int(integrator)
+        self.dipoles = bool(dipoles)
+        self.pois_ions = bool(pois_ions)
 
     def as_dict(self):
         return dict(N=self.N, r=self.r, dt=self.dt, mpp=self.mpp, soft=self.soft, Te=self.Te,
                     Ti=self.Ti, x_drift=self.x_drift, a=self.a, settle=self.settle,
-                    theta=self.theta, B=list(self.B), A=self.A, axis=list(self.axis))
+                    theta=self.theta, B=list(self.B), A=self.A, axis=list(self.axis), bounce=self.bounce,
+                    integrator=self.integrator, dipoles=self.dipoles, pois_ions=self.pois_ions)
+
+    def variant_flags(self) -> int:
+        """The bits of the reference harness's potref_variant_flags."""
+        return ((1 if self.dipoles else 0) | (2 if self.bounce else 0) | (4 if self.pois_ions else 0)
+                | (8 if self.integrator else 0) | (16 if self.integrator == 2 else 0))
 
 
 def _ptr(a, t=C.c_void_p):
@@ -151,6 +166,16 @@ class RefLib:
         L.potref_get_epe.argtypes = [C.c_void_p]
         L.potref_set_aspect.argtypes = [C.c_double]
         L.potref_set_aspect.restype = None
+        self.variant_flags = int(L.potref_variant_flags())
+        L.potref_bounce.restype = C.c_double
+        self.bounce = float(L.potref_bounce())
+        if self.variant_flags & 4:
+            L.potref_set_ion_temp.argtypes = [C.c_double]
+            L.potref_ion_temp.restype = C.c_double
+            L.potref_pos_rate_const.restype = C.c_double
+        if self.variant_flags & 1:
+            L.potref_tree_dipoles.argtypes = [C.c_ulong, C.c_void_p]
+            L.potref_tree_dipoles.restype = C.c_long
         self.shape = int(L.potref_shape())
         self.grain_enabled = bool(L.potref_grain_enabled())
         self.sceptic = bool(L.potref_has_sceptic())
@@ -173,6 +198,8 @@ class RefLib:
         words = splitmix64_words(seed)
         if p.shape != self.shape:
             raise ValueError("run shape %d does not match the %s program" % (p.shape, self.variant))
+        if p.variant_flags() != self.variant_flags or (p.bounce and p.bounce != self.bounce):
+            raise ValueError("run variants do not match the %s program" % self.variant)
         if self.shape:
             if p.axis != (1.0, 0.0, 0.0):
                 raise ValueError("the reference's spheroid axis is x")
@@ -290,6 +317,23 @@ class RefLib:
     def measure_chi_b(self):
         return self.lib.potref_measure_chi_b()
 
+    def set_ion_temp(self, Ti):
+        self.lib.potref_set_ion_temp(float(Ti))
+
+    def ion_temp(self):
+        return self.lib.potref_ion_temp()
+
+    def pos_rate_const(self):
+        return self.lib.potref_pos_rate_const()
+
+    def tree_dipoles(self):
+        mx = 9 * self.N + 16
+        out = np.zeros((mx, 3))
+        n = self.lib.potref_tree_dipoles(mx, _ptr(out))
+        if n < 0:
+            raise RuntimeError("tree dump overflow")
+        return out[:n]
+
 
 class _PtoCfg(C.Structure):
     _fields_ = [("N", C.c_uint64), ("r", C.c_uint32), ("dt", C.c_double), ("mpp", C.c_double),
@@ -297,7 +341,9 @@ class _PtoCfg(C.Structure):
                 ("x_drift", C.c_double), ("a", C.c_double), ("settle", C.c_double),
                 ("theta", C.c_double), ("B", C.c_double * 3), ("sceptic", C.c_int32),
                 ("quirk", C.c_int32), ("rng", C.c_int32), ("pad", C.c_int32), ("seed", C.c_uint64),
-                ("shape", C.c_int32), ("chi_ranks", C.c_int32), ("A", C.c_double), ("axis", C.c_double * 3)]
+                ("shape", C.c_int32), ("chi_ranks", C.c_int32), ("A", C.c_double), ("axis", C.c_double * 3),
+                ("bounce", C.c_double), ("integrator", C.c_int32), ("dipoles", C.c_int32),
+                ("pois_ions", C.c_int32), ("pad2", C.c_int32)]
 
 
 WELL_DTYPE = np.dtype([("abcd", "<u4", 4), ("index", "<u4"), ("state", "<u4", 16)])
@@ -362,6 +408,14 @@ class Oracle:
             L.pto_integrate_for_alpha.argtypes = [d, d, d, d]
             L.pto_integrate_for_alpha.restype = d
             L.pto_philox4x32.argtypes = [vp, vp, vp]
+            L.pto_set_ion_temp.argtypes = [vp, d]
+            L.pto_ion_temp.argtypes = [vp]
+            L.pto_ion_temp.restype = d
+            L.pto_poisson.argtypes = [vp, d]
+            L.pto_poisson.restype = u32
+            L.pto_tree_dipoles.argtypes = [vp, u64, vp]
+            L.pto_tree_dipoles.restype = C.c_int64
+            L.pto_last_step_variant_stats.argtypes = [vp, vp, vp]
             assert L.pto_sizeof_particle() == 56
             cls._lib = L
         return cls._lib
@@ -383,6 +437,10 @@ class Oracle:
         cfg.A = p.A
         for k in range(3):
             cfg.axis[k] = p.axis[k]
+        cfg.bounce = p.bounce
+        cfg.integrator = p.integrator
+        cfg.dipoles = 1 if p.dipoles else 0
+        cfg.pois_ions = 1 if p.pois_ions else 0
         self.cfg = cfg
         self.params = p
         self.mode = mode
@@ -528,6 +586,30 @@ class Oracle:
                                        C.byref(npush), _ptr(epe))
         return dict(dq=dq.value, de=de.value, n_absorbed=na.value, n_reinjected=nr.value,
                     n_pushed=npush.value, epe=epe)
+
+    def variant_stats(self):
+        """Charges the Poisson ion collection added, and particles found in
+        the wall moving inwards (OUT_BOUNCE), in the last step."""
+        a, b = C.c_uint32(), C.c_uint32()
+        self.lib().pto_last_step_variant_stats(self.h, C.byref(a), C.byref(b))
+        return dict(n_pois=a.value, n_wall=b.value)
+
+    def set_ion_temp(self, Ti):
+        self.lib().pto_set_ion_temp(self.h, float(Ti))
+
+    def ion_temp(self):
+        return self.lib().pto_ion_temp(self.h)
+
+    def poisson(self, lam):
+        return self.lib().pto_poisson(self.h, float(lam))
+
+    def tree_dipoles(self):
+        mx = 9 * self.N + 16
+        out = np.zeros((mx, 3))
+        n = self.lib().pto_tree_dipoles(self.h, mx, _ptr(out))
+        if n < 0:
+            raise RuntimeError("tree dump overflow")
+        return out[:n]
 
     def sample_reinject(self, n, species):
         out = np.zeros(int(n), PARTICLE_DTYPE)

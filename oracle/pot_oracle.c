@@ -52,6 +52,7 @@ typedef struct onode {
 	int32_t q;
 	uint32_t aq;
 	uint32_t ch[8];
+	double px, py, pz;  /* dipole moment about (cx, cy, cz), DIPOLES (pot.c:319-323) */
 } onode;
 
 /* slot of the child containing a point, by octal digit (gx<<2 | gy<<1 | gz) */
@@ -88,6 +89,12 @@ struct pto_ctx {
 	uint32_t st_de, st_nabs, st_nrein;
 	uint64_t st_npush;
 	long double epe[3];
+	/* variants */
+	long double* acc;        /* first-half accelerations (Proc.a_x1..a_z1), non-Boris integrators */
+	double ion_temp;         /* Proc.Ti, POIS_POS_COLLECTION (pot.c:390) */
+	double pos_rate_const;   /* Proc.pos_rate_const (pot.c:391) */
+	uint32_t st_pois;        /* charges added by the Poisson collection this step */
+	uint32_t st_wall;        /* OUT_BOUNCE: particles found in the wall moving inwards */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -181,6 +188,28 @@ static void o_nrv_pair(pto_ctx* c, double sd, double* nrv1, double* nrv2)
 	*nrv1 = sd * r * cos(theta);
 	*nrv2 = sd * r * sin(theta);
 }
+
+/* Poisson variate by inversion, prng.c:50-70: walk the CDF from k = 0
+   until the uniform draw is used up.  The reference loops until the
+   term underflows; the cap only guards against a non-terminating loop
+   (a rate of NaN or infinity) and returns 0 as the reference's exit does. */
+static uint32_t o_prv(pto_ctx* c, double lambda)
+{
+	double exp_lambda = exp(-lambda);
+	uint32_t k = 0;
+	double ratio_term = 1.0;
+	double uni = o_rnd(c, 1.0L);
+	while (ratio_term) {
+		uni -= ratio_term * exp_lambda;
+		if (uni < 0.0) break;
+		k++;
+		ratio_term *= lambda / k;
+		if (k >= (1u << 20)) return 0;
+	}
+	return ratio_term ? k : 0;
+}
+
+uint32_t pto_poisson(pto_ctx* c, double lambda) { return o_prv(c, lambda); }
 
 /* Inverse CDF of |u| at infinity without flow (Hutchinson 2003, eqs 18-19),
    Newton iteration as prng.c:138-156.  The iteration cap only guards
@@ -470,9 +499,10 @@ pto_ctx* pto_create(const pto_cfg* cfg)
 	c->parts = calloc(cfg->N, sizeof(pto_particle));
 	c->new_parts = calloc(cfg->N, sizeof(pto_particle));
 	c->prev = calloc(3 * cfg->N, sizeof(double));
+	c->acc = calloc(3 * cfg->N, sizeof(long double));
 	c->n_alloc = 9 * cfg->N + 9;   /* pot.c:4143 */
 	c->nodes = malloc(sizeof(onode) * c->n_alloc);
-	if (!c->parts || !c->new_parts || !c->prev || !c->nodes) {
+	if (!c->parts || !c->new_parts || !c->prev || !c->acc || !c->nodes) {
 		pto_destroy(c);
 		return NULL;
 	}
@@ -512,8 +542,21 @@ pto_ctx* pto_create(const pto_cfg* cfg)
 	c->tss[O_ELECTRON] = 1;
 	c->tss[O_ION] = (int) sqrt(cfg->Te * c->mass[O_ION] / (cfg->Ti * c->mass[O_ELECTRON]));
 	c->tss[O_DUST] = c->tss[O_ION] * (int) sqrt(0.1 * c->mass[O_DUST] / c->mass[O_ION]);
+	/* POIS_POS_COLLECTION set-up, pot.c:4251-4255: the cached ion temperature
+	   starts at the injection temperature; the constant part of the rate */
+	c->ion_temp = cfg->Ti;
+	{
+		const long double n = (cfg->N - 1) / ((4.0 / 3.0) * O_PI * powl(cfg->r * cfg->mpp, 3.0));
+		double k = 4.0 * O_PI * cfg->a * cfg->a * O_CHARGE[O_ION];
+		k /= sqrt(2.0 * O_PI * c->mass[O_ION]);
+		k *= c->dt * n / 2.0;
+		c->pos_rate_const = k;
+	}
 	return c;
 }
+
+void pto_set_ion_temp(pto_ctx* c, double Ti) { c->ion_temp = Ti; }
+double pto_ion_temp(const pto_ctx* c) { return c->ion_temp; }
 
 void pto_destroy(pto_ctx* c)
 {
@@ -521,6 +564,7 @@ void pto_destroy(pto_ctx* c)
 	free(c->parts);
 	free(c->new_parts);
 	free(c->prev);
+	free(c->acc);
 	free(c->nodes);
 	free(c);
 }
@@ -606,12 +650,23 @@ static void o_init_children(onode* nl, uint64_t k)
 	}
 }
 
-/* running |q|-weighted centre, pot.c:1290-1310 (monopole form) */
-static void o_update_moments(onode* node, const onode* chi)
+/* running |q|-weighted centre, pot.c:1290-1310; with dipoles the node's
+   moment is first moved to the new centre, then the child's, moved there
+   too, is added */
+static void o_update_moments(onode* node, const onode* chi, int dipoles)
 {
+	const double ocx = node->cx, ocy = node->cy, ocz = node->cz;
 	node->cx = (node->aq * node->cx + chi->aq * chi->cx) / (node->aq + chi->aq);
 	node->cy = (node->aq * node->cy + chi->aq * chi->cy) / (node->aq + chi->aq);
 	node->cz = (node->aq * node->cz + chi->aq * chi->cz) / (node->aq + chi->aq);
+	if (dipoles) {
+		node->px -= (node->cx - ocx) * node->q;
+		node->py -= (node->cy - ocy) * node->q;
+		node->pz -= (node->cz - ocz) * node->q;
+		node->px += chi->px - (node->cx - chi->cx) * chi->q;
+		node->py += chi->py - (node->cy - chi->cy) * chi->q;
+		node->pz += chi->pz - (node->cz - chi->cz) * chi->q;
+	}
 	node->q += chi->q;
 	node->aq += chi->aq;
 }
@@ -627,17 +682,19 @@ static void o_node_values(pto_ctx* c, uint64_t k)
 		node->cx = p->x;
 		node->cy = p->y;
 		node->cz = p->z;
+		node->px = node->py = node->pz = 0.0;
 		return;
 	}
 	node->q = 0;
 	node->aq = 0;
 	node->cx = node->cy = node->cz = 0.0;
+	node->px = node->py = node->pz = 0.0;
 	for (int s = 0; s < 8; s++) {
 		uint32_t ck = c->nodes[k].ch[s];
 		if (ck) {
 			o_node_values(c, ck);
 			node = &c->nodes[k];
-			if (c->nodes[ck].aq) o_update_moments(node, &c->nodes[ck]);
+			if (c->nodes[ck].aq) o_update_moments(node, &c->nodes[ck], c->cfg.dipoles);
 		}
 	}
 }
@@ -747,6 +804,33 @@ int pto_tree_dump(const pto_ctx* c, uint64_t max_nodes,
 	*n_int = ni;
 	*n_leaf = nl;
 	return 0;
+}
+
+/* Dipole moments of the internal nodes in pto_tree_dump's order; returns the
+   node count or -1. */
+int64_t pto_tree_dipoles(const pto_ctx* c, uint64_t max_nodes, double* int_p)
+{
+	uint32_t sn[1024];
+	int sl[1024];
+	int sp = 1;
+	uint64_t ni = 0;
+	sn[0] = 0; sl[0] = 0;
+	while (sp) {
+		sp--;
+		const onode* t = &c->nodes[sn[sp]];
+		const int lev = sl[sp];
+		if (t->part == O_NONE && t->ch[0]) {
+			if (ni >= max_nodes || lev >= 21 || sp + 8 > 1024) return -1;
+			int_p[3 * ni] = t->px; int_p[3 * ni + 1] = t->py; int_p[3 * ni + 2] = t->pz;
+			ni++;
+			for (int s = 0; s < 8; s++) {
+				sn[sp] = t->ch[s];
+				sl[sp] = lev + 1;
+				sp++;
+			}
+		}
+	}
+	return (int64_t) ni;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -912,13 +996,22 @@ static int o_field(const pto_ctx* c, uint32_t part, double x, double y, double z
 			dz = z - node->cz;
 			dist2 = (dx * dx) + (dy * dy) + (dz * dz);
 			if (((node->x2 - node->x1) * (node->x2 - node->x1)) < (oap * oap * dist2)) {
-				if (node->q) {
+				if (c->cfg.dipoles ? node->aq != 0 : node->q != 0) {
 					dist = sqrt(dist2);
 					E_scale = O_QE / (4 * O_PI * O_EPSILON0 * dist2 * dist);
-					E_scale *= node->q;
-					E[0] += E_scale * dx;
-					E[1] += E_scale * dy;
-					E[2] += E_scale * dz;
+					if (c->cfg.dipoles) {
+						/* pot.c:1739-1745 */
+						double r_dot_p_d2 = (dx * node->px) + (dy * node->py) + (dz * node->pz);
+						r_dot_p_d2 /= dist2;
+						E[0] += E_scale * ((node->q * dx) - node->px + (3 * dx * r_dot_p_d2));
+						E[1] += E_scale * ((node->q * dy) - node->py + (3 * dy * r_dot_p_d2));
+						E[2] += E_scale * ((node->q * dz) - node->pz + (3 * dz * r_dot_p_d2));
+					} else {
+						E_scale *= node->q;
+						E[0] += E_scale * dx;
+						E[1] += E_scale * dy;
+						E[2] += E_scale * dz;
+					}
 				}
 			} else {
 				if ((len + 8) > O_MAX_PATH) return -1;
@@ -1029,7 +1122,15 @@ double pto_phi_at(const pto_ctx* c, double x, double y, double z)
 			dz = z - node->cz;
 			dist2 = (dx * dx) + (dy * dy) + (dz * dz);
 			if (((node->x2 - node->x1) * (node->x2 - node->x1)) < (oap * oap * dist2)) {
-				if (node->q) phi += O_QE * node->q / (4 * O_PI * O_EPSILON0 * sqrt(dist2));
+				if (c->cfg.dipoles) {
+					if (node->aq) {  /* pot.c:1860-1868 */
+						dist = sqrt(dist2);
+						double r_dot_p = (dx * node->px) + (dy * node->py) + (dz * node->pz);
+						phi += (O_QE / (4 * O_PI * O_EPSILON0)) * ((node->q / dist) + (r_dot_p / (dist * dist2)));
+					}
+				} else if (node->q) {
+					phi += O_QE * node->q / (4 * O_PI * O_EPSILON0 * sqrt(dist2));
+				}
 				len--;
 			} else {
 				len--;
@@ -1065,7 +1166,15 @@ static long double o_phi_particle(const pto_ctx* c, uint32_t part)
 			dz = t->z - node->cz;
 			dist2 = (dx * dx) + (dy * dy) + (dz * dz);
 			if (((node->x2 - node->x1) * (node->x2 - node->x1)) < (oap * oap * dist2)) {
-				if (node->q) phi += O_QE * node->q / (4 * O_PI * O_EPSILON0 * sqrt(dist2));
+				if (c->cfg.dipoles) {
+					if (node->aq) {  /* pot.c:1966-1974 */
+						dist = sqrt(dist2);
+						double r_dot_p = (dx * node->px) + (dy * node->py) + (dz * node->pz);
+						phi += O_QE * ((node->q / dist) + (r_dot_p / (dist * dist2))) / (4 * O_PI * O_EPSILON0);
+					}
+				} else if (node->q) {
+					phi += O_QE * node->q / (4 * O_PI * O_EPSILON0 * sqrt(dist2));
+				}
 			} else {
 				if ((len + 8) > O_MAX_PATH) return NAN;
 				if (node->ch[0]) {
@@ -1216,6 +1325,35 @@ static int o_move(pto_ctx* c, int compute_epe, uint64_t time_steps)
 		long double dt = c->dt * c->tss[p->species];
 		double hx, hy, hz;
 		long double E[3], qom, ax, ay, az;
+		if (ru->integrator) {
+			/* velocity Verlet / Euler-Richardson, first half (pot.c:2533-2552):
+			   the field at the old position, no half drift */
+			int rc = o_field(c, (uint32_t) i, p->x, p->y, p->z, E);
+			if (rc) return rc == -1 ? -4 : -2;
+			if (p->species == O_DUST) {
+				qom = O_QE * c->grain_q;
+			} else {
+				qom = O_QE * O_CHARGE[p->species];
+			}
+			qom /= c->mass[p->species];
+			long double* a1 = &c->acc[3 * (i - start)];
+			a1[0] = qom * (E[0] + p->vy * B[2] - p->vz * B[1]);
+			a1[1] = qom * (E[1] + p->vz * B[0] - p->vx * B[2]);
+			a1[2] = qom * (E[2] + p->vx * B[1] - p->vy * B[0]);
+			np[i].vx += 0.5 * dt * a1[0];
+			np[i].vy += 0.5 * dt * a1[1];
+			np[i].vz += 0.5 * dt * a1[2];
+			if (ru->integrator == 2) {
+				np[i].x += 0.5 * dt * p->vx;
+				np[i].y += 0.5 * dt * p->vy;
+				np[i].z += 0.5 * dt * p->vz;
+			} else {
+				np[i].x += dt * (p->vx + (0.5 * dt * a1[0]));
+				np[i].y += dt * (p->vy + (0.5 * dt * a1[1]));
+				np[i].z += dt * (p->vz + (0.5 * dt * a1[2]));
+			}
+			continue;
+		}
 		if (ru->quirk) {
 			p->x += 0.5 * dt * p->vx;
 			p->y += 0.5 * dt * p->vy;
@@ -1252,17 +1390,57 @@ static int o_move(pto_ctx* c, int compute_epe, uint64_t time_steps)
 		np[i].z = hz + (0.5 * dt * np[i].vz);
 	}
 
+	/* the non-Boris integrators' mid-step exchange (pot.c:2556-2597): every
+	   particle's intermediate state replaces the old one, so the second
+	   field evaluation sees leaf particles there while the cells keep the
+	   moments of the tree built at the start of the step */
+	if (ru->integrator) memcpy(parts, np, sizeof(pto_particle) * N);
+
 	const double rad = ru->r * ru->mpp;
+	uint32_t n_wall = 0;
 	for (i = start; i < N; i++) {
 		pto_particle* pn = &np[i];
 		uint64_t ims = i - start;
 		uint32_t attempt = 0;
+		if (ru->integrator) {
+			/* second half (pot.c:2605-2638) */
+			const pto_particle* p = &parts[i];
+			long double E[3], qom, a_x2, a_y2, a_z2;
+			int rc = o_field(c, (uint32_t) i, p->x, p->y, p->z, E);
+			if (rc) return rc == -1 ? -4 : -2;
+			if (p->species == O_DUST) {
+				qom = O_QE * c->grain_q;
+			} else {
+				qom = O_QE * O_CHARGE[p->species];
+			}
+			qom /= c->mass[p->species];
+			a_x2 = qom * (E[0] + p->vy * B[2] - p->vz * B[1]);
+			a_y2 = qom * (E[1] + p->vz * B[0] - p->vx * B[2]);
+			a_z2 = qom * (E[2] + p->vx * B[1] - p->vy * B[0]);
+			long double dt = c->dt * c->tss[p->species];
+			const long double* a1 = &c->acc[3 * ims];
+			if (ru->integrator == 2) {
+				pn->x = (p->x - 0.5 * dt * (p->vx - 0.5 * dt * a1[0])) + dt * p->vx;
+				pn->y = (p->y - 0.5 * dt * (p->vy - 0.5 * dt * a1[1])) + dt * p->vy;
+				pn->z = (p->z - 0.5 * dt * (p->vz - 0.5 * dt * a1[2])) + dt * p->vz;
+				pn->vx = (p->vx - 0.5 * dt * a1[0]) + dt * a_x2;
+				pn->vy = (p->vy - 0.5 * dt * a1[1]) + dt * a_y2;
+				pn->vz = (p->vz - 0.5 * dt * a1[2]) + dt * a_z2;
+			} else {
+				pn->vx += 0.5 * dt * a_x2;
+				pn->vy += 0.5 * dt * a_y2;
+				pn->vz += 0.5 * dt * a_z2;
+			}
+		}
 		if ((i > 0) && ((time_steps * c->dt) > ru->settle)) {
 			double d[3] = { pn->x - c->prev[3 * ims], pn->y - c->prev[3 * ims + 1], pn->z - c->prev[3 * ims + 2] };
 			if (pto_cross_grain_run(c, pn, d, &np[0])) {
 				if (pn->species == O_ELECTRON) absorbed_e++;
 				absorbed_m += c->mass[pn->species];
 				absorbed_q += O_CHARGE[pn->species];
+				/* POIS_POS_COLLECTION: a positive particle's charge is undone
+				   (pot.c:2664-2670) */
+				if (ru->pois_ions && O_CHARGE[pn->species] > 0) absorbed_q -= O_CHARGE[pn->species];
 				dpx += c->mass[pn->species] * pn->vx;
 				dpy += c->mass[pn->species] * pn->vy;
 				dpz += c->mass[pn->species] * pn->vz;
@@ -1272,6 +1450,36 @@ static int o_move(pto_ctx* c, int compute_epe, uint64_t time_steps)
 				n_abs++;
 				n_rein++;
 			}
+		}
+		if (ru->bounce > 0.0) {
+			/* check_particle_in_sim_area with OUT_BOUNCE, pot.c:2036-2069: a
+			   particle outside the sphere moving outwards has its radial
+			   velocity reversed, every component scaled by the coefficient
+			   of restitution, and goes back to its position at the start of
+			   the step; one moving inwards is left where it is (the
+			   reference's warning, pot.c:2719-2722) */
+			const double bounce = ru->bounce;
+			double r[3], v[3];
+			r[0] = sqrt((pn->x - rad) * (pn->x - rad) + (pn->y - rad) * (pn->y - rad) + (pn->z - rad) * (pn->z - rad));
+			if (r[0] > rad) {
+				r[1] = atan2l(pn->y - rad, pn->x - rad);
+				r[2] = acosl((pn->z - rad) / r[0]);
+				v[0] = pn->vx * cos(r[1]) * sin(r[2]) + pn->vy * sin(r[1]) * sin(r[2]) + pn->vz * cos(r[2]);
+				v[1] = -pn->vx * sin(r[1]) + pn->vy * cos(r[1]);
+				v[2] = pn->vx * cos(r[1]) * cos(r[2]) + pn->vy * sin(r[1]) * cos(r[2]) - pn->vz * sin(r[2]);
+				if (v[0] > 0.0) {
+					v[0] *= -bounce;
+					v[1] *= bounce;
+					v[2] *= bounce;
+					o_vel_cart(v, r[1], r[2], &pn->vx, &pn->vy, &pn->vz);
+					pn->x = c->prev[3 * ims];
+					pn->y = c->prev[3 * ims + 1];
+					pn->z = c->prev[3 * ims + 2];
+				} else {
+					n_wall++;
+				}
+			}
+			continue;
 		}
 		/* check_particle_in_sim_area, pot.c:2025-2076 (spherical, no bounce) */
 		{
@@ -1300,6 +1508,19 @@ static int o_move(pto_ctx* c, int compute_epe, uint64_t time_steps)
 	np[0].vz += dpz / c->grain_m;
 	c->grain_q += absorbed_q;
 	c->tot_absor_e += absorbed_e;
+	c->st_pois = 0;
+	if (ru->pois_ions && ((time_steps * c->dt) > ru->settle)) {
+		/* POIS_POS_COLLECTION, pot.c:2837-2854: an OML ion flux at the cached
+		   ion temperature, Poisson-sampled once per step */
+		double kb_ti = O_KB * c->ion_temp;
+		double phi_normed = O_CHARGE[O_ION] * O_QE * O_QE * c->grain_q;
+		phi_normed /= 4.0 * O_PI * O_EPSILON0 * ru->a * kb_ti;
+		double lambda = c->pos_rate_const * sqrt(kb_ti) * (1.0 - phi_normed);
+		if (ru->rng) ph_stream(c, 0, time_steps, 0x30000u);
+		c->st_pois = o_prv(c, lambda);
+		c->grain_q += c->st_pois;
+	}
+	c->st_wall = n_wall;
 	if (compute_epe) {
 		c->epe[O_DUST] = c->grain_q ? c->grain_q * O_QE * o_phi_particle(c, 0) : 0.0;
 	}
@@ -1339,6 +1560,12 @@ void pto_last_step_stats(const pto_ctx* c, int64_t* dq, uint32_t* de, uint32_t* 
 	*n_reinjected = c->st_nrein;
 	*n_pushed = c->st_npush;
 	for (int k = 0; k < 3; k++) epe3[k] = (double) c->epe[k];
+}
+
+void pto_last_step_variant_stats(const pto_ctx* c, uint32_t* n_pois, uint32_t* n_wall)
+{
+	*n_pois = c->st_pois;
+	*n_wall = c->st_wall;
 }
 
 void pto_sample_reinject(pto_ctx* c, uint64_t n, int32_t species, pto_particle* out)

@@ -69,6 +69,15 @@ typedef struct pto_cfg {
 	double A;         /* aspect ratio (pot-spheroid.c -A) */
 	double axis[3];   /* symmetry axis, unit vector; (1, 0, 0) in the reference,
 	                     anything else is an extension (unpinned) */
+	/* the reference's other compile-time variants (pot.c:99-196), off = 0 */
+	double bounce;      /* OUT_BOUNCE (pot.c:113-119): the domain wall's coefficient of
+	                       restitution; 0 = reinject particles that leave */
+	int32_t integrator; /* 0 Boris (BORIS), 1 velocity Verlet (BORIS off), 2 Euler-Richardson
+	                       (EULER_RICHARDSON), pot.c:121-133 */
+	int32_t dipoles;    /* DIPOLES (pot.c:99-104): cell dipole moments in fields and potentials */
+	int32_t pois_ions;  /* POIS_POS_COLLECTION (pot.c:165-173): absorbed ions add no charge; the
+	                       grain gains a Poisson number of elementary charges each step */
+	int32_t pad2;
 } pto_cfg;
 
 typedef struct pto_ctx pto_ctx;
@@ -93,6 +102,8 @@ int pto_tree_dump(const pto_ctx* c, uint64_t max_nodes,
                   uint64_t* n_int, int32_t* int_level, uint64_t* int_path, int32_t* int_q,
                   uint32_t* int_aq, double* int_c, double* int_w,
                   uint64_t* n_leaf, uint32_t* leaf_part, int32_t* leaf_level, uint64_t* leaf_path);
+/* DIPOLES: the internal nodes' dipole moments (3 per node) in pto_tree_dump's order */
+int64_t pto_tree_dipoles(const pto_ctx* c, uint64_t max_nodes, double* int_p);
 void pto_field_many(const pto_ctx* c, uint64_t n, const uint32_t* idx, const double* xyz,
                     double* hi, double* lo);
 void pto_field_direct_many(const pto_ctx* c, uint64_t n, const uint32_t* idx, const double* xyz,
@@ -109,6 +120,13 @@ double pto_grain_phi(const pto_ctx* c, double x, double y, double z);
 double pto_measure_chi_b(const pto_ctx* c);
 /* the mean of measure_chi_b over P ranks' azimuths 2 pi k / P (pot.c:2268, 2409-2418) */
 double pto_measure_chi_b_ranks(const pto_ctx* c, int32_t P);
+/* POIS_POS_COLLECTION: the cached ion temperature (Proc.Ti) that sets the
+   collection rate; the run's Ti at set-up (pot.c:4252), then whatever the
+   macroscopic summary last measured (pot.c:3444-3448) */
+void pto_set_ion_temp(pto_ctx* c, double Ti);
+double pto_ion_temp(const pto_ctx* c);
+/* Poisson variate of prng.c:50-70 on the context's stream, for tests */
+uint32_t pto_poisson(pto_ctx* c, double lambda);
 
 /* One step: t_steps++, build the tree, move the particles (pot.c:4261-4386).
    Returns 0, or a negative status (tree build failure). */
@@ -116,6 +134,9 @@ int pto_step(pto_ctx* c, int32_t compute_epe);
 int pto_run_steps(pto_ctx* c, uint64_t n, int32_t compute_epe);
 void pto_last_step_stats(const pto_ctx* c, int64_t* dq, uint32_t* de, uint32_t* n_absorbed,
                          uint32_t* n_reinjected, uint64_t* n_pushed, double* epe3);
+/* charges added by the Poisson ion collection, and particles found in the
+   wall moving inwards (OUT_BOUNCE), in the last step */
+void pto_last_step_variant_stats(const pto_ctx* c, uint32_t* n_pois, uint32_t* n_wall);
 
 /* Reinjection sampler, for distribution tests: n draws of `species` through
    inject(reinjection = 1) on the context's RNG; out holds n particles. */

@@ -44,6 +44,35 @@ int potref_shape(void)
 #endif
 }
 
+/* the other variant switches compiled in: 1 DIPOLES, 2 OUT_BOUNCE,
+   4 POIS_POS_COLLECTION, 8 BORIS off (velocity Verlet), 16 EULER_RICHARDSON */
+int potref_variant_flags(void)
+{
+	int f = 0;
+#ifdef DIPOLES
+	f |= 1;
+#endif
+#ifdef OUT_BOUNCE
+	f |= 2;
+#endif
+#ifdef POIS_POS_COLLECTION
+	f |= 4;
+#endif
+#ifndef BORIS
+	f |= 8;
+#endif
+#ifdef EULER_RICHARDSON
+	f |= 16;
+#endif
+	return f;
+}
+
+#ifdef OUT_BOUNCE
+double potref_bounce(void) { return OUT_BOUNCE; }
+#else
+double potref_bounce(void) { return 0.0; }
+#endif
+
 /* 1 when the grain absorbs (DISABLE_GRAIN off), 0 otherwise */
 int potref_grain_enabled(void)
 {
@@ -155,12 +184,26 @@ int potref_setup(unsigned long N, unsigned int r, double dt, double mpp, double 
 	H.tss[ELECTRON] = 1;
 	H.tss[ION] = (int) sqrt(R.Te * MASS[ION] / (R.Ti * MASS[ELECTRON]));
 	H.tss[DUST] = H.tss[ION] * (int) sqrt(0.1 * MASS[DUST] / MASS[ION]);
+#ifdef POIS_POS_COLLECTION
+	/* run()'s set-up of the Poisson collection (pot.c:4251-4255) */
+	H.Ti = R.Ti;
+	H.pos_rate_const = 4.0 * PI * R.a * R.a * CHARGE[ION];
+	H.pos_rate_const /= sqrt(2.0 * PI * MASS[ION]);
+	H.pos_rate_const *= R.dt * total_number_density(R) / 2.0;
+#endif
 	H_ready = 1;
 	if (init) init_particles(&H, R);
 	return 0;
 }
 
 void potref_free(void) { h_free(); }
+
+#ifdef POIS_POS_COLLECTION
+/* Proc.Ti, the cached ion temperature of the Poisson collection rate */
+void potref_set_ion_temp(double Ti) { H.Ti = Ti; }
+double potref_ion_temp(void) { return H.Ti; }
+double potref_pos_rate_const(void) { return H.pos_rate_const; }
+#endif
 
 void potref_get_tss(unsigned int* out3) { out3[0] = H.tss[0]; out3[1] = H.tss[1]; out3[2] = H.tss[2]; }
 
@@ -260,6 +303,38 @@ int potref_tree_dump(unsigned long max_nodes,
 	*n_leaf = nl;
 	return 0;
 }
+
+#ifdef DIPOLES
+/* Dipole moments (px, py, pz) of the internal nodes, in the order of
+   potref_tree_dump.  Returns the node count or -1. */
+long potref_tree_dipoles(unsigned long max_nodes, double* int_p)
+{
+	unsigned int stack_node[1024];
+	int stack_level[1024];
+	int sp = 1;
+	unsigned long ni = 0;
+	stack_node[0] = 0;
+	stack_level[0] = 0;
+	while (sp) {
+		sp--;
+		const Tree* t = &(H.root[stack_node[sp]]);
+		const int lev = stack_level[sp];
+		if (t->part == UINT_MAX && t->gxlylz) {
+			if (ni >= max_nodes || lev >= 21 || sp + 8 > 1024) return -1;
+			int_p[3 * ni] = t->px;
+			int_p[3 * ni + 1] = t->py;
+			int_p[3 * ni + 2] = t->pz;
+			ni++;
+			for (int s = 0; s < 8; s++) {
+				stack_node[sp] = slot_child(t, s);
+				stack_level[sp] = lev + 1;
+				sp++;
+			}
+		}
+	}
+	return (long) ni;
+}
+#endif
 
 static void split_ld(long double v, double* hi, double* lo)
 {

@@ -1,6 +1,7 @@
 // C ABI (include/pot_gpu.h): run context, host <-> device transfers, the
 // per-step launch sequence, inspection queries and the kernel timer.
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -25,6 +26,10 @@ struct pot_gpu_ctx {
 	int cur = 0;
 	double4* src64 = nullptr;
 	float4* src32 = nullptr;
+	// non-Boris integrators: first-half accelerations and intermediate sources
+	double4* acc = nullptr;
+	double4* src64b = nullptr;
+	float4* src32b = nullptr;
 	uint64_t* keys[2] = { nullptr, nullptr };
 	uint32_t* vals[2] = { nullptr, nullptr };
 	int kb = 0;  // which key buffer holds the sorted keys
@@ -356,6 +361,25 @@ static int fill_params(pot_gpu_ctx* c)
 		}
 		P.t_settle = t0;
 	}
+	// the reference's other compile-time variants (pot.c:99-133, 165-173)
+	if (r.flags & ~(POT_CFG_SCEPTIC | POT_CFG_DISABLE_GRAIN | POT_CFG_DIPOLES | POT_CFG_POIS_IONS))
+		return POT_E_ARG;
+	if (!(r.bounce >= 0.0) || !std::isfinite(r.bounce)) return POT_E_ARG;
+	if (r.integrator > POT_INT_EULER_RICHARDSON) return POT_E_ARG;
+	if ((r.flags & POT_CFG_DIPOLES) && c->opts.form != POT_FORM_PLAIN) return POT_E_ARG;
+	P.bounce = r.bounce;
+	P.integrator = r.integrator;
+	for (int k = 0; k < 3; k++) P.B[k] = r.B[k];
+	// POIS_POS_COLLECTION's constant rate factor, pot.c:4253-4255, with the
+	// density of pot.c:3581-3588; MASS[ION], Run.dt and the density are long
+	// double there
+	{
+		const long double n = (r.N - 1) / ((4.0 / 3.0) * PI_REF * powl((long double)(r.r * r.mpp), 3.0L));
+		double k = 4.0 * PI_REF * r.a * r.a * 1;
+		k /= std::sqrt((double)(2.0 * PI_REF * m_ion));
+		k *= (long double)r.dt * n / 2.0;
+		P.pos_rate_const = k;
+	}
 	return POT_OK;
 }
 
@@ -571,6 +595,12 @@ static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu
 	AL(T.aq, cap);
 	AL(T.cq, cap);
 	AL(T.w2, cap);
+	if (cfg->flags & POT_CFG_DIPOLES) AL(T.dip, cap);
+	if (cfg->integrator != POT_INT_BORIS) {
+		AL(c->acc, n);
+		AL(c->src64b, n);
+		if (fast) AL(c->src32b, n);
+	}
 	AL(T.ovf, OVF_CAP);
 	if (fast) {
 		AL(T.f, cap);
@@ -599,6 +629,7 @@ static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu
 	std::memset(&r0, 0, sizeof(r0));
 	r0.grain_m = MASS_DUST;
 	r0.grain_slot = 0xFFFFFFFFu;
+	r0.ion_temp = cfg->Ti;  // Proc.Ti starts at the injection temperature, pot.c:4252
 	if (cudaMemcpy(c->rec, &r0, sizeof(r0), cudaMemcpyHostToDevice) != cudaSuccess) {
 		pot_gpu_destroy(c);
 		return POT_E_CUDA;
@@ -626,7 +657,9 @@ static int set_rec_from_grain(pot_gpu_ctx* c, const pot_grain_state* g, const do
 		r.grain_vel[0] = g_vel.x; r.grain_vel[1] = g_vel.y; r.grain_vel[2] = g_vel.z;
 	}
 	r.grain_slot = 0xFFFFFFFFu;
-	CK(cudaMemcpyAsync(c->rec, &r, sizeof(r), cudaMemcpyHostToDevice, c->stream));
+	// the record up to the per-step variant counters: the cached ion
+	// temperature after them survives uploads
+	CK(cudaMemcpyAsync(c->rec, &r, offsetof(RunRec, n_collected), cudaMemcpyHostToDevice, c->stream));
 	CK(cudaStreamSynchronize(c->stream));
 	c->sticky = POT_OK;
 	return POT_OK;
@@ -663,7 +696,7 @@ int pot_gpu_init_particles(pot_gpu_ctx* c)
 	r.grain_m = MASS_DUST;
 	r.grain_pos[0] = r.grain_pos[1] = r.grain_pos[2] = c->P.rad;
 	r.grain_slot = 0xFFFFFFFFu;
-	CK(cudaMemcpyAsync(c->rec, &r, sizeof(r), cudaMemcpyHostToDevice, c->stream));
+	CK(cudaMemcpyAsync(c->rec, &r, offsetof(RunRec, n_collected), cudaMemcpyHostToDevice, c->stream));
 	c->cur = 0;
 	launch_init(c->pos[0], c->vel[0], c->pid[0], c->P, c->rec, c->stream, c->timer);
 	CK(cudaGetLastError());
@@ -700,13 +733,31 @@ static void enqueue_step(pot_gpu_ctx* c, uint32_t flags)
 	compact_flags(c->due, c->n, c->due_list, c->block_sums, &c->rec->n_due, s, c->timer, c->due_prefix);
 	if (P.form == POT_FORM_FAST) launch_groups(c->T, c->due_prefix, c->groups, P, c->rec, s, c->timer);
 	launch_chi_b(c->T, c->src64, P, c->rec, 0, s, c->timer);
-	launch_push(c->pos[c->cur], c->vel[c->cur], c->T, c->src64, c->src32, c->due_list, c->groups, c->rein_list, P,
-	            c->rec, s, c->timer);
+	if (P.integrator == POT_INT_BORIS) {
+		launch_push(c->pos[c->cur], c->vel[c->cur], c->T, c->src64, c->src32, c->due_list, c->groups, c->rein_list,
+		            P, c->rec, StageBufs { 0, nullptr, nullptr, nullptr }, s, c->timer);
+	} else {
+		// two field evaluations (pot.c:2533-2639): the second sees every
+		// particle that moved at its intermediate position
+		StageBufs sb { 1, c->acc, c->src64b, c->src32b };
+		cudaMemcpyAsync(c->src64b, c->src64, sizeof(double4) * c->n, cudaMemcpyDeviceToDevice, s);
+		if (c->src32b) cudaMemcpyAsync(c->src32b, c->src32, sizeof(float4) * c->n, cudaMemcpyDeviceToDevice, s);
+		launch_push(c->pos[c->cur], c->vel[c->cur], c->T, c->src64, c->src32, c->due_list, c->groups, c->rein_list,
+		            P, c->rec, sb, s, c->timer);
+		cudaMemsetAsync(&c->rec->work_ctr, 0, sizeof(unsigned int), s);
+		sb.stage = 2;
+		launch_push(c->pos[c->cur], c->vel[c->cur], c->T, c->src64, c->src32, c->due_list, c->groups, c->rein_list,
+		            P, c->rec, sb, s, c->timer);
+	}
 	launch_absorb_late(c->pos[c->cur], c->vel[c->cur], c->src64, c->due_list, c->rein_list, P, c->rec, s, c->timer);
 	if (epe) {
-		launch_epe(c->pos[c->cur], c->T, c->src64, c->src32, c->groups_all, c->epe_partial, P, c->rec, s, c->timer);
+		// with two field evaluations the energies are those of the
+		// intermediate state, whose sources the second evaluation used
+		const bool two = P.integrator != POT_INT_BORIS;
+		launch_epe(c->pos[c->cur], c->T, two ? c->src64b : c->src64, two ? c->src32b : c->src32, c->groups_all,
+		           c->epe_partial, P, c->rec, s, c->timer);
 	}
-	launch_reinject(c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->rein_list, P, c->rec, s, c->timer);
+	launch_reinject(c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->rein_list, c->src64, P, c->rec, s, c->timer);
 	launch_grain_end(c->pos[c->cur], c->vel[c->cur], c->hist, P, c->rec, epe, s, c->timer);
 }
 
@@ -743,6 +794,9 @@ int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats
 		for (int k = 0; k < 3; k++) out->epe[k] = h.epe[k];
 		out->q_sum = r.q_sum;
 		out->warn = r.warn;
+		out->n_collected = r.n_collected;
+		out->n_wall = r.n_wall;
+		out->n_bounced = r.n_bounced;
 	}
 	return st;
 }
@@ -1017,7 +1071,7 @@ int pot_gpu_macro(pot_gpu_ctx* c, pot_macro_sums* out)
 	if (!c || !out) return POT_E_ARG;
 	if (!c->uploaded) return POT_E_STATE;
 	CK(cudaSetDevice(c->device));
-	launch_macro(c->pos[c->cur], c->vel[c->cur], c->P, c->macro, c->stream, c->timer);
+	launch_macro(c->pos[c->cur], c->vel[c->cur], c->P, c->macro, c->rec, c->stream, c->timer);
 	CK(cudaGetLastError());
 	CK(cudaMemcpyAsync(out, c->macro + (macro_scratch_doubles() - 80), sizeof(pot_macro_sums),
 	                   cudaMemcpyDeviceToHost, c->stream));
@@ -1041,6 +1095,24 @@ int pot_gpu_grain(pot_gpu_ctx* c, pot_grain_state* g)
 	g->t_steps = r.t_steps;
 	g->chi_b = r.chi_b;
 	return st;
+}
+
+int pot_gpu_set_ion_temp(pot_gpu_ctx* c, double Ti)
+{
+	if (!c || !(Ti >= 0.0) || !std::isfinite(Ti)) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	CK(cudaMemcpyAsync(&c->rec->ion_temp, &Ti, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	return POT_OK;
+}
+
+int pot_gpu_ion_temp(pot_gpu_ctx* c, double* Ti)
+{
+	if (!c || !Ti) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	CK(cudaMemcpy(Ti, &c->rec->ion_temp, sizeof(double), cudaMemcpyDeviceToHost));
+	return POT_OK;
 }
 
 int pot_gpu_kernel_times(pot_gpu_ctx* c, int max, const char** names, double* ms, uint64_t* launches)

@@ -15,7 +15,7 @@
 // Every loop that the reference leaves unbounded (Newton iterations, the
 // u^2 < chi_b rejection, the retry on NaN alpha) has a cap here; reaching one
 // sets POT_E_ITER and leaves the particle at a valid boundary state.
-#include "pot_tree.cuh"
+#include "pot_push.cuh"
 
 namespace pot {
 
@@ -369,9 +369,11 @@ __device__ __forceinline__ bool outside_sphere(const double4& p, const Params& P
 
 // Reinjection list entries: slot | reason << 30, reason 1 = absorbed by
 // the grain (reinjected, then tested against the boundary once more, as
-// pot.c:2676 followed by pot.c:2691), 2 = left the domain.
+// pot.c:2676 followed by pot.c:2691 -- with OUT_BOUNCE that test is the
+// wall's, against the start-of-step position in src64), 2 = left the domain.
 __global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel, const uint32_t* __restrict__ pid,
-                           const uint32_t* __restrict__ list, Params P, RunRec* rec)
+                           const uint32_t* __restrict__ list, const double4* __restrict__ src64, Params P,
+                           RunRec* rec)
 {
 	if (rec->status != POT_OK) return;
 	const uint32_t n = rec->n_rein;
@@ -393,11 +395,17 @@ __global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel,
 		Stream st;
 		st.init(P.seed, id, t, 0x10000u | attempt++);
 		inject<true>(st, sp, true, chi_b, P, p, v, fail);
-		if ((reason & 1u) && outside_sphere(p, P)) {
+		int wall = 0;
+		if ((reason & 1u) && P.bounce > 0.0) {
+			double3 x = make_double3(p.x, p.y, p.z);
+			wall = bounce_wall(src64[s], x, v, P);
+			p = make_double4(x.x, x.y, x.z, p.w);
+		} else if ((reason & 1u) && outside_sphere(p, P)) {
 			st.init(P.seed, id, t, 0x10000u | attempt++);
 			inject<true>(st, sp, true, chi_b, P, p, v, fail);
 		}
 		if (lane == 0) {
+			count_wall(rec, wall);
 			if (fail) { atomicOr(&rec->warn, fail); set_status(rec, POT_E_ITER); }
 			pos[s] = p;
 			vel[s] = v;
@@ -430,10 +438,10 @@ __global__ void k_init(double4* __restrict__ pos, double4* __restrict__ vel, uin
 }
 
 void launch_reinject(double4* pos, double4* vel, const uint32_t* pid, const uint32_t* rein_list,
-                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+                     const double4* src64, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
 {
 	ScopedKernel k(tm, "reinject");
-	k_reinject<<<148, 128, 0, s>>>(pos, vel, pid, rein_list, P, rec);
+	k_reinject<<<148, 128, 0, s>>>(pos, vel, pid, rein_list, src64, P, rec);
 }
 
 void launch_init(double4* pos, double4* vel, uint32_t* pid, const Params& P, RunRec* rec, cudaStream_t s,

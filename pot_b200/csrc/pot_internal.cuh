@@ -59,6 +59,10 @@ constexpr uint32_t OVF_CAP = 4096;
 constexpr uint32_t GROUP_MAX = 64;
 constexpr uint32_t FLAG_SCEPTIC = POT_CFG_SCEPTIC;
 constexpr uint32_t FLAG_NO_GRAIN = POT_CFG_DISABLE_GRAIN;
+constexpr uint32_t FLAG_DIPOLES = POT_CFG_DIPOLES;
+constexpr uint32_t FLAG_POIS = POT_CFG_POIS_IONS;
+constexpr uint32_t WARN_WALL = 128u;     // OUT_BOUNCE: a particle in the wall moving inwards
+constexpr uint32_t WARN_POISSON = 256u;  // the Poisson variate's iteration cap
 
 // Device-resident record of one run; the host reads it only at sync points.
 struct RunRec {
@@ -96,6 +100,11 @@ struct RunRec {
 	unsigned int epe_step;   // 1 when this step computes them
 	unsigned int epe_pad;
 	long long q_sum;         // sum over completed steps of the grain charge after each step (moving means)
+	unsigned int n_collected;  // Poisson ion collection: charges added this step
+	unsigned int n_wall;       // OUT_BOUNCE: particles outside moving inwards this step
+	unsigned int n_bounced;    // OUT_BOUNCE: particles bounced this step
+	unsigned int pad_v;
+	double ion_temp;           // cached ion temperature of the Poisson collection (Proc.Ti)
 };
 
 constexpr double VFIX = 1048576.0;  // 2^20
@@ -160,6 +169,11 @@ struct Params {
 	uint32_t s_tilted;    // symmetry axis other than x (an extension of the reference)
 	uint32_t chi_ranks;   // azimuths averaged for chi_b (ranks of an MPI run), >= 1
 	double s_ax[3], s_e1[3], s_e2[3];  // spheroid frame
+	double B[3];          // EXTERNAL_B_X/Y/Z as given (non-Boris accelerations)
+	double bounce;        // OUT_BOUNCE coefficient of restitution; 0 = reinjection at the wall
+	double pos_rate_const;  // Poisson ion collection: constant part of the rate (pot.c:4253-4255)
+	uint32_t integrator;  // POT_INT_*
+	uint32_t pad_v;
 };
 
 // ---- exactly rounded double helpers (no FMA contraction) ---------------

@@ -165,20 +165,24 @@ __global__ void __launch_bounds__(MACRO_THREADS) k_macro2(const double4* __restr
 	block_reduce<M2>(a, &partial[M2 * blockIdx.x]);
 }
 
-__global__ void k_macro2_final(const double* __restrict__ partial, double* __restrict__ sums2)
+// With the Poisson ion collection the ions' temperature from the velocity
+// dispersion becomes the cached Proc.Ti, as pot.c:3442-3448 does.
+__global__ void k_macro2_final(const double* __restrict__ partial, const double* __restrict__ sums1,
+                               double* __restrict__ sums2, Params P, RunRec* rec)
 {
 	if (threadIdx.x < M2) {
 		double s = 0.0;
 		for (int b = 0; b < MACRO_BLOCKS; b++) s += partial[M2 * b + threadIdx.x];
 		sums2[threadIdx.x] = s;
+		if (rec && threadIdx.x == 15 && sums1[1] > 0.0) rec->ion_temp = s * ((P.m_ion / (3.0 * KB)) / sums1[1]);
 	}
 }
 
 size_t macro_scratch_doubles() { return (size_t)MACRO_BLOCKS * 20 + 64 + 16; }
 
 // scratch: partials (MACRO_BLOCKS x 20), then sums1[20], sums2[M2], means
-void launch_macro(const double4* pos, const double4* vel, const Params& P, double* scratch, cudaStream_t s,
-                  Timer& tm)
+void launch_macro(const double4* pos, const double4* vel, const Params& P, double* scratch, RunRec* rec,
+                  cudaStream_t s, Timer& tm)
 {
 	double* partial = scratch;
 	double* sums1 = scratch + (size_t)MACRO_BLOCKS * 20;
@@ -188,7 +192,7 @@ void launch_macro(const double4* pos, const double4* vel, const Params& P, doubl
 	k_macro1<<<MACRO_BLOCKS, MACRO_THREADS, 0, s>>>(pos, vel, P, partial);
 	k_macro1_final<<<1, 32, 0, s>>>(partial, sums1, means);
 	k_macro2<<<MACRO_BLOCKS, MACRO_THREADS, 0, s>>>(pos, vel, P, means, partial);
-	k_macro2_final<<<1, 32, 0, s>>>(partial, sums2);
+	k_macro2_final<<<1, 32, 0, s>>>(partial, sums1, sums2, P, (P.flags & FLAG_POIS) ? rec : nullptr);
 }
 
 }  // namespace pot

@@ -172,8 +172,102 @@ __device__ __forceinline__ void boris(double4& v, double3 h, const double E[3], 
 	v = make_double4(vx, vy, vz, 0.0);
 }
 
-// Absorption tally (pot.c:2646-2666) for one absorbed particle.
-__device__ __forceinline__ void tally_absorbed(RunRec* rec, int sp, const double4& v)
+// Non-Boris integrators (pot.c:2533-2639), velocity Verlet and
+// Euler-Richardson: the acceleration a = q/m (E + v x B) at the old state,
+// then again at an intermediate state.
+__device__ __forceinline__ double3 accel_lorentz(const double E[3], const double4& v, double qom, const Params& P)
+{
+	return make_double3(qom * dsub(dadd(E[0], dmul(v.y, P.B[2])), dmul(v.z, P.B[1])),
+	                    qom * dsub(dadd(E[1], dmul(v.z, P.B[0])), dmul(v.x, P.B[2])),
+	                    qom * dsub(dadd(E[2], dmul(v.x, P.B[1])), dmul(v.y, P.B[0])));
+}
+
+// First half (pot.c:2536-2551): v += dt/2 a1; x += dt/2 v0 (Euler-Richardson)
+// or x += dt (v0 + dt/2 a1) (velocity Verlet).
+__device__ __forceinline__ void half_first(double4& p, double4& v, const double3& a1, double dt, const Params& P)
+{
+	const double hd = 0.5 * dt;
+	const double4 v0 = v;
+	v.x = dadd(v0.x, dmul(hd, a1.x));
+	v.y = dadd(v0.y, dmul(hd, a1.y));
+	v.z = dadd(v0.z, dmul(hd, a1.z));
+	if (P.integrator == POT_INT_EULER_RICHARDSON) {
+		p.x = dadd(p.x, dmul(hd, v0.x));
+		p.y = dadd(p.y, dmul(hd, v0.y));
+		p.z = dadd(p.z, dmul(hd, v0.z));
+	} else {
+		p.x = dadd(p.x, dmul(dt, dadd(v0.x, dmul(hd, a1.x))));
+		p.y = dadd(p.y, dmul(dt, dadd(v0.y, dmul(hd, a1.y))));
+		p.z = dadd(p.z, dmul(dt, dadd(v0.z, dmul(hd, a1.z))));
+	}
+}
+
+// Second half (pot.c:2624-2636) from the intermediate state (p, v): the
+// Euler-Richardson position and velocity in the reference's round-trip form,
+// or the velocity Verlet kick v += dt/2 a2.
+__device__ __forceinline__ void half_second(double3& xn, double4& v, const double4& p, const double3& a1,
+                                            const double3& a2, double dt, const Params& P)
+{
+	const double hd = 0.5 * dt;
+	xn = make_double3(p.x, p.y, p.z);
+	if (P.integrator == POT_INT_EULER_RICHARDSON) {
+		const double4 vm = v;
+		xn.x = dadd(dsub(p.x, dmul(hd, dsub(vm.x, dmul(hd, a1.x)))), dmul(dt, vm.x));
+		xn.y = dadd(dsub(p.y, dmul(hd, dsub(vm.y, dmul(hd, a1.y)))), dmul(dt, vm.y));
+		xn.z = dadd(dsub(p.z, dmul(hd, dsub(vm.z, dmul(hd, a1.z)))), dmul(dt, vm.z));
+		v.x = dadd(dsub(vm.x, dmul(hd, a1.x)), dmul(dt, a2.x));
+		v.y = dadd(dsub(vm.y, dmul(hd, a1.y)), dmul(dt, a2.y));
+		v.z = dadd(dsub(vm.z, dmul(hd, a1.z)), dmul(dt, a2.z));
+	} else {
+		v.x = dadd(v.x, dmul(hd, a2.x));
+		v.y = dadd(v.y, dmul(hd, a2.y));
+		v.z = dadd(v.z, dmul(hd, a2.z));
+	}
+}
+
+// OUT_BOUNCE at the spherical wall (pot.c:2036-2069): a particle outside the
+// sphere and moving outwards has its radial velocity reversed, every
+// spherical component scaled by the coefficient of restitution, and goes back
+// to its start-of-step position; one moving inwards stays where it is (the
+// reference's warning, pot.c:2719-2722).  Returns 0 inside, 1 bounced, 2 left
+// in the wall.  The angles come from atan2 and acos in FP64 (atan2l and acosl,
+// rounded to double, in the reference).
+__device__ __forceinline__ int bounce_wall(const double4& p_old, double3& xn, double4& vn, const Params& P)
+{
+	const double dx = dsub(xn.x, P.rad), dy = dsub(xn.y, P.rad), dz = dsub(xn.z, P.rad);
+	const double r0 = sqrt(dsq3(dx, dy, dz));
+	if (!(r0 > P.rad)) return 0;
+	const double ph = atan2(dy, dx);
+	const double th = acos(ddiv(dz, r0));
+	const double cp = cos(ph), sp = sin(ph), ct = cos(th), st = sin(th);
+	double v0 = dadd(dadd(dmul(dmul(vn.x, cp), st), dmul(dmul(vn.y, sp), st)), dmul(vn.z, ct));
+	double v1 = dadd(dmul(-vn.x, sp), dmul(vn.y, cp));
+	double v2 = dsub(dadd(dmul(dmul(vn.x, cp), ct), dmul(dmul(vn.y, sp), ct)), dmul(vn.z, st));
+	if (!(v0 > 0.0)) return 2;
+	v0 = dmul(v0, -P.bounce);
+	v1 = dmul(v1, P.bounce);
+	v2 = dmul(v2, P.bounce);
+	// velocity_in_cartesian_coords, coord.c:6-13
+	vn.x = dadd(dsub(dmul(dmul(v0, cp), st), dmul(v1, sp)), dmul(dmul(v2, cp), ct));
+	vn.y = dadd(dadd(dmul(dmul(v0, sp), st), dmul(v1, cp)), dmul(dmul(v2, sp), ct));
+	vn.z = dsub(dmul(v0, ct), dmul(v2, st));
+	xn = make_double3(p_old.x, p_old.y, p_old.z);
+	return 1;
+}
+
+__device__ __forceinline__ void count_wall(RunRec* rec, int b)
+{
+	if (b == 1) {
+		atomicAdd(&rec->n_bounced, 1u);
+	} else if (b == 2) {
+		atomicAdd(&rec->n_wall, 1u);
+		atomicOr(&rec->warn, WARN_WALL);
+	}
+}
+
+// Absorption tally (pot.c:2646-2666) for one absorbed particle.  With the
+// Poisson ion collection an absorbed ion adds no charge (pot.c:2664-2670).
+__device__ __forceinline__ void tally_absorbed(RunRec* rec, int sp, const double4& v, const Params& P)
 {
 	if (sp == SP_E) {
 		atomicAdd(&rec->de, 1ull);
@@ -184,7 +278,7 @@ __device__ __forceinline__ void tally_absorbed(RunRec* rec, int sp, const double
 		atomicAdd((unsigned long long*)&rec->sumv_e[2], (unsigned long long)llrint(v.z * VFIX));
 	} else {
 		atomicAdd(&rec->nabs_ion, 1ull);
-		atomicAdd((unsigned long long*)&rec->dq, 1ull);
+		if (!(P.flags & FLAG_POIS)) atomicAdd((unsigned long long*)&rec->dq, 1ull);
 		atomicAdd((unsigned long long*)&rec->sumv_ion[0], (unsigned long long)llrint(v.x * VFIX));
 		atomicAdd((unsigned long long*)&rec->sumv_ion[1], (unsigned long long)llrint(v.y * VFIX));
 		atomicAdd((unsigned long long*)&rec->sumv_ion[2], (unsigned long long)llrint(v.z * VFIX));
@@ -192,9 +286,10 @@ __device__ __forceinline__ void tally_absorbed(RunRec* rec, int sp, const double
 }
 
 // After the push: absorption (then reinjection, whose result is re-tested
-// against the boundary by the reinjection kernel), else the boundary test.
-// Returns the reinjection reason bits (1 absorbed, 2 outside).
-__device__ __forceinline__ uint32_t after_push(int sp, const double4& p_old, const double3& xn, const double4& vn,
+// against the boundary by the reinjection kernel), else the boundary test:
+// reinjection, or with OUT_BOUNCE the wall's bounce applied to (xn, vn) in
+// place.  Returns the reinjection reason bits (1 absorbed, 2 outside).
+__device__ __forceinline__ uint32_t after_push(int sp, const double4& p_old, double3& xn, double4& vn,
                                                const Params& P, RunRec* rec, bool absorb_on, double gx,
                                                double gy, double gz)
 {
@@ -206,8 +301,10 @@ __device__ __forceinline__ uint32_t after_push(int sp, const double4& p_old, con
 		              : cross_grain(xn.x, xn.y, xn.z, ddx, ddy, ddz, gx, gy, gz, P.a);
 	}
 	if (hit) {
-		tally_absorbed(rec, sp, vn);
+		tally_absorbed(rec, sp, vn, P);
 		reason = 1;
+	} else if (P.bounce > 0.0) {
+		count_wall(rec, bounce_wall(p_old, xn, vn, P));
 	} else if (outside_domain(xn.x, xn.y, xn.z, P)) {
 		reason = 2;
 	}

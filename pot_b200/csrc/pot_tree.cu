@@ -91,6 +91,9 @@ __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ k
 		for (int k = 0; k < 3; k++) { rec->sumv_ion[k] = 0; rec->sumv_e[k] = 0; }
 		rec->interactions = 0;
 		rec->n_pushed = 0;
+		rec->n_collected = 0;
+		rec->n_wall = 0;
+		rec->n_bounced = 0;
 		rec->grain_slot = 0xFFFFFFFFu;
 	}
 	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -305,11 +308,34 @@ __device__ __forceinline__ void add_moment(int& q, uint32_t& aq, double& cx, dou
 	aq += caq;
 }
 
+// DIPOLES (pot.c:1290-1310): the node's dipole moves to the new centre of
+// |q|, then the child's, moved there too, is added; q and |q| last
+__device__ __forceinline__ void add_moment_dip(int& q, uint32_t& aq, double& cx, double& cy, double& cz, double& px,
+                                               double& py, double& pz, int cq, uint32_t caq, double ccx, double ccy,
+                                               double ccz, double cpx, double cpy, double cpz)
+{
+	const double ox = cx, oy = cy, oz = cz;
+	const double a0 = (double)aq, a1 = (double)caq, den = (double)(aq + caq);
+	cx = ddiv(dadd(dmul(a0, cx), dmul(a1, ccx)), den);
+	cy = ddiv(dadd(dmul(a0, cy), dmul(a1, ccy)), den);
+	cz = ddiv(dadd(dmul(a0, cz), dmul(a1, ccz)), den);
+	const double qd = (double)q, cqd = (double)cq;
+	px = dsub(px, dmul(dsub(cx, ox), qd));
+	py = dsub(py, dmul(dsub(cy, oy), qd));
+	pz = dsub(pz, dmul(dsub(cz, oz), qd));
+	px = dadd(px, dsub(cpx, dmul(dsub(cx, ccx), cqd)));
+	py = dadd(py, dsub(cpy, dmul(dsub(cy, ccy), cqd)));
+	pz = dadd(pz, dsub(cpz, dmul(dsub(cz, ccz), cqd)));
+	q += cq;
+	aq += caq;
+}
+
 __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec)
 {
 	const uint32_t M = rec->n_nodes;
 	if (M > T.cap) return;
 	const uint32_t L = P.leaf_size;
+	const bool dip = T.dip != nullptr;
 	for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < M; k0 += gridDim.x * blockDim.x) {
 	if (T.nint[k0] != 0) continue;
 	uint32_t k = k0;
@@ -317,6 +343,7 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 		int q = 0;
 		uint32_t aq = 0;
 		double cx = 0.0, cy = 0.0, cz = 0.0;
+		double px = 0.0, py = 0.0, pz = 0.0;
 		const float w_child = 0.5f * (float)(sqrt(T.w2[k]) * P.inv_rad);
 		for (int s = 0; s < 8; s++) {
 			const int d = slot_digit(s);
@@ -325,6 +352,7 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 			int cq;
 			uint32_t caq;
 			double ccx, ccy, ccz;
+			double cpx = 0.0, cpy = 0.0, cpz = 0.0;
 			if (code >= 0) {
 				cq = __ldcg(&T.q[code]);
 				caq = __ldcg(&T.aq[code]);
@@ -332,6 +360,11 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 				const double2 c01 = __ldcg(cp2), c23 = __ldcg(cp2 + 1);
 				const double4 c = make_double4(c01.x, c01.y, c23.x, c23.y);
 				ccx = c.x; ccy = c.y; ccz = c.z;
+				if (dip) {
+					const double2* dp2 = reinterpret_cast<const double2*>(&T.dip[code]);
+					const double2 d01 = __ldcg(dp2), d23 = __ldcg(dp2 + 1);
+					cpx = d01.x; cpy = d01.y; cpz = d23.x;
+				}
 			} else if (L == 1 && leaf_payload(code) < P.n_tree) {
 				const double4 sp = src64[leaf_payload(code)];
 				cq = (int)sp.w;
@@ -348,7 +381,13 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 					const double4 sp = src64[j];
 					const int pq = (int)sp.w;
 					const uint32_t paq = (uint32_t)abs(pq);
-					if (paq) add_moment(cq, caq, ccx, ccy, ccz, pq, paq, sp.x, sp.y, sp.z);
+					if (!paq) continue;
+					if (dip) {
+						add_moment_dip(cq, caq, ccx, ccy, ccz, cpx, cpy, cpz, pq, paq, sp.x, sp.y, sp.z, 0.0, 0.0,
+						               0.0);
+					} else {
+						add_moment(cq, caq, ccx, ccy, ccz, pq, paq, sp.x, sp.y, sp.z);
+					}
 				}
 				if (T.lf && L > 1) {
 					T.lf[e] = make_float4((float)((ccx - P.rad) * P.inv_rad), (float)((ccy - P.rad) * P.inv_rad),
@@ -356,11 +395,18 @@ __global__ void k_moments(TreeDev T, const double4* __restrict__ src64, Params P
 					T.lr2[e] = w_child * w_child / P.oap2_f;
 				}
 			}
-			if (caq) add_moment(q, aq, cx, cy, cz, cq, caq, ccx, ccy, ccz);
+			if (caq) {
+				if (dip) {
+					add_moment_dip(q, aq, cx, cy, cz, px, py, pz, cq, caq, ccx, ccy, ccz, cpx, cpy, cpz);
+				} else {
+					add_moment(q, aq, cx, cy, cz, cq, caq, ccx, ccy, ccz);
+				}
+			}
 		}
 		T.q[k] = q;
 		T.aq[k] = aq;
 		T.cq[k] = make_double4(cx, cy, cz, (double)q);
+		if (dip) T.dip[k] = make_double4(px, py, pz, 0.0);
 		if (T.f) {
 			T.f[k] = make_float4((float)((cx - P.rad) * P.inv_rad), (float)((cy - P.rad) * P.inv_rad),
 			                     (float)((cz - P.rad) * P.inv_rad), (float)q);

@@ -23,6 +23,7 @@ struct TreeDev {
 	uint32_t* aq;      // absolute charge (Tree.aq)
 	double4* cq;       // centre of |q| and q
 	double* w2;        // (x2 - x1)^2
+	double4* dip;      // DIPOLES (plain form): dipole moment about cq; null otherwise
 	// FP32 walk (fast form only; null otherwise)
 	float4* f;         // centre relative to the domain centre, q
 	float* r2;         // w2 / OAP^2: accepted when d^2 > r2
@@ -47,13 +48,23 @@ void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const 
 
 // walk.cu
 size_t macro_scratch_doubles();
-void launch_macro(const double4* pos, const double4* vel, const Params& P, double* scratch, cudaStream_t s,
-                  Timer& tm);
+void launch_macro(const double4* pos, const double4* vel, const Params& P, double* scratch, RunRec* rec,
+                  cudaStream_t s, Timer& tm);
 void launch_chi_b(const TreeDev& T, const double4* src64, const Params& P, RunRec* rec, int force,
                   cudaStream_t s, Timer& tm);
+// Buffers of the non-Boris integrators' two-launch step: stage 0 is the
+// one-launch Boris step; stage 1 writes each due particle's first-half
+// acceleration (acc) and its intermediate source entry (src64b, and src32b in
+// the fast form); stage 2 reads them.
+struct StageBufs {
+	int stage;
+	double4* acc;
+	double4* src64b;
+	float4* src32b;
+};
 void launch_push(double4* pos, double4* vel, const TreeDev& T, const double4* src64, const float4* src32,
                  const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P, RunRec* rec,
-                 cudaStream_t s, Timer& tm);
+                 const StageBufs& sb, cudaStream_t s, Timer& tm);
 void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const Params& P, RunRec* rec,
                    cudaStream_t s, Timer& tm);
 void launch_absorb_late(double4* pos, double4* vel, const double4* src64, const uint32_t* due_list,
@@ -70,7 +81,7 @@ void launch_phi_query(const TreeDev& T, const double4* src64, const double* xyz,
 
 // inject.cu
 void launch_reinject(double4* pos, double4* vel, const uint32_t* pid, const uint32_t* rein_list,
-                     const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+                     const double4* src64, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 void launch_init(double4* pos, double4* vel, uint32_t* pid, const Params& P, RunRec* rec, cudaStream_t s,
                  Timer& tm);
 

@@ -34,7 +34,19 @@ __device__ int field_plain(uint32_t self, double x, double y, double z, const Tr
 			const double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
 			const double dist2 = dsq3(dx, dy, dz);
 			if (T.w2[code] < dmul(P.oap2, dist2)) {
-				if (c.w != 0.0) {
+				if (T.dip) {
+					if (T.aq[code] != 0) {
+						// DIPOLES, pot.c:1739-1745: the cell's dipole term too
+						const double dist = sqrt(dist2);
+						const double es = ddiv(QE, dmul(dmul(P.k4, dist2), dist));
+						const double4 pd = T.dip[code];
+						const double rp = ddiv(dadd(dadd(dmul(dx, pd.x), dmul(dy, pd.y)), dmul(dz, pd.z)), dist2);
+						ex = fma(es, dadd(dsub(dmul(c.w, dx), pd.x), dmul(dmul(3.0, dx), rp)), ex);
+						ey = fma(es, dadd(dsub(dmul(c.w, dy), pd.y), dmul(dmul(3.0, dy), rp)), ey);
+						ez = fma(es, dadd(dsub(dmul(c.w, dz), pd.z), dmul(dmul(3.0, dz), rp)), ez);
+						n_inter++;
+					}
+				} else if (c.w != 0.0) {
 					const double dist = sqrt(dist2);
 					const double es = dmul(ddiv(QE, dmul(dmul(P.k4, dist2), dist)), c.w);
 					ex = fma(es, dx, ex);
@@ -104,7 +116,16 @@ __device__ double phi_plain(uint32_t self, double x, double y, double z, const T
 			const double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
 			const double dist2 = dsq3(dx, dy, dz);
 			if (T.w2[code] < dmul(P.oap2, dist2)) {
-				if (c.w != 0.0) phi += ddiv(dmul(QE, c.w), dmul(P.k4, sqrt(dist2)));
+				if (T.dip) {
+					if (T.aq[code] != 0) {  // DIPOLES, pot.c:1966-1974
+						const double dist = sqrt(dist2);
+						const double4 pd = T.dip[code];
+						const double rp = dadd(dadd(dmul(dx, pd.x), dmul(dy, pd.y)), dmul(dz, pd.z));
+						phi += ddiv(dmul(QE, dadd(ddiv(c.w, dist), ddiv(rp, dmul(dist, dist2)))), P.k4);
+					}
+				} else if (c.w != 0.0) {
+					phi += ddiv(dmul(QE, c.w), dmul(P.k4, sqrt(dist2)));
+				}
 			} else {
 				if (len + 8 > WALK_STACK) {
 					rc = POT_E_WALK;
@@ -209,18 +230,33 @@ __device__ __forceinline__ void warp_add_u64(unsigned long long* dst, unsigned l
 	if (lane_id() == 0 && v) atomicAdd(dst, v);
 }
 
+// The walk fused with the push.  STG 0: Boris (half drift, field, kick,
+// rotate, kick, half drift), then absorption and the boundary.  The
+// non-Boris integrators take two launches: STG 1 evaluates the field at the
+// old position and writes the intermediate state, its acceleration and its
+// source entry (sb); STG 2 evaluates the field at the intermediate state over
+// those sources (leaf particles moved, cells as built) and finishes the step
+// (pot.c:2533-2639), then absorption and the boundary against the
+// start-of-step position in src64.
+template <int STG>
 __global__ void __launch_bounds__(128) k_push_plain(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T,
                                                     const double4* __restrict__ src64,
                                                     const uint32_t* __restrict__ due_list,
-                                                    uint32_t* __restrict__ rein_list, Params P, RunRec* rec)
+                                                    uint32_t* __restrict__ rein_list, Params P, RunRec* rec,
+                                                    StageBufs sb)
 {
 	if (rec->status != POT_OK) return;
 	const uint32_t n_due = rec->n_due;
 	const unsigned long long t = rec->t_steps;
 	const bool grain_due = rec->grain_due != 0;
 	const bool absorb_on = !(P.flags & FLAG_NO_GRAIN) && t >= P.t_settle;
-	const double gx = rec->grain_pos[0], gy = rec->grain_pos[1], gz = rec->grain_pos[2];
+	double gx = rec->grain_pos[0], gy = rec->grain_pos[1], gz = rec->grain_pos[2];
+	if (STG == 2 && grain_due && rec->grain_slot < P.n) {
+		const double4 g = pos[rec->grain_slot];  // the grain's intermediate position
+		gx = g.x; gy = g.y; gz = g.z;
+	}
 	const double qg = (double)rec->grain_q;
+	const double4* __restrict__ src = STG == 2 ? sb.src64b : src64;
 	unsigned long long n_inter = 0, n_push = 0;
 	for (;;) {
 		uint32_t base = 0;
@@ -235,20 +271,36 @@ __global__ void __launch_bounds__(128) k_push_plain(double4* __restrict__ pos, d
 		const int sp = (int)p.w;
 		const double dt = P.dt * (double)P.tss[sp];
 		const double half = 0.5 * dt;
-		const double3 h = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
+		const double3 h = STG == 0 ? make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z))
+		                           : make_double3(p.x, p.y, p.z);
 		double E[3] = { 0.0, 0.0, 0.0 };
 		if (P.shape && sp != SP_DUST) spheroid_field(P, qg, dsub(h.x, gx), dsub(h.y, gy), dsub(h.z, gz), E);
 		uint32_t ni = 0;
-		const int rc = field_plain(s, h.x, h.y, h.z, T, src64, P, E, ni);
+		const int rc = field_plain(s, h.x, h.y, h.z, T, src, P, E, ni);
 		if (rc != POT_OK) set_status(rec, rc);
 		n_inter += ni;
-		n_push++;
 		const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
 		const double qom = (QE * charge) / mass_of(sp, P);
+		if (STG == 1) {
+			const double3 a1 = accel_lorentz(E, v, qom, P);
+			double4 pm = p;
+			half_first(pm, v, a1, dt, P);
+			pos[s] = pm;
+			vel[s] = v;
+			sb.acc[s] = make_double4(a1.x, a1.y, a1.z, 0.0);
+			sb.src64b[s] = make_double4(pm.x, pm.y, pm.z, src64[s].w);
+			continue;
+		}
+		n_push++;
 		double3 xn;
-		boris(v, h, E, qom, dt, P, xn);
+		if (STG == 0) {
+			boris(v, h, E, qom, dt, P, xn);
+		} else {
+			const double4 a = sb.acc[s];
+			half_second(xn, v, p, make_double3(a.x, a.y, a.z), accel_lorentz(E, v, qom, P), dt, P);
+		}
 		uint32_t reason = 0;
-		if (!grain_due) reason = after_push(sp, p, xn, v, P, rec, absorb_on, gx, gy, gz);
+		if (!grain_due) reason = after_push(sp, STG == 0 ? p : src64[s], xn, v, P, rec, absorb_on, gx, gy, gz);
 		pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
 		vel[s] = v;
 		if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
@@ -271,13 +323,40 @@ __global__ void k_absorb_late(double4* __restrict__ pos, double4* __restrict__ v
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_due; i += gridDim.x * blockDim.x) {
 		const uint32_t s = due_list[i];
 		const double4 p = pos[s];
-		const double4 v = vel[s];
+		double4 v = vel[s];
 		const double4 p_old = src64[s];
 		const int sp = (int)p.w;
-		const uint32_t reason =
-		    after_push(sp, p_old, make_double3(p.x, p.y, p.z), v, P, rec, absorb_on, g.x, g.y, g.z);
+		double3 xn = make_double3(p.x, p.y, p.z);
+		const uint32_t reason = after_push(sp, p_old, xn, v, P, rec, absorb_on, g.x, g.y, g.z);
+		if (P.bounce > 0.0 && !reason) {  // a bounce moved it
+			pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
+			vel[s] = v;
+		}
 		if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
 	}
+}
+
+// Poisson variate by inversion (prng.c:50-70): walk the CDF from k = 0 until
+// the uniform draw is used up.  The reference loops until the term
+// underflows; the cap (the oracle's too) only ends a loop that cannot end
+// (a rate of NaN or infinity), returning 0 as the reference's exit does.
+constexpr uint32_t POISSON_CAP = 1u << 20;
+__device__ uint32_t poisson_inv(double lambda, double uni, bool& capped)
+{
+	const double e = exp(-lambda);
+	uint32_t k = 0;
+	double ratio = 1.0;
+	while (ratio != 0.0) {
+		uni = dsub(uni, dmul(ratio, e));
+		if (uni < 0.0) break;
+		k++;
+		ratio = dmul(ratio, ddiv(lambda, (double)k));
+		if (k >= POISSON_CAP) {
+			capped = true;
+			return 0;
+		}
+	}
+	return ratio != 0.0 ? k : 0;
 }
 
 // Grain update of pot.c:2825-2848 and the step's statistics.
@@ -308,6 +387,21 @@ __global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel
 	for (int k = 0; k < 3; k++) rec->grain_vel[k] = gv[k];
 	rec->grain_m = m;
 	rec->grain_q += rec->dq;
+	if ((P.flags & FLAG_POIS) && rec->t_steps >= P.t_settle) {
+		// POIS_POS_COLLECTION, pot.c:2837-2854: the OML ion flux at the cached
+		// ion temperature and the grain's charge after this step's absorptions
+		const double kb_ti = KB * rec->ion_temp;
+		double phi_normed = dmul(dmul(QE, QE), (double)rec->grain_q);
+		phi_normed = ddiv(phi_normed, dmul(dmul(dmul(4.0 * PI_REF, EPSILON0), P.a), kb_ti));
+		const double lambda = dmul(dmul(P.pos_rate_const, sqrt(kb_ti)), dsub(1.0, phi_normed));
+		Stream st;
+		st.init(P.seed, 0u, (uint32_t)rec->t_steps, 0x30000u);
+		bool capped = false;
+		const uint32_t k = poisson_inv(lambda, st.rnd(1.0), capped);
+		if (capped) rec->warn |= WARN_POISSON;
+		rec->n_collected = k;
+		rec->grain_q += k;
+	}
 	rec->q_sum += rec->grain_q;
 	rec->tot_absor_e += rec->de;
 	if (epe) {
@@ -360,7 +454,16 @@ __device__ double warp_phi(double x, double y, double z, const TreeDev& T, const
 			const double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
 			const double dist2 = dsq3(dx, dy, dz);
 			if (T.w2[code] < dmul(P.oap2, dist2)) {
-				if (c.w != 0.0) acc += ddiv(dmul(QE, c.w), dmul(P.k4, sqrt(dist2)));
+				if (T.dip) {
+					if (T.aq[code] != 0) {  // DIPOLES, pot.c:1860-1868
+						const double dist = sqrt(dist2);
+						const double4 pd = T.dip[code];
+						const double rp = dadd(dadd(dmul(dx, pd.x), dmul(dy, pd.y)), dmul(dz, pd.z));
+						acc += dmul(ddiv(QE, P.k4), dadd(ddiv(c.w, dist), ddiv(rp, dmul(dist, dist2))));
+					}
+				} else if (c.w != 0.0) {
+					acc += ddiv(dmul(QE, c.w), dmul(P.k4, sqrt(dist2)));
+				}
 			} else {
 				const int32_t* cp = &T.child[8u * (uint32_t)code];
 #pragma unroll
@@ -495,7 +598,7 @@ __global__ void k_field_query_plain(TreeDev T, const double4* __restrict__ src64
 // ---------------------------------------------------------------------------
 void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,
                       const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P,
-                      RunRec* rec, cudaStream_t s, Timer& tm);
+                      RunRec* rec, const StageBufs& sb, cudaStream_t s, Timer& tm);
 void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, const double4* src64,
                      uint2* groups_all, double* partial, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 void launch_field_query_fast(const TreeDev& T, const float4* src32, const double* xyz, const uint32_t* self_slot,
@@ -523,14 +626,21 @@ void launch_chi_b(const TreeDev& T, const double4* src64, const Params& P, RunRe
 
 void launch_push(double4* pos, double4* vel, const TreeDev& T, const double4* src64, const float4* src32,
                  const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P, RunRec* rec,
-                 cudaStream_t s, Timer& tm)
+                 const StageBufs& sb, cudaStream_t s, Timer& tm)
 {
 	if (P.form == POT_FORM_FAST) {
-		launch_push_fast(pos, vel, T, src32, src64, due_list, groups, rein_list, P, rec, s, tm);
+		launch_push_fast(pos, vel, T, src32, src64, due_list, groups, rein_list, P, rec, sb, s, tm);
 		return;
 	}
-	ScopedKernel k(tm, "walk_push_plain");
-	k_push_plain<<<sm_count() * 8, 128, 0, s>>>(pos, vel, T, src64, due_list, rein_list, P, rec);
+	ScopedKernel k(tm, sb.stage == 0 ? "walk_push_plain" : (sb.stage == 1 ? "walk_half1_plain" : "walk_half2_plain"));
+	const int nb = sm_count() * 8;
+	if (sb.stage == 0) {
+		k_push_plain<0><<<nb, 128, 0, s>>>(pos, vel, T, src64, due_list, rein_list, P, rec, sb);
+	} else if (sb.stage == 1) {
+		k_push_plain<1><<<nb, 128, 0, s>>>(pos, vel, T, src64, due_list, rein_list, P, rec, sb);
+	} else {
+		k_push_plain<2><<<nb, 128, 0, s>>>(pos, vel, T, src64, due_list, rein_list, P, rec, sb);
+	}
 }
 
 void launch_absorb_late(double4* pos, double4* vel, const double4* src64, const uint32_t* due_list,

@@ -521,13 +521,16 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 	}
 }
 
-template <int TPL>
+// STG as in k_push_plain: 0 the Boris step; 1 and 2 the two halves of the
+// non-Boris integrators (stage 2 walks over the intermediate sources).
+template <int TPL, int STG>
 __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel,
                                                             TreeDev T, const float4* __restrict__ src32,
                                                             const uint32_t* __restrict__ due_list,
                                                             const uint2* __restrict__ groups,
                                                             uint32_t* __restrict__ rein_list, Params P,
-                                                            RunRec* rec)
+                                                            RunRec* rec, const double4* __restrict__ src64,
+                                                            StageBufs sb)
 {
 	__shared__ FastSmem<TPL> smem[FW_WARPS];
 	FastSmem<TPL>& sm = smem[threadIdx.x >> 5];
@@ -536,7 +539,12 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 	const unsigned long long t_step = rec->t_steps;
 	const bool grain_due = rec->grain_due != 0;
 	const bool absorb_on = !(P.flags & FLAG_NO_GRAIN) && t_step >= P.t_settle;
-	const double gx = rec->grain_pos[0], gy = rec->grain_pos[1], gz = rec->grain_pos[2];
+	double gx = rec->grain_pos[0], gy = rec->grain_pos[1], gz = rec->grain_pos[2];
+	if (STG == 2 && grain_due && rec->grain_slot < P.n) {
+		const double4 gp = pos[rec->grain_slot];  // the grain's intermediate position
+		gx = gp.x; gy = gp.y; gz = gp.z;
+	}
+	const float4* __restrict__ srcf = STG == 2 ? sb.src32b : src32;
 	const double qg = (double)rec->grain_q;
 	const double escale = QE / (P.k4 * P.rad * P.rad);
 	unsigned long long n_inter = 0, n_push = 0;
@@ -564,9 +572,13 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 			if (tg.valid[k]) {
 				slot[k] = due_list[grp.x + m];
 				const double4 p = pos[slot[k]];
-				const double4 v = vel[slot[k]];
-				const double half = 0.5 * (P.dt * (double)P.tss[(int)p.w]);
-				h[k] = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
+				if (STG == 0) {
+					const double4 v = vel[slot[k]];
+					const double half = 0.5 * (P.dt * (double)P.tss[(int)p.w]);
+					h[k] = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
+				} else {
+					h[k] = make_double3(p.x, p.y, p.z);
+				}
 			}
 			tg.self[k] = slot[k];
 			tg.t[k] = make_float3((float)((h[k].x - P.rad) * P.inv_rad), (float)((h[k].y - P.rad) * P.inv_rad),
@@ -574,7 +586,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 		}
 		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, depth, err, split);
+		const Field<TPL> ef = group_walk<TPL>(tg, T, srcf, P, sm, ne, depth, err, split);
 		stack_max = max(stack_max, depth);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
@@ -589,7 +601,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 			const int sp = (int)p.w;
 			const double dt = P.dt * (double)P.tss[sp];
 			n_inter += ne;
-			n_push++;
+			if (STG != 1) n_push++;
 			double E[3] = { (double)ef.x[k] * escale, (double)ef.y[k] * escale, (double)ef.z[k] * escale };
 			if (P.shape && sp != SP_DUST) {
 				// the spheroid's own field in FP64 (pot-spheroid.c:1815-1819)
@@ -601,10 +613,27 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 			}
 			const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
 			const double qom = (QE * charge) / mass_of(sp, P);
+			if (STG == 1) {
+				const double3 a1 = accel_lorentz(E, v, qom, P);
+				double4 pm = p;
+				half_first(pm, v, a1, dt, P);
+				pos[s] = pm;
+				vel[s] = v;
+				sb.acc[s] = make_double4(a1.x, a1.y, a1.z, 0.0);
+				sb.src32b[s] = make_float4((float)((pm.x - P.rad) * P.inv_rad), (float)((pm.y - P.rad) * P.inv_rad),
+				                           (float)((pm.z - P.rad) * P.inv_rad), src32[s].w);
+				sb.src64b[s] = make_double4(pm.x, pm.y, pm.z, src64[s].w);
+				continue;
+			}
 			double3 xn;
-			boris(v, h[k], E, qom, dt, P, xn);
+			if (STG == 0) {
+				boris(v, h[k], E, qom, dt, P, xn);
+			} else {
+				const double4 a = sb.acc[s];
+				half_second(xn, v, p, make_double3(a.x, a.y, a.z), accel_lorentz(E, v, qom, P), dt, P);
+			}
 			uint32_t reason = 0;
-			if (!grain_due) reason = after_push(sp, p, xn, v, P, rec, absorb_on, gx, gy, gz);
+			if (!grain_due) reason = after_push(sp, STG == 0 ? p : src64[s], xn, v, P, rec, absorb_on, gx, gy, gz);
 			pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
 			vel[s] = v;
 			if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
@@ -778,18 +807,32 @@ void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, 
 	}
 }
 
+template <int STG>
+static void push_fast_stage(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,
+                            const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P,
+                            RunRec* rec, const StageBufs& sb, cudaStream_t s)
+{
+	const int nb = sm_count_fast() * 6;
+	if (P.group_max > 32) {
+		k_push_fast<2, STG><<<nb, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list, P, rec,
+		                                                 src64, sb);
+	} else {
+		k_push_fast<1, STG><<<nb, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list, P, rec,
+		                                                 src64, sb);
+	}
+}
+
 void launch_push_fast(double4* pos, double4* vel, const TreeDev& T, const float4* src32, const double4* src64,
                       const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P,
-                      RunRec* rec, cudaStream_t s, Timer& tm)
+                      RunRec* rec, const StageBufs& sb, cudaStream_t s, Timer& tm)
 {
-	(void)src64;
-	ScopedKernel k(tm, "walk_push_fast");
-	if (P.group_max > 32) {
-		k_push_fast<2><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list,
-		                                                            P, rec);
+	ScopedKernel k(tm, sb.stage == 0 ? "walk_push_fast" : (sb.stage == 1 ? "walk_half1_fast" : "walk_half2_fast"));
+	if (sb.stage == 0) {
+		push_fast_stage<0>(pos, vel, T, src32, src64, due_list, groups, rein_list, P, rec, sb, s);
+	} else if (sb.stage == 1) {
+		push_fast_stage<1>(pos, vel, T, src32, src64, due_list, groups, rein_list, P, rec, sb, s);
 	} else {
-		k_push_fast<1><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list,
-		                                                            P, rec);
+		push_fast_stage<2>(pos, vel, T, src32, src64, due_list, groups, rein_list, P, rec, sb, s);
 	}
 }
 

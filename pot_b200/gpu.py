@@ -38,7 +38,8 @@ STATUS_NAMES = {0: "POT_OK", -1: "POT_E_ARG", -2: "POT_E_CUDA", -3: "POT_E_NOMEM
 NOALLOC_MAX_POINTS = 65536
 FORM_PLAIN, FORM_FAST = 0, 1
 STEP_EPE = 0x1
-CFG_SCEPTIC, CFG_DISABLE_GRAIN = 0x1, 0x2
+CFG_SCEPTIC, CFG_DISABLE_GRAIN, CFG_DIPOLES, CFG_POIS_IONS = 0x1, 0x2, 0x4, 0x8
+INT_BORIS, INT_VERLET, INT_EULER_RICHARDSON = 0, 1, 2
 OPT_TIMING = 0x1
 
 
@@ -53,7 +54,8 @@ class _RunCfg(C.Structure):
     _fields_ = [("N", C.c_uint64), ("r", C.c_uint32), ("flags", C.c_uint32), ("dt", C.c_double),
                 ("mpp", C.c_double), ("soft", C.c_double), ("Te", C.c_double), ("Ti", C.c_double),
                 ("x_drift", C.c_double), ("a", C.c_double), ("settle", C.c_double), ("theta", C.c_double),
-                ("B", C.c_double * 3), ("A", C.c_double), ("axis", C.c_double * 3)]
+                ("B", C.c_double * 3), ("A", C.c_double), ("axis", C.c_double * 3), ("bounce", C.c_double),
+                ("integrator", C.c_uint32), ("pad", C.c_uint32)]
 
 
 class _Opts(C.Structure):
@@ -73,7 +75,8 @@ class _Stats(C.Structure):
                 ("n_absorbed", C.c_uint64), ("n_reinjected", C.c_uint64), ("n_pushed", C.c_uint64),
                 ("interactions", C.c_uint64), ("n_nodes", C.c_uint64), ("chi_b", C.c_double),
                 ("status", C.c_int32), ("stack_max", C.c_uint32), ("epe", C.c_double * 3),
-                ("q_sum", C.c_int64), ("warn", C.c_uint32), ("pad2", C.c_uint32)]
+                ("q_sum", C.c_int64), ("warn", C.c_uint32), ("n_collected", C.c_uint32),
+                ("n_wall", C.c_uint32), ("n_bounced", C.c_uint32)]
 
 
 _LIB = None
@@ -127,6 +130,8 @@ def load_library(path: str = LIB_PATH, build_if_stale: bool = True):
     L.pot_gpu_launch_count.argtypes = [vp, C.POINTER(u64)]
     L.pot_gpu_macro.argtypes = [vp, C.POINTER(_MacroSums)]
     L.pot_gpu_grain.argtypes = [vp, C.POINTER(_Grain)]
+    L.pot_gpu_set_ion_temp.argtypes = [vp, C.c_double]
+    L.pot_gpu_ion_temp.argtypes = [vp, C.POINTER(C.c_double)]
     L.pot_gpu_bytes_needed.argtypes = [C.POINTER(_RunCfg), C.POINTER(_Opts), C.POINTER(u64)]
     L.pot_gpu_tune.argtypes = [C.POINTER(_RunCfg), C.POINTER(_Opts), u32, C.POINTER(C.c_double)]
     L.pot_batch_create.argtypes = [C.POINTER(_BatchOpts), C.POINTER(vp)]
@@ -189,11 +194,19 @@ class RunConfig:
     sceptic: bool = True
     disable_grain: bool = False
     axis: Sequence[float] = field(default_factory=lambda: (0.0, 0.0, 0.0))
+    # the reference's other compile-time variants (pot.c:99-133, 165-173)
+    bounce: float = 0.0          # OUT_BOUNCE coefficient of restitution; 0 = reinjection
+    integrator: int = INT_BORIS  # INT_BORIS, INT_VERLET or INT_EULER_RICHARDSON
+    dipoles: bool = False        # DIPOLES (plain form)
+    pois_ions: bool = False      # POIS_POS_COLLECTION
 
     def to_c(self) -> _RunCfg:
         c = _RunCfg()
         c.N, c.r = int(self.N), int(self.r)
-        c.flags = (CFG_SCEPTIC if self.sceptic else 0) | (CFG_DISABLE_GRAIN if self.disable_grain else 0)
+        c.flags = ((CFG_SCEPTIC if self.sceptic else 0) | (CFG_DISABLE_GRAIN if self.disable_grain else 0)
+                   | (CFG_DIPOLES if self.dipoles else 0) | (CFG_POIS_IONS if self.pois_ions else 0))
+        c.bounce = float(self.bounce)
+        c.integrator = int(self.integrator)
         c.dt, c.mpp, c.soft, c.Te, c.Ti = self.dt, self.mpp, self.soft, self.Te, self.Ti
         c.x_drift, c.a, c.settle, c.theta, c.A = self.x_drift, self.a, self.settle, self.theta, self.A
         for k in range(3):
@@ -328,6 +341,15 @@ class Run:
         g = _Grain()
         self._check(self.lib.pot_gpu_grain(self.h, C.byref(g)), "pot_gpu_grain")
         return _grain_dict(g)
+
+    def set_ion_temp(self, Ti: float):
+        """The cached ion temperature of the Poisson ion collection."""
+        self._check(self.lib.pot_gpu_set_ion_temp(self.h, float(Ti)), "pot_gpu_set_ion_temp")
+
+    def ion_temp(self) -> float:
+        t = C.c_double()
+        self._check(self.lib.pot_gpu_ion_temp(self.h, C.byref(t)), "pot_gpu_ion_temp")
+        return t.value
 
     # -- inspection ---------------------------------------------------------------
     def build_tree(self) -> int:
