@@ -19,7 +19,12 @@
  *   --oap X (OAP, pot.c:97), --bx/--by/--bz T (EXTERNAL_B_*, pot.c:55-57),
  *   --no-sceptic (SCEPTIC_REINJECTION, pot.c:181), --disable-grain
  *   (DISABLE_GRAIN, pot.c:30), --prolate / --oblate (pot-spheroid.c's
- *   PROLATE / OBLATE programs, with that program's defaults), and for the
+ *   PROLATE / OBLATE programs, with that program's defaults), --dipoles
+ *   (DIPOLES, pot.c:99-104; plain form), --bounce C (OUT_BOUNCE C,
+ *   pot.c:113-119), --integrator boris|verlet|euler-richardson (BORIS,
+ *   EULER_RICHARDSON, pot.c:121-133), --pois-ions (POIS_POS_COLLECTION,
+ *   pot.c:165-173; the macroscopic summary refreshes the cached ion
+ *   temperature as pot.c:3444-3448 does), and for the
  *   GPU: --form fast|plain, --leaf N, --group 32|64, --seed S, --axis x,y,z
  *   (spheroid axis; x in the reference), --output-dir DIR.
  * Random numbers: the device draws from Philox4x32-10 streams keyed by a
@@ -72,6 +77,9 @@ typedef struct {
 	double oap;
 	double B[3];
 	bool sceptic, disable_grain;
+	bool dipoles, pois_ions;
+	double bounce;             /* 0: reinjection at the wall */
+	unsigned int integrator;   /* POT_INT_* */
 	int shape; /* 0 sphere, 1 prolate, 2 oblate */
 	double A;
 	double axis[3];
@@ -151,8 +159,9 @@ static void usage(const char* prog)
 	e_puts("  -x [NUMBER]   drift velocity in x-direction");
 	e_puts("The reference's compile-time switches:");
 	e_puts("  --oap X  --bx T --by T --bz T  --no-sceptic  --disable-grain  --prolate  --oblate");
+	e_puts("  --dipoles  --bounce C  --integrator boris|verlet|euler-richardson  --pois-ions");
 	e_puts("GPU execution:");
-	e_puts("  --form fast|plain  --leaf N  --group 32|64  --seed S  --axis X,Y,Z  --output-dir DIR");
+	e_puts("  --form fast|plain  --leaf N  --group 8|16|32|64  --seed S  --axis X,Y,Z  --output-dir DIR");
 	e_puts("  --host-macro  compute the summary from downloaded particles (default: on the device)");
 }
 
@@ -176,12 +185,26 @@ static int parse_args(int argc, char** argv, Run* ru)
 			if (!strcmp(f, "--no-sceptic")) { ru->sceptic = false; continue; }
 			if (!strcmp(f, "--disable-grain")) { ru->disable_grain = true; continue; }
 			if (!strcmp(f, "--host-macro")) { ru->host_macro = true; continue; }
+			if (!strcmp(f, "--dipoles")) { ru->dipoles = true; continue; }
+			if (!strcmp(f, "--pois-ions")) { ru->pois_ions = true; continue; }
 			if (!want(&n, argc)) return 1;
 			const char* v = argv[n];
 			if (!strcmp(f, "--oap")) ru->oap = strtod(v, NULL);
 			else if (!strcmp(f, "--bx")) ru->B[0] = strtod(v, NULL);
 			else if (!strcmp(f, "--by")) ru->B[1] = strtod(v, NULL);
 			else if (!strcmp(f, "--bz")) ru->B[2] = strtod(v, NULL);
+			else if (!strcmp(f, "--bounce")) {
+				ru->bounce = strtod(v, NULL);
+				if (!(ru->bounce >= 0.0)) {
+					e_puts("Coefficient of restitution must be non-negative.");
+					return 2;
+				}
+			} else if (!strcmp(f, "--integrator")) {
+				if (!strcmp(v, "boris")) ru->integrator = POT_INT_BORIS;
+				else if (!strcmp(v, "verlet")) ru->integrator = POT_INT_VERLET;
+				else if (!strcmp(v, "euler-richardson")) ru->integrator = POT_INT_EULER_RICHARDSON;
+				else return 1;
+			}
 			else if (!strcmp(f, "--form")) {
 				if (!strcmp(v, "fast")) ru->form = POT_FORM_FAST;
 				else if (!strcmp(v, "plain")) ru->form = POT_FORM_PLAIN;
@@ -317,6 +340,11 @@ static void output_args_for_run(const char* prog, const Run* ru)
 	if (ru->B[0] != 0.0 || ru->B[1] != 0.0 || ru->B[2] != 0.0) printf(" --bx %g --by %g --bz %g", ru->B[0], ru->B[1], ru->B[2]);
 	if (!ru->sceptic) printf(" --no-sceptic");
 	if (ru->disable_grain) printf(" --disable-grain");
+	if (ru->dipoles) printf(" --dipoles");
+	if (ru->bounce > 0.0) printf(" --bounce %g", ru->bounce);
+	if (ru->integrator == POT_INT_VERLET) printf(" --integrator verlet");
+	if (ru->integrator == POT_INT_EULER_RICHARDSON) printf(" --integrator euler-richardson");
+	if (ru->pois_ions) printf(" --pois-ions");
 	if (ru->shape == 1) printf(" --prolate");
 	if (ru->shape == 2) printf(" --oblate");
 	printf(" --form %s", ru->form == POT_FORM_PLAIN ? "plain" : "fast");
@@ -448,13 +476,19 @@ static void write_run_description(const Run* ru)
 	fputs(ru->disable_grain ? "grain:                disabled\n" : "grain:                enabled\n", fp);
 	fputs("OpenGL interface:     no\n", fp);
 	fputs("trajectory length:    N/A\n", fp);
-	fputs(ru->sceptic ? "containment:          reinjection (SCEPTIC-style)\n"
-	                  : "containment:          reinjection (old-style)\n", fp);
+	if (ru->bounce > 0.0) {
+		fprintf(fp, "containment:          bouncing (c.o.e. %g)\n", ru->bounce);
+	} else {
+		fputs(ru->sceptic ? "containment:          reinjection (SCEPTIC-style)\n"
+		                  : "containment:          reinjection (old-style)\n", fp);
+	}
 	fputs("FP exceptions:        no\n", fp);
-	fputs("multipole expansion:  monopole\n", fp);
+	fputs(ru->dipoles ? "multipole expansion:  dipole\n" : "multipole expansion:  monopole\n", fp);
 	fputs("simulation shape:     spherical\n", fp);
-	fputs("numerical integrator: Boris\n", fp);
-	fputs("pos. Pois. collec'n:  no\n", fp);
+	fputs(ru->integrator == POT_INT_EULER_RICHARDSON ? "numerical integrator: Euler-Richardson\n"
+	      : ru->integrator == POT_INT_VERLET ? "numerical integrator: velocity Verlet\n"
+	                                         : "numerical integrator: Boris\n", fp);
+	fputs(ru->pois_ions ? "pos. Pois. collec'n:  yes\n" : "pos. Pois. collec'n:  no\n", fp);
 	fputs("Langmuir test wave:   no\n", fp);
 	fputs("P-P interactions:     yes\n", fp);
 	fputs(ru->shape == 1 ? "Grain shape:          prolate spheroid\n\n"
@@ -589,6 +623,13 @@ static int record_row(FILE* fp, const Run* ru, pot_gpu_ctx* ctx, pot_particle* P
 	if (ru->host_macro) {
 		if ((rc = pot_gpu_download(ctx, P, g)) != POT_OK) return rc;
 		host_macro_sums(ru, P, &m);
+		if (ru->pois_ions && m.n_i > 0.0) {
+			/* the measured ion temperature becomes the cached one, pot.c:3442-3448
+			   (pot_gpu_macro does this on the device) */
+			double Ti = m.T_i;
+			Ti *= (mass_of(ru, ION) / (3.0 * KB)) / m.n_i;
+			if ((rc = pot_gpu_set_ion_temp(ctx, Ti)) != POT_OK) return rc;
+		}
 	} else {
 		if ((rc = pot_gpu_macro(ctx, &m)) != POT_OK) return rc;
 		if ((rc = pot_gpu_grain(ctx, g)) != POT_OK) return rc;
@@ -863,7 +904,10 @@ int main(int argc, char** argv)
 	memset(&opt, 0, sizeof(opt));
 	cfg.N = ru.N;
 	cfg.r = ru.r;
-	cfg.flags = (ru.sceptic ? POT_CFG_SCEPTIC : 0u) | (ru.disable_grain ? POT_CFG_DISABLE_GRAIN : 0u);
+	cfg.flags = (ru.sceptic ? POT_CFG_SCEPTIC : 0u) | (ru.disable_grain ? POT_CFG_DISABLE_GRAIN : 0u) |
+	            (ru.dipoles ? POT_CFG_DIPOLES : 0u) | (ru.pois_ions ? POT_CFG_POIS_IONS : 0u);
+	cfg.bounce = ru.bounce;
+	cfg.integrator = ru.integrator;
 	cfg.dt = (double)ru.dt;
 	cfg.mpp = ru.mpp;
 	cfg.soft = ru.soft;

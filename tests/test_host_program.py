@@ -170,3 +170,30 @@ def test_spheroid_program_flags(potgpu, tmp_path):
     assert "ion/electron mass ratio: 1836.15" in d
     rows = (out / "pot-macroscopic.dat").read_text().splitlines()[1:]
     assert len(rows) == 30
+
+
+def test_variant_switches_listed(potgpu):
+    p = run(["-l", "--dipoles", "--bounce", "0.9", "--integrator", "euler-richardson", "--pois-ions"])
+    assert p.returncode == 0
+    assert "--dipoles --bounce 0.9 --integrator euler-richardson --pois-ions" in p.stdout
+    p = run(["--integrator", "leapfrog"])
+    assert p.returncode != 0
+    p = run(["--bounce", "-1"])
+    assert p.returncode != 0 and "restitution" in p.stderr
+
+
+@pytest.mark.gpu
+def test_variant_program_run(potgpu, tmp_path):
+    """A run with every variant of pot.c's switches (plain form, since the
+    dipole moments are plain-form): the description names them and the
+    summary rows are written."""
+    out = tmp_path / "v"
+    out.mkdir()
+    p = run(SMALL_FLAGS + ["-i", "12", "--seed", "3", "--form", "plain", "--dipoles", "--bounce", "0.95",
+                           "--integrator", "verlet", "--pois-ions", "--output-dir", str(out)])
+    assert p.returncode == 0, p.stderr
+    d = (out / "pot-run-descrip.txt").read_text()
+    assert "multipole expansion:  dipole" in d and "numerical integrator: velocity Verlet" in d
+    assert "pos. Pois. collec'n:  yes" in d and "containment:          bouncing (c.o.e. 0.95)" in d
+    rows = (out / "pot-macroscopic.dat").read_text().splitlines()[1:]
+    assert len(rows) == 12
