@@ -172,14 +172,19 @@ def cpu_baseline_reference(cfg_name: str):
 
 
 def _ref_rank_worker(args):
-    cfg_name, nprocs, rank, n_steps, q = args
+    cfg_name, nprocs, rank, n_steps, budget_s, q = args
     from oracle.oracle import RefLib, RunParams
     from pot_b200.configs import run_params, variant
     p = RunParams(**run_params(cfg_name, untilted=True))
     ref = RefLib(variant(cfg_name), build=False)
     ref.setup(p, seed=1, nprocs=nprocs, rank=rank)
     times = []
-    for _ in range(n_steps):
+    start = time.perf_counter()
+    # the run is a bounded sample: steps stop at n_steps or once budget_s of
+    # stepping has passed (at least two steps)
+    for k in range(n_steps):
+        if k >= 2 and time.perf_counter() - start > budget_s:
+            break
         t0 = time.perf_counter()
         ref.step()
         times.append(time.perf_counter() - t0)
@@ -205,20 +210,38 @@ def run_reference_arm(args):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     n = args.warmup + args.steps
-    procs = [ctx.Process(target=_ref_rank_worker, args=((args.config, P, r, n, q),)) for r in range(P)]
+    budget_s = 150.0
+    procs = [ctx.Process(target=_ref_rank_worker, args=((args.config, P, r, n, budget_s, q),)) for r in range(P)]
     for pr in procs:
         pr.start()
     res = {}
-    for _ in range(P):
-        r, times = q.get()
-        res[r] = times
+    import queue as _queue
+    failed = None
+    while len(res) < P and failed is None:
+        try:
+            r, times = q.get(timeout=10)
+            res[r] = times
+        except _queue.Empty:
+            dead = [pr.exitcode for pr in procs if pr.exitcode not in (None, 0)]
+            if dead:
+                failed = "a reference rank exited with status %d" % dead[0]
     for pr in procs:
+        if failed is not None and pr.is_alive():
+            pr.terminate()
         pr.join()
-    per_step = [max(res[r][k] for r in range(P)) for k in range(n)][args.warmup:]
+    if failed is not None:
+        print(json.dumps({"impl": "reference", "unavailable": failed}), flush=True)
+        return 1
+    # every rank ran the same steps up to its budget; the common prefix, less
+    # the warm-up steps (at most half of it), is timed
+    common = min(len(res[r]) for r in range(P))
+    w = min(args.warmup, common // 2)
+    per_step = [max(res[r][k] for r in range(P)) for k in range(common)][w:]
+    timed = len(per_step)
     t = sum(per_step)
-    value = (N - 1) * args.steps / t
+    value = (N - 1) * timed / t
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / timed,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/x87",
             "data": "synthetic", "config": {"workload": WORKLOADS.get(args.config, args.config), "N": N,
                                             "reference_axis": "x (the reference cannot tilt its grain)"
@@ -227,7 +250,8 @@ def run_reference_arm(args):
                              "sample": "%d processes, each one MPI rank of a %d-rank run of the reference pot.c "
                                        "(gcc -O2, single-rank MPI stand-in): full tree build plus its own block "
                                        "of ~%d particles per step; step time = max over ranks; no MPI "
-                                       "communication counted" % (P, P, N // P)},
+                                       "communication counted; %d timed steps after %d warm-up (at most %.0f s "
+                                       "of stepping per rank)" % (P, P, N // P, timed, w, budget_s)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0

@@ -400,6 +400,16 @@ int potref_step(int compute_epe)
 	H.t_steps++;
 	if (build_tree(&H, R) == NULL) return -1;
 	move_particles(&H, R, H.root, H_mpi_particle, compute_epe != 0, H.t_steps);
+	if (H.rank) {
+		/* A worker rank of a multi-rank run: its stepped block reaches its
+		   own particle array only through the master's broadcast at the
+		   next step (pot.c:4299), which the single-rank stand-in does not
+		   carry, so copy the block back here.  Without it the in-place
+		   half drifts (pot.c:2478-2485) accumulate and the block leaves the
+		   domain unreinjected. */
+		const unsigned int a = H.pits[H.rank][0], b = H.pits[H.rank][1];
+		memcpy(&H.parts[a], &H.new_parts[a], sizeof(Particle) * (b - a + 1));
+	}
 	return 0;
 }
 

@@ -143,6 +143,17 @@ __device__ __forceinline__ void eval_src(Acc<2>& E, const TgtE<2>& t, const floa
 	}
 }
 
+// Two staged sources (x, y, z, q) in float4 slots 2p and 2p + 1 become one
+// FP32x2 operand pair, (-xa, -xb, -ya, -yb) and (-za, -zb, qa, qb), in place:
+// with one target per lane the packed instructions evaluate two sources at
+// once against the (duplicated) target.
+__device__ __forceinline__ void pair_pack(float4* buf, int p)
+{
+	const float4 a = buf[2 * p], b = buf[2 * p + 1];
+	buf[2 * p] = make_float4(-a.x, -b.x, -a.y, -b.y);
+	buf[2 * p + 1] = make_float4(-a.z, -b.z, a.w, b.w);
+}
+
 __device__ __forceinline__ void add_xor(Acc<1>& E, int o)
 {
 	E.x += __shfl_xor_sync(0xffffffffu, E.x, o);
@@ -255,10 +266,26 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 	const float eps2 = fmaxf(P.soft2_f, 1e-20f);
 	const bool single_leaves = P.leaf_size == 1;
 	const int sub = (int)lane / (32 / split);  // this lane's share of each staged list
-	TgtE<TPL> te;
-	Acc<TPL> E;
-	to_eval(tg, te, E);
+	// Evaluation is FP32x2 in both forms.  Two targets per lane: each pair is
+	// the lane's two targets against one duplicated source.  One target per
+	// lane: each pair is two sources (packed by pair_pack at the flush)
+	// against the duplicated target, and the two halves are added at the end.
+	TgtE<2> te;
+	Acc<2> E;
+	if constexpr (TPL == 1) {
+		te.x = make_float2(tg.t[0].x, tg.t[0].x);
+		te.y = make_float2(tg.t[0].y, tg.t[0].y);
+		te.z = make_float2(tg.t[0].z, tg.t[0].z);
+		E.x = E.y = E.z = make_float2(0.f, 0.f);
+	} else {
+		to_eval(tg, te, E);
+	}
 	Acc<TPL>* tag = nullptr;  // selects the staging layout
+	// staged sources per evaluation (a pair of sources with one target per lane)
+	constexpr int PER_EV = TPL == 1 ? 2 : 1;
+	// cell evaluations unrolled per lane: 8, or 4 for a split list of pairs
+	// (so that the padded list fits the cell buffer)
+	const int cell_unroll = (TPL == 1 && split > 1) ? 4 : 8;
 	int len = 1, ncell = 0, nleaf = 0;
 	uint32_t n_cells_ev = 0, n_parts_ev = 0;
 	if (lane == 0) sm.stack[0] = 0;
@@ -341,20 +368,25 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		// flush staged monopoles, padded to a multiple of 8 with zero-charge
 		// cells far outside the domain so the loop needs no remainder
 		if (ncell >= FW_CELL_FLUSH || (done && ncell > 0)) {
-			const int unit = 8 * split;
+			const int unit = cell_unroll * PER_EV * split;  // <= 32: the padding is one store per lane
 			const int padded = (ncell + unit - 1) / unit * unit;
 			if ((int)lane < padded - ncell) stage_src(sm.cells, ncell + lane, make_float4(64.f, 64.f, 64.f, 0.f), tag);
 			__syncwarp();
+			if (TPL == 1) {
+				for (int p = (int)lane; p < padded / 2; p += 32) pair_pack(sm.cells, p);
+				__syncwarp();
+			}
+			const int nev = padded / PER_EV;
 			if (split == 1) {
-				for (int j = 0; j < padded; j += 8) {
+				for (int j = 0; j < nev; j += 8) {
 #pragma unroll
 					for (int u = 0; u < 8; u++) eval_src<false, POT>(E, te, sm.cells, j + u, eps2);
 				}
 			} else {
-				const int per = padded / split;
-				for (int j = 0; j < per; j += 8) {
+				const int per = nev / split;
+				for (int j = 0; j < per; j += 4) {
 #pragma unroll
-					for (int u = 0; u < 8; u++) eval_src<false, POT>(E, te, sm.cells, (j + u) * split + sub, eps2);
+					for (int u = 0; u < 4; u++) eval_src<false, POT>(E, te, sm.cells, (j + u) * split + sub, eps2);
 				}
 			}
 			n_cells_ev += ncell;
@@ -387,11 +419,16 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 				}
 				stage_src(sm.pbuf, (int)lane, p, tag);
 				__syncwarp();
+				if (TPL == 1) {
+					if (lane < 16) pair_pack(sm.pbuf, (int)lane);
+					__syncwarp();
+				}
+				constexpr int nev = 32 / PER_EV;
 				if (split == 1) {
 #pragma unroll 16
-					for (int m = 0; m < 32; m++) eval_src<true, POT>(E, te, sm.pbuf, m, eps2);
+					for (int m = 0; m < nev; m++) eval_src<true, POT>(E, te, sm.pbuf, m, eps2);
 				} else {
-					const int per = 32 / split;
+					const int per = nev / split;
 #pragma unroll 8
 					for (int m = 0; m < per; m++) eval_src<true, POT>(E, te, sm.pbuf, m * split + sub, eps2);
 				}
@@ -403,10 +440,19 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		}
 		if (done) break;
 	}
-	if (split > 1) {  // add the split partial fields (lanes l, l ^ 16, l ^ 8, ... share a member)
-		for (int o = 16; o >= 32 / split; o >>= 1) add_xor(E, o);
+	Field<TPL> F;
+	if constexpr (TPL == 1) {
+		Acc<1> e1;
+		e1.x = E.x.x + E.x.y;
+		e1.y = E.y.x + E.y.y;
+		e1.z = E.z.x + E.z.y;
+		if (split > 1) {  // add the split partial fields (lanes l, l ^ 16, l ^ 8, ... share a member)
+			for (int o = 16; o >= 32 / split; o >>= 1) add_xor(e1, o);
+		}
+		F = from_eval(e1);
+	} else {
+		F = from_eval(E);
 	}
-	Field<TPL> F = from_eval(E);
 	// take back the members' own terms
 #pragma unroll
 	for (int k = 0; k < TPL; k++) {
