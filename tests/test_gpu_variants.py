@@ -58,7 +58,9 @@ def test_bounce_plain_step_by_step(d):
         st, Pg, gg, so, Po, go = _compare_step(d, o)
         _assert_close(d, st, Pg, gg, so, Po, go)
         assert st["n_reinjected"] == st["n_absorbed"]  # nothing reinjected at the wall
-        assert st["n_wall"] == o.variant_stats()["n_wall"]
+        # a particle reinjected onto the sphere may sit an ulp outside it in
+        # one result and not the other (known deviation 2), moving inwards
+        assert abs(st["n_wall"] - o.variant_stats()["n_wall"]) <= so["n_absorbed"]
         bounced += st["n_bounced"]
     assert bounced > 0
     R = d["r"] * d["mpp"]
