@@ -3,15 +3,18 @@
 //
 // Groups.  Targets are the particles due this step, in Morton order.  A group
 // is a run of at most GROUP_MAX (64) of them lying inside one tree cell (see
-// k_groups), so its bounding box is compact.  A warp owns one group, two
-// targets per lane (lane l holds group members l and l + 32).
+// k_groups), so its bounding box is compact.  A warp owns one group, one or
+// two targets per lane.
 //
 // Walk.  The warp walks the tree once for the whole group:
-//   * opening test per cell against the group's bounding box: accept when
-//     the squared distance from the box to the cell's centre of charge
-//     exceeds (x2 - x1)^2 / OAP^2.  Every target in the box is at least that
-//     far, so each accepted cell also passes the reference's per-target test
-//     (pot.c:1729): the group's list refines every member's list;
+//   * opening test per cell: the reference's test (pot.c:1729), accept when
+//     (x2 - x1)^2 < OAP^2 d^2, with d the distance from the centre of the
+//     group's bounding box to the cell's centre of charge -- the test of the
+//     group's typical member -- and only if no member can lie inside the
+//     cell: the box must be farther from the centre of charge than the
+//     cell's diagonal, sqrt(3) (x2 - x1), so a cell never holds a target it
+//     is accepted for (the reference's self-inclusion at OAP >= 1/sqrt(3)
+//     does not occur);
 //   * accepted cells (monopoles, unsoftened as pot.c:1737-1749) are staged in
 //     shared memory; opened leaves (particle ranges, Plummer-softened as
 //     pot.c:1789-1798, the target excluded by slot) are staged as ranges and
@@ -57,6 +60,16 @@ __device__ __forceinline__ float box_d2(float3 bmin, float3 bmax, float4 c)
 	const float dy = fmaxf(fmaxf(bmin.y - c.y, c.y - bmax.y), 0.0f);
 	const float dz = fmaxf(fmaxf(bmin.z - c.z, c.z - bmax.z), 0.0f);
 	return dx * dx + dy * dy + dz * dz;
+}
+
+// The group's opening test (see the file comment).  r2 = (x2 - x1)^2 / OAP^2
+// in units of R^2, th2 = OAP^2; bc the centre of the group's box.
+__device__ __forceinline__ bool group_accepts(float3 bmin, float3 bmax, float3 bc, float4 c, float r2, float th2)
+{
+	const float db2 = box_d2(bmin, bmax, c);
+	if (db2 <= 3.0f * th2 * r2) return false;  // a member may lie inside the cell
+	const float dx = bc.x - c.x, dy = bc.y - c.y, dz = bc.z - c.z;
+	return dx * dx + dy * dy + dz * dz > r2;
 }
 
 __device__ __forceinline__ int warp_excl(int v, int& total)
@@ -264,6 +277,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		bmax.z = fmaxf(bmax.z, __shfl_xor_sync(0xffffffffu, bmax.z, o));
 	}
 	const float eps2 = fmaxf(P.soft2_f, 1e-20f);
+	const float3 bc = make_float3(0.5f * (bmin.x + bmax.x), 0.5f * (bmin.y + bmax.y), 0.5f * (bmin.z + bmax.z));
 	const bool single_leaves = P.leaf_size == 1;
 	const int sub = (int)lane / (32 / split);  // this lane's share of each staged list
 	// Evaluation is FP32x2 in both forms.  Two targets per lane: each pair is
@@ -306,7 +320,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
 			if (code >= 0) {
 				cell = T.f[code];
-				if (box_d2(bmin, bmax, cell) > T.r2[code]) {
+				if (group_accepts(bmin, bmax, bc, cell, T.r2[code], P.oap2_f)) {
 					acc = cell.w != 0.f;
 				} else {
 					const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * (uint32_t)code]);
@@ -323,7 +337,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
 				} else {
 					cell = T.lf[e];
-					if (box_d2(bmin, bmax, cell) > T.lr2[e]) {
+					if (group_accepts(bmin, bmax, bc, cell, T.lr2[e], P.oap2_f)) {
 						acc = cell.w != 0.f;
 					} else {
 						leafr = true;
