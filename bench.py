@@ -327,11 +327,13 @@ def time_config(name, stream, dev, flush, steps=10, warmup=3, plain_steps=3):
         st = run.step(0)
         return sum(a.elapsed_time(b) for a, b in ev) / k, st
 
-    with Run(cfg, form="fast", leaf_size=cfgd["leaf_size"], seed=cfgd.get("seed", 1), stream=stream.cuda_stream,
-             device=dev.index) as run:
+    group = cfgd.get("group_size", 32)
+    with Run(cfg, form="fast", leaf_size=cfgd["leaf_size"], group_size=group, seed=cfgd.get("seed", 1),
+             stream=stream.cuda_stream, device=dev.index) as run:
         ms, st = timed(run, steps)
     out["fast"] = {"value": (cfg.N - 1) / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
-                   "form": "fast FP32 walk / FP64 state, leaf %d" % cfgd["leaf_size"], "status": st["status"]}
+                   "form": "fast FP32 walk / FP64 state, leaf %d, groups of %d" % (cfgd["leaf_size"], group),
+                   "status": st["status"]}
     with Run(cfg, form="plain", seed=cfgd.get("seed", 1), stream=stream.cuda_stream, device=dev.index) as run:
         msp, stp = timed(run, plain_steps)
     out["plain_fp64"] = {"value": (cfg.N - 1) / (msp / 1e3), "unit": UNIT, "ms_per_step": msp,

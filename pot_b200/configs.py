@@ -36,7 +36,7 @@ CONFIGS = {
                Te=11600.0, Ti=1160.0, x_drift=9785.26, settle=0.0, theta=0.5, steps=10000, leaf_size=16),
     "4m": dict(N=4000001, r=1000, mpp=6.00218e-08, a=7.21387e-07, A=3.0, soft=5.00182e-08, dt=5.96447e-14,
                Te=11600.0, Ti=1160.0, x_drift=4892.63, settle=0.0, theta=0.4, B=(0.0, 0.0, 0.9533),
-               axis=(0.8660254037844387, 0.5, 0.0), steps=20000, leaf_size=16, seed=3,
+               axis=(0.8660254037844387, 0.5, 0.0), steps=20000, leaf_size=16, group_size=64, seed=3,
                variant="prolate_sceptic"),
 }
 
