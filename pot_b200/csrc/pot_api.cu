@@ -61,6 +61,11 @@ struct pot_gpu_ctx {
 	uint64_t bytes = 0;     // device bytes held (or needed, when dry)
 	Timer timer;
 	std::vector<void*> allocs;
+	// one step as a CUDA graph, per buffer parity before the step and per
+	// POT_STEP_EPE (captured on first use; not with event timing)
+	cudaGraphExec_t step_exec[2][2] = { { nullptr, nullptr }, { nullptr, nullptr } };
+	uint64_t step_launches[2][2] = { { 0, 0 }, { 0, 0 } };
+	bool graphs_off = false;  // a capture failed once: enqueue kernel by kernel
 };
 
 // ---------------------------------------------------------------------------
@@ -471,6 +476,9 @@ void pot_gpu_destroy(pot_gpu_ctx* c)
 	if (!c) return;
 	cudaSetDevice(c->device);
 	if (c->stream) cudaStreamSynchronize(c->stream);
+	for (auto& row : c->step_exec)
+		for (auto& g : row)
+			if (g) cudaGraphExecDestroy(g);
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 	delete c;
@@ -762,6 +770,52 @@ static void enqueue_step(pot_gpu_ctx* c, uint32_t flags)
 }
 
 
+// One step: replay of the step's CUDA graph for the current parity (the
+// step's ~25 launches become one), captured the first time; kernel by kernel
+// when timing events are on, when the caller's stream is itself being
+// captured, or after a failed capture.
+static int step_once(pot_gpu_ctx* c, uint32_t flags)
+{
+	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+	if (c->graphs_off || c->timer.enabled || cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess ||
+	    cs != cudaStreamCaptureStatusNone) {
+		enqueue_step(c, flags);
+		return POT_OK;
+	}
+	const int e = (flags & POT_STEP_EPE) ? 1 : 0;
+	const int p = c->cur;
+	if (!c->step_exec[p][e]) {
+		const uint64_t l0 = c->timer.launches;
+		cudaGraph_t g = nullptr;
+		if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+			c->graphs_off = true;
+			enqueue_step(c, flags);
+			return POT_OK;
+		}
+		enqueue_step(c, flags);  // records the launches; flips c->cur
+		const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+		const uint64_t per_step = c->timer.launches - l0;
+		c->cur = p;
+		c->timer.launches = l0;
+		cudaGraphExec_t x = nullptr;
+		if (ec == cudaSuccess && g && cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+			c->step_exec[p][e] = x;
+		}
+		if (g) cudaGraphDestroy(g);
+		if (!c->step_exec[p][e]) {
+			cudaGetLastError();
+			c->graphs_off = true;
+			enqueue_step(c, flags);
+			return POT_OK;
+		}
+		c->step_launches[p][e] = per_step;
+	}
+	CK(cudaGraphLaunch(c->step_exec[p][e], c->stream));
+	c->timer.launches += c->step_launches[p][e];
+	c->cur = p ^ 1;
+	return POT_OK;
+}
+
 int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats* out)
 {
 	if (!c) return POT_E_ARG;
@@ -769,7 +823,10 @@ int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats
 	if (!c->uploaded) return POT_E_STATE;
 	if (c->sticky != POT_OK) return c->sticky;
 	CK(cudaSetDevice(c->device));
-	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c, flags);
+	for (uint32_t k = 0; k < nsteps; k++) {
+		const int rc = step_once(c, flags);
+		if (rc != POT_OK) return rc;
+	}
 	CK(cudaGetLastError());
 	c->tree_valid = true;
 	const int st = sync_status(c);
@@ -808,7 +865,10 @@ int pot_gpu_step_async(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags)
 	if (!c->uploaded) return POT_E_STATE;
 	if (c->sticky != POT_OK) return c->sticky;
 	CK(cudaSetDevice(c->device));
-	for (uint32_t k = 0; k < nsteps; k++) enqueue_step(c, flags);
+	for (uint32_t k = 0; k < nsteps; k++) {
+		const int rc = step_once(c, flags);
+		if (rc != POT_OK) return rc;
+	}
 	CK(cudaGetLastError());
 	c->tree_valid = true;
 	return POT_OK;
