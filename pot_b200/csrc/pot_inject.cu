@@ -123,6 +123,38 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 	double alpha = 0.0, xi0 = 0.0, y0 = s;
 	int intervals = 0;
 	for (;;) {
+		// Most intervals pass within the first few halvings, so halvings 1-8
+		// are tried first: their end points need a recursion 8 deep, not 32.
+		// The full 32-lane batch below runs only when none of them passes,
+		// so the interval chosen is the same either way.
+		{
+			double e = 1.0;
+			const uint32_t top = lane < 8u ? lane : 7u;
+			for (uint32_t k = 0; k <= top; k++) e = (xi0 + e) / 2.0;  // e_{lane+1}
+			double y = 1.0 - (chu2 * e * exp(Rol * (1.0 - (1.0 / e))));
+			y = 1.0 / sqrt((y / s2) - (e * e));
+			const double y_up = __shfl_up_sync(0xffffffffu, y, 1);
+			const double e_up = __shfl_up_sync(0xffffffffu, e, 1);
+			const double y_ek = lane == 0 ? y_one : y_up;
+			const double e_k = lane == 0 ? 1.0 : e_up;
+			const bool linear = lane < 8u && !(fabs(y_ek - y - (y - y0)) > mld);
+			const uint32_t pass = __ballot_sync(0xffffffffu, linear);
+			if (pass) {
+				const int k = __ffs(pass) - 1;
+				const double xk = __shfl_sync(0xffffffffu, e_k, k);
+				const double yk = __shfl_sync(0xffffffffu, y_ek, k);
+				const double ym = __shfl_sync(0xffffffffu, y, k);
+				alpha += (xk - xi0) * (y0 + (4.0 * ym) + yk) / 6.0;
+				xi0 = xk;
+				y0 = yk;
+				if (!(xi0 < 1.0)) break;
+				if (++intervals > SIMPSON_CAP) {
+					fail |= FAIL_SIMPSON;
+					return 0.0;
+				}
+				continue;
+			}
+		}
 		// end points e_0 .. e_32 (lane k holds e_{k+1} and its integrand)
 		double e = 1.0, ek1 = 0.0;
 		for (uint32_t k = 0; k <= lane; k++) e = (xi0 + e) / 2.0;  // e_{lane+1}
