@@ -42,6 +42,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -139,6 +141,78 @@ class Clocks:
             pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
                 "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def reference_tree_field(cfg_name: str, parts, grain, idx, xyz):
+    """The reference's own field_particle_feels_at (pot.c:1696-1808) on its
+    own tree built from the snapshot `parts` (reference order), for the
+    targets idx at xyz; None where the compiled reference is absent."""
+    from oracle.oracle import RefLib, RunParams
+    from pot_b200.configs import run_params, variant
+    try:
+        ref = RefLib(variant(cfg_name), build=False)
+    except Exception:
+        return None
+    p = RunParams(**run_params(cfg_name, untilted=True))
+    ref.setup(p, seed=1, init=False)
+    ref.set_particles(parts)
+    ref.set_grain(q=int(grain["q"]), m=float(grain["m"]), tot_absor_e=int(grain["tot_absor_e"]),
+                  t_steps=int(grain["t_steps"]), chi_b=float(grain["chi_b"]))
+    ref.build_tree()
+    hi, lo = ref.field_many(idx, xyz)
+    return hi + lo
+
+
+def direct_field_fp64(parts, grain, idx, xyz, soft, dev):
+    """FP64 direct sum of the field at xyz for the targets idx over every
+    other particle, every pair softened as the reference's own accuracy check
+    softens them (pot.c:2197-2238); torch on the GPU as the checker's
+    arithmetic."""
+    import torch
+    q = np.where(parts["species"] == 0, float(grain["q"]), np.where(parts["species"] == 1, 1.0, -1.0))
+    src = torch.tensor(np.stack([parts["x"], parts["y"], parts["z"]], 1), dtype=torch.float64, device=dev)
+    qs = torch.tensor(q, dtype=torch.float64, device=dev)
+    tgt = torch.tensor(np.asarray(xyz), dtype=torch.float64, device=dev)
+    tid = torch.tensor(np.asarray(idx, np.int64), device=dev)
+    E = torch.zeros((len(idx), 3), dtype=torch.float64, device=dev)
+    n = len(parts)
+    chunk = 4096
+    for j0 in range(0, n, chunk):
+        s = src[j0:j0 + chunk]
+        d = tgt[:, None, :] - s[None, :, :]
+        r2 = (d * d).sum(-1) + soft * soft
+        w = qs[j0:j0 + chunk][None, :] * torch.rsqrt(r2) / r2
+        jj = torch.arange(j0, j0 + s.shape[0], device=dev)
+        w = w.masked_fill(tid[:, None] == jj[None, :], 0.0)
+        E += (w[..., None] * d).sum(1)
+    return (E * (1.6021766e-19 / (4 * 3.14159265358979 * 8.85419e-12))).cpu().numpy()
+
+
+def force_accuracy(run, cfg_name: str, cfg, dev, n_targets: int = 8192):
+    """Field of the fast form at n_targets sampled particles of the run's
+    current state against an FP64 direct sum and against the reference's own
+    tree on the same snapshot: RMS and 99th percentile of |dE| / |E_direct|."""
+    parts, grain = run.download()
+    rng = np.random.default_rng(12345)
+    idx = np.sort(rng.choice(np.arange(1, len(parts)), n_targets, replace=False)).astype(np.uint32)
+    xyz = np.stack([parts["x"][idx], parts["y"][idx], parts["z"][idx]], 1)
+    run.build_tree()
+    e_fast = run.field_at(idx, xyz)
+    e_dir = direct_field_fp64(parts, grain, idx, xyz, cfg.soft, dev)
+    e_ref = reference_tree_field(cfg_name, parts, grain, idx, xyz)
+    mag2 = (e_dir ** 2).sum(1)
+
+    def stat(e):
+        rel = np.sqrt(((e - e_dir) ** 2).sum(1) / mag2)
+        return {"rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99))}
+
+    out = {"targets": n_targets, "state": "after the timed steps", "direct": "FP64, every pair softened",
+           "fast_vs_direct": stat(e_fast)}
+    if e_ref is not None:
+        out["reference_tree_vs_direct"] = stat(e_ref)
+        rel = np.sqrt(((e_fast - e_ref) ** 2).sum(1) / (e_ref ** 2).sum(1))
+        out["fast_vs_reference_tree"] = {"rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99))}
+    return out
 
 
 def cpu_baseline_reference(cfg_name: str):
@@ -487,8 +561,12 @@ def run_ours(args):
         e2e["value"] = n_plasma * ws * args.e2e_steps / reduce_max(t_e2e, dev)
 
     cpu = None
+    accuracy = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        # the reference leg: the reference's own step for the CPU baseline, and
+        # its own tree for the force comparison
         cpu = cpu_baseline_reference(args.config)
+        accuracy = force_accuracy(run, args.config, cfg, dev)
 
     batch = None
     if ws == 1 and args.batch_runs > 0:
@@ -518,7 +596,8 @@ def run_ours(args):
             "walk_compute": walk_compute(inter, dom_name, per_launch_s, clk),
             "kernels_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
             "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
-            "walk_stack_max": st.get("stack_max"), "extra_configs": extra or None, "batch": batch,
+            "walk_stack_max": st.get("stack_max"), "force_accuracy": accuracy, "extra_configs": extra or None,
+            "batch": batch,
             "status": st["status"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
