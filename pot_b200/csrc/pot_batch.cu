@@ -397,7 +397,8 @@ int pot_gpu_tune(const pot_run_cfg* cfg, pot_gpu_opts* opts, uint32_t steps, dou
 		pot_gpu_ctx* c = nullptr;
 		int rc = pot_gpu_create(cfg, &o, &c);
 		if (rc == POT_OK) rc = pot_gpu_init_particles(c);
-		if (rc == POT_OK) rc = pot_gpu_step(c, 2, 0, nullptr);  // warm-up
+		if (rc == POT_OK) rc = ctx_enqueue(c, 2);  // warm-up, kernel by kernel as the batch enqueues them
+		if (rc == POT_OK) rc = pot_gpu_sync(c);
 		float ms = 0.f;
 		if (rc == POT_OK) {
 			cudaStream_t s = ctx_stream(c);
