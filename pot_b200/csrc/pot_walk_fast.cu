@@ -319,12 +319,15 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 #pragma unroll
 			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
 			if (code >= 0) {
+				// the child codes are loaded with the cell's moments, before the
+				// test, so an opened cell costs one round trip to L2, not two
+				const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * (uint32_t)code]);
 				cell = T.f[code];
-				if (group_accepts(bmin, bmax, bc, cell, T.r2[code], P.oap2_f)) {
+				const float r2 = T.r2[code];
+				const int4 c0 = cp[0], c1 = cp[1];
+				if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
 					acc = cell.w != 0.f;
 				} else {
-					const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * (uint32_t)code]);
-					const int4 c0 = cp[0], c1 = cp[1];
 					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
 					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
 #pragma unroll
@@ -337,11 +340,13 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
 				} else {
 					cell = T.lf[e];
-					if (group_accepts(bmin, bmax, bc, cell, T.lr2[e], P.oap2_f)) {
+					const float r2 = T.lr2[e];
+					const uint2 lr = T.lrange[e];  // with the moments, as for cells
+					if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
 						acc = cell.w != 0.f;
 					} else {
 						leafr = true;
-						range = T.lrange[e];
+						range = lr;
 					}
 				}
 			}
