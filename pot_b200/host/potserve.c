@@ -140,6 +140,15 @@ static bool converged(const Job* j, uint32_t epoch)
 	return fabs(m1 - m0) <= 0.005 * fabs(m1);
 }
 
+/* the grain charge averaged over the run's last 500 steps (NaN if shorter) */
+static double final_mean(const Job* j, uint32_t epoch)
+{
+	const uint32_t w = 500 / epoch;
+	if (j->n_qs < w + 1) return NAN;
+	const uint32_t e = j->n_qs - 1;
+	return (double)(j->qs[e] - j->qs[e - w]) / 500.0;
+}
+
 static void push_q(Job* j, int64_t q)
 {
 	if (j->n_qs == j->cap_qs) {
@@ -392,7 +401,10 @@ int main(int argc, char** argv)
 		const int K = plain_sample < n_jobs ? plain_sample : n_jobs;
 		double t_sum = 0.0, ps_p = 0.0;
 		int conv_p = 0;
+		double* q_fast = calloc((size_t)K, sizeof(double));
+		double* q_plain = calloc((size_t)K, sizeof(double));
 		for (int i = 0; i < K; i++) {
+			q_fast[i] = q_plain[i] = NAN;
 			Job* j = &jobs[i];
 			pot_gpu_opts o;
 			memset(&o, 0, sizeof(o));
@@ -420,6 +432,8 @@ int main(int argc, char** argv)
 			}
 			const double dt = now_s() - t0;
 			pot_gpu_destroy(c);
+			q_fast[i] = final_mean(j, epoch);
+			q_plain[i] = final_mean(&jj, epoch);
 			free(jj.qs);
 			t_sum += dt;
 			ps_p += (double)st * (double)(j->cfg.N - 1);
@@ -429,6 +443,17 @@ int main(int argc, char** argv)
 		       "\"mean_s_per_job\": %.4f, \"particle_steps_per_s\": %.6e, \"note\": \"the first %d jobs, each alone in "
 		       "the plain FP64 form from creation to convergence or --max-steps\"}",
 		       K, conv_p, t_sum, K ? t_sum / K : 0.0, t_sum > 0 ? ps_p / t_sum : 0.0, K);
+		/* the same jobs' charge in both forms: the mean over each run's last
+		   500 steps (fast in the batch, plain alone) */
+		printf(", \"final_charge_fast_vs_plain\": [");
+		for (int i = 0; i < K; i++) {
+			char f1[32], f2[32];
+			printf("%s{\"job\": %d, \"N\": %lu, \"fast\": %s, \"plain\": %s}", i ? ", " : "", i,
+			       (unsigned long)jobs[i].cfg.N, jnum(f1, q_fast[i]), jnum(f2, q_plain[i]));
+		}
+		printf("]");
+		free(q_fast);
+		free(q_plain);
 	}
 	printf("}\n");
 	for (int i = 0; i < n_jobs; i++) free(jobs[i].qs);
