@@ -371,7 +371,8 @@ static int fill_params(pot_gpu_ctx* c)
 		return POT_E_ARG;
 	if (!(r.bounce >= 0.0) || !std::isfinite(r.bounce)) return POT_E_ARG;
 	if (r.integrator > POT_INT_EULER_RICHARDSON) return POT_E_ARG;
-	if ((r.flags & POT_CFG_DIPOLES) && c->opts.form != POT_FORM_PLAIN) return POT_E_ARG;
+	// the fast form's dipole cells are evaluated with one target per lane
+	if ((r.flags & POT_CFG_DIPOLES) && c->opts.form == POT_FORM_FAST && c->opts.group_size > 32) return POT_E_ARG;
 	P.bounce = r.bounce;
 	P.integrator = r.integrator;
 	for (int k = 0; k < 3; k++) P.B[k] = r.B[k];
@@ -615,6 +616,12 @@ static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu
 		AL(T.r2, cap);
 		AL(T.mom_pre, 5 * mom_prefix_entries(n));
 		AL(T.mom_blk, 5 * mom_block_entries(n));
+		if (cfg->flags & POT_CFG_DIPOLES) {
+			AL(T.mom_pre_d, 5 * mom_prefix_entries(n));
+			AL(T.mom_blk_d, 5 * mom_block_entries(n));
+			AL(T.fd, cap);
+			if (L > 1) AL(T.lfd, 8ull * cap);
+		}
 		if (L > 1) {
 			AL(T.lf, 8ull * cap);
 			AL(T.lr2, 8ull * cap);

@@ -538,8 +538,12 @@ __device__ __forceinline__ Mom5 mom_add(const Mom5& u, const Mom5& v)
 	return Mom5 { u.q + v.q, u.a + v.a, u.x + v.x, u.y + v.y, u.z + v.z };
 }
 
+// K = 0: (q, |q|, |q| x, |q| y, |q| z); K = 1 (DIPOLES): (q x, q y, q z, 0, 0);
+// positions relative to the domain centre c
+template <int K>
 __device__ __forceinline__ Mom5 mom_of(const double4& p, double c)
 {
+	if (K == 1) return Mom5 { p.w * (p.x - c), p.w * (p.y - c), p.w * (p.z - c), 0.0, 0.0 };
 	const double a = fabs(p.w);
 	return Mom5 { p.w, a, a * (p.x - c), a * (p.y - c), a * (p.z - c) };
 }
@@ -603,6 +607,7 @@ __device__ __forceinline__ Mom5 mom_shfl(const Mom5& m, int src)
 	              __shfl_sync(0xffffffffu, m.z, src) };
 }
 
+template <int K>
 __global__ void __launch_bounds__(MOM_THREADS) k_mom_reduce(const double4* __restrict__ src64, uint32_t n, double c,
                                                            Mom5* __restrict__ bsum)
 {
@@ -612,7 +617,7 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_reduce(const double4* __res
 	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
 	for (int k = 0; k < MOM_ITEMS; k++) {
 		const size_t i = base + (size_t)k * 32 + lane;
-		if (i < n) s = mom_add(s, mom_of(src64[i], c));
+		if (i < n) s = mom_add(s, mom_of<K>(src64[i], c));
 	}
 	mom_block_excl(s, &tot);
 	if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
@@ -636,6 +641,7 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_top(Mom5* __restrict__ bsum
 	}
 }
 
+template <int K>
 __global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restrict__ src64, uint32_t n, double c,
                                                          const Mom5* __restrict__ bsum, Mom5* __restrict__ pre)
 {
@@ -646,7 +652,7 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restr
 	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
 	for (int k = 0; k < MOM_ITEMS; k++) {
 		const size_t i = base + (size_t)k * 32 + lane;
-		if (i < n) s = mom_add(s, mom_of(src64[i], c));
+		if (i < n) s = mom_add(s, mom_of<K>(src64[i], c));
 	}
 	// reduce the per-lane partial sums to the warp total on lane 0
 	Mom5 wt = s;
@@ -661,7 +667,7 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restr
 	carry = mom_shfl(carry, 0);
 	for (int k = 0; k < MOM_ITEMS; k++) {
 		const size_t i = base + (size_t)k * 32 + lane;
-		const Mom5 v = i < n ? mom_of(src64[i], c) : Mom5 { 0, 0, 0, 0, 0 };
+		const Mom5 v = i < n ? mom_of<K>(src64[i], c) : Mom5 { 0, 0, 0, 0, 0 };
 		const Mom5 inc = mom_warp_incl(v);
 		if (i < n) {
 			pre[i] = mom_add(carry, Mom5 { inc.q - v.q, inc.a - v.a, inc.x - v.x, inc.y - v.y, inc.z - v.z });
@@ -677,7 +683,16 @@ __device__ __forceinline__ Mom5 mom_range(const Mom5* __restrict__ pre, uint32_t
 	return Mom5 { u.q - v.q, u.a - v.a, u.x - v.x, u.y - v.y, u.z - v.z };
 }
 
-__global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, Params P, RunRec* rec)
+// DIPOLES: the dipole about the centre of |q| from the prefix sums of q x
+// (pd) and the cell's charge and centre (relative to the domain centre),
+// p = sum q (x - c) = sum q x - Q c
+__device__ __forceinline__ double3 dipole_of(const Mom5& pd, double q, double cx, double cy, double cz)
+{
+	return make_double3(pd.q - q * cx, pd.a - q * cy, pd.x - q * cz);
+}
+
+__global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, const Mom5* __restrict__ pre_d, Params P,
+                                 RunRec* rec)
 {
 	const uint32_t M = rec->n_nodes;
 	if (M > T.cap) return;
@@ -692,6 +707,11 @@ __global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, Params
 		T.cq[k] = make_double4(cx + P.rad, cy + P.rad, cz + P.rad, (double)q);
 		T.f[k] = make_float4((float)(cx * P.inv_rad), (float)(cy * P.inv_rad), (float)(cz * P.inv_rad), (float)q);
 		T.r2[k] = (float)(T.w2[k] * P.inv_rad * P.inv_rad / P.oap2);
+		if (pre_d) {
+			const double3 d = dipole_of(mom_range(pre_d, T.first[k], T.last[k] + 1), (double)q, cx, cy, cz);
+			T.dip[k] = make_double4(d.x, d.y, d.z, 0.0);
+			T.fd[k] = make_float4((float)(d.x * P.inv_rad), (float)(d.y * P.inv_rad), (float)(d.z * P.inv_rad), 0.f);
+		}
 		if (L > 1) {
 			const float w_child = 0.5f * (float)(sqrt(T.w2[k]) * P.inv_rad);
 			for (int d = 0; d < 8; d++) {
@@ -704,6 +724,12 @@ __global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, Params
 				T.lf[e] = make_float4((float)(lm.x * li * P.inv_rad), (float)(lm.y * li * P.inv_rad),
 				                      (float)(lm.z * li * P.inv_rad), (float)llrint(lm.q));
 				T.lr2[e] = w_child * w_child / P.oap2_f;
+				if (pre_d) {
+					const double3 d = dipole_of(mom_range(pre_d, r.x, r.x + r.y), (double)llrint(lm.q), lm.x * li,
+					                            lm.y * li, lm.z * li);
+					T.lfd[e] = make_float4((float)(d.x * P.inv_rad), (float)(d.y * P.inv_rad),
+					                       (float)(d.z * P.inv_rad), 0.f);
+				}
 			}
 		}
 	}
@@ -754,15 +780,25 @@ void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const 
 		k_finish_nodes<<<blocks_for(n, 256), 256, 0, s>>>(keys, n, L, T.lvl8, T.base, T, P, rec);
 	}
 	{
-		ScopedKernel k(tm, "tree_moments");
-		if (P.form == POT_FORM_FAST && T.mom_pre) {
+		const bool prefix = P.form == POT_FORM_FAST && T.mom_pre;
+		const bool dip = prefix && T.mom_pre_d;
+		ScopedKernel k(tm, "tree_moments", prefix ? (dip ? 7 : 4) : 1);
+		if (prefix) {
 			const uint32_t nb = (uint32_t)((n + MOM_TILE - 1) / MOM_TILE);
 			Mom5* pre = reinterpret_cast<Mom5*>(T.mom_pre);
 			Mom5* bs = reinterpret_cast<Mom5*>(T.mom_blk);
-			k_mom_reduce<<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs);
+			k_mom_reduce<0><<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs);
 			k_mom_top<<<1, MOM_THREADS, 0, s>>>(bs, nb);
-			k_mom_down<<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs, pre);
-			k_moments_prefix<<<blocks_for(n / 4 + 1, 256), 256, 0, s>>>(T, pre, P, rec);
+			k_mom_down<0><<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs, pre);
+			Mom5* pre_d = nullptr;
+			if (dip) {  // DIPOLES: prefix sums of q x as well
+				pre_d = reinterpret_cast<Mom5*>(T.mom_pre_d);
+				Mom5* bs_d = reinterpret_cast<Mom5*>(T.mom_blk_d);
+				k_mom_reduce<1><<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs_d);
+				k_mom_top<<<1, MOM_THREADS, 0, s>>>(bs_d, nb);
+				k_mom_down<1><<<nb, MOM_THREADS, 0, s>>>(src64, n, P.rad, bs_d, pre_d);
+			}
+			k_moments_prefix<<<blocks_for(n / 4 + 1, 256), 256, 0, s>>>(T, pre, pre_d, P, rec);
 		} else if (P.form == POT_FORM_FAST) {
 			k_moments_fast<<<blocks_for(n, 256), 256, 0, s>>>(T, src64, P, rec);
 		} else {

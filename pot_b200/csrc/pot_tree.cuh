@@ -34,6 +34,12 @@ struct TreeDev {
 	// fast form: exclusive prefix sums of (q, |q|, |q| x, |q| y, |q| z), 5 doubles each
 	double* mom_pre;   // [n + 1]
 	double* mom_blk;   // [blocks + 1]
+	// fast form with DIPOLES: prefix sums of (q x, q y, q z) in the same layout,
+	// and the cells' and bucket leaves' dipoles in FP32 units of q R
+	double* mom_pre_d;
+	double* mom_blk_d;
+	float4* fd;        // [cap]
+	float4* lfd;       // [8 * cap]
 };
 
 size_t mom_prefix_entries(size_t n);

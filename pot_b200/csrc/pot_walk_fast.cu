@@ -43,10 +43,12 @@ static_assert(GROUP_MAX == 32 * FW_TPL_MAX, "one group per warp, at most FW_TPL_
 // with two it is stored duplicated and negated as (-x, -x, -y, -y),
 // (-z, -z, q, q) so that each half is a ready operand of the packed FP32x2
 // instructions that evaluate both targets of a lane at once.
-template <int TPL>
+// With DIPOLES (one target per lane) the cell buffer has a second half that
+// holds each staged cell's dipole moment, packed in pairs like the positions.
+template <int TPL, bool DIP = false>
 struct FastSmem {
 	int32_t stack[FW_STACK];
-	float4 cells[FW_CELLS * TPL];
+	float4 cells[FW_CELLS * TPL * (DIP ? 2 : 1)];
 	uint2 leaves[FW_LEAVES];
 	uint32_t loff[FW_LEAVES];  // exclusive prefix of the staged leaves' particle counts
 	float4 pbuf[32 * TPL];     // one 32-particle chunk of opened leaves
@@ -167,6 +169,50 @@ __device__ __forceinline__ void pair_pack(float4* buf, int p)
 	buf[2 * p + 1] = make_float4(-a.z, -b.z, a.w, b.w);
 }
 
+// the dipoles of two staged cells, (px, py, pz, 0) in slots 2p and 2p + 1,
+// become (pxa, pxb, pya, pyb), (pza, pzb, 0, 0), in place
+__device__ __forceinline__ void pair_pack_dip(float4* buf, int p)
+{
+	const float4 a = buf[2 * p], b = buf[2 * p + 1];
+	buf[2 * p] = make_float4(a.x, b.x, a.y, b.y);
+	buf[2 * p + 1] = make_float4(a.z, b.z, 0.f, 0.f);
+}
+
+// Two staged cells with their dipoles (DIPOLES, pot.c:1739-1745) against the
+// duplicated target: E += (q + 3 (p.r) / r^2) r / r^3 - p / r^3, or for the
+// potential q / r + (p.r) / r^3 (pot.c:1966-1974), r from the cell's centre
+// of charge to the target; cells unsoftened.
+template <bool POT>
+__device__ __forceinline__ void eval_cell_dip(Acc<2>& E, const TgtE<2>& t, const float4* buf, const float4* dbuf,
+                                              int i)
+{
+	const float4 a = buf[2 * i], b = buf[2 * i + 1], pa = dbuf[2 * i], pb = dbuf[2 * i + 1];
+	const float2 dx = __fadd2_rn(t.x, make_float2(a.x, a.y));
+	const float2 dy = __fadd2_rn(t.y, make_float2(a.z, a.w));
+	const float2 dz = __fadd2_rn(t.z, make_float2(b.x, b.y));
+	const float2 q = make_float2(b.z, b.w);
+	const float2 px = make_float2(pa.x, pa.y), py = make_float2(pa.z, pa.w), pz = make_float2(pb.x, pb.y);
+	float2 r2 = __fmul2_rn(dz, dz);
+	r2 = __ffma2_rn(dy, dy, r2);
+	r2 = __ffma2_rn(dx, dx, r2);
+	const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+	const float2 ri2 = __fmul2_rn(ri, ri);
+	const float2 ri3 = __fmul2_rn(ri2, ri);
+	float2 pr = __fmul2_rn(pz, dz);
+	pr = __ffma2_rn(py, dy, pr);
+	pr = __ffma2_rn(px, dx, pr);
+	if (POT) {
+		E.x = __ffma2_rn(q, ri, E.x);
+		E.x = __ffma2_rn(pr, ri3, E.x);
+	} else {
+		const float2 w = __fmul2_rn(ri3, __ffma2_rn(make_float2(3.f, 3.f), __fmul2_rn(pr, ri2), q));
+		const float2 nri3 = make_float2(-ri3.x, -ri3.y);
+		E.x = __ffma2_rn(nri3, px, __ffma2_rn(w, dx, E.x));
+		E.y = __ffma2_rn(nri3, py, __ffma2_rn(w, dy, E.y));
+		E.z = __ffma2_rn(nri3, pz, __ffma2_rn(w, dz, E.z));
+	}
+}
+
 __device__ __forceinline__ void add_xor(Acc<1>& E, int o)
 {
 	E.x += __shfl_xor_sync(0xffffffffu, E.x, o);
@@ -235,9 +281,9 @@ __device__ __forceinline__ Field<2> from_eval(const Acc<2>& E)
 // the lanes are split instead: lane l holds member l mod 32/split and
 // evaluates the staged entries with index = sub (mod split), sub = l div
 // 32/split; the split partial fields are added across lanes at the end.
-template <int TPL, bool POT = false>
+template <int TPL, bool POT = false, bool DIP = false>
 __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const float4* __restrict__ src32,
-                                 const Params& P, FastSmem<TPL>& sm, uint32_t& n_eval, uint32_t& stack_max,
+                                 const Params& P, FastSmem<TPL, DIP>& sm, uint32_t& n_eval, uint32_t& stack_max,
                                  int& err, int split = 1)
 {
 	const uint32_t lane = lane_f();
@@ -313,6 +359,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			len -= take;
 			bool acc = false, leafr = false;
 			float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
+			float4 dipole = make_float4(0.f, 0.f, 0.f, 0.f);
 			uint2 range = make_uint2(0u, 0u);
 			int nch = 0;
 			int32_t cc[8];
@@ -325,8 +372,9 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 				cell = T.f[code];
 				const float r2 = T.r2[code];
 				const int4 c0 = cp[0], c1 = cp[1];
+				if (DIP) dipole = T.fd[code];
 				if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
-					acc = cell.w != 0.f;
+					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
 				} else {
 					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
 					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
@@ -342,8 +390,9 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 					cell = T.lf[e];
 					const float r2 = T.lr2[e];
 					const uint2 lr = T.lrange[e];  // with the moments, as for cells
+					if (DIP) dipole = T.lfd[e];
 					if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
-						acc = cell.w != 0.f;
+						acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
 					} else {
 						leafr = true;
 						range = lr;
@@ -359,6 +408,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			const int co = off & 0x3FF, lo = (off >> 10) & 0x3FF, po = off >> 20;
 			const int tcell = tot & 0x3FF, tleaf = (tot >> 10) & 0x3FF, tch = tot >> 20;
 			if (acc) stage_src(sm.cells, ncell + co, cell, tag);
+			if (DIP && acc) sm.cells[FW_CELLS + ncell + co] = dipole;
 			ncell += tcell;
 			if (leafr) sm.leaves[nleaf + lo] = range;
 			nleaf += tleaf;
@@ -389,14 +439,27 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		if (ncell >= FW_CELL_FLUSH || (done && ncell > 0)) {
 			const int unit = cell_unroll * PER_EV * split;  // <= 32: the padding is one store per lane
 			const int padded = (ncell + unit - 1) / unit * unit;
-			if ((int)lane < padded - ncell) stage_src(sm.cells, ncell + lane, make_float4(64.f, 64.f, 64.f, 0.f), tag);
+			if ((int)lane < padded - ncell) {
+				stage_src(sm.cells, ncell + lane, make_float4(64.f, 64.f, 64.f, 0.f), tag);
+				if (DIP) sm.cells[FW_CELLS + ncell + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+			}
 			__syncwarp();
 			if (TPL == 1) {
-				for (int p = (int)lane; p < padded / 2; p += 32) pair_pack(sm.cells, p);
+				for (int p = (int)lane; p < padded / 2; p += 32) {
+					pair_pack(sm.cells, p);
+					if (DIP) pair_pack_dip(sm.cells + FW_CELLS, p);
+				}
 				__syncwarp();
 			}
 			const int nev = padded / PER_EV;
-			if (split == 1) {
+			if (DIP) {  // one target per lane (creation checks the group size)
+				const int stride = split, per = nev / split;
+				for (int j = 0; j < per; j += 4) {
+#pragma unroll
+					for (int u = 0; u < 4; u++)
+						eval_cell_dip<POT>(E, te, sm.cells, sm.cells + FW_CELLS, (j + u) * stride + sub);
+				}
+			} else if (split == 1) {
 				for (int j = 0; j < nev; j += 8) {
 #pragma unroll
 					for (int u = 0; u < 8; u++) eval_src<false, POT>(E, te, sm.cells, j + u, eps2);
@@ -588,7 +651,7 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 
 // STG as in k_push_plain: 0 the Boris step; 1 and 2 the two halves of the
 // non-Boris integrators (stage 2 walks over the intermediate sources).
-template <int TPL, int STG>
+template <int TPL, int STG, bool DIP = false>
 __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel,
                                                             TreeDev T, const float4* __restrict__ src32,
                                                             const uint32_t* __restrict__ due_list,
@@ -597,8 +660,8 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
                                                             RunRec* rec, const double4* __restrict__ src64,
                                                             StageBufs sb)
 {
-	__shared__ FastSmem<TPL> smem[FW_WARPS];
-	FastSmem<TPL>& sm = smem[threadIdx.x >> 5];
+	__shared__ FastSmem<TPL, DIP> smem[FW_WARPS];
+	FastSmem<TPL, DIP>& sm = smem[threadIdx.x >> 5];
 	if (rec->status != POT_OK) return;
 	const uint32_t n_groups = rec->n_groups;
 	const unsigned long long t_step = rec->t_steps;
@@ -651,7 +714,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 		}
 		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> ef = group_walk<TPL>(tg, T, srcf, P, sm, ne, depth, err, split);
+		const Field<TPL> ef = group_walk<TPL, false, DIP>(tg, T, srcf, P, sm, ne, depth, err, split);
 		stack_max = max(stack_max, depth);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
@@ -717,15 +780,15 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 	}
 }
 
-template <int TPL>
+template <int TPL, bool DIP = false>
 __global__ void __launch_bounds__(FW_WARPS * 32) k_field_query_fast(TreeDev T, const float4* __restrict__ src32,
                                                                    const double* __restrict__ xyz,
                                                                    const uint32_t* __restrict__ self_slot,
                                                                    uint32_t nq, double* __restrict__ E, Params P,
                                                                    RunRec* rec)
 {
-	__shared__ FastSmem<TPL> smem[FW_WARPS];
-	FastSmem<TPL>& sm = smem[threadIdx.x >> 5];
+	__shared__ FastSmem<TPL, DIP> smem[FW_WARPS];
+	FastSmem<TPL, DIP>& sm = smem[threadIdx.x >> 5];
 	const uint32_t gsize = 32u * TPL;
 	const uint32_t n_groups = (nq + gsize - 1) / gsize;
 	const double escale = QE / (P.k4 * P.rad * P.rad);
@@ -748,7 +811,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_field_query_fast(TreeDev T, c
 		}
 		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> ef = group_walk<TPL>(tg, T, src32, P, sm, ne, depth, err);
+		const Field<TPL> ef = group_walk<TPL, false, DIP>(tg, T, src32, P, sm, ne, depth, err);
 		if (err != POT_OK && lane_f() == 0) set_status(rec, err);
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
@@ -789,15 +852,15 @@ void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const 
 // compute_epe (pot.c:2771-2804), fast form: groups of up to 32 TPL over
 // every particle, the group walk accumulating potentials; per-group partial
 // sums of q e phi per species, summed in group order by k_epe_final.
-template <int TPL>
+template <int TPL, bool DIP = false>
 __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __restrict__ pos, TreeDev T,
                                                            const float4* __restrict__ src32,
                                                            const double4* __restrict__ src64,
                                                            const uint2* __restrict__ groups,
                                                            double* __restrict__ partial, Params P, RunRec* rec)
 {
-	__shared__ FastSmem<TPL> smem[FW_WARPS];
-	FastSmem<TPL>& sm = smem[threadIdx.x >> 5];
+	__shared__ FastSmem<TPL, DIP> smem[FW_WARPS];
+	FastSmem<TPL, DIP>& sm = smem[threadIdx.x >> 5];
 	if (rec->status != POT_OK) return;
 	const uint32_t n_groups = rec->n_groups_all;
 	const uint32_t gs = rec->grain_slot;
@@ -824,7 +887,7 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 		}
 		uint32_t ne = 0, depth = 0;
 		int err = POT_OK;
-		const Field<TPL> f = group_walk<TPL, true>(tg, T, src32, P, sm, ne, depth, err, split);
+		const Field<TPL> f = group_walk<TPL, true, DIP>(tg, T, src32, P, sm, ne, depth, err, split);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
 			break;
@@ -866,6 +929,9 @@ void launch_epe_fast(const double4* pos, const TreeDev& T, const float4* src32, 
 	if (two) {
 		k_epe_fast<2><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, src64, groups_all, partial, P,
 		                                                            rec);
+	} else if (T.fd) {
+		k_epe_fast<1, true><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, src64, groups_all, partial,
+		                                                                  P, rec);
 	} else {
 		k_epe_fast<1><<<sm_count_fast() * 6, FW_WARPS * 32, 0, s>>>(pos, T, src32, src64, groups_all, partial, P,
 		                                                            rec);
@@ -881,6 +947,9 @@ static void push_fast_stage(double4* pos, double4* vel, const TreeDev& T, const 
 	if (P.group_max > 32) {
 		k_push_fast<2, STG><<<nb, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list, P, rec,
 		                                                 src64, sb);
+	} else if (T.fd) {  // DIPOLES
+		k_push_fast<1, STG, true><<<nb, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list, P,
+		                                                       rec, src64, sb);
 	} else {
 		k_push_fast<1, STG><<<nb, FW_WARPS * 32, 0, s>>>(pos, vel, T, src32, due_list, groups, rein_list, P, rec,
 		                                                 src64, sb);
@@ -912,7 +981,10 @@ void launch_field_query_fast(const TreeDev& T, const float4* src32, const double
 	if (gsize == 64) {
 		k_field_query_fast<2><<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
 	} else {
-		k_field_query_fast<1><<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
+		if (T.fd)
+			k_field_query_fast<1, true><<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
+		else
+			k_field_query_fast<1><<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
 	}
 }
 

@@ -186,3 +186,64 @@ def test_fast_integrator_field_matches_plain(integrator):
           for f in out}
     rel = np.sqrt(((dv["fast"] - dv["plain"]) ** 2).sum(1) / (dv["plain"] ** 2).sum(1))
     assert np.sqrt(np.mean(rel ** 2)) < 0.4
+
+
+def _direct_rms(o, idx, xyz, E):
+    hi, lo = o.field_direct_many(idx, xyz, soften_all=True)
+    E_dir = ld(hi, lo).astype(np.float64)
+    return float(np.sqrt(np.mean(((E - E_dir) ** 2).sum(1) / (E_dir ** 2).sum(1))))
+
+
+@pytest.mark.parametrize("leaf", [1, 16])
+def test_fast_dipoles_field_and_potential(leaf):
+    """DIPOLES in the fast form: cell dipoles from prefix sums of q x, the
+    dipole term in the FP32 walk.  Against an FP64 direct sum the field is
+    more accurate than the same form's monopole field, and the edge
+    potential and potential energies agree with the plain form's dipole
+    results (FP64, the reference's arithmetic) to the FP32 walk's error."""
+    d = dict(SMALL, N=30001)
+    o = oracle_snapshot(d, seed=33, mode="gpu", steps=1)
+    o.set_grain(q=-300)
+    rng = np.random.default_rng(8)
+    P = o.particles()
+    idx = np.sort(rng.choice(np.arange(1, d["N"]), 2048, replace=False)).astype(np.uint32)
+    xyz = np.stack([P["x"][idx], P["y"][idx], P["z"][idx]], 1)
+    out = {}
+    for dip in (False, True):
+        dd = dict(d, dipoles=dip)
+        with gpu_from_oracle(dd, o, form="fast", leaf_size=leaf, group_size=32) as r:
+            r.build_tree()
+            out[dip] = r.field_at(idx, xyz)
+    err_mono, err_dip = _direct_rms(o, idx, xyz, out[False]), _direct_rms(o, idx, xyz, out[True])
+    assert err_dip < 0.8 * err_mono, (err_dip, err_mono)
+    dd = dict(d, dipoles=True)
+    res = {}
+    for form, kw in (("plain", {}), ("fast", dict(leaf_size=leaf, group_size=32))):
+        with gpu_from_oracle(dd, o, form=form, **kw) as r:
+            st = r.step(1, epe=True)
+            res[form] = st
+    assert res["fast"]["status"] == 0
+    # the edge potential: the fast form's FP64 walk over its own (bucket-leaf) tree
+    assert abs(res["fast"]["chi_b"] - res["plain"]["chi_b"]) <= 0.05 * abs(res["plain"]["chi_b"])
+    ep, ef = res["plain"]["epe"], res["fast"]["epe"]
+    assert np.all(np.abs(ef - ep) <= 0.1 * np.abs(ep).max()), (ef, ep)
+
+
+def test_fast_dipoles_run_and_limits():
+    """A fast-form run with dipoles steps and conserves charge; groups of 64
+    (two targets per lane) are refused with dipoles."""
+    from pot_b200.gpu import PotError, Run
+    from common import run_config
+    d = dict(SMALL, N=20001, dipoles=True)
+    o = oracle_snapshot(d, seed=35, mode="gpu", steps=1)
+    o.set_grain(q=-400)
+    with gpu_from_oracle(d, o, form="fast", leaf_size=16, group_size=32) as r:
+        q0 = r.download()[1]["q"]
+        tot = 0
+        for _ in range(10):
+            st = r.step(1)
+            assert st["status"] == 0
+            tot += st["dq"]
+        assert r.download()[1]["q"] == q0 + tot
+    with pytest.raises(PotError):
+        Run(run_config(d), form="fast", leaf_size=16, group_size=64)
