@@ -84,7 +84,8 @@ typedef struct pot_run_cfg {
 #define POT_CFG_SCEPTIC 0x1u        /* SCEPTIC_REINJECTION (pot.c:181): flux-weighted reinjection */
 #define POT_CFG_DISABLE_GRAIN 0x2u  /* DISABLE_GRAIN (pot.c:30): no absorption */
 #define POT_CFG_DIPOLES 0x4u        /* DIPOLES (pot.c:99-104): cells carry dipole moments about their
-                                       centre of charge, used in fields and potentials; plain form */
+                                       centre of charge, used in fields and potentials; in the fast
+                                       form with groups of at most 32 (one target per lane) */
 #define POT_CFG_POIS_IONS 0x8u      /* POIS_POS_COLLECTION (pot.c:165-173, 2837-2854): absorbed ions
                                        add no charge; each step after the settling time the grain
                                        gains a Poisson number of elementary charges at the OML ion

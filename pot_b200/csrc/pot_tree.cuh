@@ -23,7 +23,7 @@ struct TreeDev {
 	uint32_t* aq;      // absolute charge (Tree.aq)
 	double4* cq;       // centre of |q| and q
 	double* w2;        // (x2 - x1)^2
-	double4* dip;      // DIPOLES (plain form): dipole moment about cq; null otherwise
+	double4* dip;      // DIPOLES: dipole moment about cq (FP64, both forms); null otherwise
 	// FP32 walk (fast form only; null otherwise)
 	float4* f;         // centre relative to the domain centre, q
 	float* r2;         // w2 / OAP^2: accepted when d^2 > r2

@@ -197,7 +197,7 @@ class RunConfig:
     # the reference's other compile-time variants (pot.c:99-133, 165-173)
     bounce: float = 0.0          # OUT_BOUNCE coefficient of restitution; 0 = reinjection
     integrator: int = INT_BORIS  # INT_BORIS, INT_VERLET or INT_EULER_RICHARDSON
-    dipoles: bool = False        # DIPOLES (plain form)
+    dipoles: bool = False        # DIPOLES (fast form: groups of at most 32)
     pois_ions: bool = False      # POIS_POS_COLLECTION
 
     def to_c(self) -> _RunCfg:

@@ -20,7 +20,7 @@
  *   --no-sceptic (SCEPTIC_REINJECTION, pot.c:181), --disable-grain
  *   (DISABLE_GRAIN, pot.c:30), --prolate / --oblate (pot-spheroid.c's
  *   PROLATE / OBLATE programs, with that program's defaults), --dipoles
- *   (DIPOLES, pot.c:99-104; plain form), --bounce C (OUT_BOUNCE C,
+ *   (DIPOLES, pot.c:99-104), --bounce C (OUT_BOUNCE C,
  *   pot.c:113-119), --integrator boris|verlet|euler-richardson (BORIS,
  *   EULER_RICHARDSON, pot.c:121-133), --pois-ions (POIS_POS_COLLECTION,
  *   pot.c:165-173; the macroscopic summary refreshes the cached ion
