@@ -209,7 +209,11 @@ int pot_gpu_download(pot_gpu_ctx* ctx, pot_particle* parts, pot_grain_state* gra
 
 /* Drop-in for one iteration of run()'s hot path (pot.c:4299-4386): upload
    `parts` (N records, reference order) and `grain`, t_steps++, build the
-   tree, move the particles, download both back into the same arrays. */
+   tree, move the particles, download both back into the same arrays.  The
+   transfers run in chunks that overlap the conversions (page-locked host
+   memory lets them overlap the most).  On an error status the particle
+   array holds the device's state at the failure (kernels skip their work
+   once a status is set) and `grain` is left as passed. */
 int pot_gpu_move_particles(pot_gpu_ctx* ctx, pot_particle* parts, uint64_t N,
                            pot_grain_state* grain, pot_step_stats* out);
 

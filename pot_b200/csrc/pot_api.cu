@@ -66,6 +66,11 @@ struct pot_gpu_ctx {
 	cudaGraphExec_t step_exec[2][2] = { { nullptr, nullptr }, { nullptr, nullptr } };
 	uint64_t step_launches[2][2] = { { 0, 0 }, { 0, 0 } };
 	bool graphs_off = false;  // a capture failed once: enqueue kernel by kernel
+	// the drop-in call's copy stream, chunk events and pinned records
+	cudaStream_t xfer = nullptr;
+	cudaEvent_t xev[2 * 4 + 1] = {};
+	RunRec* h_rec = nullptr;
+	StepHist* h_hist = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -188,6 +193,45 @@ __global__ void k_to_aos(const double4* __restrict__ pos, const double4* __restr
 	o.species = (int32_t)p.w;
 	o.pad = 0;
 	aos[pid[s]] = o;
+}
+
+// The drop-in call's chunked forms: particles [i0, i0 + cnt) from the host
+// record array, and (gathered through the inverse permutation) back into it
+// with coalesced writes.
+__global__ void k_from_aos_range(const pot_particle* __restrict__ aos, uint32_t i0, uint32_t cnt,
+                                 double4* __restrict__ pos, double4* __restrict__ vel, uint32_t* __restrict__ pid,
+                                 RunRec* rec)
+{
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= cnt) return;
+	const uint32_t i = i0 + k;
+	const pot_particle p = aos[i];
+	int sp = p.species;
+	if (sp < 0 || sp > 2) {
+		set_status(rec, POT_E_ARG);
+		sp = SP_E;
+	}
+	pos[i] = make_double4(p.x, p.y, p.z, (double)sp);
+	vel[i] = make_double4(p.vx, p.vy, p.vz, 0.0);
+	pid[i] = i;
+}
+
+__global__ void k_to_aos_gather(const double4* __restrict__ pos, const double4* __restrict__ vel,
+                                const uint32_t* __restrict__ inv, uint32_t i0, uint32_t cnt,
+                                pot_particle* __restrict__ aos)
+{
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= cnt) return;
+	const uint32_t i = i0 + k;
+	const uint32_t s = inv[i];
+	const double4 p = pos[s];
+	const double4 v = vel[s];
+	pot_particle o;
+	o.x = p.x; o.y = p.y; o.z = p.z;
+	o.vx = v.x; o.vy = v.y; o.vz = v.z;
+	o.species = (int32_t)p.w;
+	o.pad = 0;
+	aos[i] = o;
 }
 
 __global__ void k_inverse(const uint32_t* __restrict__ pid, uint32_t n, uint32_t* __restrict__ inv)
@@ -480,6 +524,12 @@ void pot_gpu_destroy(pot_gpu_ctx* c)
 	for (auto& row : c->step_exec)
 		for (auto& g : row)
 			if (g) cudaGraphExecDestroy(g);
+	if (c->xfer) cudaStreamSynchronize(c->xfer);
+	for (auto& e : c->xev)
+		if (e) cudaEventDestroy(e);
+	if (c->xfer) cudaStreamDestroy(c->xfer);
+	if (c->h_rec) cudaFreeHost(c->h_rec);
+	if (c->h_hist) cudaFreeHost(c->h_hist);
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 	delete c;
@@ -911,14 +961,131 @@ int pot_gpu_download(pot_gpu_ctx* c, pot_particle* parts, pot_grain_state* grain
 	return r.status;
 }
 
+// The drop-in call as one pipeline: the upload in chunks on a copy stream,
+// each chunk converted as soon as it has arrived; the step; the download
+// gathered in chunks in reference order, each chunk copied back while the
+// next is gathered; the run record and step history copied with it.  One
+// wait for the host at the end.  Same results as pot_gpu_upload, pot_gpu_step
+// and pot_gpu_download in turn.
+constexpr int XFER_CHUNKS = 4;
+
+static int xfer_setup(pot_gpu_ctx* c)
+{
+	if (c->xfer) return POT_OK;
+	CK(cudaStreamCreateWithFlags(&c->xfer, cudaStreamNonBlocking));
+	for (auto& e : c->xev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+	CK(cudaMallocHost((void**)&c->h_rec, sizeof(RunRec)));
+	CK(cudaMallocHost((void**)&c->h_hist, sizeof(StepHist) * HIST));
+	return POT_OK;
+}
+
 int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_grain_state* grain,
                            pot_step_stats* out)
 {
-	int rc = pot_gpu_upload(c, parts, N, grain);
+	if (!c || !parts || N != c->cfg.N) return POT_E_ARG;
+	if (parts[0].species != SP_DUST) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	if (!c->aos) {
+		const int ra = dalloc(c, &c->aos, c->n);
+		if (ra) return ra;
+	}
+	int rc = xfer_setup(c);
 	if (rc) return rc;
-	rc = pot_gpu_step(c, 1, 0, out);
-	if (rc) return rc;
-	return pot_gpu_download(c, parts, grain);
+	const uint32_t n = c->n;
+	const int K = n >= 4u * 65536u ? XFER_CHUNKS : 1;
+	// upload: chunk k lands on the copy stream, then is converted on the
+	// context's stream (after whatever that stream already holds)
+	c->cur = 0;
+	CK(cudaEventRecord(c->xev[2 * XFER_CHUNKS], c->stream));  // the copies follow the stream's earlier work
+	CK(cudaStreamWaitEvent(c->xfer, c->xev[2 * XFER_CHUNKS], 0));
+	for (int k = 0; k < K; k++) {
+		const uint32_t i0 = (uint32_t)((uint64_t)n * k / K), i1 = (uint32_t)((uint64_t)n * (k + 1) / K);
+		CK(cudaMemcpyAsync(c->aos + i0, parts + i0, sizeof(pot_particle) * (i1 - i0), cudaMemcpyHostToDevice,
+		                   c->xfer));
+		CK(cudaEventRecord(c->xev[k], c->xfer));
+		CK(cudaStreamWaitEvent(c->stream, c->xev[k], 0));
+		k_from_aos_range<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->aos, i0, i1 - i0, c->pos[0], c->vel[0],
+		                                                              c->pid[0], c->rec);
+	}
+	// the run record, as set_rec_from_grain writes it, from pinned memory
+	{
+		RunRec& r = *c->h_rec;
+		std::memset(&r, 0, sizeof(r));
+		if (grain) {
+			r.grain_q = grain->q;
+			r.grain_m = grain->m;
+			r.grain_pos[0] = grain->x; r.grain_pos[1] = grain->y; r.grain_pos[2] = grain->z;
+			r.grain_vel[0] = grain->vx; r.grain_vel[1] = grain->vy; r.grain_vel[2] = grain->vz;
+			r.tot_absor_e = grain->tot_absor_e;
+			r.t_steps = grain->t_steps;
+			r.chi_b = grain->chi_b;
+		} else {
+			r.grain_m = MASS_DUST;
+			r.grain_pos[0] = parts[0].x; r.grain_pos[1] = parts[0].y; r.grain_pos[2] = parts[0].z;
+			r.grain_vel[0] = parts[0].vx; r.grain_vel[1] = parts[0].vy; r.grain_vel[2] = parts[0].vz;
+		}
+		r.grain_slot = 0xFFFFFFFFu;
+		CK(cudaMemcpyAsync(c->rec, &r, offsetof(RunRec, n_collected), cudaMemcpyHostToDevice, c->stream));
+	}
+	c->sticky = POT_OK;  // as pot_gpu_upload: a new state clears the run's status
+	c->uploaded = true;
+	c->tree_valid = false;
+	// the step
+	rc = step_once(c, 0);
+	if (rc != POT_OK) return rc;
+	c->tree_valid = true;
+	// download in reference order: slot of each particle, then gather and copy by chunks
+	k_inverse<<<nblk(n, 256), 256, 0, c->stream>>>(c->pid[c->cur], n, c->inv);
+	for (int k = 0; k < K; k++) {
+		const uint32_t i0 = (uint32_t)((uint64_t)n * k / K), i1 = (uint32_t)((uint64_t)n * (k + 1) / K);
+		k_to_aos_gather<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->vel[c->cur], c->inv, i0,
+		                                                             i1 - i0, c->aos);
+		CK(cudaEventRecord(c->xev[XFER_CHUNKS + k], c->stream));
+		CK(cudaStreamWaitEvent(c->xfer, c->xev[XFER_CHUNKS + k], 0));
+		CK(cudaMemcpyAsync(parts + i0, c->aos + i0, sizeof(pot_particle) * (i1 - i0), cudaMemcpyDeviceToHost,
+		                   c->xfer));
+	}
+	CK(cudaMemcpyAsync(c->h_rec, c->rec, sizeof(RunRec), cudaMemcpyDeviceToHost, c->stream));
+	if (out) CK(cudaMemcpyAsync(c->h_hist, c->hist, sizeof(StepHist) * HIST, cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaGetLastError());
+	CK(cudaStreamSynchronize(c->xfer));
+	CK(cudaStreamSynchronize(c->stream));
+	c->timer.resolve();
+	const RunRec& r = *c->h_rec;
+	if (r.status != POT_OK && c->sticky == POT_OK) c->sticky = r.status;
+	if (out) {
+		const StepHist& h = c->h_hist[r.t_steps % HIST];
+		std::memset(out, 0, sizeof(*out));
+		out->t_steps = r.t_steps;
+		out->grain_q = r.grain_q;
+		out->dq = h.dq;
+		out->de = h.de;
+		out->n_absorbed = h.n_absorbed;
+		out->n_reinjected = h.n_reinjected;
+		out->n_pushed = h.n_pushed;
+		out->interactions = h.interactions;
+		out->n_nodes = h.n_nodes;
+		out->chi_b = r.chi_b;
+		out->status = r.status;
+		out->stack_max = r.stack_max;
+		for (int k = 0; k < 3; k++) out->epe[k] = h.epe[k];
+		out->q_sum = r.q_sum;
+		out->warn = r.warn;
+		out->n_collected = r.n_collected;
+		out->n_wall = r.n_wall;
+		out->n_bounced = r.n_bounced;
+	}
+	if (r.status != POT_OK) return r.status;
+	if (grain) {
+		grain->q = r.grain_q;
+		grain->m = r.grain_m;
+		grain->x = r.grain_pos[0]; grain->y = r.grain_pos[1]; grain->z = r.grain_pos[2];
+		grain->vx = r.grain_vel[0]; grain->vy = r.grain_vel[1]; grain->vz = r.grain_vel[2];
+		grain->tot_absor_e = r.tot_absor_e;
+		grain->t_steps = r.t_steps;
+		grain->chi_b = r.chi_b;
+	}
+	return POT_OK;
 }
 
 int pot_gpu_build_tree(pot_gpu_ctx* c, uint64_t* n_nodes)

@@ -383,3 +383,31 @@ def test_fast_push_field_accuracy(leaf, group):
         return np.sqrt(np.mean(((a - E_dir) ** 2).sum(1) / (E_dir ** 2).sum(1)))
 
     assert rms(E_fast) <= rms(E_ref) + 1e-3, (rms(E_fast), rms(E_ref))
+
+
+@pytest.mark.parametrize("N,form", [(300001, "fast"), (8193, "fast"), (8193, "plain")])
+def test_move_particles_matches_upload_step_download(N, form):
+    """The drop-in call (chunked transfers overlapping the conversions, one
+    host wait) gives bit for bit what pot_gpu_upload, one step and
+    pot_gpu_download give, twice in a row."""
+    cfg = run_config(dict(SMALL, N=N))
+    kw = dict(leaf_size=16) if form == "fast" else {}
+    with Run(cfg, form=form, seed=3, **kw) as r0:
+        r0.init_particles()
+        r0.step(2)
+        P0, g0 = r0.download()
+    a_parts, a_grain = P0.copy(), dict(g0)
+    b_parts, b_grain = P0.copy(), dict(g0)
+    with Run(cfg, form=form, seed=3, **kw) as ra, Run(cfg, form=form, seed=3, **kw) as rb:
+        for _ in range(2):
+            a_grain, sa = ra.move_particles(a_parts, a_grain)
+            rb.upload(b_parts, b_grain)
+            sb = rb.step(1)
+            b_parts, b_grain = rb.download()
+            assert a_parts.tobytes() == b_parts.tobytes()
+            for k in ("q", "m", "tot_absor_e", "t_steps", "chi_b"):
+                assert a_grain[k] == b_grain[k], k
+            assert np.array_equal(a_grain["pos"], b_grain["pos"]) and np.array_equal(a_grain["vel"], b_grain["vel"])
+            for k in ("t_steps", "grain_q", "dq", "de", "n_absorbed", "n_reinjected", "n_pushed", "interactions",
+                      "n_nodes", "chi_b", "status", "q_sum"):
+                assert sa[k] == sb[k], k
