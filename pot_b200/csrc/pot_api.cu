@@ -741,12 +741,13 @@ int pot_gpu_upload(pot_gpu_ctx* c, const pot_particle* parts, uint64_t N, const 
 	}
 	CK(cudaMemcpyAsync(c->aos, parts, sizeof(pot_particle) * c->n, cudaMemcpyHostToDevice, c->stream));
 	c->cur = 0;
-	k_from_aos<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->aos, c->n, c->pos[0], c->vel[0], c->pid[0], c->rec);
-	CK(cudaGetLastError());
+	// the record first, so a bad species found by the conversion is kept
 	const double4 gp = make_double4(parts[0].x, parts[0].y, parts[0].z, 0.0);
 	const double4 gv = make_double4(parts[0].vx, parts[0].vy, parts[0].vz, 0.0);
 	int rc = set_rec_from_grain(c, grain, gp, gv);
 	if (rc) return rc;
+	k_from_aos<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->aos, c->n, c->pos[0], c->vel[0], c->pid[0], c->rec);
+	CK(cudaGetLastError());
 	c->uploaded = true;
 	c->tree_valid = false;
 	return POT_OK;
@@ -979,35 +980,15 @@ static int xfer_setup(pot_gpu_ctx* c)
 	return POT_OK;
 }
 
-int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_grain_state* grain,
-                           pot_step_stats* out)
+// the copies and kernels of the drop-in call; the caller waits for both
+// streams whatever this returns, so no copy outlives the call
+static int move_enqueue(pot_gpu_ctx* c, pot_particle* parts, const pot_grain_state* grain, bool want_hist)
 {
-	if (!c || !parts || N != c->cfg.N) return POT_E_ARG;
-	if (parts[0].species != SP_DUST) return POT_E_ARG;
-	CK(cudaSetDevice(c->device));
-	if (!c->aos) {
-		const int ra = dalloc(c, &c->aos, c->n);
-		if (ra) return ra;
-	}
-	int rc = xfer_setup(c);
-	if (rc) return rc;
+	int rc = POT_OK;
 	const uint32_t n = c->n;
 	const int K = n >= 4u * 65536u ? XFER_CHUNKS : 1;
-	// upload: chunk k lands on the copy stream, then is converted on the
-	// context's stream (after whatever that stream already holds)
-	c->cur = 0;
-	CK(cudaEventRecord(c->xev[2 * XFER_CHUNKS], c->stream));  // the copies follow the stream's earlier work
-	CK(cudaStreamWaitEvent(c->xfer, c->xev[2 * XFER_CHUNKS], 0));
-	for (int k = 0; k < K; k++) {
-		const uint32_t i0 = (uint32_t)((uint64_t)n * k / K), i1 = (uint32_t)((uint64_t)n * (k + 1) / K);
-		CK(cudaMemcpyAsync(c->aos + i0, parts + i0, sizeof(pot_particle) * (i1 - i0), cudaMemcpyHostToDevice,
-		                   c->xfer));
-		CK(cudaEventRecord(c->xev[k], c->xfer));
-		CK(cudaStreamWaitEvent(c->stream, c->xev[k], 0));
-		k_from_aos_range<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->aos, i0, i1 - i0, c->pos[0], c->vel[0],
-		                                                              c->pid[0], c->rec);
-	}
-	// the run record, as set_rec_from_grain writes it, from pinned memory
+	// the run record first (as set_rec_from_grain writes it, from pinned
+	// memory), so a bad species found by the conversion below is not overwritten
 	{
 		RunRec& r = *c->h_rec;
 		std::memset(&r, 0, sizeof(r));
@@ -1026,6 +1007,20 @@ int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_
 		}
 		r.grain_slot = 0xFFFFFFFFu;
 		CK(cudaMemcpyAsync(c->rec, &r, offsetof(RunRec, n_collected), cudaMemcpyHostToDevice, c->stream));
+	}
+	// upload: chunk k lands on the copy stream, then is converted on the
+	// context's stream (after whatever that stream already holds)
+	c->cur = 0;
+	CK(cudaEventRecord(c->xev[2 * XFER_CHUNKS], c->stream));  // the copies follow the stream's earlier work
+	CK(cudaStreamWaitEvent(c->xfer, c->xev[2 * XFER_CHUNKS], 0));
+	for (int k = 0; k < K; k++) {
+		const uint32_t i0 = (uint32_t)((uint64_t)n * k / K), i1 = (uint32_t)((uint64_t)n * (k + 1) / K);
+		CK(cudaMemcpyAsync(c->aos + i0, parts + i0, sizeof(pot_particle) * (i1 - i0), cudaMemcpyHostToDevice,
+		                   c->xfer));
+		CK(cudaEventRecord(c->xev[k], c->xfer));
+		CK(cudaStreamWaitEvent(c->stream, c->xev[k], 0));
+		k_from_aos_range<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->aos, i0, i1 - i0, c->pos[0], c->vel[0],
+		                                                              c->pid[0], c->rec);
 	}
 	c->sticky = POT_OK;  // as pot_gpu_upload: a new state clears the run's status
 	c->uploaded = true;
@@ -1046,10 +1041,28 @@ int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_
 		                   c->xfer));
 	}
 	CK(cudaMemcpyAsync(c->h_rec, c->rec, sizeof(RunRec), cudaMemcpyDeviceToHost, c->stream));
-	if (out) CK(cudaMemcpyAsync(c->h_hist, c->hist, sizeof(StepHist) * HIST, cudaMemcpyDeviceToHost, c->stream));
+	if (want_hist) CK(cudaMemcpyAsync(c->h_hist, c->hist, sizeof(StepHist) * HIST, cudaMemcpyDeviceToHost, c->stream));
 	CK(cudaGetLastError());
-	CK(cudaStreamSynchronize(c->xfer));
-	CK(cudaStreamSynchronize(c->stream));
+	return POT_OK;
+}
+
+int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_grain_state* grain,
+                           pot_step_stats* out)
+{
+	if (!c || !parts || N != c->cfg.N) return POT_E_ARG;
+	if (parts[0].species != SP_DUST) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	if (!c->aos) {
+		const int ra = dalloc(c, &c->aos, c->n);
+		if (ra) return ra;
+	}
+	int rc = xfer_setup(c);
+	if (rc) return rc;
+	rc = move_enqueue(c, parts, grain, out != nullptr);
+	const cudaError_t e1 = cudaStreamSynchronize(c->xfer);
+	const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+	if (rc != POT_OK) return rc;
+	if (e1 != cudaSuccess || e2 != cudaSuccess) return POT_E_CUDA;
 	c->timer.resolve();
 	const RunRec& r = *c->h_rec;
 	if (r.status != POT_OK && c->sticky == POT_OK) c->sticky = r.status;
