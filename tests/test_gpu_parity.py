@@ -411,3 +411,23 @@ def test_move_particles_matches_upload_step_download(N, form):
             for k in ("t_steps", "grain_q", "dq", "de", "n_absorbed", "n_reinjected", "n_pushed", "interactions",
                       "n_nodes", "chi_b", "status", "q_sum"):
                 assert sa[k] == sb[k], k
+
+
+def test_bad_species_is_reported():
+    """A record whose species is not 0, 1 or 2 makes the upload (and the
+    drop-in call) fail with POT_E_ARG at the next step instead of being
+    stepped as an electron silently."""
+    cfg = run_config(dict(SMALL, N=8193))
+    with Run(cfg, form="fast", leaf_size=16, seed=2) as r:
+        r.init_particles()
+        P, g = r.download()
+    P[5]["species"] = 7
+    with Run(cfg, form="fast", leaf_size=16, seed=2) as r:
+        with pytest.raises(PotError) as e:
+            r.move_particles(P.copy(), g)
+        assert e.value.status == -1
+    with Run(cfg, form="plain", seed=2) as r:
+        r.upload(P, g)
+        with pytest.raises(PotError) as e:
+            r.step(1)
+        assert e.value.status == -1
