@@ -63,3 +63,34 @@ def test_no_cpu_fallback_without_device():
     cfg = gpu.RunConfig(N=100, r=1000, dt=1e-15, mpp=1e-9, soft=1e-9, Te=1e4, Ti=1e4).to_c()
     opts = gpu._Opts()
     assert L.pot_gpu_create(C.byref(cfg), C.byref(opts), C.byref(h)) == -2
+
+
+def test_python_mirror_matches_the_c_header(tmp_path):
+    """Every field offset and record size of the ctypes mirror against the
+    header as gcc lays it out."""
+    import os
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    mirrors = {"pot_run_cfg": gpu._RunCfg, "pot_gpu_opts": gpu._Opts, "pot_grain_state": gpu._Grain,
+               "pot_step_stats": gpu._Stats, "pot_macro_sums": gpu._MacroSums, "pot_batch_opts": gpu._BatchOpts}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pot_gpu.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in cls._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([cc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.splitlines())
+    for cname, cls in mirrors.items():
+        assert int(got[cname]) == C.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert int(got["%s.%s" % (cname, f)]) == getattr(cls, f).offset, (cname, f)
