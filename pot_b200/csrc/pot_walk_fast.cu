@@ -32,7 +32,7 @@ namespace pot {
 constexpr int FW_WARPS = 4;        // warps per block
 constexpr int FW_TPL_MAX = 2;      // targets per lane (1 or 2; groups of 32 or 64)
 constexpr int FW_STACK = POT_WALK_STACK;  // cells awaiting a test, per warp
-constexpr int FW_CELLS = 104;      // staged monopoles (flush at >= 64, padded to a multiple of 8)
+constexpr int FW_CELLS = 104;      // staged monopoles (flush at >= 64; at most 95 staged, 96 padded)
 constexpr int FW_CELL_FLUSH = 64;
 constexpr int FW_LEAVES = 64;      // staged leaf ranges (flush at >= 32)
 constexpr int FW_LEAF_FLUSH = 32;
@@ -108,6 +108,18 @@ template <int TPL> struct TgtE;
 template <> struct TgtE<1> { float x, y, z; };
 template <> struct TgtE<2> { float2 x, y, z; };
 
+// FP32 reciprocal square root: the hardware approximation with subnormal
+// input flushed to zero (PTX rsqrt.approx.ftz.f32), one instruction.  Its
+// arguments are squared distances to accepted cells or softened (floor
+// 1e-20 R^2) squared distances to particles, never subnormal, where the
+// flushing and the non-flushing forms give the same result.
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+	float r;
+	asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+	return r;
+}
+
 __device__ __forceinline__ void stage_src(float4* buf, int i, float4 c, Acc<1>*) { buf[i] = c; }
 __device__ __forceinline__ void stage_src(float4* buf, int i, float4 c, Acc<2>*)
 {
@@ -125,7 +137,7 @@ __device__ __forceinline__ void eval_src(Acc<1>& E, const TgtE<1>& t, const floa
 	const float4 q = buf[i];
 	const float dx = t.x - q.x, dy = t.y - q.y, dz = t.z - q.z;
 	const float r2 = fmaf(dx, dx, fmaf(dy, dy, SOFT ? fmaf(dz, dz, eps2) : dz * dz));
-	const float ri = rsqrtf(r2);
+	const float ri = rsqrt_ftz(r2);
 	if (POT) {
 		E.x = fmaf(q.w, ri, E.x);
 	} else {
@@ -147,7 +159,7 @@ __device__ __forceinline__ void eval_src(Acc<2>& E, const TgtE<2>& t, const floa
 	float2 r2 = SOFT ? __ffma2_rn(dz, dz, make_float2(eps2, eps2)) : __fmul2_rn(dz, dz);
 	r2 = __ffma2_rn(dy, dy, r2);
 	r2 = __ffma2_rn(dx, dx, r2);
-	const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+	const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
 	if (POT) {
 		E.x = __ffma2_rn(q, ri, E.x);
 	} else {
@@ -195,7 +207,7 @@ __device__ __forceinline__ void eval_cell_dip(Acc<2>& E, const TgtE<2>& t, const
 	float2 r2 = __fmul2_rn(dz, dz);
 	r2 = __ffma2_rn(dy, dy, r2);
 	r2 = __ffma2_rn(dx, dx, r2);
-	const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+	const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
 	const float2 ri2 = __fmul2_rn(ri, ri);
 	const float2 ri3 = __fmul2_rn(ri2, ri);
 	float2 pr = __fmul2_rn(pz, dz);
@@ -399,6 +411,7 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 					}
 				}
 			}
+			leafr = leafr && range.y > 0u;  // the leaf flush relies on no staged leaf being empty
 			// one warp scan for the three appends: accepted cells in bits 0-9,
 			// leaf ranges in bits 10-19, children in bits 20-31 (totals <= 32,
 			// <= 32 and <= 256 fit)
@@ -434,12 +447,14 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			maxlen = max(maxlen, len);
 			__syncwarp();
 		}
-		// flush staged monopoles, padded to a multiple of 8 with zero-charge
-		// cells far outside the domain so the loop needs no remainder
+		// flush staged monopoles in whole units of the unrolled loop, so it
+		// needs no remainder: a flush during the walk evaluates the whole units
+		// and carries the rest (fewer than a unit) to the next; the last one
+		// pads to a whole unit with zero-charge cells far outside the domain
 		if (ncell >= FW_CELL_FLUSH || (done && ncell > 0)) {
 			const int unit = cell_unroll * PER_EV * split;  // <= 32: the padding is one store per lane
-			const int padded = (ncell + unit - 1) / unit * unit;
-			if ((int)lane < padded - ncell) {
+			const int padded = done ? (ncell + unit - 1) / unit * unit : ncell / unit * unit;
+			if (done && (int)lane < padded - ncell) {
 				stage_src(sm.cells, ncell + lane, make_float4(64.f, 64.f, 64.f, 0.f), tag);
 				if (DIP) sm.cells[FW_CELLS + ncell + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
 			}
@@ -471,8 +486,17 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 					for (int u = 0; u < 4; u++) eval_src<false, POT>(E, te, sm.cells, (j + u) * split + sub, eps2);
 				}
 			}
-			n_cells_ev += ncell;
-			ncell = 0;
+			// carried cells (unpacked, fewer than 32) move to the front; the
+			// ranges [padded, ncell) and [0, ncell - padded) are disjoint
+			const int rem = ncell > padded ? ncell - padded : 0;
+			n_cells_ev += ncell - rem;
+			__syncwarp();
+			if ((int)lane < rem) {
+#pragma unroll
+				for (int k = 0; k < TPL; k++) sm.cells[TPL * (int)lane + k] = sm.cells[TPL * (padded + (int)lane) + k];
+				if (DIP) sm.cells[FW_CELLS + lane] = sm.cells[FW_CELLS + padded + lane];
+			}
+			ncell = rem;
 			__syncwarp();
 		}
 		// flush staged leaves: their particles are gathered 32 at a time into
@@ -486,19 +510,27 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			sm.loff[lane] = (uint32_t)e0;
 			sm.loff[lane + 32] = (uint32_t)(t0 + e1);
 			const uint32_t total = (uint32_t)(t0 + t1);
+			// start offsets of this lane's two staged leaves, ~0 for none
+			const uint32_t st0 = (int)lane < nleaf ? (uint32_t)e0 : 0xFFFFFFFFu;
+			const uint32_t st1 = (int)lane + 32 < nleaf ? (uint32_t)(t0 + e1) : 0xFFFFFFFFu;
+			const uint32_t le_mask = (2u << lane) - 1u;  // lanes 0..lane (all for lane 31)
+			int before = 0;  // staged leaves that start before this chunk
 			__syncwarp();
 			for (uint32_t base = 0; base < total; base += 32) {
 				const uint32_t g = base + lane;
+				// the staged leaves that start inside this chunk, one bit per
+				// start offset (no leaf is empty, so no two share a start)
+				uint32_t bits = 0u;
+				if (st0 - base < 32u) bits |= 1u << (st0 - base);
+				if (st1 - base < 32u) bits |= 1u << (st1 - base);
+				const uint32_t starts = __reduce_or_sync(0xffffffffu, bits);
 				// padding: zero charge far outside the domain
 				float4 p = make_float4(64.f, 64.f, 64.f, 0.f);
 				if (g < total) {
-					int a = 0, b = nleaf - 1;
-					while (a < b) {  // last staged leaf whose offset <= g
-						const int mid = (a + b + 1) >> 1;
-						if (sm.loff[mid] <= g) a = mid; else b = mid - 1;
-					}
+					const int a = before + __popc(starts & le_mask) - 1;  // the last leaf starting at or before g
 					p = __ldg(&src32[sm.leaves[a].x + (g - sm.loff[a])]);
 				}
+				before += __popc(starts);
 				stage_src(sm.pbuf, (int)lane, p, tag);
 				__syncwarp();
 				if (TPL == 1) {
