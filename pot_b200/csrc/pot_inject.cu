@@ -124,21 +124,35 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 	int intervals = 0;
 	for (;;) {
 		// Most intervals pass within the first few halvings, so halvings 1-8
-		// are tried first: their end points need a recursion 8 deep, not 32.
-		// The full 32-lane batch below runs only when none of them passes,
-		// so the interval chosen is the same either way.
+		// are tried first (lanes 0-7): their end points need a recursion 8
+		// deep, not 32.  The full 32-lane batch below runs only when none of
+		// them passes, so the interval chosen is the same either way.
+		// Lanes 8-31 meanwhile try the next interval, in groups of 8, for
+		// the three likeliest outcomes (the interval ends at e_2, e_3 or e_4,
+		// together about 70 % of intervals): group g = lane / 8 starts its
+		// halvings at e_{g+1}, computed by the same recursion, with y(e_{g+1})
+		// from lane g.  When the outcome was guessed, one round takes two
+		// intervals, with the values the sequential loop would compute.
 		{
-			double e = 1.0;
-			const uint32_t top = lane < 8u ? lane : 7u;
-			for (uint32_t k = 0; k <= top; k++) e = (xi0 + e) / 2.0;  // e_{lane+1}
-			double y = 1.0 - (chu2 * e * exp(Rol * (1.0 - (1.0 / e))));
-			y = 1.0 / sqrt((y / s2) - (e * e));
+			const uint32_t grp = lane >> 3, j = lane & 7u;
+			double x_lo = xi0;  // start of this group's interval
+			if (grp) {
+				x_lo = 1.0;
+				for (uint32_t k = 0; k <= grp; k++) x_lo = (xi0 + x_lo) / 2.0;  // e_{grp+1}
+			}
+			double ep = 1.0;
+			for (uint32_t k = 0; k <= j; k++) ep = (x_lo + ep) / 2.0;  // this group's e_{j+1}
+			double y = 1.0 - (chu2 * ep * exp(Rol * (1.0 - (1.0 / ep))));
+			y = 1.0 / sqrt((y / s2) - (ep * ep));
+			const double y_lo_g = __shfl_sync(0xffffffffu, y, grp);  // y(e_{grp+1}) from lane grp
+			const double y_lo = grp ? y_lo_g : y0;
 			const double y_up = __shfl_up_sync(0xffffffffu, y, 1);
-			const double e_up = __shfl_up_sync(0xffffffffu, e, 1);
-			const double y_ek = lane == 0 ? y_one : y_up;
-			const double e_k = lane == 0 ? 1.0 : e_up;
-			const bool linear = lane < 8u && !(fabs(y_ek - y - (y - y0)) > mld);
-			const uint32_t pass = __ballot_sync(0xffffffffu, linear);
+			const double e_up = __shfl_up_sync(0xffffffffu, ep, 1);
+			const double y_ek = j == 0 ? y_one : y_up;
+			const double e_k = j == 0 ? 1.0 : e_up;
+			const bool linear = !(fabs(y_ek - y - (y - y_lo)) > mld);
+			const uint32_t pass_all = __ballot_sync(0xffffffffu, linear);
+			const uint32_t pass = pass_all & 0xFFu;
 			if (pass) {
 				const int k = __ffs(pass) - 1;
 				const double xk = __shfl_sync(0xffffffffu, e_k, k);
@@ -151,6 +165,22 @@ __device__ double d_integrate_for_alpha_warp(double s, double chi_b, double u2, 
 				if (++intervals > SIMPSON_CAP) {
 					fail |= FAIL_SIMPSON;
 					return 0.0;
+				}
+				// the interval ended at e_k: group k - 1 started there
+				const uint32_t pass2 = (k >= 2 && k <= 4) ? (pass_all >> (8 * (k - 1))) & 0xFFu : 0u;
+				if (pass2) {
+					const int k2 = 8 * (k - 1) + __ffs(pass2) - 1;
+					const double xk2 = __shfl_sync(0xffffffffu, e_k, k2);
+					const double yk2 = __shfl_sync(0xffffffffu, y_ek, k2);
+					const double ym2 = __shfl_sync(0xffffffffu, y, k2);
+					alpha += (xk2 - xi0) * (y0 + (4.0 * ym2) + yk2) / 6.0;
+					xi0 = xk2;
+					y0 = yk2;
+					if (!(xi0 < 1.0)) break;
+					if (++intervals > SIMPSON_CAP) {
+						fail |= FAIL_SIMPSON;
+						return 0.0;
+					}
 				}
 				continue;
 			}

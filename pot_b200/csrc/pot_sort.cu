@@ -162,6 +162,7 @@ constexpr uint32_t OS_FLAG_AGG = 1u << 30;
 constexpr uint32_t OS_FLAG_PRE = 2u << 30;
 constexpr uint32_t OS_COUNT = (1u << 30) - 1u;
 constexpr long OS_SPIN_CAP = 1L << 24;
+constexpr int OS_LOOKBACK = 8;      // earlier tiles read per round of the look-back
 
 // Digit counts of every pass in one read of the keys: hist[p * 256 + d].
 __global__ void __launch_bounds__(OS_THREADS) k_os_hist(const uint64_t* __restrict__ keys, size_t n, int low_bit,
@@ -201,10 +202,9 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restri
                                                         uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                         int* __restrict__ err)
 {
+	constexpr int NW = OS_THREADS / 32;
 	__shared__ uint32_t s_tile;
-	__shared__ uint32_t s_run[RS_BINS];       // running per-digit count in this tile
-	__shared__ uint32_t s_wcnt[8][RS_BINS];
-	__shared__ uint32_t s_wpre[8][RS_BINS];
+	__shared__ uint32_t s_wcnt[NW][RS_BINS];  // per-warp running count, then per-warp exclusive prefix
 	__shared__ uint32_t s_loc[RS_BINS];       // digit start inside the staged tile
 	__shared__ uint32_t s_glob[RS_BINS];      // digit start in the output
 	__shared__ uint64_t s_key[OS_TILE];
@@ -212,19 +212,20 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restri
 	const int t = threadIdx.x, w = t >> 5, lane = t & 31;
 	const uint32_t lt_mask = (1u << lane) - 1u;
 	if (t == 0) s_tile = atomicAdd(tile_ctr, 1u);
-	s_run[t] = 0;
 #pragma unroll
-	for (int k = 0; k < 8; k++) s_wcnt[k][t] = 0;
+	for (int k = 0; k < NW; k++) s_wcnt[k][t] = 0;
 	__syncthreads();
 	const uint32_t tile = s_tile;
 	const size_t base = (size_t)tile * OS_TILE;
+	// warp w holds the tile's keys [256 w, 256 w + 256), round r the 32 at
+	// 256 w + 32 r, so a key's index in the tile is (warp, round, lane) in order
 	uint64_t key[OS_ITEMS];
 	uint32_t val[OS_ITEMS];
 	uint32_t rank[OS_ITEMS];
 	int dig[OS_ITEMS];
 #pragma unroll
 	for (int r = 0; r < OS_ITEMS; r++) {
-		const size_t i = base + (size_t)r * OS_THREADS + t;
+		const size_t i = base + (size_t)(w * 32 * OS_ITEMS + r * 32 + lane);
 		dig[r] = RS_BINS;
 		key[r] = 0;
 		val[r] = 0;
@@ -234,51 +235,61 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restri
 			dig[r] = (int)((key[r] >> shift) & 0xFF);
 		}
 	}
-	// stable local ranks: rounds in index order, then warps, then lanes
+	// stable ranks inside the warp: a running count per digit in the warp's
+	// own row, updated once per round by the lowest lane of each digit
 #pragma unroll
 	for (int r = 0; r < OS_ITEMS; r++) {
 		const int d = dig[r];
 		const uint32_t peers = __match_any_sync(0xffffffffu, d);
-		const uint32_t lrank = __popc(peers & lt_mask);
-		if (d < RS_BINS && lrank == 0) s_wcnt[w][d] = __popc(peers);
-		__syncthreads();
-		{
-			uint32_t run = 0;
-#pragma unroll
-			for (int k = 0; k < 8; k++) {
-				const uint32_t c = s_wcnt[k][t];
-				s_wcnt[k][t] = 0;
-				s_wpre[k][t] = run;
-				run += c;
-			}
-			s_loc[t] = run;  // this round's count of digit t
-		}
-		__syncthreads();
-		if (d < RS_BINS) rank[r] = s_run[d] + s_wpre[w][d] + lrank;
-		__syncthreads();
-		s_run[t] += s_loc[t];
+		const uint32_t before = d < RS_BINS ? s_wcnt[w][d] : 0u;
+		rank[r] = before + __popc(peers & lt_mask);
+		__syncwarp();
+		if (d < RS_BINS && (peers & lt_mask) == 0u) s_wcnt[w][d] = before + __popc(peers);
+		__syncwarp();
 	}
 	__syncthreads();
-	// publish this tile's count of digit t, then look back for its prefix
-	const uint32_t cnt = s_run[t];
+	// digit t: each warp's exclusive prefix over the warps before it, and
+	// the tile's count
+	uint32_t cnt = 0;
+#pragma unroll
+	for (int k = 0; k < NW; k++) {
+		const uint32_t c = s_wcnt[k][t];
+		s_wcnt[k][t] = cnt;
+		cnt += c;
+	}
+	// publish this tile's count of digit t, then look back for its prefix,
+	// OS_LOOKBACK earlier tiles per round of reads
 	volatile uint32_t* st = status;
 	st[(size_t)tile * RS_BINS + t] = (tile == 0 ? OS_FLAG_PRE : OS_FLAG_AGG) | cnt;
 	uint32_t excl = 0;
 	if (tile > 0) {
 		long spins = 0;
-		for (int64_t j = (int64_t)tile - 1; j >= 0;) {
-			const uint32_t v = st[(size_t)j * RS_BINS + t];
-			const uint32_t flag = v & ~OS_COUNT;
-			if (flag == 0) {
-				if (++spins > OS_SPIN_CAP) {
-					atomicCAS(err, 0, POT_E_ITER);
-					break;
+		int64_t j = (int64_t)tile - 1;  // next tile to read
+		bool found = false;
+		while (!found) {
+			uint32_t v[OS_LOOKBACK];
+#pragma unroll
+			for (int q = 0; q < OS_LOOKBACK; q++) v[q] = j - q >= 0 ? st[(size_t)(j - q) * RS_BINS + t] : 0u;
+			int used = 0;
+			bool stalled = false;
+#pragma unroll
+			for (int q = 0; q < OS_LOOKBACK; q++) {
+				if (found || stalled) continue;
+				const uint32_t flag = v[q] & ~OS_COUNT;
+				if (flag == 0) {  // not yet published (tile 0 always is, so j - q >= 0 here)
+					stalled = true;
+					continue;
 				}
-				continue;
+				excl += v[q] & OS_COUNT;
+				used++;
+				if (flag == OS_FLAG_PRE) found = true;
 			}
-			excl += v & OS_COUNT;
-			if (flag == OS_FLAG_PRE) break;
-			j--;
+			if (found) break;
+			j -= used;
+			if (used == 0 && ++spins > OS_SPIN_CAP) {
+				atomicCAS(err, 0, POT_E_ITER);
+				break;
+			}
 		}
 		st[(size_t)tile * RS_BINS + t] = OS_FLAG_PRE | (excl + cnt);
 	}
@@ -293,7 +304,7 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restri
 #pragma unroll
 	for (int r = 0; r < OS_ITEMS; r++) {
 		if (dig[r] < RS_BINS) {
-			const uint32_t p = s_loc[dig[r]] + rank[r];
+			const uint32_t p = s_loc[dig[r]] + s_wcnt[w][dig[r]] + rank[r];
 			s_key[p] = key[r];
 			s_val[p] = val[r];
 		}
