@@ -193,16 +193,95 @@ __global__ void k_fill_nodes(const int8_t* __restrict__ lvl8, const uint32_t* __
 	}
 }
 
-// first index in [a, b) whose child digit at `shift` is >= c (digits are
-// non-decreasing over a cell's sorted key range)
-__device__ __forceinline__ uint32_t lower_digit(const uint64_t* __restrict__ keys, uint32_t a, uint32_t b,
-                                                int shift, uint32_t c)
+// The searches below run over a cell's sorted key range, where the tested
+// property holds on a prefix of the range.  They make several independent
+// reads per round, so that the chain of dependent loads -- which sets the
+// time of the cells near the root -- is short.
+
+// First index in [a, b) at which `pred` fails, b if it holds throughout:
+// seven probes per round keep one eighth of the range; the last eight or
+// fewer are read at once.
+template <class Pred>
+__device__ __forceinline__ uint32_t first_fail8(const uint64_t* __restrict__ keys, uint32_t a, uint32_t b, Pred pred)
 {
-	while (a < b) {
-		const uint32_t m = a + ((b - a) >> 1);
-		if (((keys[m] >> shift) & 7u) < c) a = m + 1; else b = m;
+	while (b - a > 8u) {
+		const uint64_t span = b - a;
+		uint32_t p[7];
+		bool ok[7];
+#pragma unroll
+		for (int i = 0; i < 7; i++) p[i] = a + (uint32_t)((span * (uint64_t)(i + 1)) >> 3);  // a < p[0] < ... < p[6] < b
+#pragma unroll
+		for (int i = 0; i < 7; i++) ok[i] = pred(keys[p[i]]);
+		uint32_t na = a, nb = b;
+#pragma unroll
+		for (int i = 0; i < 7; i++)
+			if (ok[i]) na = p[i] + 1;  // the last probe that holds
+#pragma unroll
+		for (int i = 6; i >= 0; i--)
+			if (!ok[i]) nb = p[i];  // the first probe that fails
+		a = na;
+		b = nb;
 	}
-	return a;
+	uint32_t c = 0;
+#pragma unroll
+	for (int i = 0; i < 8; i++) c += (a + (uint32_t)i < b && pred(keys[a + i])) ? 1u : 0u;
+	return a + c;
+}
+
+// One past the last slot of the cell that starts at slot f with key prefix
+// pfx (key >> shift): f + 2^e is probed for seven exponents per round until
+// one leaves the cell, then the bracket is searched.
+__device__ __forceinline__ uint32_t cell_end(const uint64_t* __restrict__ keys, uint32_t f, uint32_t n, int shift,
+                                             uint64_t pfx)
+{
+	const auto same = [=](uint64_t k) { return (k >> shift) == pfx; };
+	uint32_t a = f + 1, b = n;
+	for (int e0 = 0; e0 < 32; e0 += 7) {
+		uint64_t q[7];
+		bool ok[7];
+#pragma unroll
+		for (int i = 0; i < 7; i++) {
+			q[i] = (uint64_t)f + (1ull << (e0 + i));
+			ok[i] = q[i] < n && same(keys[q[i]]);
+		}
+		bool left = false;
+#pragma unroll
+		for (int i = 0; i < 7; i++)
+			if (ok[i]) a = (uint32_t)q[i] + 1;
+#pragma unroll
+		for (int i = 6; i >= 0; i--) {
+			if (!ok[i]) {
+				b = q[i] < n ? (uint32_t)q[i] : n;
+				left = true;
+			}
+		}
+		if (left) break;
+	}
+	return first_fail8(keys, a, b, same);
+}
+
+// s[c] for c = 1..7: the first slot of [f, e) whose child digit at `shift`
+// is >= c; seven bisections side by side.
+__device__ __forceinline__ void child_starts(const uint64_t* __restrict__ keys, uint32_t f, uint32_t e, int shift,
+                                             uint32_t s[9])
+{
+	uint32_t lo[7], hi[7];
+#pragma unroll
+	for (int c = 0; c < 7; c++) {
+		lo[c] = f;
+		hi[c] = e;
+	}
+	for (uint32_t span = e - f; span > 0u; span >>= 1) {
+#pragma unroll
+		for (int c = 0; c < 7; c++) {
+			if (lo[c] < hi[c]) {
+				const uint32_t m = lo[c] + ((hi[c] - lo[c]) >> 1);
+				if (((keys[m] >> shift) & 7u) < (uint32_t)(c + 1)) lo[c] = m + 1; else hi[c] = m;
+			}
+		}
+	}
+#pragma unroll
+	for (int c = 0; c < 7; c++) s[c + 1] = lo[c];
 }
 
 __global__ void k_finish_nodes(const uint64_t* __restrict__ keys, uint32_t n, uint32_t L,
@@ -219,27 +298,15 @@ __global__ void k_finish_nodes(const uint64_t* __restrict__ keys, uint32_t n, ui
 		const int l = T.level[k];
 		const int shift = 63 - 3 * l;
 		const uint64_t pfx = keys[f] >> shift;
-		// last particle of the cell: gallop, then bisect
-		uint32_t good = f, step = 1, probe = f + 1;
-		while (probe < n && (keys[probe] >> shift) == pfx) {
-			good = probe;
-			step <<= 1;
-			probe = f + step;
-		}
-		uint32_t a = good + 1, b = probe < n ? probe : n;
-		while (a < b) {
-			const uint32_t m = a + ((b - a) >> 1);
-			if ((keys[m] >> shift) == pfx) a = m + 1; else b = m;
-		}
-		const uint32_t last = a - 1;
+		// last particle of the cell
+		const uint32_t last = cell_end(keys, f, n, shift, pfx) - 1;
 		T.last[k] = last;
 		// children by digit at the next level
 		const int cshift = shift - 3;
 		uint32_t s[9];
 		s[0] = f;
 		s[8] = last + 1;
-#pragma unroll
-		for (int c = 1; c < 8; c++) s[c] = lower_digit(keys, s[c - 1], last + 1, cshift, (uint32_t)c);
+		child_starts(keys, f, last + 1, cshift, s);
 		int nint = 0;
 #pragma unroll
 		for (int c = 0; c < 8; c++) {
