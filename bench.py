@@ -596,7 +596,9 @@ def run_ours(args):
             "walk_compute": walk_compute(inter, dom_name, per_launch_s, clk),
             "kernels_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
             "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
-            "walk_stack_max": st.get("stack_max"), "force_accuracy": accuracy, "extra_configs": extra or None,
+            "walk_stack_max": st.get("stack_max"),
+            "targets_per_group": (st["n_pushed"] / st["n_groups"]) if st.get("n_groups") else None,
+            "force_accuracy": accuracy, "extra_configs": extra or None,
             "batch": batch,
             "status": st["status"]}
     if rank == 0:

@@ -160,6 +160,9 @@ typedef struct pot_step_stats {
 	uint32_t n_collected;  /* POT_CFG_POIS_IONS: charges the Poisson ion collection added */
 	uint32_t n_wall;       /* OUT_BOUNCE: particles found outside moving inwards, left in place */
 	uint32_t n_bounced;    /* OUT_BOUNCE: particles bounced off the wall */
+	uint32_t n_groups;     /* fast form: target groups the walk ran this step, one warp each
+	                          (n_pushed / n_groups targets per group on average); 0 in the plain form */
+	uint32_t pad;
 } pot_step_stats;
 
 /* capacity of the fast form's per-warp stack of cells awaiting a test;

@@ -912,6 +912,7 @@ int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats
 		out->n_collected = r.n_collected;
 		out->n_wall = r.n_wall;
 		out->n_bounced = r.n_bounced;
+		out->n_groups = c->P.form == POT_FORM_FAST ? r.n_groups : 0u;
 	}
 	return st;
 }
@@ -1087,6 +1088,7 @@ int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_
 		out->n_collected = r.n_collected;
 		out->n_wall = r.n_wall;
 		out->n_bounced = r.n_bounced;
+		out->n_groups = c->P.form == POT_FORM_FAST ? r.n_groups : 0u;
 	}
 	if (r.status != POT_OK) return r.status;
 	if (grain) {

@@ -538,9 +538,19 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 					__syncwarp();
 				}
 				constexpr int nev = 32 / PER_EV;
-				if (split == 1) {
+				const uint32_t in_chunk = total - base < 32u ? total - base : 32u;
+				if (split == 1 && in_chunk == 32u) {
 #pragma unroll 16
 					for (int m = 0; m < nev; m++) eval_src<true, POT>(E, te, sm.pbuf, m, eps2);
+				} else if (split == 1) {
+					// a flush's last, partial chunk: whole quads of evaluations that
+					// cover its particles (the padding beyond has zero charge)
+					const int need = TPL == 1 ? ((int)in_chunk + 1) / 2 : (int)in_chunk;
+					const int nq = (need + 3) & ~3;  // <= nev
+					for (int m = 0; m < nq; m += 4) {
+#pragma unroll
+						for (int u = 0; u < 4; u++) eval_src<true, POT>(E, te, sm.pbuf, m + u, eps2);
+					}
 				} else {
 					const int per = nev / split;
 #pragma unroll 8
