@@ -13,8 +13,9 @@
 //     more than L particles iff keys i and i + L share its 3l-bit prefix;
 //     pair i = (i, i + L) "owns" the cells whose first particle is i, i.e.
 //     the levels (lvl[i-1], lvl[i]], which numbers cells in pre-order;
-//   * a cell's last particle and its 8 children are found by binary search
-//     over its key range.
+//   * a cell's last particle and its 8 children are found by searches over
+//     its key range that make several independent reads per round
+//     (cell_end, child_starts).
 // Leaf size L = 1 reproduces the reference's tree; L > 1 gives bucket leaves.
 //
 // Moments.  Net charge q, absolute charge aq and the |q|-weighted centre of
