@@ -69,3 +69,24 @@ def test_morton_key_matches_midpoint_descent():
                 h = m
             want = (want << 3) | (b * 7)
         assert int(ki) == want
+
+
+@pytest.mark.parametrize("N,L,seed", [(20000, 16, 1), (3001, 1, 2), (50000, 8, 3)])
+def test_device_searches_find_cell_ends_and_children(N, L, seed):
+    """The searches of k_finish_nodes (cell_end, child_starts), restated in
+    tree_model.py, give every cell's last slot and child boundaries of the
+    model tree, including clustered keys that make deep, lopsided cells."""
+    rng = np.random.default_rng(seed)
+    pts = rng.normal(0.5, 0.12, size=(N, 3)).clip(0.001, 0.999)
+    keys = np.sort(tm.morton_keys(pts[:, 0], pts[:, 1], pts[:, 2], 1.0))
+    tree = tm.build(keys, L)
+    n = len(keys)
+    for c in range(tree["M"]):
+        f, l = int(tree["first"][c]), int(tree["level"][c])
+        shift = 63 - 3 * l
+        pfx = int(keys[f]) >> shift
+        end = tm.cell_end(keys, f, n, shift, pfx)
+        assert end == int(tree["last"][c]) + 1, c
+        digits = (keys[f:end] >> np.uint64(shift - 3)) & np.uint64(7)
+        want = [f + int(np.searchsorted(digits, np.uint64(d), side="left")) for d in range(1, 8)]
+        assert tm.child_starts(keys, f, end, shift - 3) == want, c

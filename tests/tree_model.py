@@ -122,3 +122,61 @@ def canonical(keys_sorted, perm, tree):
                 for j in range(cnt):
                     leaves.append((int(perm[s0 + j]), l + 1, (pfx << 3) | d))
     return sorted(ints), sorted(leaves)
+
+
+# ---- the device's searches over a cell's key range (k_finish_nodes) ----
+
+def _first_fail8(k, a, b, pred):
+    """first_fail8: seven probes per round keep one eighth of [a, b); the
+    last eight or fewer are read at once."""
+    while b - a > 8:
+        span = b - a
+        p = [a + ((span * (i + 1)) >> 3) for i in range(7)]
+        ok = [pred(int(k[q])) for q in p]
+        na, nb = a, b
+        for i in range(7):
+            if ok[i]:
+                na = p[i] + 1
+        for i in range(6, -1, -1):
+            if not ok[i]:
+                nb = p[i]
+        a, b = na, nb
+    return a + sum(1 for i in range(8) if a + i < b and pred(int(k[a + i])))
+
+
+def cell_end(k, f, n, shift, pfx):
+    """cell_end: f + 2^e probed for seven exponents per round until one
+    leaves the cell (key >> shift != pfx), then the bracket searched."""
+    same = lambda key: (key >> shift) == pfx
+    a, b = f + 1, n
+    for e0 in range(0, 32, 7):
+        q = [f + (1 << (e0 + i)) for i in range(7)]
+        ok = [qq < n and same(int(k[qq])) for qq in q]
+        left = False
+        for i in range(7):
+            if ok[i]:
+                a = q[i] + 1
+        for i in range(6, -1, -1):
+            if not ok[i]:
+                b = min(q[i], n)
+                left = True
+        if left:
+            break
+    return _first_fail8(k, a, b, same)
+
+
+def child_starts(k, f, e, shift):
+    """child_starts: s[c] for c = 1..7, the first slot of [f, e) whose digit
+    at shift is >= c, by seven bisections side by side."""
+    lo, hi = [f] * 7, [e] * 7
+    span = e - f
+    while span > 0:
+        for c in range(7):
+            if lo[c] < hi[c]:
+                m = lo[c] + ((hi[c] - lo[c]) >> 1)
+                if ((int(k[m]) >> shift) & 7) < c + 1:
+                    lo[c] = m + 1
+                else:
+                    hi[c] = m
+        span >>= 1
+    return lo
