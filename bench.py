@@ -2,11 +2,14 @@
 """Throughput of pot's per-timestep particle loop on B200.
 
 Metric: particle-steps/s (plasma particles x base time steps; ions keep the
-reference's sub-cycling, pot.c:4157-4159) for the 1,000,001-particle plasma
-(Te/Ti = 10, Mach-1 ion drift, R = 10 Debye lengths, grain 0.2 Debye
-lengths, theta = 0.5), fast form (FP32 leaf-grouped walk, FP64 positions and
-push, leaf size 16).  Synthetic data: particles initialised on the device by
-the reference's init_particles sampler with a fixed seed.
+reference's sub-cycling, pot.c:4157-4159).  Headline workload: the
+4,000,001-particle spheroid plasma of pot-spheroid.c (prolate grain of
+semi-axes 0.3 / 0.1 / 0.1 Debye lengths with its axis along the flow axis x,
+as the reference program has it; Te/Ti = 10, Mach-0.5 drift, B = 0.9533 T,
+R = 12 Debye lengths, theta = 0.4), fast form (FP32 leaf-grouped walk, FP64
+positions and push, leaf size 16, groups of 64).  Synthetic data: particles
+initialised on the device by the reference's init_particles sampler with a
+fixed seed.
 
 Our arm (default):
   * value: K device-timed steps with every input resident in HBM, CUDA events
@@ -18,12 +21,16 @@ Our arm (default):
     wall-clock around the loop;
   * plain_fp64: the same workload with the plain FP64 form (the reference's
     arithmetic, leaf size 1);
-  * roofline: the dominant kernel's algorithmic bytes per launch over its
-    CUDA-event duration, against MEASURED_PEAKS.json; the per-kernel events
-    come from a second pass over the same K steps from the same start, with
-    an event pair around every kernel (events cannot sit inside the graph);
+  * roofline: the dominant kernel (the walk) against its bound, FP32
+    arithmetic (flops per interaction x interactions per launch over the
+    launch's CUDA-event time), with its HBM bytes beside it; the per-kernel
+    events come from a second pass over the same K steps from the same
+    start, with an event pair around every kernel (events cannot sit inside
+    the graph);
+  * kernels: every kernel's time per launch, algorithmic bytes and fraction
+    of the measured HBM bandwidth;
   * cpu_baseline: the reference program itself (oracle/_ref, one core, one
-    MPI rank) for one step of the same configuration.
+    MPI rank) on a bounded sample of the same configuration.
 Reference arm (--impl reference): the compiled reference on the host cores,
 P processes each playing one MPI rank of a P-rank run (full tree build,
 its own block of particles pushed), max over ranks per step.
@@ -54,12 +61,16 @@ WORKLOADS = {
            "Mach-1 ion drift along x, R = 10 lambda_De, a = 0.2 lambda_De, theta = 0.5, "
            "SCEPTIC reinjection, dt = 0.005/omega_pe"),
     "4m": ("4m spheroid plasma (pot-spheroid.c): 4,000,001 particles, prolate grain 0.3/0.1/0.1 lambda_De "
-           "tilted 30 deg to the flow, Te/Ti = 10, Mach-0.5 drift, B = 0.9533 T (electron gyroradius "
-           "0.5 lambda_De), R = 12 lambda_De, theta = 0.4, SCEPTIC reinjection"),
+           "with its axis along the flow (x, as the reference has it), Te/Ti = 10, Mach-0.5 drift, "
+           "B = 0.9533 T (electron gyroradius 0.5 lambda_De), R = 12 lambda_De, theta = 0.4, SCEPTIC "
+           "reinjection, dt = 0.005/omega_pe"),
+    "4m_tilt": ("4m spheroid plasma with the grain tilted 30 deg to the flow (GPU only: the reference cannot "
+                "tilt its grain): 4,000,001 particles, prolate grain 0.3/0.1/0.1 lambda_De, Te/Ti = 10, "
+                "Mach-0.5 drift, B = 0.9533 T, R = 12 lambda_De, theta = 0.4, SCEPTIC reinjection"),
     "small": ("small plasma: 8,193 particles, Te = Ti, no flow, R = 5 lambda_De, a = 0.1 lambda_De, "
               "theta = 0.5"),
 }
-WORKLOAD = WORKLOADS["1m"]
+WORKLOAD = WORKLOADS["4m"]
 
 
 def peaks():
@@ -163,13 +174,32 @@ def reference_tree_field(cfg_name: str, parts, grain, idx, xyz):
     return hi + lo
 
 
-def direct_field_fp64(parts, grain, idx, xyz, soft, dev):
+def grain_field_fp64(cfg_name: str, grain, xyz):
+    """The spheroidal grain's own analytic field (pot-spheroid.c:1689-1779)
+    at the points xyz, from the oracle's FP64 restatement (the spheroid is
+    not a tree source, so a direct sum over the plasma leaves it out)."""
+    from oracle.oracle import Oracle, RunParams
+    from pot_b200.configs import run_params
+    from pot_b200.gpu import PARTICLE_DTYPE
+    p = RunParams(**run_params(cfg_name, N=3))
+    o = Oracle(p, mode="gpu", init=False)
+    parts = np.zeros(3, PARTICLE_DTYPE)
+    parts["species"] = [0, 1, 2]
+    parts[0]["x"], parts[0]["y"], parts[0]["z"] = grain["x"], grain["y"], grain["z"]
+    o.set_particles(parts)
+    o.set_grain(q=int(grain["q"]))
+    return np.array([o.grain_field(*map(float, r)) for r in np.asarray(xyz)])
+
+
+def direct_field_fp64(parts, grain, idx, xyz, soft, dev, grain_source=True):
     """FP64 direct sum of the field at xyz for the targets idx over every
     other particle, every pair softened as the reference's own accuracy check
     softens them (pot.c:2197-2238); torch on the GPU as the checker's
-    arithmetic."""
+    arithmetic.  grain_source=False leaves the grain (slot 0) out of the sum
+    (a spheroid, whose field is analytic)."""
     import torch
-    q = np.where(parts["species"] == 0, float(grain["q"]), np.where(parts["species"] == 1, 1.0, -1.0))
+    q = np.where(parts["species"] == 0, float(grain["q"]) if grain_source else 0.0,
+                 np.where(parts["species"] == 1, 1.0, -1.0))
     src = torch.tensor(np.stack([parts["x"], parts["y"], parts["z"]], 1), dtype=torch.float64, device=dev)
     qs = torch.tensor(q, dtype=torch.float64, device=dev)
     tgt = torch.tensor(np.asarray(xyz), dtype=torch.float64, device=dev)
@@ -198,7 +228,11 @@ def force_accuracy(run, cfg_name: str, cfg, dev, n_targets: int = 8192):
     xyz = np.stack([parts["x"][idx], parts["y"][idx], parts["z"][idx]], 1)
     run.build_tree()
     e_fast = run.field_at(idx, xyz)
-    e_dir = direct_field_fp64(parts, grain, idx, xyz, cfg.soft, dev)
+    spheroid = bool(cfg.A)
+    e_dir = direct_field_fp64(parts, grain, idx, xyz, cfg.soft, dev, grain_source=not spheroid)
+    if spheroid:
+        g = dict(grain, x=parts[0]["x"], y=parts[0]["y"], z=parts[0]["z"])
+        e_dir = e_dir + grain_field_fp64(cfg_name, g, xyz)
     e_ref = reference_tree_field(cfg_name, parts, grain, idx, xyz)
     mag2 = (e_dir ** 2).sum(1)
 
@@ -206,7 +240,8 @@ def force_accuracy(run, cfg_name: str, cfg, dev, n_targets: int = 8192):
         rel = np.sqrt(((e - e_dir) ** 2).sum(1) / mag2)
         return {"rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99))}
 
-    out = {"targets": n_targets, "state": "after the timed steps", "direct": "FP64, every pair softened",
+    out = {"targets": n_targets, "state": "after the timed steps",
+           "direct": "FP64, every pair softened" + (", plus the spheroid's analytic field" if spheroid else ""),
            "fast_vs_direct": stat(e_fast)}
     if e_ref is not None:
         out["reference_tree_vs_direct"] = stat(e_ref)
@@ -216,35 +251,68 @@ def force_accuracy(run, cfg_name: str, cfg, dev, n_targets: int = 8192):
 
 
 def cpu_baseline_reference(cfg_name: str):
-    """One step of the reference program (compiled from its own sources,
-    one MPI rank on one core) on the same configuration."""
+    """The reference program (compiled from its own sources, one MPI rank on
+    one core) on a bounded sample of the same configuration.
+
+    Up to 1.5M particles the sample is one whole step.  Above that a whole
+    step takes minutes on one core, so the sample is the reference's own
+    16-rank decomposition seen from its last rank (pot.c:2936-2998 blocks,
+    reference order grain, ions, electrons: the last block is all
+    electrons): its build_tree alone, then one step of that rank (the tree
+    again plus its block pushed).  The one-core step is the tree plus every
+    due electron at the block's push rate."""
     from oracle.oracle import RefLib, RunParams
     from pot_b200.configs import run_params, variant
     p = RunParams(**run_params(cfg_name, untilted=True))
-    kind = "reference"
+    n_plasma = p.N - 1
     try:
         ref = RefLib(variant(cfg_name), build=False)
     except Exception:
         ref = None
-    if ref is not None:
+    if ref is not None and p.N <= 1_500_000:
         t0 = time.perf_counter()
         ref.setup(p, seed=1)
         t_init = time.perf_counter() - t0
         t0 = time.perf_counter()
         ref.step()
         t_step = time.perf_counter() - t0
-        n_plasma = p.N - 1
-        return {"value": n_plasma / t_step, "unit": UNIT, "cores": 1, "kind": kind,
+        return {"value": n_plasma / t_step, "unit": UNIT, "cores": 1, "kind": "reference",
                 "sample": "one step (t = 1: tree over %d particles, %d electrons pushed) of the %s config by the "
                           "reference pot.c compiled with gcc -O2 and a single-rank MPI stand-in, after its own "
                           "init_particles (%.1f s); step took %.1f s" % (p.N, n_plasma // 2, cfg_name, t_init,
                                                                          t_step)}
+    if ref is not None:
+        P = 16
+        t0 = time.perf_counter()
+        ref.setup(p, seed=1, nprocs=P, rank=P - 1)
+        t_init = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.build_tree()
+        t_tree = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.step()
+        t_rank = time.perf_counter() - t0
+        # the last block [lo, N): init_particles lays out each block as its
+        # ions then its electrons (pot.c:908-930); at t = 1 only electrons
+        # are due
+        lo = (P - 1) * (p.N // P)
+        sp = ref.particles()["species"]
+        e_block = int((sp[lo:] == 2).sum())
+        n_e = int((sp == 2).sum())
+        t_push = max(t_rank - t_tree, 1e-9)
+        t_one = t_tree + t_push * n_e / max(e_block, 1)
+        return {"value": n_plasma / t_one, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "the reference (pot-spheroid.c / pot.c, gcc -O2, single-rank MPI stand-in) as the last "
+                          "rank of an %d-rank run of the %s config (t = 1, after its own init_particles, %.1f s): "
+                          "build_tree over %d particles %.2f s, then one step of that rank %.2f s (tree + its %d "
+                          "electrons pushed); one-core step = tree + all %d electrons at that push rate = %.1f s"
+                          % (P, cfg_name, t_init, p.N, t_tree, t_rank, e_block, n_e, t_one)}
     from oracle.oracle import Oracle
     o = Oracle(p, mode="reference", seed=1, sceptic=variant(cfg_name).endswith("sceptic"))
     t0 = time.perf_counter()
     o.step()
     t_step = time.perf_counter() - t0
-    return {"value": (p.N - 1) / t_step, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": n_plasma / t_step, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": "one step of the %s config by the C restatement (reference not built here)" % cfg_name}
 
 
@@ -321,8 +389,9 @@ def run_reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / timed,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64/x87",
             "data": "synthetic", "config": {"workload": WORKLOADS.get(args.config, args.config), "N": N,
-                                            "reference_axis": "x (the reference cannot tilt its grain)"
-                                            if "axis" in CONFIGS[args.config] else None},
+                                            "reference_axis": "x (pot-spheroid.c's spheroid axis; the reference "
+                                                              "cannot tilt its grain)"
+                                            if CONFIGS[args.config].get("A") else None},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": "reference",
                              "sample": "%d processes, each one MPI rank of a %d-rank run of the reference pot.c "
                                        "(gcc -O2, single-rank MPI stand-in): full tree build plus its own block "
@@ -336,9 +405,13 @@ def run_reference_arm(args):
 
 def run_batches(args, device):
     """The batched sweep and the serving loop (pot_b200/potserve), short
-    versions: a sweep of --batch-runs runs (16k-256k particles) and a serving
-    window of Poisson arrivals (8k-1M particles), each run capped at
-    --batch-steps steps.  The full-length runs are separate invocations."""
+    versions sized so that most runs converge inside them: a sweep of
+    --batch-runs runs of 16k-64k particles and a serving window of Poisson
+    arrivals (20 per second for --serve-seconds, 8k-128k particles), each run
+    to a converged charge (the 500-step moving mean changing by under 0.5 %)
+    or --batch-steps steps.  Packed launches, autotuned group and leaf sizes,
+    the sampler's edge-potential cap on (POT_OPT_CHI_CAP).  The full-length
+    sweep (16k-256k) and serving load (8k-1M) are separate invocations."""
     from pot_b200 import build as gpu_build
     try:
         exe = os.path.join(os.path.dirname(gpu_build.HOST_BIN), "potserve")
@@ -348,9 +421,9 @@ def run_batches(args, device):
         return {"unavailable": str(e)}
     out = {}
     common = ["--max-steps", str(args.batch_steps), "--tune", "--device", str(device)]
-    runs = [("sweep", ["--mode", "sweep", "--runs", str(args.batch_runs), "--nmin", "16000", "--nmax", "256000"]),
+    runs = [("sweep", ["--mode", "sweep", "--runs", str(args.batch_runs), "--nmin", "16000", "--nmax", "64000"]),
             ("serve", ["--mode", "serve", "--rate", "20", "--duration", str(args.serve_seconds), "--nmin", "8000",
-                       "--nmax", "1000000", "--bmax", "1.0"])]
+                       "--nmax", "128000", "--bmax", "1.0"])]
     for name, extra in runs:
         try:
             p = subprocess.run([exe] + extra + common, capture_output=True, text=True, timeout=600)
@@ -360,20 +433,64 @@ def run_batches(args, device):
     return out
 
 
-def walk_compute(interactions, kernel, launch_s, clk):
-    """FP32 rate of the fast walk, the kernel's real bound (it is issue- and
-    FP32-pipe-limited, not HBM-bound): 17 FP32 flops and one rsqrt per
-    target-source interaction, against 148 SMs x 128 FP32 lanes x 2 flops x
-    the median SM clock sampled during the timed region (nominal peak; no
-    measured FP32 figure exists)."""
-    if not interactions or not kernel.startswith("walk_push") or not launch_s:
-        return None
+def kernel_table(kt, N, pushes, hbm_peak):
+    """Per-kernel time per launch, algorithmic bytes per launch and the
+    fraction of the measured HBM bandwidth they represent.  Algorithmic
+    bytes count each array a kernel must read or write once: keys (FP64
+    position in, 64-bit key and 32-bit slot out), the sort's histogram (keys
+    in) and each onesweep pass (key and slot in and out), the reorder
+    (gather of position, velocity and identity; write of the same plus FP64
+    and FP32 sources and a due flag), the compaction (due flags in, list
+    and prefix out), the fast moments (FP32 sources in, per-particle FP64
+    prefix sums out and read back per cell) and the walk (FP64 state of each
+    pushed particle in and out).  Kernels bound by latency or L2 (tree
+    build, groups, reinjection, grain update) get none."""
+    per_particle = {"keys": 32 + 12, "sort_hist": 8, "sort_pass": 24, "reorder": 72 + 117, "compact": 1 + 8,
+                    "tree_moments": 16 + 40 + 40}
+    out = {}
+    for name, (ms, n) in sorted(kt.items(), key=lambda kv: -kv[1][0]):
+        per = ms / max(n, 1)
+        if name.startswith("walk_push") or name.startswith("walk_half2"):
+            b = 96.0 * pushes
+        elif name in per_particle:
+            b = per_particle[name] * float(N)
+        else:
+            b = None
+        e = {"ms": round(per, 4), "launches": n, "alg_bytes": b}
+        if b:
+            gbs = b / (per / 1e3) / 1e9
+            e["hbm_gbs"] = round(gbs, 1)
+            e["hbm_frac"] = round(gbs / hbm_peak, 4)
+        out[name] = e
+    return out
+
+
+def roofline(kernel, interactions, launch_s, clk, alg_bytes, hbm_achieved, hbm_peak, peak_kind, traffic, share,
+             timing):
+    """The dominant kernel against its bound.  The fast walk is bound by
+    FP32 arithmetic and instruction issue, not HBM: 17 FP32 flops (and one
+    reciprocal square root) per target-source interaction, interactions per
+    launch from the device counter, over the launch's CUDA-event time,
+    against 148 SMs x 128 FP32 lanes x 2 flops x the median SM clock sampled
+    during the timed region (a nominal peak: no measured FP32 figure
+    exists).  Its HBM figures (96 B per push: the FP64 state read and
+    written) sit beside it; `traffic` is the DRAM bytes of one launch from
+    an ncu capture of the same workload."""
     mhz = (clk or {}).get("sm_mhz") or 1965.0
-    achieved = interactions * 17.0 / launch_s / 1e12
-    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_kind": "nominal at the sampled SM clock", "flop_per_interaction": 17,
-            "interactions_per_launch": interactions}
+    out = {"kernel": kernel, "ms_per_launch": launch_s * 1e3, "share_of_step": share, "timing": timing,
+           "alg_bytes_per_launch": alg_bytes, "traffic": traffic,
+           "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+                   "frac": hbm_achieved / hbm_peak}}
+    if interactions and kernel.startswith("walk_push") and launch_s:
+        achieved = interactions * 17.0 / launch_s / 1e12
+        peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+        out.update({"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "peak_kind": "nominal FP32 at the sampled SM clock (%.0f MHz)" % mhz,
+                    "flop_per_interaction": 17, "interactions_per_launch": interactions})
+    else:
+        out.update({"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": hbm_achieved / hbm_peak, "peak_kind": peak_kind})
+    return out
 
 
 def time_config(name, stream, dev, flush, steps=10, warmup=3, plain_steps=3):
@@ -448,9 +565,11 @@ def run_ours(args):
     seed0 = cfgd.get("seed", 1)
     flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device=dev)
 
-    def timed_region(r):
+    def timed_region(r, per_step_stats=False):
         """args.steps steps of r, each between CUDA events on the library's
-        stream, L2 flushed after each; barrier + synchronize on both sides."""
+        stream, L2 flushed after each; barrier + synchronize on both sides.
+        per_step_stats: read each step's statistics after it (a host wait
+        per step: the instrumented pass only)."""
         for _ in range(args.warmup):
             r.step_async(1)
         r.sync()
@@ -463,18 +582,26 @@ def run_ours(args):
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
+        sums = {"interactions": 0, "n_pushed": 0, "n_groups": 0}
         for k in range(args.steps):
             ev[k][0].record(stream)
             r.step_async(1)
             ev[k][1].record(stream)
             flush.zero_()
+            if per_step_stats:
+                stk = r.step(0)
+                for key in sums:
+                    sums[key] += int(stk.get(key) or 0)
         torch.cuda.synchronize(dev)
         if ws > 1:
             dist.barrier()
         clk_ = clocks.stop()
         r.sync()
         t = sum(a.elapsed_time(b) for a, b in ev)
-        return t, r.launch_count() - l0, r.step(0), clk_
+        stl = r.step(0)
+        if per_step_stats:
+            stl = dict(stl, **{"sum_" + key: v for key, v in sums.items()})
+        return t, r.launch_count() - l0, stl, clk_
 
     def make_run(timing):
         r = Run(cfg, form=args.form, leaf_size=args.leaf or cfgd["leaf_size"], group_size=group, seed=seed0 + rank,
@@ -490,33 +617,32 @@ def run_ours(args):
     # the same steps from the same start once more with a CUDA event pair
     # around every kernel: the per-kernel times behind the roofline
     runk = make_run(True)
-    tk_ms, _, _, _ = timed_region(runk)
+    tk_ms, _, stk, _ = timed_region(runk, per_step_stats=True)
     kt = runk.kernel_times()
     runk.close()
 
-    # dominant kernel and its roofline (algorithmic bytes per launch)
+    # dominant kernel: its time per launch and algorithmic bytes
     dom = max(kt.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
     n_e = n_plasma - (N - 1) // 2
     tss_ion = int((cfg.Te * 1836.15 / cfg.Ti) ** 0.5)
     pushes_per_step = n_e + ((N - 1) // 2) / tss_ion  # average due particles per step
     per_launch_s = dom_ms / dom_n / 1e3
-    if dom_name.startswith("walk_push"):
-        alg_bytes = pushes_per_step * 96.0  # FP64 state read + write per push
-    elif dom_name.startswith("sort"):
-        alg_bytes = N * 24.0 * 2
-    else:
-        alg_bytes = N * 48.0
+    kernels = kernel_table(kt, N, pushes_per_step, hbm_peak)
+    alg_bytes = kernels[dom_name]["alg_bytes"] or 0.0
     achieved = alg_bytes / per_launch_s / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get(dom_name)
+                tj = json.load(f)
+            if tj.get("workload") == args.config and not args.particles:
+                traffic = tj.get(dom_name)
         except Exception:
             traffic = None
-    inter = st["interactions"]  # last timed step
+    # interactions per walk launch, averaged over the instrumented pass's steps
+    inter = stk["sum_interactions"] / args.steps if stk.get("sum_interactions") else st["interactions"]
 
     # plain FP64 form on the same workload (fewer steps: it is the slow form)
     plain = None
@@ -537,7 +663,8 @@ def run_ours(args):
         runp.sync()
         tp = sum(a.elapsed_time(b) for a, b in evp)
         plain = {"value": n_plasma * args.plain_steps / (tp / 1e3), "unit": UNIT,
-                 "ms_per_step": tp / args.plain_steps, "steps": args.plain_steps, "form": "plain FP64, leaf 1"}
+                 "ms_per_step": tp / args.plain_steps, "steps": args.plain_steps, "form": "plain FP64, leaf 1",
+                 "fast_over_plain": (tp / args.plain_steps) / (t_ms / args.steps)}
         runp.close()
 
     # end to end: drop-in call on pinned host buffers
@@ -547,6 +674,19 @@ def run_ours(args):
     parts[:] = P
     grain = g
     run.move_particles(parts, grain)  # warm
+    # records the call copies back: the grain's and the reference-index range
+    # of the species due at step t (host arithmetic, for the byte count only)
+    sp = parts["species"]
+    span = {s_: (int(np.flatnonzero(sp == s_)[0]), int(np.flatnonzero(sp == s_)[-1])) for s_ in (0, 1, 2)
+            if (sp == s_).any()}
+    tss = {0: tss_ion * int((0.1 * 1.67e-12 / (1836.15 * 9.109383e-31)) ** 0.5), 1: tss_ion, 2: 1}
+
+    def d2h_records(t):
+        due = [span[s_] for s_ in span if t % tss[s_] == 0]
+        lo, hi = min(a for a, _ in due), max(b for _, b in due)
+        return (hi - lo + 1) + (1 if lo > 0 else 0)
+    t_first = int(grain["t_steps"]) + 1
+    d2h_rec = sum(d2h_records(t_first + k) for k in range(args.e2e_steps))
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
@@ -555,8 +695,10 @@ def run_ours(args):
     t_e2e = time.perf_counter() - t0
     e2e = {"value": n_plasma * args.e2e_steps / t_e2e, "unit": UNIT,
            "h2d_bytes_per_step": int(N * PARTICLE_DTYPE.itemsize + 96),
-           "d2h_bytes_per_step": int(N * PARTICLE_DTYPE.itemsize + 96 + 88),
-           "steps": args.e2e_steps, "timing": "wall clock around pot_gpu_move_particles calls"}
+           "d2h_bytes_per_step": int(d2h_rec * PARTICLE_DTYPE.itemsize / args.e2e_steps + 8 + 88),
+           "steps": args.e2e_steps, "first_step": t_first,
+           "timing": "wall clock around pot_gpu_move_particles calls: the whole Particle array uploaded, the "
+                     "grain's record and the range of the particles due copied back"}
     if ws > 1:
         e2e["value"] = n_plasma * ws * args.e2e_steps / reduce_max(t_e2e, dev)
 
@@ -573,9 +715,9 @@ def run_ours(args):
         batch = run_batches(args, local)
 
     extra = {}
-    if ws == 1 and args.extra_config not in ("none", "", args.config):
-        extra[args.extra_config] = time_config(args.extra_config, stream, dev, flush, steps=min(args.steps, 10),
-                                               warmup=3, plain_steps=min(args.plain_steps, 3) or 2)
+    for name in ([] if ws > 1 else [c for c in args.extra_config.split(",") if c and c not in ("none", args.config)]):
+        extra[name] = time_config(name, stream, dev, flush, steps=min(args.steps, 10), warmup=3,
+                                  plain_steps=min(args.plain_steps, 3) or 2)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -585,19 +727,17 @@ def run_ours(args):
                        "group_size": group,
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
                        "parallelism": "replicas" if ws > 1 else "1 GPU"},
-            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm_peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
-                         "ms_per_launch": per_launch_s * 1e3,
-                         "share_of_step": dom_ms / tk_ms if tk_ms else None,
-                         "timing": "per-kernel CUDA events in a second, instrumented pass over the same %d steps "
-                                   "(%.4f ms per step with the events)" % (args.steps, tk_ms / args.steps)},
+            "roofline": roofline(dom_name, inter, per_launch_s, clk, alg_bytes, achieved, hbm_peak, peak_kind,
+                                 traffic, dom_ms / tk_ms if tk_ms else None,
+                                 "per-kernel CUDA events in a second, instrumented pass over the same %d steps "
+                                 "(%.4f ms per step with the events)" % (args.steps, tk_ms / args.steps)),
             "interactions_per_s": (inter * ws / (t_ms / args.steps / 1e3)) if inter else None,
-            "walk_compute": walk_compute(inter, dom_name, per_launch_s, clk),
-            "kernels_ms": {k: round(v[0] / max(v[1], 1), 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
+            "interactions_per_push": (stk["sum_interactions"] / stk["sum_n_pushed"])
+            if stk.get("sum_n_pushed") else None,
+            "kernels": kernels,
             "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
             "walk_stack_max": st.get("stack_max"),
-            "targets_per_group": (st["n_pushed"] / st["n_groups"]) if st.get("n_groups") else None,
+            "targets_per_group": (stk["sum_n_pushed"] / stk["sum_n_groups"]) if stk.get("sum_n_groups") else None,
             "force_accuracy": accuracy, "extra_configs": extra or None,
             "batch": batch,
             "status": st["status"]}
@@ -616,7 +756,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--config", default="1m")
+    ap.add_argument("--config", default="4m")
     ap.add_argument("--form", choices=("fast", "plain"), default="fast")
     ap.add_argument("--leaf", type=int, default=0)
     ap.add_argument("--group", type=int, default=0, help="targets per warp group (32 or 64; default per config)")
@@ -625,13 +765,13 @@ def main(argv=None):
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-runs", type=int, default=64,
+    ap.add_argument("--batch-runs", type=int, default=32,
                     help="runs in the short batched sweep (0 to skip the batch and serving measurements)")
-    ap.add_argument("--batch-steps", type=int, default=400, help="step cap per run in the short batch measurements")
+    ap.add_argument("--batch-steps", type=int, default=4000, help="step cap per run in the short batch measurements")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window of the short serving run")
-    ap.add_argument("--extra-config", default="4m",
-                    help="also time this configuration (fast and plain FP64 form, N=1 only) into the line's "
-                         "extra_configs; 'none' to skip")
+    ap.add_argument("--extra-config", default="4m_tilt,1m",
+                    help="also time these configurations (comma-separated; fast and plain FP64 form, N=1 only) "
+                         "into the line's extra_configs; 'none' to skip")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

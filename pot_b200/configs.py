@@ -15,11 +15,14 @@ domain radius R = r * mpp.
 * ``4m``     the spheroidal-grain program (pot-spheroid.c, PROLATE):
   4,000,001 particles, a prolate spheroid of semi-axes 0.3 / 0.1 / 0.1
   lambda (-a 7.21387e-07 -A 3: a is the volume-equivalent radius, the
-  semi-axes a A^(2/3) and a A^(-1/3)) tilted 30 degrees from the flow axis x
-  towards y, Te/Ti = 10, Mach 0.5 drift, B = 0.9533 T along z (electron
-  gyroradius sqrt(k Te / m_e) / omega_ce = 0.5 lambda), domain 12 lambda,
-  theta 0.4, 20,000 steps, seed 3.  The reference cannot tilt its grain;
-  its runs of this plasma use the untilted spheroid (axis x).
+  semi-axes a A^(2/3) and a A^(-1/3)) with its axis along the flow axis x,
+  as the reference program has it (pot-spheroid.c:1689-1779, 2448-2537),
+  Te/Ti = 10, Mach 0.5 drift, B = 0.9533 T along z (electron gyroradius
+  sqrt(k Te / m_e) / omega_ce = 0.5 lambda), domain 12 lambda, theta 0.4,
+  20,000 steps, seed 3.
+* ``4m_tilt`` the same plasma with the spheroid tilted 30 degrees from the
+  flow axis x towards y.  The reference cannot tilt its grain, so this one
+  runs on the GPU only.
 
 Keys beyond the run's flags: ``steps`` (run length), ``leaf_size`` (fast
 form), ``seed`` and ``variant`` (the reference program that realises it:
@@ -36,9 +39,9 @@ CONFIGS = {
                Te=11600.0, Ti=1160.0, x_drift=9785.26, settle=0.0, theta=0.5, steps=10000, leaf_size=16),
     "4m": dict(N=4000001, r=1000, mpp=6.00218e-08, a=7.21387e-07, A=3.0, soft=5.00182e-08, dt=5.96447e-14,
                Te=11600.0, Ti=1160.0, x_drift=4892.63, settle=0.0, theta=0.4, B=(0.0, 0.0, 0.9533),
-               axis=(0.8660254037844387, 0.5, 0.0), steps=20000, leaf_size=16, group_size=64, seed=3,
-               variant="prolate_sceptic"),
+               steps=20000, leaf_size=16, group_size=64, seed=3, variant="prolate_sceptic"),
 }
+CONFIGS["4m_tilt"] = dict(CONFIGS["4m"], axis=(0.8660254037844387, 0.5, 0.0))
 
 EXTRA_KEYS = ("steps", "leaf_size", "group_size", "seed", "variant")
 
