@@ -36,7 +36,9 @@ Two things are built here, both with gcc, both outside the GPU product path:
    opening angle and field; C evaluates ``OAP * OAP * dist2`` identically for
    a literal and for a variable holding the same double.
 
-Usage: ``python oracle/build.py [--ref-root PATH] [--force]``.
+Usage: ``python oracle/build.py [--ref-root PATH] [--force]``.  The reference
+checkout is ``$POT_REFERENCE_ROOT`` if set, else ``--ref-root``, else a
+directory named ``reference`` beside this repository's own directory.
 """
 from __future__ import annotations
 
@@ -49,7 +51,10 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF_ROOT = os.environ.get("POT_REFERENCE_ROOT", "/root/reference")
+# The reference checkout: $POT_REFERENCE_ROOT, else --ref-root, else a
+# directory named "reference" beside this repository.
+DEFAULT_REF_ROOT = os.environ.get("POT_REFERENCE_ROOT") or \
+    os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 
 VARIANTS = ("sphere", "sceptic")
 SPHEROID_VARIANTS = ("prolate", "prolate_sceptic", "oblate", "oblate_sceptic")

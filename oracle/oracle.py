@@ -176,6 +176,12 @@ class RefLib:
         if self.variant_flags & 1:
             L.potref_tree_dipoles.argtypes = [C.c_ulong, C.c_void_p]
             L.potref_tree_dipoles.restype = C.c_long
+        L.potref_write_state.argtypes = [C.c_char_p]
+        L.potref_read_state.argtypes = [C.c_char_p]
+        L.potref_read_state.restype = C.c_int
+        self.has_write_phi = bool(L.potref_has_write_phi())
+        if self.has_write_phi:
+            L.potref_write_phi.argtypes = [C.c_char_p, C.c_ulong]
         self.shape = int(L.potref_shape())
         self.grain_enabled = bool(L.potref_grain_enabled())
         self.sceptic = bool(L.potref_has_sceptic())
@@ -240,6 +246,20 @@ class RefLib:
         buf = (C.c_char * self.prng_size)()
         self.lib.potref_get_prng(buf)
         return bytes(buf)
+
+    def write_state(self, path: str):
+        """The reference's write_sim_state_to_file (format C, pot.c:3816-3901)."""
+        self.lib.potref_write_state(os.fsencode(path))
+
+    def read_state(self, path: str):
+        """The reference's read_sim_state_from_file (pot.c:3904-4019)."""
+        if self.lib.potref_read_state(os.fsencode(path)) != 0:
+            raise RuntimeError("the reference failed to read the state file %s" % path)
+
+    def write_phi(self, path: str, time_step: int):
+        """The reference's write_phi_data_to_file (pot.c:3001-3042) over the
+        tree last built, rows appended to path."""
+        self.lib.potref_write_phi(os.fsencode(path), int(time_step))
 
     def set_prng(self, blob: bytes):
         buf = (C.c_char * self.prng_size).from_buffer_copy(blob)

@@ -392,6 +392,32 @@ double potref_integrate_for_alpha(double s, double chi_b, double u2, double Rol)
 }
 #endif
 
+/* The reference's own state-file writer and reader (pot.c:3816-3901,
+   3904-4019), on the harness's run: format C, one worker record.  read
+   returns 0 on success (read_sim_state_from_file's nonzero is success). */
+void potref_write_state(const char* path)
+{
+	/* run() writes at the top of an iteration, after its t_steps++
+	   (pot.c:4261, 4353-4356), and the file holds t_steps - 1: the steps
+	   completed, which is what H.t_steps counts here */
+	H.t_steps++;
+	write_sim_state_to_file((unsigned int) R.N, &H, path);
+	H.t_steps--;
+}
+int potref_read_state(const char* path) { return read_sim_state_from_file((unsigned int) R.N, &H, path) ? 0 : -1; }
+
+#ifdef RECORD_PHI_DATA
+/* write_phi_data_to_file (pot.c:3001-3042) for the tree last built, the
+   rows appended to `path` with time time_step * dt. */
+void potref_write_phi(const char* path, unsigned long time_step)
+{
+	write_phi_data_to_file(path, &H, R, time_step, H.root);
+}
+int potref_has_write_phi(void) { return 1; }
+#else
+int potref_has_write_phi(void) { return 0; }
+#endif
+
 /* One iteration of run()'s loop body for the hot path (pot.c:4261 t_steps++,
    4308 build_tree, 4386 move_particles), without the writers.
    Returns 0, or -1 if build_tree failed. */
