@@ -1,0 +1,120 @@
+"""Bit-exact parity at the benchmark sizes, against the compiled reference.
+
+The small-size tests pin the GPU to the oracle; these pin it to the
+reference program itself (oracle/_ref, compiled from pot.c and
+pot-spheroid.c) at the sizes the benchmark runs, where 21-level keys and
+deep cells occur:
+
+* the 1m plasma (1,000,001 particles): the reference's own init_particles
+  and build_tree (pot.c:658-996, 1457-1643) against the GPU's plain-form
+  tree of the same particles -- every internal cell (level, path, q, aq,
+  FP64 centre of |q|, width) and every leaf (particle, level, path) bit for
+  bit;
+* the 4m spheroid plasma (4,000,001 particles, pot-spheroid.c's prolate
+  grain along x, kept out of the tree as pot-spheroid.c:1516-1518 does);
+* one plain step of the 1m plasma against the oracle (GPU semantics): the
+  absorption tallies and grain charge exact, positions within 1e-12 of the
+  domain radius -- once with the benchmark's grain and once with a grain of
+  two Debye lengths, which absorbs particles in every step.
+
+Comparisons are vectorised: both dumps are put in (level, path) order and
+compared as arrays (the FP64 values as their bit patterns).
+"""
+import numpy as np
+import pytest
+
+from common import oracle_snapshot, run_config
+from oracle.oracle import RefLib, RunParams
+from pot_b200.configs import run_params, variant
+from pot_b200.gpu import Run
+
+pytestmark = pytest.mark.gpu
+
+
+def _sorted_dump(d):
+    o = np.lexsort((d["int_path"], d["int_level"]))
+    cells = {k: np.ascontiguousarray(d[k][o]) for k in ("int_level", "int_path", "int_q", "int_aq", "int_c", "int_w")}
+    ol = np.lexsort((d["leaf_path"], d["leaf_level"], d["leaf_part"]))
+    leaves = {k: np.ascontiguousarray(d[k][ol]) for k in ("leaf_part", "leaf_level", "leaf_path")}
+    return cells, leaves
+
+
+def _assert_same_tree(gd, rd):
+    gc, gl = _sorted_dump(gd)
+    rc, rl = _sorted_dump(rd)
+    assert len(gc["int_level"]) == len(rc["int_level"])
+    for k in ("int_level", "int_path", "int_q", "int_aq"):
+        assert np.array_equal(gc[k], rc[k]), k
+    for k in ("int_c", "int_w"):  # FP64, bit for bit
+        assert np.array_equal(gc[k].view(np.uint64), rc[k].view(np.uint64)), k
+    assert len(gl["leaf_part"]) == len(rl["leaf_part"])
+    for k in ("leaf_part", "leaf_level", "leaf_path"):
+        assert np.array_equal(gl[k], rl[k]), k
+
+
+def _reference_and_gpu_trees(cfg_name, seed, grain_q):
+    p = run_params(cfg_name, untilted=True)
+    ref = RefLib(variant(cfg_name), build=False)
+    ref.setup(RunParams(**p), seed=seed)
+    ref.set_grain(q=grain_q)
+    P = ref.particles()
+    ref.build_tree()
+    rd = ref.tree_dump()
+    g = dict(q=grain_q, pos=(P[0]["x"], P[0]["y"], P[0]["z"]))
+    with Run(run_config(p), form="plain", seed=seed) as r:
+        r.upload(P, g)
+        r.build_tree()
+        gd = r.tree_dump()
+    return gd, rd
+
+
+def test_tree_bit_exact_vs_reference_1m():
+    gd, rd = _reference_and_gpu_trees("1m", seed=11, grain_q=-2500)
+    assert len(rd["int_level"]) > 400000  # a leaf-size-1 tree over a million particles
+    _assert_same_tree(gd, rd)
+
+
+def test_tree_bit_exact_vs_reference_4m_spheroid():
+    gd, rd = _reference_and_gpu_trees("4m", seed=3, grain_q=-4000)
+    assert len(rd["leaf_part"]) == 4000000  # every plasma particle, the spheroid left out
+    assert 0 not in set(rd["leaf_part"][:16].tolist()) and not (rd["leaf_part"] == 0).any()
+    _assert_same_tree(gd, rd)
+
+
+@pytest.mark.parametrize("a_debye", [0.2, 2.0])
+def test_one_plain_step_1m_vs_oracle(a_debye):
+    p = run_params("1m")
+    lam = p["a"] / 0.2
+    p["a"] = a_debye * lam
+    o = oracle_snapshot(p, seed=4, mode="gpu")
+    o.set_grain(q=-3000)
+    P0 = o.particles()
+    g = dict(q=-3000, pos=(P0[0]["x"], P0[0]["y"], P0[0]["z"]))
+    with Run(run_config(p), form="plain", seed=4) as r:
+        r.upload(P0, g)
+        st = r.step(1)
+        Pg, gg = r.download()
+    o.step()
+    Po = o.particles()
+    go = o.grain()
+    so = o.last_step_stats()
+    assert st["status"] == 0
+    assert gg["q"] == go["q"] and gg["tot_absor_e"] == go["tot_absor_e"]
+    assert st["dq"] == so["dq"] and st["de"] == so["de"]
+    assert st["n_absorbed"] == so["n_absorbed"]
+    assert st["n_reinjected"] == so["n_reinjected"] and st["n_pushed"] == so["n_pushed"]
+    if a_debye >= 1.0:
+        assert st["n_absorbed"] > 0
+    assert np.array_equal(Pg["species"], Po["species"])
+    R = p["r"] * p["mpp"]
+    pos_g = np.stack([Pg["x"], Pg["y"], Pg["z"]], 1)
+    pos_o = np.stack([Po["x"], Po["y"], Po["z"]], 1)
+    # a particle absorbed and reinjected onto the boundary sphere is tested
+    # against the boundary again (pot.c:2676 then 2691): an ulp-level coin flip
+    # of libm, so the two may reinject it differently; each such particle lies
+    # on the sphere in both results, at most one per absorption
+    bad = np.nonzero(np.abs(pos_g - pos_o).max(1) >= 1e-12 * R)[0]
+    assert len(bad) <= so["n_absorbed"]
+    for P in (Pg, Po):
+        rr = np.sqrt((P["x"][bad] - R) ** 2 + (P["y"][bad] - R) ** 2 + (P["z"][bad] - R) ** 2)
+        assert np.all(np.abs(rr - R) < 1e-9 * R)

@@ -197,3 +197,79 @@ def test_variant_program_run(potgpu, tmp_path):
     assert "pos. Pois. collec'n:  yes" in d and "containment:          bouncing (c.o.e. 0.95)" in d
     rows = (out / "pot-macroscopic.dat").read_text().splitlines()[1:]
     assert len(rows) == 12
+
+
+def _reference_state(path, steps=5, seed=1):
+    """The reference itself (oracle/_ref, SCEPTIC) runs the small plasma
+    `steps` steps and writes its format C state file (pot.c:3816-3901)."""
+    from oracle.oracle import RefLib, RunParams
+    from common import SMALL
+    ref = RefLib("sceptic", build=False)
+    ref.setup(RunParams(**SMALL), seed=seed)
+    ref.set_grain(q=-40)
+    ref.run_steps(steps)
+    ref.write_state(str(path))
+    return ref
+
+
+def _parse_state_c(path, N):
+    """Header fields, PRNG blocks and particles of a one-worker format C file."""
+    raw = open(path, "rb").read()
+    nl = raw.index(b"\n")
+    head = raw[:nl].split()
+    assert head[0] == b"C" and int(head[1]) == 1
+    parts = np.frombuffer(raw[nl + 1 + 84:], PARTICLE_DTYPE)
+    assert len(parts) == N
+    return dict(q=int(head[2]), m=float(head[3]), t_steps=int(head[4]), tot_absor_e=int(head[8]),
+                chi_b=float(head[9])), parts
+
+
+def test_read_out_reference_state_file(potgpu, tmp_path):
+    """-R reads a state file the reference program itself wrote."""
+    path = tmp_path / "ref_state"
+    ref = _reference_state(path)
+    P = ref.particles()
+    p = run(SMALL_FLAGS + ["-R", str(path)])
+    assert p.returncode == 0, p.stderr
+    lines = p.stdout.strip().splitlines()
+    assert lines[0] == "NO S X Y Z VX VY VZ" and len(lines) == 8193 + 1
+    for i in (0, 1, 4096, 4097, 8192):
+        f = lines[1 + i].split()
+        assert int(f[0]) == i and f[1] == '"%s"' % "die"[P["species"][i]]
+        assert np.allclose([float(v) for v in f[2:]], [P[k][i] for k in ("x", "y", "z", "vx", "vy", "vz")],
+                           rtol=1e-5)
+
+
+@pytest.mark.gpu
+def test_state_files_and_phi_exchange_with_reference(potgpu, tmp_path):
+    """The reference writes a state file after 30 steps; potgpu -g resumes
+    from it (plain form, theta 0.5) and writes pot-phi.dat for that state
+    (--phi-start), which agrees row by row with the reference's own
+    write_phi_data_to_file (pot.c:3001-3042) over the same particles; after
+    one step potgpu -f writes its state, which the reference's
+    read_sim_state_from_file (pot.c:3904-4019) reads back: the particles
+    it holds are the file's, bit for bit."""
+    a = tmp_path / "ref_state"
+    ref = _reference_state(a, steps=30)
+    ref.build_tree()
+    ref_phi = tmp_path / "ref_phi.dat"
+    ref.write_phi(str(ref_phi), 30)
+    out = tmp_path / "out"
+    out.mkdir()
+    b = tmp_path / "gpu_state"
+    p = run(SMALL_FLAGS + ["--oap", "0.5", "--form", "plain", "-g", str(a), "-i", "31", "--phi-start",
+                           "--output-dir", str(out), "-f", str(b)])
+    assert p.returncode == 0, p.stderr
+    rows_g = (out / "pot-phi.dat").read_text().splitlines()
+    rows_r = ref_phi.read_text().splitlines()
+    assert len(rows_r) == 50 * 4 * 11 and rows_g[:len(rows_r)] and len(rows_g) >= len(rows_r)
+    for lg, lr in zip(rows_g, rows_r):
+        fg, fr = lg.split(), lr.split()
+        assert fg[:4] == fr[:4]
+        assert abs(float(fg[4]) - float(fr[4])) <= 2e-5 * abs(float(fr[4])) + 1e-12
+    head, parts = _parse_state_c(b, 8193)
+    assert head["t_steps"] == 31
+    ref.read_state(str(b))
+    g = ref.grain()
+    assert g["t_steps"] == 31 and g["q"] == head["q"] and g["tot_absor_e"] == head["tot_absor_e"]
+    assert ref.particles().tobytes() == parts.tobytes()
