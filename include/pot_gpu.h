@@ -116,6 +116,18 @@ typedef struct pot_gpu_opts {
 #define POT_FORM_FAST 1u   /* FP32 leaf-grouped warp walk, FP64 positions and push */
 
 #define POT_OPT_TIMING 0x1u  /* record CUDA events around each kernel (pot_gpu_kernel_times) */
+/* SCEPTIC reinjection with the edge potential capped (no counterpart in the
+   reference): the speed sampler is given min(chi, 0.9 (U^2 + 1/2)) for each
+   species, U its drift in units of its normalisation speed.  Above about
+   U^2 + 1/2 the reference's inverse CDF is NaN for every draw
+   (prng.c:171-214) and sceptically_reinject retries without end
+   (pot.c:582-599); a noisy single-point edge potential of a small grain in
+   cold ions can read that high.  Off, such a run stops with POT_E_ITER and
+   warn bit 64 (the reference's behaviour made finite); on, it goes on and
+   sets warn bit 512 (kept, like the other warn bits) once the cap has
+   applied.  A run whose edge potential stays below the cap gives the same
+   results either way. */
+#define POT_OPT_CHI_CAP 0x2u
 
 /* Grain state: the reference keeps it in Proc (pot.c:370-371, 397) and in
    parts[0] (pot.c:890-899). */
@@ -156,7 +168,8 @@ typedef struct pot_step_stats {
 	                          distribution for the edge potential (the reference's inverse
 	                          CDF is NaN there and it retries without end); 128 a particle in
 	                          the domain wall moving inwards (OUT_BOUNCE, the reference's
-	                          warning at pot.c:2719-2722); 256 the Poisson variate's cap */
+	                          warning at pot.c:2719-2722); 256 the Poisson variate's cap;
+	                          512 POT_OPT_CHI_CAP capped the edge potential for the sampler */
 	uint32_t n_collected;  /* POT_CFG_POIS_IONS: charges the Poisson ion collection added */
 	uint32_t n_wall;       /* OUT_BOUNCE: particles found outside moving inwards, left in place */
 	uint32_t n_bounced;    /* OUT_BOUNCE: particles bounced off the wall */
@@ -214,9 +227,13 @@ int pot_gpu_download(pot_gpu_ctx* ctx, pot_particle* parts, pot_grain_state* gra
    `parts` (N records, reference order) and `grain`, t_steps++, build the
    tree, move the particles, download both back into the same arrays.  The
    transfers run in chunks that overlap the conversions (page-locked host
-   memory lets them overlap the most).  On an error status the particle
-   array holds the device's state at the failure (kernels skip their work
-   once a status is set) and `grain` is left as passed. */
+   memory lets them overlap the most).  Only the records the step can have
+   changed are copied back: the grain's and the contiguous range of
+   reference indices holding every particle due this step (species s is due
+   when t_steps % tss[s] == 0); the records outside it are neither pushed
+   nor reinjected and keep their values.  On an error status the particles
+   in that range hold the device's state at the failure (kernels skip their
+   work once a status is set) and `grain` is left as passed. */
 int pot_gpu_move_particles(pot_gpu_ctx* ctx, pot_particle* parts, uint64_t N,
                            pot_grain_state* grain, pot_step_stats* out);
 
@@ -251,8 +268,11 @@ int pot_gpu_field_at(pot_gpu_ctx* ctx, uint64_t n, const uint32_t* idx, const do
    device which loads the library holds until the process exits; hence at
    most POT_NOALLOC_MAX_POINTS points per call, larger n returns
    POT_E_LIMIT.  The first call on each device looks the array's device
-   address up (make that call before any stream capture).  All calls on a
-   device share the array: calls whose work overlaps on the GPU race. */
+   address up and keeps it (make that call before any stream capture); the
+   kept address is valid while the device's primary context lives, so a
+   program that calls cudaDeviceReset must not call this function again.
+   All calls on a device share the array: calls whose work overlaps on the
+   GPU race. */
 #define POT_NOALLOC_MAX_POINTS 65536u
 int pot_gpu_field_at_noalloc(pot_gpu_ctx* ctx, uint64_t n, const uint32_t* idx, const double* xyz,
                              double* E);
@@ -317,16 +337,24 @@ int pot_gpu_bytes_needed(const pot_run_cfg* cfg, const pot_gpu_opts* opts, uint6
 
 /* ---- batches of independent runs ---------------------------------------
    No counterpart in the reference, which runs one grain per MPI job.  A
-   batch holds many runs (each its own context and stream) and advances all
-   of them with one CUDA-graph launch per `steps_per_launch` steps; runs are
-   admitted while free HBM allows and evicted when done.  Runs share no
-   state: each result is bit-identical to the same run stepped alone. */
+   batch holds many runs (each its own context) and advances all of them
+   with one CUDA-graph launch per `steps_per_launch` steps; runs are admitted
+   while free HBM allows and evicted when done.  Fast-form Boris runs with
+   the same group size and key depth are packed: each kernel of their step
+   is one launch over all of them (a grid shared out by run size, the walk
+   one persistent launch over every run's target groups).  Other runs step
+   as their own kernel sequences in the same graph.  Runs share no state:
+   each result is bit-identical to the same run stepped alone. */
 typedef struct pot_batch pot_batch;
+
+#define POT_BATCH_NO_PACK 0x1u  /* step every run as its own kernel sequence */
 
 typedef struct pot_batch_opts {
 	int32_t device;
 	uint32_t steps_per_launch;  /* steps per graph launch, even; 0 = 2 */
 	uint64_t reserve_bytes;     /* HBM left free when admitting */
+	uint32_t flags;             /* POT_BATCH_* */
+	uint32_t pad;
 } pot_batch_opts;
 
 /* One member's state, gathered on the device for the whole batch. */
@@ -362,8 +390,10 @@ int pot_batch_count(pot_batch* b, uint32_t* runs, uint64_t* particles, uint64_t*
 int pot_batch_ctx(pot_batch* b, int32_t slot, pot_gpu_ctx** ctx);
 
 /* Autotuner: time `steps` steps of each candidate (leaf size, group size)
-   of the fast form on a fresh run of cfg and write the fastest into opts
-   (its ms per step into *ms_per_step). */
+   of the fast form -- (8, 32), (16, 32), (32, 32), (16, 64), (32, 64) -- on
+   one run of cfg (created once, its particles initialised again for each
+   candidate) and write the fastest into opts (its ms per step into
+   *ms_per_step). */
 int pot_gpu_tune(const pot_run_cfg* cfg, pot_gpu_opts* opts, uint32_t steps, double* ms_per_step);
 
 #ifdef __cplusplus

@@ -71,6 +71,12 @@ struct pot_gpu_ctx {
 	cudaEvent_t xev[2 * 4 + 1] = {};
 	RunRec* h_rec = nullptr;
 	StepHist* h_hist = nullptr;
+	// reference-index range [lo, hi] of the particles due in the drop-in
+	// call's step (device and pinned host copies) and the event after which
+	// the host reads it
+	uint32_t* due_rng = nullptr;
+	uint32_t* h_due_rng = nullptr;
+	cudaEvent_t rng_ev = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -216,6 +222,40 @@ __global__ void k_from_aos_range(const pot_particle* __restrict__ aos, uint32_t 
 	pid[i] = i;
 }
 
+// k_from_aos_range that also records the smallest and largest reference
+// index of the particles due at step t (t % tss[species] == 0, as the
+// reorder's due flags have it) in rng[0] (atomicMin) and rng[1] (atomicMax).
+__global__ void k_from_aos_range_due(const pot_particle* __restrict__ aos, uint32_t i0, uint32_t cnt,
+                                     double4* __restrict__ pos, double4* __restrict__ vel,
+                                     uint32_t* __restrict__ pid, RunRec* rec, unsigned long long t, uint3 tss,
+                                     uint32_t* __restrict__ rng)
+{
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	bool due = false;
+	uint32_t i = 0;
+	if (k < cnt) {
+		i = i0 + k;
+		const pot_particle p = aos[i];
+		int sp = p.species;
+		if (sp < 0 || sp > 2) {
+			set_status(rec, POT_E_ARG);
+			sp = SP_E;
+		}
+		pos[i] = make_double4(p.x, p.y, p.z, (double)sp);
+		vel[i] = make_double4(p.vx, p.vy, p.vz, 0.0);
+		pid[i] = i;
+		const uint32_t m = sp == SP_DUST ? tss.x : (sp == SP_ION ? tss.y : tss.z);
+		due = (t % m) == 0;
+	}
+	// one atomic pair per warp
+	const unsigned int b = __ballot_sync(0xffffffffu, due);
+	if (b && (threadIdx.x & 31u) == 0) {
+		const uint32_t w0 = i0 + (blockIdx.x * blockDim.x + (threadIdx.x & ~31u));
+		atomicMin(&rng[0], w0 + (uint32_t)(__ffs(b) - 1));
+		atomicMax(&rng[1], w0 + (uint32_t)(31 - __clz(b)));
+	}
+}
+
 __global__ void k_to_aos_gather(const double4* __restrict__ pos, const double4* __restrict__ vel,
                                 const uint32_t* __restrict__ inv, uint32_t i0, uint32_t cnt,
                                 pot_particle* __restrict__ aos)
@@ -287,7 +327,7 @@ static int fill_params(pot_gpu_ctx* c)
 	P.n_ions = (uint32_t)((r.N - 1) / 2);
 	P.r_pix = r.r;
 	P.leaf_size = c->opts.leaf_size;
-	P.flags = r.flags;
+	P.flags = r.flags | ((c->opts.flags & POT_OPT_CHI_CAP) ? FLAG_CHI_CAP : 0u);
 	P.form = c->opts.form;
 	// Fast form: bucket leaves of 8 or more need few levels (a level-10 cell holds on
 	// average N / 5.6e8 particles, 0.03 at the largest N), and 30 key bits sort in
@@ -493,6 +533,70 @@ int ctx_enqueue(pot_gpu_ctx* c, uint32_t nsteps)
 	return POT_OK;
 }
 void ctx_mark_error(pot_gpu_ctx* c, int rc) { if (c->sticky == POT_OK) c->sticky = rc; }
+void ctx_set_tree_valid(pot_gpu_ctx* c) { c->tree_valid = true; }
+// The autotuner's candidates on one context: a fast-form context created
+// with leaf size 8 (the largest tree capacity of the sizes that key ten
+// levels) takes any leaf size of 8 or more and any group size; its step
+// graphs are dropped and its particles initialised again.
+int ctx_retune(pot_gpu_ctx* c, uint32_t leaf, uint32_t group)
+{
+	if (c->P.form != POT_FORM_FAST || c->opts.leaf_size != 8 || leaf < 8 || leaf > 64 ||
+	    (group != 32 && group != 64) || (c->cfg.flags & POT_CFG_DIPOLES))
+		return POT_E_ARG;
+	if (c->cfg.N <= (uint64_t)leaf + (c->cfg.A != 0.0 ? 1u : 0u)) return POT_E_ARG;
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	for (auto& row : c->step_exec)
+		for (auto& g : row)
+			if (g) {
+				cudaGraphExecDestroy(g);
+				g = nullptr;
+			}
+	c->graphs_off = false;
+	pot_gpu_opts o = c->opts;
+	o.leaf_size = leaf;
+	o.group_size = group;
+	c->opts = o;
+	int rc = fill_params(c);
+	if (rc != POT_OK) return rc;
+	c->opts.leaf_size = 8;  // the allocation's leaf size: the next retune checks it
+	c->P.leaf_size = leaf;
+	return pot_gpu_init_particles(c);
+}
+// The packed-batch view of a run (pot_batch.cu); false when the run cannot
+// join a packed launch: the plain form, dipoles or a non-Boris integrator
+// (their steps have other kernels), or a query-only context.
+bool ctx_member_view(pot_gpu_ctx* c, MemberView* v)
+{
+	if (c->P.form != POT_FORM_FAST || c->P.integrator != POT_INT_BORIS || (c->cfg.flags & POT_CFG_DIPOLES) ||
+	    !c->T.mom_pre || !c->src32)
+		return false;
+	std::memset(v, 0, sizeof(*v));
+	v->P = c->P;
+	v->T = c->T;
+	v->rec = c->rec;
+	v->hist = c->hist;
+	for (int b = 0; b < 2; b++) {
+		v->pos[b] = c->pos[b];
+		v->vel[b] = c->vel[b];
+		v->pid[b] = c->pid[b];
+		v->keys[b] = c->keys[b];
+		v->vals[b] = c->vals[b];
+	}
+	v->src64 = c->src64;
+	v->src32 = c->src32;
+	v->counts = c->counts;
+	v->block_sums = c->block_sums;
+	v->due = c->due;
+	v->due_list = c->due_list;
+	v->due_prefix = c->due_prefix;
+	v->groups = c->groups;
+	v->rein_list = c->rein_list;
+	v->cur = (uint32_t)c->cur;
+	v->kb = (uint32_t)(radix_passes((int)c->P.key_bits) & 1);
+	v->tiles = radix_tiles(c->n);
+	return true;
+}
 }  // namespace pot
 
 extern "C" {
@@ -528,8 +632,10 @@ void pot_gpu_destroy(pot_gpu_ctx* c)
 	for (auto& e : c->xev)
 		if (e) cudaEventDestroy(e);
 	if (c->xfer) cudaStreamDestroy(c->xfer);
+	if (c->rng_ev) cudaEventDestroy(c->rng_ev);
 	if (c->h_rec) cudaFreeHost(c->h_rec);
 	if (c->h_hist) cudaFreeHost(c->h_hist);
+	if (c->h_due_rng) cudaFreeHost(c->h_due_rng);
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 	delete c;
@@ -964,11 +1070,13 @@ int pot_gpu_download(pot_gpu_ctx* c, pot_particle* parts, pot_grain_state* grain
 }
 
 // The drop-in call as one pipeline: the upload in chunks on a copy stream,
-// each chunk converted as soon as it has arrived; the step; the download
-// gathered in chunks in reference order, each chunk copied back while the
-// next is gathered; the run record and step history copied with it.  One
-// wait for the host at the end.  Same results as pot_gpu_upload, pot_gpu_step
-// and pot_gpu_download in turn.
+// each chunk converted as soon as it has arrived; the step; the download of
+// the records the step can have changed (the grain's and the range of the
+// particles due), gathered in chunks in reference order, each chunk copied
+// back while the next is gathered; the run record and step history copied
+// with it.  The host waits twice: for the upload (to learn the due range,
+// while the step runs) and at the end.  Same results as pot_gpu_upload,
+// pot_gpu_step and pot_gpu_download in turn.
 constexpr int XFER_CHUNKS = 4;
 
 static int xfer_setup(pot_gpu_ctx* c)
@@ -976,20 +1084,29 @@ static int xfer_setup(pot_gpu_ctx* c)
 	if (c->xfer) return POT_OK;
 	CK(cudaStreamCreateWithFlags(&c->xfer, cudaStreamNonBlocking));
 	for (auto& e : c->xev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+	CK(cudaEventCreateWithFlags(&c->rng_ev, cudaEventDisableTiming));
 	CK(cudaMallocHost((void**)&c->h_rec, sizeof(RunRec)));
 	CK(cudaMallocHost((void**)&c->h_hist, sizeof(StepHist) * HIST));
+	CK(cudaMallocHost((void**)&c->h_due_rng, 2 * sizeof(uint32_t)));
+	const int ra = dalloc(c, &c->due_rng, 2);
+	if (ra) return ra;
 	return POT_OK;
 }
 
-// the copies and kernels of the drop-in call; the caller waits for both
-// streams whatever this returns, so no copy outlives the call
-static int move_enqueue(pot_gpu_ctx* c, pot_particle* parts, const pot_grain_state* grain, bool want_hist)
+// The drop-in call's first half: the run record, the upload in chunks on the
+// copy stream with each chunk converted on the context's stream as soon as
+// it has landed (recording the reference-index range of the particles due
+// this step), that range copied to pinned memory behind rng_ev, and the
+// step.  The caller waits for both streams whatever this returns, so no copy
+// outlives the call.
+static int move_enqueue_in(pot_gpu_ctx* c, pot_particle* parts, const pot_grain_state* grain)
 {
 	int rc = POT_OK;
 	const uint32_t n = c->n;
 	const int K = n >= 4u * 65536u ? XFER_CHUNKS : 1;
 	// the run record first (as set_rec_from_grain writes it, from pinned
 	// memory), so a bad species found by the conversion below is not overwritten
+	unsigned long long t_prev = 0;
 	{
 		RunRec& r = *c->h_rec;
 		std::memset(&r, 0, sizeof(r));
@@ -1007,8 +1124,13 @@ static int move_enqueue(pot_gpu_ctx* c, pot_particle* parts, const pot_grain_sta
 			r.grain_vel[0] = parts[0].vx; r.grain_vel[1] = parts[0].vy; r.grain_vel[2] = parts[0].vz;
 		}
 		r.grain_slot = 0xFFFFFFFFu;
+		t_prev = r.t_steps;
 		CK(cudaMemcpyAsync(c->rec, &r, offsetof(RunRec, n_collected), cudaMemcpyHostToDevice, c->stream));
 	}
+	// due range: lo starts at ~0 (every byte 0xFF), hi at 0
+	CK(cudaMemsetAsync(&c->due_rng[0], 0xFF, sizeof(uint32_t), c->stream));
+	CK(cudaMemsetAsync(&c->due_rng[1], 0, sizeof(uint32_t), c->stream));
+	const uint3 tss = make_uint3(c->P.tss[SP_DUST], c->P.tss[SP_ION], c->P.tss[SP_E]);
 	// upload: chunk k lands on the copy stream, then is converted on the
 	// context's stream (after whatever that stream already holds)
 	c->cur = 0;
@@ -1020,9 +1142,12 @@ static int move_enqueue(pot_gpu_ctx* c, pot_particle* parts, const pot_grain_sta
 		                   c->xfer));
 		CK(cudaEventRecord(c->xev[k], c->xfer));
 		CK(cudaStreamWaitEvent(c->stream, c->xev[k], 0));
-		k_from_aos_range<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->aos, i0, i1 - i0, c->pos[0], c->vel[0],
-		                                                              c->pid[0], c->rec);
+		k_from_aos_range_due<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->aos, i0, i1 - i0, c->pos[0], c->vel[0],
+		                                                                  c->pid[0], c->rec, t_prev + 1ull, tss,
+		                                                                  c->due_rng);
 	}
+	CK(cudaMemcpyAsync(c->h_due_rng, c->due_rng, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaEventRecord(c->rng_ev, c->stream));
 	c->sticky = POT_OK;  // as pot_gpu_upload: a new state clears the run's status
 	c->uploaded = true;
 	c->tree_valid = false;
@@ -1030,16 +1155,38 @@ static int move_enqueue(pot_gpu_ctx* c, pot_particle* parts, const pot_grain_sta
 	rc = step_once(c, 0);
 	if (rc != POT_OK) return rc;
 	c->tree_valid = true;
-	// download in reference order: slot of each particle, then gather and copy by chunks
+	CK(cudaGetLastError());
+	return POT_OK;
+}
+
+// The second half, once the host has the due range [lo, hi]: only those
+// records and the grain's (index 0) can have changed in the step (a particle
+// not due is neither pushed nor reinjected), so only they are gathered in
+// reference order and copied back, in chunks, each copied while the next is
+// gathered; the caller's other records already hold the same values.  Then
+// the run record and step history.
+static int move_enqueue_out(pot_gpu_ctx* c, pot_particle* parts, uint32_t lo, uint32_t hi, bool want_hist)
+{
+	const uint32_t n = c->n;
 	k_inverse<<<nblk(n, 256), 256, 0, c->stream>>>(c->pid[c->cur], n, c->inv);
-	for (int k = 0; k < K; k++) {
-		const uint32_t i0 = (uint32_t)((uint64_t)n * k / K), i1 = (uint32_t)((uint64_t)n * (k + 1) / K);
-		k_to_aos_gather<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->vel[c->cur], c->inv, i0,
-		                                                             i1 - i0, c->aos);
-		CK(cudaEventRecord(c->xev[XFER_CHUNKS + k], c->stream));
-		CK(cudaStreamWaitEvent(c->xfer, c->xev[XFER_CHUNKS + k], 0));
-		CK(cudaMemcpyAsync(parts + i0, c->aos + i0, sizeof(pot_particle) * (i1 - i0), cudaMemcpyDeviceToHost,
-		                   c->xfer));
+	if (lo > 0 || hi < lo) {  // the grain's record on its own
+		k_to_aos_gather<<<1, 32, 0, c->stream>>>(c->pos[c->cur], c->vel[c->cur], c->inv, 0u, 1u, c->aos);
+		CK(cudaEventRecord(c->xev[2 * XFER_CHUNKS], c->stream));
+		CK(cudaStreamWaitEvent(c->xfer, c->xev[2 * XFER_CHUNKS], 0));
+		CK(cudaMemcpyAsync(parts, c->aos, sizeof(pot_particle), cudaMemcpyDeviceToHost, c->xfer));
+	}
+	if (hi >= lo && hi < n) {
+		const uint32_t m = hi - lo + 1u;
+		const int K = m >= 4u * 65536u ? XFER_CHUNKS : 1;
+		for (int k = 0; k < K; k++) {
+			const uint32_t i0 = lo + (uint32_t)((uint64_t)m * k / K), i1 = lo + (uint32_t)((uint64_t)m * (k + 1) / K);
+			k_to_aos_gather<<<nblk(i1 - i0, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->vel[c->cur], c->inv, i0,
+			                                                             i1 - i0, c->aos);
+			CK(cudaEventRecord(c->xev[XFER_CHUNKS + k], c->stream));
+			CK(cudaStreamWaitEvent(c->xfer, c->xev[XFER_CHUNKS + k], 0));
+			CK(cudaMemcpyAsync(parts + i0, c->aos + i0, sizeof(pot_particle) * (i1 - i0), cudaMemcpyDeviceToHost,
+			                   c->xfer));
+		}
 	}
 	CK(cudaMemcpyAsync(c->h_rec, c->rec, sizeof(RunRec), cudaMemcpyDeviceToHost, c->stream));
 	if (want_hist) CK(cudaMemcpyAsync(c->h_hist, c->hist, sizeof(StepHist) * HIST, cudaMemcpyDeviceToHost, c->stream));
@@ -1059,7 +1206,16 @@ int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_
 	}
 	int rc = xfer_setup(c);
 	if (rc) return rc;
-	rc = move_enqueue(c, parts, grain, out != nullptr);
+	rc = move_enqueue_in(c, parts, grain);
+	if (rc == POT_OK) {
+		// the host waits for the upload and the due range only; the step is
+		// already queued behind them, so the GPU does not wait for the host
+		if (cudaEventSynchronize(c->rng_ev) != cudaSuccess) {
+			rc = POT_E_CUDA;
+		} else {
+			rc = move_enqueue_out(c, parts, c->h_due_rng[0], c->h_due_rng[1], out != nullptr);
+		}
+	}
 	const cudaError_t e1 = cudaStreamSynchronize(c->xfer);
 	const cudaError_t e2 = cudaStreamSynchronize(c->stream);
 	if (rc != POT_OK) return rc;
@@ -1251,8 +1407,10 @@ struct NoAllocScratch {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
 // Device address of g_noalloc_scratch on `device` (the current device),
-// looked up once per device.  In host code the symbol names a host-side
-// stand-in, never device memory, so kernels only ever get this address.
+// looked up once per device and kept for the life of the process: valid
+// while that device's primary context lives (cudaDeviceReset would leave it
+// stale).  In host code the symbol names a host-side stand-in, never device
+// memory, so kernels only ever get this address.
 static int noalloc_scratch(int device, NoAllocScratch** out)
 {
 	static std::mutex mu;

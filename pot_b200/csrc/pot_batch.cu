@@ -29,6 +29,9 @@ uint64_t ctx_particles(const pot_gpu_ctx* c);
 int ctx_ready(const pot_gpu_ctx* c);
 int ctx_enqueue(pot_gpu_ctx* c, uint32_t nsteps);
 void ctx_mark_error(pot_gpu_ctx* c, int rc);
+bool ctx_member_view(pot_gpu_ctx* c, MemberView* v);
+void ctx_set_tree_valid(pot_gpu_ctx* c);
+int ctx_retune(pot_gpu_ctx* c, uint32_t leaf, uint32_t group);
 
 // one member's summary row
 struct BatchRow {
@@ -64,6 +67,19 @@ struct BatchSlot {
 	cudaEvent_t join = nullptr;
 };
 
+// Members that share one packed launch per kernel: fast-form Boris runs
+// with the same group size and the same radix passes.  Its device block
+// holds the members' views, each stage's block prefix, the walk's group
+// prefix and work counter.
+struct PackClass {
+	uint32_t group_max = 0, npass = 0;
+	std::vector<int> slots;
+	void* mem = nullptr;
+	PackDev B {};
+	cudaStream_t st = nullptr;
+	cudaEvent_t join = nullptr;
+};
+
 struct pot_batch {
 	int device = 0;
 	uint32_t spl = 2;            // steps per graph launch (even)
@@ -79,8 +95,20 @@ struct pot_batch {
 	BatchRow* h_rows = nullptr;  // pinned
 	uint32_t cap_rows = 0;
 	std::vector<int> order;      // slot of each summary row
+	std::vector<PackClass> packs;  // packed launches of the last capture
+	bool pack = true;            // pack the members that can be packed
 	int sticky = POT_OK;
 };
+
+static void free_packs(pot_batch* b)
+{
+	for (auto& pc : b->packs) {
+		if (pc.mem) cudaFree(pc.mem);
+		if (pc.join) cudaEventDestroy(pc.join);
+		if (pc.st) cudaStreamDestroy(pc.st);
+	}
+	b->packs.clear();
+}
 
 #define BCK(x)                                                        \
 	do {                                                              \
@@ -108,6 +136,7 @@ int pot_batch_create(const pot_batch_opts* opts, pot_batch** out)
 	b->device = o.device;
 	b->spl = o.steps_per_launch;
 	b->reserve = o.reserve_bytes;
+	b->pack = (o.flags & POT_BATCH_NO_PACK) == 0;
 	if (cudaSetDevice(b->device) != cudaSuccess ||
 	    cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) != cudaSuccess ||
 	    cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
@@ -124,6 +153,7 @@ void pot_batch_destroy(pot_batch* b)
 	cudaSetDevice(b->device);
 	if (b->origin) cudaStreamSynchronize(b->origin);
 	if (b->exec) cudaGraphExecDestroy(b->exec);
+	free_packs(b);
 	for (auto& s : b->slots) {
 		if (s.ctx) pot_gpu_destroy(s.ctx);
 		if (s.join) cudaEventDestroy(s.join);
@@ -215,6 +245,108 @@ static int ensure_rows(pot_batch* b, uint32_t n)
 	return POT_OK;
 }
 
+static inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// Blocks of each packed stage for one member (the single run's grids,
+// except where a kernel strides over a device-side count: there a share
+// proportional to the member's size).
+static void member_blocks(const MemberView& v, uint32_t out[PS_COUNT])
+{
+	const uint32_t n = v.P.n, nt = v.P.n_tree, L = v.P.leaf_size;
+	out[PS_N256] = div_up(n, 256);
+	out[PS_HIST] = std::min<uint32_t>(v.tiles, 1024u);
+	out[PS_TILES] = v.tiles;
+	out[PS_CMP] = pack_scan_blocks(n);
+	out[PS_PAIRS] = div_up(nt - 1, 256);
+	out[PS_NODES] = pack_scan_blocks(nt - L);
+	out[PS_FILL] = div_up(nt - L, 256);
+	out[PS_FINISH] = div_up(nt, 256);
+	out[PS_MOM] = div_up(nt, PACK_MOM_TILE);
+	out[PS_MOMPRE] = div_up(nt / 4 + 1, 256);
+	out[PS_GROUPS] = std::min<uint32_t>(592u, std::max<uint32_t>(1u, div_up(nt, 2048)));
+	out[PS_ONE] = 1;
+	out[PS_SMALL] = std::max<uint32_t>(1u, std::min<uint32_t>(148u, n / 16384u));
+}
+
+// Sort the batch's live members into packed classes (left in b->packs,
+// with their device blocks filled) and the rest (`chains`), which step as
+// their own kernel sequences.
+static int plan_packs(pot_batch* b, std::vector<int>& chains)
+{
+	free_packs(b);
+	chains.clear();
+	std::vector<std::vector<MemberView>> views;
+	for (int k : b->order) {
+		MemberView v;
+		if (!b->pack || !ctx_member_view(b->slots[k].ctx, &v)) {
+			chains.push_back(k);
+			continue;
+		}
+		const uint32_t npass = (uint32_t)radix_passes((int)v.P.key_bits);
+		size_t c = 0;
+		while (c < b->packs.size() && (b->packs[c].group_max != v.P.group_max || b->packs[c].npass != npass)) c++;
+		if (c == b->packs.size()) {
+			b->packs.emplace_back();
+			b->packs.back().group_max = v.P.group_max;
+			b->packs.back().npass = npass;
+			views.emplace_back();
+		}
+		b->packs[c].slots.push_back(k);
+		views[c].push_back(v);
+	}
+	for (size_t c = 0; c < b->packs.size(); c++) {
+		PackClass& pc = b->packs[c];
+		const uint32_t M = (uint32_t)views[c].size();
+		// device block: views, then per stage M + 1 prefix words, the group prefix, the counter
+		const size_t views_b = (sizeof(MemberView) * M + 255) / 256 * 256;
+		const size_t words = (size_t)PS_COUNT * (M + 1) + (M + 1) + 1;
+		std::vector<uint32_t> h(words, 0u);
+		for (uint32_t m = 0; m < M; m++) {
+			uint32_t nb[PS_COUNT];
+			member_blocks(views[c][m], nb);
+			for (int st = 0; st < PS_COUNT; st++) h[(size_t)st * (M + 1) + m + 1] = h[(size_t)st * (M + 1) + m] + nb[st];
+		}
+		BCK(cudaMalloc(&pc.mem, views_b + words * sizeof(uint32_t)));
+		char* base = static_cast<char*>(pc.mem);
+		uint32_t* w = reinterpret_cast<uint32_t*>(base + views_b);
+		BCK(cudaMemcpy(base, views[c].data(), sizeof(MemberView) * M, cudaMemcpyHostToDevice));
+		BCK(cudaMemcpy(w, h.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+		pc.B.mv = reinterpret_cast<const MemberView*>(base);
+		pc.B.M = M;
+		pc.B.npass = pc.npass;
+		for (int st = 0; st < PS_COUNT; st++) {
+			pc.B.pre[st] = w + (size_t)st * (M + 1);
+			pc.B.blocks[st] = h[(size_t)st * (M + 1) + M];
+		}
+		pc.B.gpre = w + (size_t)PS_COUNT * (M + 1);
+		pc.B.ctr = w + (size_t)PS_COUNT * (M + 1) + (M + 1);
+		BCK(cudaStreamCreateWithFlags(&pc.st, cudaStreamNonBlocking));
+		BCK(cudaEventCreateWithFlags(&pc.join, cudaEventDisableTiming));
+	}
+	return POT_OK;
+}
+
+// One packed class's `spl` steps: every kernel of the fast Boris step once
+// for all its members (enqueue_step's sequence).
+static void enqueue_pack(const PackClass& pc, uint32_t spl)
+{
+	const PackDev& B = pc.B;
+	cudaStream_t s = pc.st;
+	for (uint32_t k = 0; k < spl; k++) {
+		pack_keys(B, (int)k, s);
+		pack_sort(B, s);
+		pack_reorder(B, (int)k, s);
+		pack_build(B, s);
+		pack_compact(B, s);
+		pack_groups(B, s);
+		pack_chi_b(B, s);
+		pack_push(B, (int)k, pc.group_max > 32 ? 2u : 1u, s);
+		pack_absorb_late(B, (int)k, s);
+		pack_reinject(B, (int)k, s);
+		pack_grain_end(B, (int)k, s);
+	}
+}
+
 // Capture every member's `spl` steps and the summary gather into one graph.
 static int capture(pot_batch* b)
 {
@@ -238,10 +370,29 @@ static int capture(pot_batch* b)
 	BCK(cudaStreamSynchronize(b->origin));
 	// every member's own queue must be idle before it joins the capture
 	for (int k : b->order) BCK(cudaStreamSynchronize(ctx_stream(b->slots[k].ctx)));
+	std::vector<int> chains;
+	rc = plan_packs(b, chains);
+	if (rc != POT_OK) return rc;
 	BCK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
 	cudaError_t ce = cudaEventRecord(b->fork, b->origin);
 	int first_err = ce == cudaSuccess ? POT_OK : POT_E_CUDA;
-	for (int k : b->order) {
+	for (auto& pc : b->packs) {
+		if (first_err != POT_OK) break;
+		if (cudaStreamWaitEvent(pc.st, b->fork, 0) != cudaSuccess) {
+			first_err = POT_E_CUDA;
+			break;
+		}
+		enqueue_pack(pc, b->spl);
+		if (cudaGetLastError() != cudaSuccess) first_err = POT_E_CUDA;
+		if (cudaEventRecord(pc.join, pc.st) != cudaSuccess || cudaStreamWaitEvent(b->origin, pc.join, 0) != cudaSuccess) {
+			if (first_err == POT_OK) first_err = POT_E_CUDA;
+		}
+		for (int k : pc.slots) {
+			b->slots[k].parity = ctx_parity(b->slots[k].ctx);
+			ctx_set_tree_valid(b->slots[k].ctx);
+		}
+	}
+	for (int k : chains) {
 		if (first_err != POT_OK) break;
 		BatchSlot& s = b->slots[k];
 		cudaStream_t st = ctx_stream(s.ctx);
@@ -382,21 +533,27 @@ int pot_gpu_tune(const pot_run_cfg* cfg, pot_gpu_opts* opts, uint32_t steps, dou
 	steps += steps % 2;
 	static const uint32_t cand[][2] = { { 8, 32 }, { 16, 32 }, { 32, 32 }, { 16, 64 }, { 32, 64 } };
 	double best = -1.0;
-	pot_gpu_opts best_o = *opts;
+	uint32_t best_l = 0, best_g = 0;
 	if (cudaSetDevice(opts->device) != cudaSuccess) return POT_E_CUDA;
+	// one context for every candidate: created with leaf size 8, the largest
+	// tree of the candidates, and switched between them (ctx_retune)
+	pot_gpu_opts o = *opts;
+	o.leaf_size = 8;
+	o.group_size = 32;
+	o.flags &= ~POT_OPT_TIMING;
+	o.stream = nullptr;
+	pot_gpu_ctx* c = nullptr;
+	int rc = pot_gpu_create(cfg, &o, &c);
+	if (rc != POT_OK) return rc;
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
-	BCK(cudaEventCreate(&e0));
-	BCK(cudaEventCreate(&e1));
+	if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+		if (e0) cudaEventDestroy(e0);
+		pot_gpu_destroy(c);
+		return POT_E_CUDA;
+	}
 	int last_rc = POT_OK;
 	for (const auto& c2 : cand) {
-		pot_gpu_opts o = *opts;
-		o.leaf_size = c2[0];
-		o.group_size = c2[1];
-		o.flags &= ~POT_OPT_TIMING;
-		o.stream = nullptr;
-		pot_gpu_ctx* c = nullptr;
-		int rc = pot_gpu_create(cfg, &o, &c);
-		if (rc == POT_OK) rc = pot_gpu_init_particles(c);
+		rc = ctx_retune(c, c2[0], c2[1]);
 		if (rc == POT_OK) rc = ctx_enqueue(c, 2);  // warm-up, kernel by kernel as the batch enqueues them
 		if (rc == POT_OK) rc = pot_gpu_sync(c);
 		float ms = 0.f;
@@ -409,22 +566,24 @@ int pot_gpu_tune(const pot_run_cfg* cfg, pot_gpu_opts* opts, uint32_t steps, dou
 			if (rc == POT_OK) cudaEventElapsedTime(&ms, e0, e1);
 			if (rc == POT_OK) rc = pot_gpu_sync(c);
 		}
-		if (c) pot_gpu_destroy(c);
 		if (rc != POT_OK) {
 			last_rc = rc;
+			if (rc == POT_E_CUDA) break;
 			continue;
 		}
 		const double per = ms / steps;
 		if (best < 0.0 || per < best) {
 			best = per;
-			best_o = o;
+			best_l = c2[0];
+			best_g = c2[1];
 		}
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
+	pot_gpu_destroy(c);
 	if (best < 0.0) return last_rc != POT_OK ? last_rc : POT_E_CUDA;
-	opts->leaf_size = best_o.leaf_size;
-	opts->group_size = best_o.group_size;
+	opts->leaf_size = best_l;
+	opts->group_size = best_g;
 	if (ms_per_step) *ms_per_step = best;
 	return POT_OK;
 }

@@ -72,6 +72,9 @@ size_t radix_counts_words(size_t n);
 // LSD radix sort of (keys, vals) on bits [low_bit, 64) in 8-bit passes;
 // result in keys[0]/vals[0] when the number of passes is even, keys[1]/vals[1]
 // otherwise (returns the index).
+// tiles and 8-bit passes of radix_sort_pairs for n keys sorted from low_bit
+uint32_t radix_tiles(size_t n);
+int radix_passes(int low_bit);
 int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* counts, uint32_t* block_sums,
                      int low_bit, cudaStream_t s, Timer& tm, int* err);
 

@@ -27,6 +27,9 @@ constexpr uint32_t FAIL_SIMPSON = 16u; // orbit-integral halvings (pot.c:433-492
 constexpr uint32_t FAIL_SHELL = 32u;   // initial radius outside the grain (pot.c:703-708)
 constexpr uint32_t FAIL_SPEED = 64u;   // no speed distribution for this chi_b: the inverse CDF is NaN
                                        // (u_icdf for chi_b above about U^2 + 1/2, prng.c:171-214)
+// Not a failure: POT_OPT_CHI_CAP capped the edge potential (warn bit 512,
+// no status).
+constexpr uint32_t FAIL_CAPPED = WARN_CHI_CAP;
 constexpr int NEWTON_CAP = 200;
 constexpr int REJECT_CAP = 10000;
 // NaN alpha means the sampled orbit meets a potential barrier; with cold ions
@@ -316,6 +319,16 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 	for (int attempt = 0;; attempt++) {
 		chi_b = chi_b_in;
 		if (sp == SP_E) chi_b *= -P.Ti / P.Te;
+		if (P.flags & FLAG_CHI_CAP) {
+			// POT_OPT_CHI_CAP: keep the speed distribution defined (its inverse
+			// CDF needs chi below about U^2 + 1/2); nine tenths of that
+			const double U = P.x_drift / v_n;
+			const double cap = 0.9 * ((U * U) + 0.5);
+			if (chi_b > cap) {
+				chi_b = cap;
+				fail |= FAIL_CAPPED;
+			}
+		}
 		if (P.x_drift != 0.0) {
 			const double U = P.x_drift / v_n;
 			int k = 0;
@@ -433,18 +446,19 @@ __device__ __forceinline__ bool outside_sphere(const double4& p, const Params& P
 // the grain (reinjected, then tested against the boundary once more, as
 // pot.c:2676 followed by pot.c:2691 -- with OUT_BOUNCE that test is the
 // wall's, against the start-of-step position in src64), 2 = left the domain.
-__global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel, const uint32_t* __restrict__ pid,
-                           const uint32_t* __restrict__ list, const double4* __restrict__ src64, Params P,
-                           RunRec* rec)
+template <class G>
+__device__ __forceinline__ void reinject_body(G grd, double4* __restrict__ pos, double4* __restrict__ vel,
+                                              const uint32_t* __restrict__ pid, const uint32_t* __restrict__ list,
+                                              const double4* __restrict__ src64, const Params& P, RunRec* rec)
 {
 	if (rec->status != POT_OK) return;
 	const uint32_t n = rec->n_rein;
 	const uint32_t t = (uint32_t)rec->t_steps;
 	const double chi_b = rec->chi_b;
 	const uint32_t lane = threadIdx.x & 31u;
-	const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+	const uint32_t warps = grd.n() * (blockDim.x >> 5);
 	// one warp per reinjected particle
-	for (uint32_t e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < n; e += warps) {
+	for (uint32_t e = grd.id() * (blockDim.x >> 5) + (threadIdx.x >> 5); e < n; e += warps) {
 		const uint32_t w = list[e];
 		const uint32_t s = w & 0x3FFFFFFFu;
 		const uint32_t reason = w >> 30;
@@ -468,11 +482,20 @@ __global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel,
 		}
 		if (lane == 0) {
 			count_wall(rec, wall);
-			if (fail) { atomicOr(&rec->warn, fail); set_status(rec, POT_E_ITER); }
+			if (fail) {
+				atomicOr(&rec->warn, fail);
+				if (fail & ~FAIL_CAPPED) set_status(rec, POT_E_ITER);
+			}
 			pos[s] = p;
 			vel[s] = v;
 		}
 	}
+}
+
+__global__ void k_reinject(double4* __restrict__ pos, double4* __restrict__ vel, const uint32_t* __restrict__ pid,
+                           const uint32_t* __restrict__ list, const double4* __restrict__ src64, Params P, RunRec* rec)
+{
+	reinject_body(GridSelf {}, pos, vel, pid, list, src64, P, rec);
 }
 
 // init_particles for one rank (pot.c:887-935), reference order: slot i holds
@@ -494,7 +517,10 @@ __global__ void k_init(double4* __restrict__ pos, double4* __restrict__ vel, uin
 	Stream st;
 	st.init(P.seed, i, 0u, 0x20000u);
 	inject<false>(st, sp, false, 0.0, P, p, v, fail);
-	if (fail) { atomicOr(&rec->warn, fail); set_status(rec, POT_E_ITER); }
+	if (fail) {
+		atomicOr(&rec->warn, fail);
+		if (fail & ~FAIL_CAPPED) set_status(rec, POT_E_ITER);
+	}
 	pos[i] = p;
 	vel[i] = v;
 }
@@ -511,6 +537,26 @@ void launch_init(double4* pos, double4* vel, uint32_t* pid, const Params& P, Run
 {
 	ScopedKernel k(tm, "init");
 	k_init<<<(P.n_total + 127) / 128, 128, 0, s>>>(pos, vel, pid, P, rec);
+}
+
+}  // namespace pot
+
+// ---------------------------------------------------------------------------
+// packed batch: the reinjection of every member in one launch
+// ---------------------------------------------------------------------------
+namespace pot {
+
+__global__ void kp_reinject(PackDev B, int k)
+{
+	const SegBlock sb = seg_block(B.pre[PS_SMALL], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const uint32_t b = pack_out(v, k);
+	reinject_body(GridSeg { sb.id, sb.n }, v.pos[b], v.vel[b], v.pid[b], v.rein_list, v.src64, v.P, v.rec);
+}
+
+void pack_reinject(const PackDev& B, int k, cudaStream_t s)
+{
+	kp_reinject<<<B.blocks[PS_SMALL], 128, 0, s>>>(B, k);
 }
 
 }  // namespace pot

@@ -63,6 +63,8 @@ constexpr uint32_t FLAG_DIPOLES = POT_CFG_DIPOLES;
 constexpr uint32_t FLAG_POIS = POT_CFG_POIS_IONS;
 constexpr uint32_t WARN_WALL = 128u;     // OUT_BOUNCE: a particle in the wall moving inwards
 constexpr uint32_t WARN_POISSON = 256u;  // the Poisson variate's iteration cap
+constexpr uint32_t WARN_CHI_CAP = 512u;  // POT_OPT_CHI_CAP: the sampler's edge potential was capped
+constexpr uint32_t FLAG_CHI_CAP = 0x100u;  // Params.flags: POT_OPT_CHI_CAP (above the run's POT_CFG_* bits)
 
 // Device-resident record of one run; the host reads it only at sync points.
 struct RunRec {
@@ -240,6 +242,38 @@ struct Stream {
 	// rnd(state, maximum) of prng.c:11-28: maximum * u / UINT32_MAX.
 	__device__ double rnd(double maximum) { return maximum * ((double)next() / 4294967295.0); }
 };
+
+// The grid a kernel body runs in.  A kernel of one run passes GridSelf (its
+// own block index and grid size); a batched launch, which covers several
+// member runs with one grid, passes each block its index and grid size
+// within its member's share (GridSeg, from seg_block).
+struct GridSelf {
+	__device__ __forceinline__ uint32_t id() const { return blockIdx.x; }
+	__device__ __forceinline__ uint32_t n() const { return gridDim.x; }
+};
+struct GridSeg {
+	uint32_t i, c;
+	__device__ __forceinline__ uint32_t id() const { return i; }
+	__device__ __forceinline__ uint32_t n() const { return c; }
+};
+
+// Block `blockIdx.x` of a batched launch: its member m (pre[m] <= blockIdx.x
+// < pre[m + 1], pre an exclusive prefix of the members' block counts) and
+// its block index and grid size within that member's share of the launch.
+struct SegBlock {
+	uint32_t m, id, n;
+};
+__device__ __forceinline__ SegBlock seg_block(const uint32_t* __restrict__ pre, uint32_t M)
+{
+	uint32_t lo = 0, hi = M;  // pre[lo] <= b < pre[hi]
+	const uint32_t b = blockIdx.x;
+	while (hi - lo > 1) {
+		const uint32_t mid = (lo + hi) >> 1;
+		if (__ldg(&pre[mid]) <= b) lo = mid; else hi = mid;
+	}
+	const uint32_t p0 = __ldg(&pre[lo]);
+	return SegBlock { lo, b - p0, __ldg(&pre[lo + 1]) - p0 };
+}
 
 __device__ __forceinline__ void set_status(RunRec* rec, int code)
 {

@@ -1,10 +1,14 @@
 // Device-wide exclusive scan, stream compaction and the 64-bit LSD radix
 // sort of (Morton key, slot) pairs that orders particles each step.
 //
-// All three are reduce-then-scan designs: no kernel waits on another
-// block, so nothing here can spin.  Work is tiled so that a block owns a
-// contiguous tile and touches only its own outputs (in-place scans are safe).
-#include "pot_host.h"
+// The scan and the compaction are reduce-then-scan designs: none of their
+// kernels waits on another block.  The radix sort's pass (k_os_pass) does
+// wait: each tile spins in its decoupled look-back on the status words of
+// tiles that took an earlier ticket (and are therefore resident), with
+// OS_SPIN_CAP as the limit after which it records POT_E_ITER and finishes.
+// Work is tiled so that a block owns a contiguous tile and touches only its
+// own outputs (in-place scans are safe).
+#include "pot_tree.cuh"
 
 namespace pot {
 
@@ -55,22 +59,30 @@ __device__ __forceinline__ uint32_t load_val(const T* in, size_t i, size_t n)
 	return i < n ? (uint32_t)(in[i] != 0 ? (sizeof(T) == 1 ? 1u : (uint32_t)in[i]) : 0u) : 0u;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const T* __restrict__ in, size_t n,
-                                                              uint32_t* __restrict__ block_sums)
+template <typename T, class G>
+__device__ __forceinline__ void scan_reduce_body(G grd, const T* __restrict__ in, size_t n,
+                                                 uint32_t* __restrict__ block_sums)
 {
-	const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
+	const size_t base = (size_t)grd.id() * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
 	uint32_t s = 0;
 #pragma unroll
 	for (int k = 0; k < SCAN_ITEMS; k++) s += load_val(in, base + k, n);
 	uint32_t tot;
 	block_excl_scan(s, &tot);
-	if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+	if (threadIdx.x == 0) block_sums[grd.id()] = tot;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const T* __restrict__ in, size_t n,
+                                                              uint32_t* __restrict__ block_sums)
+{
+	scan_reduce_body<T>(GridSelf {}, in, n, block_sums);
 }
 
 // One block scans all block sums (nb <= SCAN_TILE).
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(uint32_t* __restrict__ block_sums, size_t nb,
-                                                           unsigned int* __restrict__ total)
+template <class G>
+__device__ __forceinline__ void scan_top_body(G grd, uint32_t* __restrict__ block_sums, size_t nb,
+                                              unsigned int* __restrict__ total)
 {
 	uint32_t v[SCAN_ITEMS];
 	uint32_t s = 0;
@@ -90,13 +102,18 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(uint32_t* __restrict_
 	if (threadIdx.x == 0 && total) *total = tot;
 }
 
-template <typename T, bool COMPACT>
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const T* __restrict__ in, size_t n,
-                                                            const uint32_t* __restrict__ block_sums,
-                                                            uint32_t* __restrict__ out,
-                                                            uint32_t* __restrict__ prefix = nullptr)
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(uint32_t* __restrict__ block_sums, size_t nb,
+                                                           unsigned int* __restrict__ total)
 {
-	const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
+	scan_top_body(GridSelf {}, block_sums, nb, total);
+}
+
+template <typename T, bool COMPACT, class G>
+__device__ __forceinline__ void scan_down_body(G grd, const T* __restrict__ in, size_t n,
+                                               const uint32_t* __restrict__ block_sums, uint32_t* __restrict__ out,
+                                               uint32_t* __restrict__ prefix)
+{
+	const size_t base = (size_t)grd.id() * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
 	uint32_t v[SCAN_ITEMS];
 	uint32_t s = 0;
 #pragma unroll
@@ -105,7 +122,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const T* __restrict_
 		s += v[k];
 	}
 	uint32_t tot;
-	uint32_t run = block_excl_scan(s, &tot) + block_sums[blockIdx.x];
+	uint32_t run = block_excl_scan(s, &tot) + block_sums[grd.id()];
 #pragma unroll
 	for (int k = 0; k < SCAN_ITEMS; k++) {
 		if (base + k < n) {
@@ -119,6 +136,15 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const T* __restrict_
 		run += v[k];
 		if (COMPACT && prefix && base + k + 1 == n) prefix[n] = run;
 	}
+}
+
+template <typename T, bool COMPACT>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const T* __restrict__ in, size_t n,
+                                                            const uint32_t* __restrict__ block_sums,
+                                                            uint32_t* __restrict__ out,
+                                                            uint32_t* __restrict__ prefix = nullptr)
+{
+	scan_down_body<T, COMPACT>(GridSelf {}, in, n, block_sums, out, prefix);
 }
 
 size_t scan_blocks(size_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
@@ -165,13 +191,14 @@ constexpr long OS_SPIN_CAP = 1L << 24;
 constexpr int OS_LOOKBACK = 8;      // earlier tiles read per round of the look-back
 
 // Digit counts of every pass in one read of the keys: hist[p * 256 + d].
-__global__ void __launch_bounds__(OS_THREADS) k_os_hist(const uint64_t* __restrict__ keys, size_t n, int low_bit,
-                                                        int npass, uint32_t* __restrict__ hist)
+template <class G>
+__device__ __forceinline__ void os_hist_body(G grd, const uint64_t* __restrict__ keys, size_t n, int low_bit,
+                                             int npass, uint32_t* __restrict__ hist)
 {
 	__shared__ uint32_t h[OS_MAX_PASSES][RS_BINS];
 	for (int i = threadIdx.x; i < OS_MAX_PASSES * RS_BINS; i += OS_THREADS) (&h[0][0])[i] = 0;
 	__syncthreads();
-	for (size_t i = (size_t)blockIdx.x * OS_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * OS_THREADS) {
+	for (size_t i = (size_t)grd.id() * OS_THREADS + threadIdx.x; i < n; i += (size_t)grd.n() * OS_THREADS) {
 		const uint64_t k = keys[i];
 		for (int p = 0; p < npass; p++) atomicAdd(&h[p][(k >> (low_bit + 8 * p)) & 0xFF], 1u);
 	}
@@ -182,8 +209,15 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_hist(const uint64_t* __restri
 	}
 }
 
+__global__ void __launch_bounds__(OS_THREADS) k_os_hist(const uint64_t* __restrict__ keys, size_t n, int low_bit,
+                                                        int npass, uint32_t* __restrict__ hist)
+{
+	os_hist_body(GridSelf {}, keys, n, low_bit, npass, hist);
+}
+
 // In place: hist[p * 256 + d] <- exclusive prefix over digits (one block).
-__global__ void __launch_bounds__(RS_BINS) k_os_offsets(uint32_t* __restrict__ hist, int npass)
+template <class G>
+__device__ __forceinline__ void os_offsets_body(G grd, uint32_t* __restrict__ hist, int npass)
 {
 	for (int p = 0; p < npass; p++) {
 		uint32_t tot;
@@ -194,13 +228,17 @@ __global__ void __launch_bounds__(RS_BINS) k_os_offsets(uint32_t* __restrict__ h
 	}
 }
 
-__global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restrict__ kin,
-                                                        const uint32_t* __restrict__ vin, size_t n, int shift,
-                                                        const uint32_t* __restrict__ goff,
-                                                        uint32_t* __restrict__ status,
-                                                        unsigned int* __restrict__ tile_ctr,
-                                                        uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                        int* __restrict__ err)
+__global__ void __launch_bounds__(RS_BINS) k_os_offsets(uint32_t* __restrict__ hist, int npass)
+{
+	os_offsets_body(GridSelf {}, hist, npass);
+}
+
+template <class G>
+__device__ __forceinline__ void os_pass_body(G grd, const uint64_t* __restrict__ kin,
+                                             const uint32_t* __restrict__ vin, size_t n, int shift,
+                                             const uint32_t* __restrict__ goff, uint32_t* __restrict__ status,
+                                             unsigned int* __restrict__ tile_ctr, uint64_t* __restrict__ kout,
+                                             uint32_t* __restrict__ vout, int* __restrict__ err)
 {
 	constexpr int NW = OS_THREADS / 32;
 	__shared__ uint32_t s_tile;
@@ -320,7 +358,21 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restri
 	}
 }
 
+__global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restrict__ kin,
+                                                        const uint32_t* __restrict__ vin, size_t n, int shift,
+                                                        const uint32_t* __restrict__ goff,
+                                                        uint32_t* __restrict__ status,
+                                                        unsigned int* __restrict__ tile_ctr,
+                                                        uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                        int* __restrict__ err)
+{
+	os_pass_body(GridSelf {}, kin, vin, n, shift, goff, status, tile_ctr, kout, vout, err);
+}
+
 static inline int os_passes(int low_bit) { return (63 - low_bit + 7) / 8; }
+
+uint32_t radix_tiles(size_t n) { return (uint32_t)((n + OS_TILE - 1) / OS_TILE); }
+int radix_passes(int low_bit) { return os_passes(low_bit); }
 
 size_t radix_counts_words(size_t n)
 {
@@ -356,6 +408,154 @@ int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* c
 		src ^= 1;
 	}
 	return src;
+}
+
+}  // namespace pot
+
+// ---------------------------------------------------------------------------
+// packed batch: the sort, the due list and the cell numbering of every
+// member in one launch per kernel (the single run's sequences above)
+// ---------------------------------------------------------------------------
+namespace pot {
+
+uint32_t pack_scan_blocks(uint32_t n) { return (uint32_t)scan_blocks(n ? n : 1); }
+
+// scan_blocks(max(n, 1)) in device code
+__device__ __forceinline__ size_t dev_scan_blocks(size_t n)
+{
+	return ((n ? n : 1) + SCAN_TILE - 1) / SCAN_TILE;
+}
+
+// The radix sort's layout in a member's counts buffer (radix_sort_pairs).
+struct OsLayout {
+	uint32_t* status;
+	uint32_t* hist;
+	unsigned int* ctr;
+	__device__ OsLayout(const MemberView& v)
+	{
+		status = v.counts;
+		hist = v.counts + (size_t)OS_MAX_PASSES * v.tiles * RS_BINS;
+		ctr = hist + OS_MAX_PASSES * RS_BINS;
+	}
+};
+
+// What the single run clears with memsets before its sort, tree and groups:
+// each tile's status words of every pass; block 0 of a member the digit
+// counts, tile counters, overflow count and group count.
+__global__ void __launch_bounds__(OS_THREADS) kp_sort_clear(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_TILES], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const OsLayout L(v);
+	for (uint32_t p = 0; p < B.npass; p++)
+		L.status[((size_t)p * v.tiles + sb.id) * RS_BINS + threadIdx.x] = 0u;
+	if (sb.id == 0) {
+		for (int i = threadIdx.x; i < OS_MAX_PASSES * RS_BINS + OS_MAX_PASSES; i += OS_THREADS) L.hist[i] = 0u;
+		if (threadIdx.x == 0) {
+			v.rec->n_overflow = 0;
+			v.rec->n_groups = 0;
+		}
+	}
+}
+
+__global__ void __launch_bounds__(OS_THREADS) kp_os_hist(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_HIST], B.M);
+	const MemberView& v = B.mv[sb.m];
+	os_hist_body(GridSeg { sb.id, sb.n }, v.keys[0], (size_t)v.P.n, (int)v.P.key_bits, (int)B.npass,
+	             OsLayout(v).hist);
+}
+
+__global__ void __launch_bounds__(RS_BINS) kp_os_offsets(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_ONE], B.M);
+	const MemberView& v = B.mv[sb.m];
+	os_offsets_body(GridSeg { sb.id, sb.n }, OsLayout(v).hist, (int)B.npass);
+}
+
+// Pass p: every member's tiles; a tile's index within its member comes from
+// the member's own ticket counter, so the look-back waits only on tiles of
+// the same member that took earlier tickets (and are therefore resident).
+__global__ void __launch_bounds__(OS_THREADS) kp_os_pass(PackDev B, int p)
+{
+	const SegBlock sb = seg_block(B.pre[PS_TILES], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const OsLayout L(v);
+	const int src = p & 1;
+	os_pass_body(GridSeg { sb.id, sb.n }, v.keys[src], v.vals[src], (size_t)v.P.n, (int)v.P.key_bits + 8 * p,
+	             L.hist + p * RS_BINS, L.status + (size_t)p * v.tiles * RS_BINS, L.ctr + p, v.keys[src ^ 1],
+	             v.vals[src ^ 1], &v.rec->status);
+}
+
+void pack_sort(const PackDev& B, cudaStream_t s)
+{
+	kp_sort_clear<<<B.blocks[PS_TILES], OS_THREADS, 0, s>>>(B);
+	kp_os_hist<<<B.blocks[PS_HIST], OS_THREADS, 0, s>>>(B);
+	kp_os_offsets<<<B.blocks[PS_ONE], RS_BINS, 0, s>>>(B);
+	for (uint32_t p = 0; p < B.npass; p++) kp_os_pass<<<B.blocks[PS_TILES], OS_THREADS, 0, s>>>(B, (int)p);
+}
+
+// the due list and its prefix (compact_flags)
+__global__ void __launch_bounds__(SCAN_THREADS) kp_cmp_reduce(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_CMP], B.M);
+	const MemberView& v = B.mv[sb.m];
+	scan_reduce_body<uint8_t>(GridSeg { sb.id, sb.n }, v.due, (size_t)v.P.n, v.block_sums);
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) kp_cmp_top(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_ONE], B.M);
+	const MemberView& v = B.mv[sb.m];
+	scan_top_body(GridSeg { sb.id, sb.n }, v.block_sums, dev_scan_blocks(v.P.n), &v.rec->n_due);
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) kp_cmp_down(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_CMP], B.M);
+	const MemberView& v = B.mv[sb.m];
+	scan_down_body<uint8_t, true>(GridSeg { sb.id, sb.n }, v.due, (size_t)v.P.n, v.block_sums, v.due_list,
+	                              v.due_prefix);
+}
+
+void pack_compact(const PackDev& B, cudaStream_t s)
+{
+	kp_cmp_reduce<<<B.blocks[PS_CMP], SCAN_THREADS, 0, s>>>(B);
+	kp_cmp_top<<<B.blocks[PS_ONE], SCAN_THREADS, 0, s>>>(B);
+	kp_cmp_down<<<B.blocks[PS_CMP], SCAN_THREADS, 0, s>>>(B);
+}
+
+// cell numbering: exclusive scan of the cells each key pair owns
+// (launch_build's scan_exclusive)
+__global__ void __launch_bounds__(SCAN_THREADS) kp_node_reduce(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_NODES], B.M);
+	const MemberView& v = B.mv[sb.m];
+	scan_reduce_body<uint32_t>(GridSeg { sb.id, sb.n }, v.T.cnt, (size_t)(v.P.n_tree - v.P.leaf_size),
+	                           v.block_sums);
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) kp_node_top(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_ONE], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const size_t np = v.P.n_tree - v.P.leaf_size;
+	scan_top_body(GridSeg { sb.id, sb.n }, v.block_sums, dev_scan_blocks(np), &v.rec->n_nodes);
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) kp_node_down(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_NODES], B.M);
+	const MemberView& v = B.mv[sb.m];
+	scan_down_body<uint32_t, false>(GridSeg { sb.id, sb.n }, v.T.cnt, (size_t)(v.P.n_tree - v.P.leaf_size),
+	                                v.block_sums, v.T.base, nullptr);
+}
+
+void pack_node_scan(const PackDev& B, cudaStream_t s)
+{
+	kp_node_reduce<<<B.blocks[PS_NODES], SCAN_THREADS, 0, s>>>(B);
+	kp_node_top<<<B.blocks[PS_ONE], SCAN_THREADS, 0, s>>>(B);
+	kp_node_down<<<B.blocks[PS_NODES], SCAN_THREADS, 0, s>>>(B);
 }
 
 }  // namespace pot

@@ -72,10 +72,11 @@ __device__ __forceinline__ uint64_t scaled_key(double x, double y, double z, dou
 	return (spread3(ix) << 2) | (spread3(iy) << 1) | spread3(iz);
 }
 
-__global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ keys,
-                       uint32_t* __restrict__ vals, Params P, RunRec* rec, int begin_step)
+template <class G>
+__device__ __forceinline__ void keys_body(G grd, const double4* __restrict__ pos, uint64_t* __restrict__ keys,
+                                          uint32_t* __restrict__ vals, const Params& P, RunRec* rec, int begin_step)
 {
-	if (begin_step && blockIdx.x == 0 && threadIdx.x == 0) {
+	if (begin_step && grd.id() == 0 && threadIdx.x == 0) {
 		const unsigned long long t = rec->t_steps + 1;
 		rec->t_steps = t;
 		rec->n_due = 0;
@@ -97,7 +98,7 @@ __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ k
 		rec->n_bounced = 0;
 		rec->grain_slot = 0xFFFFFFFFu;
 	}
-	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t s = grd.id() * blockDim.x + threadIdx.x;
 	if (s >= P.n) return;
 	const double4 p = pos[s];
 	if (isnan(p.x) || isnan(p.y) || isnan(p.z)) {
@@ -114,16 +115,24 @@ __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ k
 	vals[s] = s;
 }
 
+__global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                       Params P, RunRec* rec, int begin_step)
+{
+	keys_body(GridSelf {}, pos, keys, vals, P, rec, begin_step);
+}
+
 // Gather the state into the new Morton order, write the tree sources and
 // mark the particles due this step (electrons every step, ions every
 // tss[ION] steps, the grain every tss[DUST] steps, pot.c:2430-2434).
-__global__ void k_reorder(const uint32_t* __restrict__ perm, const double4* __restrict__ pos_in,
-                          const double4* __restrict__ vel_in, const uint32_t* __restrict__ pid_in,
-                          double4* __restrict__ pos_out, double4* __restrict__ vel_out,
-                          uint32_t* __restrict__ pid_out, double4* __restrict__ src64,
-                          float4* __restrict__ src32, uint8_t* __restrict__ due, Params P, RunRec* rec)
+template <class G>
+__device__ __forceinline__ void reorder_body(G grd, const uint32_t* __restrict__ perm,
+                                             const double4* __restrict__ pos_in, const double4* __restrict__ vel_in,
+                                             const uint32_t* __restrict__ pid_in, double4* __restrict__ pos_out,
+                                             double4* __restrict__ vel_out, uint32_t* __restrict__ pid_out,
+                                             double4* __restrict__ src64, float4* __restrict__ src32,
+                                             uint8_t* __restrict__ due, const Params& P, RunRec* rec)
 {
-	const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t s = grd.id() * blockDim.x + threadIdx.x;
 	if (s >= P.n) return;
 	const uint32_t j = perm[s];
 	const double4 p = pos_in[j];
@@ -143,6 +152,15 @@ __global__ void k_reorder(const uint32_t* __restrict__ perm, const double4* __re
 	if (sp == SP_DUST) rec->grain_slot = s;
 }
 
+__global__ void k_reorder(const uint32_t* __restrict__ perm, const double4* __restrict__ pos_in,
+                          const double4* __restrict__ vel_in, const uint32_t* __restrict__ pid_in,
+                          double4* __restrict__ pos_out, double4* __restrict__ vel_out,
+                          uint32_t* __restrict__ pid_out, double4* __restrict__ src64, float4* __restrict__ src32,
+                          uint8_t* __restrict__ due, Params P, RunRec* rec)
+{
+	reorder_body(GridSelf {}, perm, pos_in, vel_in, pid_in, pos_out, vel_out, pid_out, src64, src32, due, P, rec);
+}
+
 __device__ __forceinline__ int lcp_levels(uint64_t a, uint64_t b)
 {
 	const uint64_t x = a ^ b;
@@ -152,11 +170,13 @@ __device__ __forceinline__ int lcp_levels(uint64_t a, uint64_t b)
 
 // lvl8[i] = common levels of keys i and i + L (capped at 20: a level-21
 // cell cannot split); cnt[i] = number of cells pair i owns.
-__global__ void k_pairs(const uint64_t* __restrict__ keys, const double4* __restrict__ src64, uint32_t n,
-                        uint32_t n_pairs, uint32_t L, int max_level, int8_t* __restrict__ lvl8,
-                        uint32_t* __restrict__ cnt, RunRec* rec)
+template <class G>
+__device__ __forceinline__ void pairs_body(G grd, const uint64_t* __restrict__ keys,
+                                           const double4* __restrict__ src64, uint32_t n, uint32_t n_pairs,
+                                           uint32_t L, int max_level, int8_t* __restrict__ lvl8,
+                                           uint32_t* __restrict__ cnt, RunRec* rec)
 {
-	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t i = grd.id() * blockDim.x + threadIdx.x;
 	// Two particles at one position: the reference's insertion would split
 	// forever (pot.c:1466-1470) or fail at a reallocation (pot.c:1578-1586).
 	if (i + 1 < n && keys[i] == keys[i + 1]) {
@@ -176,10 +196,19 @@ __global__ void k_pairs(const uint64_t* __restrict__ keys, const double4* __rest
 	cnt[i] = hi > prev ? (uint32_t)(hi - prev) : 0u;
 }
 
-__global__ void k_fill_nodes(const int8_t* __restrict__ lvl8, const uint32_t* __restrict__ base,
-                             uint32_t n_pairs, TreeDev T, RunRec* rec)
+__global__ void k_pairs(const uint64_t* __restrict__ keys, const double4* __restrict__ src64, uint32_t n,
+                        uint32_t n_pairs, uint32_t L, int max_level, int8_t* __restrict__ lvl8,
+                        uint32_t* __restrict__ cnt, RunRec* rec)
 {
-	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	pairs_body(GridSelf {}, keys, src64, n, n_pairs, L, max_level, lvl8, cnt, rec);
+}
+
+template <class G>
+__device__ __forceinline__ void fill_nodes_body(G grd, const int8_t* __restrict__ lvl8,
+                                                const uint32_t* __restrict__ base, uint32_t n_pairs, const TreeDev& T,
+                                                RunRec* rec)
+{
+	const uint32_t i = grd.id() * blockDim.x + threadIdx.x;
 	if (i >= n_pairs) return;
 	const int hi = lvl8[i];
 	const int lo = i == 0 ? 0 : lvl8[i - 1] + 1;
@@ -192,6 +221,12 @@ __global__ void k_fill_nodes(const int8_t* __restrict__ lvl8, const uint32_t* __
 		T.first[k] = i;
 		T.level[k] = (uint8_t)l;
 	}
+}
+
+__global__ void k_fill_nodes(const int8_t* __restrict__ lvl8, const uint32_t* __restrict__ base, uint32_t n_pairs,
+                             TreeDev T, RunRec* rec)
+{
+	fill_nodes_body(GridSelf {}, lvl8, base, n_pairs, T, rec);
 }
 
 // The searches below run over a cell's sorted key range, where the tested
@@ -285,16 +320,17 @@ __device__ __forceinline__ void child_starts(const uint64_t* __restrict__ keys, 
 	for (int c = 0; c < 7; c++) s[c + 1] = lo[c];
 }
 
-__global__ void k_finish_nodes(const uint64_t* __restrict__ keys, uint32_t n, uint32_t L,
-                               const int8_t* __restrict__ lvl8, const uint32_t* __restrict__ base,
-                               TreeDev T, Params P, RunRec* rec)
+template <class G>
+__device__ __forceinline__ void finish_nodes_body(G grd, const uint64_t* __restrict__ keys, uint32_t n, uint32_t L,
+                                                  const int8_t* __restrict__ lvl8, const uint32_t* __restrict__ base,
+                                                  const TreeDev& T, const Params& P, RunRec* rec)
 {
 	const uint32_t M = rec->n_nodes;
 	if (M > T.cap) {
-		if (blockIdx.x == 0 && threadIdx.x == 0) set_status(rec, POT_E_CAPACITY);
+		if (grd.id() == 0 && threadIdx.x == 0) set_status(rec, POT_E_CAPACITY);
 		return;
 	}
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+	for (uint32_t k = grd.id() * blockDim.x + threadIdx.x; k < M; k += grd.n() * blockDim.x) {
 		const uint32_t f = T.first[k];
 		const int l = T.level[k];
 		const int shift = 63 - 3 * l;
@@ -362,6 +398,13 @@ __global__ void k_finish_nodes(const uint64_t* __restrict__ keys, uint32_t n, ui
 		const double w = dsub(hi, lo);
 		T.w2[k] = dmul(w, w);
 	}
+}
+
+__global__ void k_finish_nodes(const uint64_t* __restrict__ keys, uint32_t n, uint32_t L,
+                               const int8_t* __restrict__ lvl8, const uint32_t* __restrict__ base, TreeDev T,
+                               Params P, RunRec* rec)
+{
+	finish_nodes_body(GridSelf {}, keys, n, L, lvl8, base, T, P, rec);
 }
 
 // running |q|-weighted update of pot.c:1290-1310
@@ -675,23 +718,31 @@ __device__ __forceinline__ Mom5 mom_shfl(const Mom5& m, int src)
 	              __shfl_sync(0xffffffffu, m.z, src) };
 }
 
-template <int K>
-__global__ void __launch_bounds__(MOM_THREADS) k_mom_reduce(const double4* __restrict__ src64, uint32_t n, double c,
-                                                           Mom5* __restrict__ bsum)
+template <int K, class G>
+__device__ __forceinline__ void mom_reduce_body(G grd, const double4* __restrict__ src64, uint32_t n, double c,
+                                                Mom5* __restrict__ bsum)
 {
 	__shared__ Mom5 tot;
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)w * (MOM_ITEMS * 32);
+	const size_t base = (size_t)grd.id() * MOM_TILE + (size_t)w * (MOM_ITEMS * 32);
 	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
 	for (int k = 0; k < MOM_ITEMS; k++) {
 		const size_t i = base + (size_t)k * 32 + lane;
 		if (i < n) s = mom_add(s, mom_of<K>(src64[i], c));
 	}
 	mom_block_excl(s, &tot);
-	if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+	if (threadIdx.x == 0) bsum[grd.id()] = tot;
 }
 
-__global__ void __launch_bounds__(MOM_THREADS) k_mom_top(Mom5* __restrict__ bsum, uint32_t nb)
+template <int K>
+__global__ void __launch_bounds__(MOM_THREADS) k_mom_reduce(const double4* __restrict__ src64, uint32_t n, double c,
+                                                            Mom5* __restrict__ bsum)
+{
+	mom_reduce_body<K>(GridSelf {}, src64, n, c, bsum);
+}
+
+template <class G>
+__device__ __forceinline__ void mom_top_body(G grd, Mom5* __restrict__ bsum, uint32_t nb)
 {
 	__shared__ Mom5 tot;
 	__shared__ Mom5 carry;
@@ -709,13 +760,18 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_top(Mom5* __restrict__ bsum
 	}
 }
 
-template <int K>
-__global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restrict__ src64, uint32_t n, double c,
-                                                         const Mom5* __restrict__ bsum, Mom5* __restrict__ pre)
+__global__ void __launch_bounds__(MOM_THREADS) k_mom_top(Mom5* __restrict__ bsum, uint32_t nb)
+{
+	mom_top_body(GridSelf {}, bsum, nb);
+}
+
+template <int K, class G>
+__device__ __forceinline__ void mom_down_body(G grd, const double4* __restrict__ src64, uint32_t n, double c,
+                                              const Mom5* __restrict__ bsum, Mom5* __restrict__ pre)
 {
 	__shared__ Mom5 tot;
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-	const size_t base = (size_t)blockIdx.x * MOM_TILE + (size_t)w * (MOM_ITEMS * 32);
+	const size_t base = (size_t)grd.id() * MOM_TILE + (size_t)w * (MOM_ITEMS * 32);
 	// this warp's chunk total, then its offset among the block's warps
 	Mom5 s = Mom5 { 0, 0, 0, 0, 0 };
 	for (int k = 0; k < MOM_ITEMS; k++) {
@@ -731,7 +787,7 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restr
 		                        __shfl_xor_sync(0xffffffffu, wt.z, o) });
 	}
 	const Mom5 mine = lane == 0 ? wt : Mom5 { 0, 0, 0, 0, 0 };
-	Mom5 carry = mom_add(bsum[blockIdx.x], mom_block_excl(mine, &tot));  // valid on lane 0
+	Mom5 carry = mom_add(bsum[grd.id()], mom_block_excl(mine, &tot));  // valid on lane 0
 	carry = mom_shfl(carry, 0);
 	for (int k = 0; k < MOM_ITEMS; k++) {
 		const size_t i = base + (size_t)k * 32 + lane;
@@ -743,6 +799,13 @@ __global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restr
 		}
 		carry = mom_add(carry, mom_shfl(inc, 31));
 	}
+}
+
+template <int K>
+__global__ void __launch_bounds__(MOM_THREADS) k_mom_down(const double4* __restrict__ src64, uint32_t n, double c,
+                                                          const Mom5* __restrict__ bsum, Mom5* __restrict__ pre)
+{
+	mom_down_body<K>(GridSelf {}, src64, n, c, bsum, pre);
 }
 
 __device__ __forceinline__ Mom5 mom_range(const Mom5* __restrict__ pre, uint32_t a, uint32_t b)
@@ -759,13 +822,14 @@ __device__ __forceinline__ double3 dipole_of(const Mom5& pd, double q, double cx
 	return make_double3(pd.q - q * cx, pd.a - q * cy, pd.x - q * cz);
 }
 
-__global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, const Mom5* __restrict__ pre_d, Params P,
-                                 RunRec* rec)
+template <class G>
+__device__ __forceinline__ void moments_prefix_body(G grd, const TreeDev& T, const Mom5* __restrict__ pre,
+                                                    const Mom5* __restrict__ pre_d, const Params& P, RunRec* rec)
 {
 	const uint32_t M = rec->n_nodes;
 	if (M > T.cap) return;
 	const uint32_t L = P.leaf_size;
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+	for (uint32_t k = grd.id() * blockDim.x + threadIdx.x; k < M; k += grd.n() * blockDim.x) {
 		const Mom5 m = mom_range(pre, T.first[k], T.last[k] + 1);
 		const double inv = m.a > 0.0 ? 1.0 / m.a : 0.0;
 		const double cx = m.x * inv, cy = m.y * inv, cz = m.z * inv;  // relative to the centre
@@ -801,6 +865,12 @@ __global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, const 
 			}
 		}
 	}
+}
+
+__global__ void k_moments_prefix(TreeDev T, const Mom5* __restrict__ pre, const Mom5* __restrict__ pre_d, Params P,
+                                 RunRec* rec)
+{
+	moments_prefix_body(GridSelf {}, T, pre, pre_d, P, rec);
 }
 
 size_t mom_prefix_entries(size_t n) { return n + 1; }
@@ -873,6 +943,109 @@ void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const 
 			k_moments<<<blocks_for(n, 256), 256, 0, s>>>(T, src64, P, rec);
 		}
 	}
+}
+
+}  // namespace pot
+
+// ---------------------------------------------------------------------------
+// packed batch: the same kernels, one launch over every member
+// ---------------------------------------------------------------------------
+namespace pot {
+
+__global__ void kp_keys(PackDev B, int k)
+{
+	const SegBlock sb = seg_block(B.pre[PS_N256], B.M);
+	const MemberView& v = B.mv[sb.m];
+	keys_body(GridSeg { sb.id, sb.n }, v.pos[pack_in(v, k)], v.keys[0], v.vals[0], v.P, v.rec, 1);
+}
+
+__global__ void kp_reorder(PackDev B, int k)
+{
+	const SegBlock sb = seg_block(B.pre[PS_N256], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const uint32_t a = pack_in(v, k), b = pack_out(v, k);
+	reorder_body(GridSeg { sb.id, sb.n }, v.vals[v.kb], v.pos[a], v.vel[a], v.pid[a], v.pos[b], v.vel[b], v.pid[b],
+	             v.src64, v.src32, v.due, v.P, v.rec);
+}
+
+__global__ void kp_pairs(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_PAIRS], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const uint32_t n = v.P.n_tree, L = v.P.leaf_size;
+	pairs_body(GridSeg { sb.id, sb.n }, v.keys[v.kb], v.src64, n, n - L, L, (int)v.P.max_level, v.T.lvl8, v.T.cnt,
+	           v.rec);
+}
+
+__global__ void kp_fill_nodes(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_FILL], B.M);
+	const MemberView& v = B.mv[sb.m];
+	fill_nodes_body(GridSeg { sb.id, sb.n }, v.T.lvl8, v.T.base, v.P.n_tree - v.P.leaf_size, v.T, v.rec);
+}
+
+__global__ void kp_finish_nodes(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_FINISH], B.M);
+	const MemberView& v = B.mv[sb.m];
+	finish_nodes_body(GridSeg { sb.id, sb.n }, v.keys[v.kb], v.P.n_tree, v.P.leaf_size, v.T.lvl8, v.T.base, v.T,
+	                  v.P, v.rec);
+}
+
+__global__ void __launch_bounds__(MOM_THREADS) kp_mom_reduce(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_MOM], B.M);
+	const MemberView& v = B.mv[sb.m];
+	mom_reduce_body<0>(GridSeg { sb.id, sb.n }, v.src64, v.P.n_tree, v.P.rad, reinterpret_cast<Mom5*>(v.T.mom_blk));
+}
+
+__global__ void __launch_bounds__(MOM_THREADS) kp_mom_top(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_ONE], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const uint32_t nb = (v.P.n_tree + MOM_TILE - 1) / MOM_TILE;
+	mom_top_body(GridSeg { sb.id, sb.n }, reinterpret_cast<Mom5*>(v.T.mom_blk), nb);
+}
+
+__global__ void __launch_bounds__(MOM_THREADS) kp_mom_down(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_MOM], B.M);
+	const MemberView& v = B.mv[sb.m];
+	mom_down_body<0>(GridSeg { sb.id, sb.n }, v.src64, v.P.n_tree, v.P.rad, reinterpret_cast<Mom5*>(v.T.mom_blk),
+	                 reinterpret_cast<Mom5*>(v.T.mom_pre));
+}
+
+__global__ void kp_moments_prefix(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_MOMPRE], B.M);
+	const MemberView& v = B.mv[sb.m];
+	moments_prefix_body(GridSeg { sb.id, sb.n }, v.T, reinterpret_cast<const Mom5*>(v.T.mom_pre), nullptr, v.P,
+	                    v.rec);
+}
+
+static_assert(MOM_TILE == (int)PACK_MOM_TILE, "moment tile");
+
+void pack_keys(const PackDev& B, int k, cudaStream_t s)
+{
+	kp_keys<<<B.blocks[PS_N256], 256, 0, s>>>(B, k);
+}
+
+void pack_reorder(const PackDev& B, int k, cudaStream_t s)
+{
+	kp_reorder<<<B.blocks[PS_N256], 256, 0, s>>>(B, k);
+}
+
+// Octree and fast-form moments of every member (launch_build's sequence).
+void pack_build(const PackDev& B, cudaStream_t s)
+{
+	kp_pairs<<<B.blocks[PS_PAIRS], 256, 0, s>>>(B);
+	pack_node_scan(B, s);
+	kp_fill_nodes<<<B.blocks[PS_FILL], 256, 0, s>>>(B);
+	kp_finish_nodes<<<B.blocks[PS_FINISH], 256, 0, s>>>(B);
+	kp_mom_reduce<<<B.blocks[PS_MOM], MOM_THREADS, 0, s>>>(B);
+	kp_mom_top<<<B.blocks[PS_ONE], MOM_THREADS, 0, s>>>(B);
+	kp_mom_down<<<B.blocks[PS_MOM], MOM_THREADS, 0, s>>>(B);
+	kp_moments_prefix<<<B.blocks[PS_MOMPRE], 256, 0, s>>>(B);
 }
 
 }  // namespace pot

@@ -42,6 +42,88 @@ struct TreeDev {
 	float4* lfd;       // [8 * cap]
 };
 
+// One member run of a packed batch as the batched kernels see it: the
+// run's parameters, tree, record and device arrays (those of its context).
+// Buffer parity: at step k of a graph launch a member's state is in
+// pos[cur ^ (k & 1)]; kb is the key buffer holding the sorted keys (the
+// number of radix passes is the same for every member of a batch).
+struct MemberView {
+	Params P;
+	TreeDev T;
+	RunRec* rec;
+	StepHist* hist;
+	double4* pos[2];
+	double4* vel[2];
+	uint32_t* pid[2];
+	double4* src64;
+	float4* src32;
+	uint64_t* keys[2];
+	uint32_t* vals[2];
+	uint32_t* counts;      // radix-sort status words, histograms and tile counters
+	uint32_t* block_sums;  // scan block sums
+	uint8_t* due;
+	uint32_t* due_list;
+	uint32_t* due_prefix;
+	uint2* groups;
+	uint32_t* rein_list;
+	uint32_t cur;
+	uint32_t kb;
+	uint32_t tiles;        // radix-sort tiles
+	uint32_t pad;
+};
+
+// A packed batch's step: each kernel of the step is one launch over every
+// member (pot_batch.cu builds this).  pre[stage] is the exclusive prefix of
+// the members' block counts for that stage's kernels (device, M + 1
+// entries), blocks[stage] its total.  Stages:
+//   PS_N256    blocks_for(n, 256): keys, reorder
+//   PS_HIST    min(tiles, 1024): the sort's histogram
+//   PS_TILES   the sort's tiles: clearing the status words, each pass
+//   PS_CMP     scan tiles over n: the due list
+//   PS_PAIRS   blocks_for(n_tree - 1, 256)
+//   PS_NODES   scan tiles over the n_tree - L key pairs: cell numbering
+//   PS_FILL    blocks_for(n_tree - L, 256)
+//   PS_FINISH  blocks_for(n_tree, 256)
+//   PS_MOM     moment tiles over n_tree: prefix sums
+//   PS_MOMPRE  blocks_for(n_tree / 4 + 1, 256): cell moments from the sums
+//   PS_GROUPS  target groups
+//   PS_ONE     one block per member: digit offsets, scan tops, chi_b, grain
+//   PS_SMALL   a few blocks per member: late absorption, reinjection
+enum PackStage : int {
+	PS_N256, PS_HIST, PS_TILES, PS_CMP, PS_PAIRS, PS_NODES, PS_FILL, PS_FINISH, PS_MOM, PS_MOMPRE, PS_GROUPS,
+	PS_ONE, PS_SMALL, PS_COUNT
+};
+struct PackDev {
+	const MemberView* mv;           // [M], device
+	uint32_t M;
+	uint32_t npass;                 // radix passes, the same for every member
+	const uint32_t* pre[PS_COUNT];
+	uint32_t blocks[PS_COUNT];
+	uint32_t* gpre;                 // [M + 1] prefix of the members' target groups this step (device)
+	unsigned int* ctr;              // the batch walk's work counter (device)
+};
+// The member's state at step k of a graph launch is in buffer cur ^ (k & 1)
+// until the reorder, which writes the other buffer.
+__device__ __forceinline__ uint32_t pack_in(const MemberView& v, int k) { return v.cur ^ (uint32_t)(k & 1); }
+__device__ __forceinline__ uint32_t pack_out(const MemberView& v, int k) { return v.cur ^ (uint32_t)(k & 1) ^ 1u; }
+
+// the packed step's launches, in stream order (tree.cu, sort.cu, walk.cu,
+// walk_fast.cu, inject.cu)
+void pack_keys(const PackDev& B, int k, cudaStream_t s);
+void pack_sort(const PackDev& B, cudaStream_t s);
+void pack_reorder(const PackDev& B, int k, cudaStream_t s);
+void pack_build(const PackDev& B, cudaStream_t s);
+void pack_compact(const PackDev& B, cudaStream_t s);
+void pack_node_scan(const PackDev& B, cudaStream_t s);
+void pack_groups(const PackDev& B, cudaStream_t s);
+void pack_chi_b(const PackDev& B, cudaStream_t s);
+void pack_push(const PackDev& B, int k, uint32_t tpl, cudaStream_t s);
+void pack_absorb_late(const PackDev& B, int k, cudaStream_t s);
+void pack_reinject(const PackDev& B, int k, cudaStream_t s);
+void pack_grain_end(const PackDev& B, int k, cudaStream_t s);
+constexpr uint32_t PACK_MOM_TILE = 256 * 16;  // moment prefix-sum tile (tree.cu MOM_TILE)
+uint32_t pack_scan_blocks(uint32_t n);        // scan tiles over n items
+
 size_t mom_prefix_entries(size_t n);
 size_t mom_block_entries(size_t n);
 void launch_keys(const double4* pos, uint64_t* keys, uint32_t* vals, const Params& P, RunRec* rec,

@@ -312,15 +312,17 @@ __global__ void __launch_bounds__(128) k_push_plain(double4* __restrict__ pos, d
 // Steps where the grain itself moves (t a multiple of tss[DUST]): the
 // reference tests absorption against the grain's new position
 // (new_parts[0], pot.c:2641-2652), so the tests run after all pushes.
-__global__ void k_absorb_late(double4* __restrict__ pos, double4* __restrict__ vel,
-                              const double4* __restrict__ src64, const uint32_t* __restrict__ due_list,
-                              uint32_t* __restrict__ rein_list, Params P, RunRec* rec)
+template <class G>
+__device__ __forceinline__ void absorb_late_body(G grd, double4* __restrict__ pos, double4* __restrict__ vel,
+                                                 const double4* __restrict__ src64,
+                                                 const uint32_t* __restrict__ due_list,
+                                                 uint32_t* __restrict__ rein_list, const Params& P, RunRec* rec)
 {
 	if (rec->status != POT_OK || !rec->grain_due) return;
 	const uint32_t n_due = rec->n_due;
 	const bool absorb_on = !(P.flags & FLAG_NO_GRAIN) && rec->t_steps >= P.t_settle;
 	const double4 g = pos[rec->grain_slot];
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_due; i += gridDim.x * blockDim.x) {
+	for (uint32_t i = grd.id() * blockDim.x + threadIdx.x; i < n_due; i += grd.n() * blockDim.x) {
 		const uint32_t s = due_list[i];
 		const double4 p = pos[s];
 		double4 v = vel[s];
@@ -334,6 +336,13 @@ __global__ void k_absorb_late(double4* __restrict__ pos, double4* __restrict__ v
 		}
 		if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
 	}
+}
+
+__global__ void k_absorb_late(double4* __restrict__ pos, double4* __restrict__ vel, const double4* __restrict__ src64,
+                              const uint32_t* __restrict__ due_list, uint32_t* __restrict__ rein_list, Params P,
+                              RunRec* rec)
+{
+	absorb_late_body(GridSelf {}, pos, vel, src64, due_list, rein_list, P, rec);
 }
 
 // Poisson variate by inversion (prng.c:50-70): walk the CDF from k = 0 until
@@ -360,10 +369,11 @@ __device__ uint32_t poisson_inv(double lambda, double uni, bool& capped)
 }
 
 // Grain update of pot.c:2825-2848 and the step's statistics.
-__global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel, StepHist* hist, Params P,
-                            RunRec* rec, int epe)
+template <class G>
+__device__ __forceinline__ void grain_end_body(G grd, double4* __restrict__ pos, double4* __restrict__ vel,
+                                               StepHist* hist, const Params& P, RunRec* rec, int epe)
 {
-	if (threadIdx.x != 0 || blockIdx.x != 0) return;
+	if (threadIdx.x != 0 || grd.id() != 0) return;
 	const double dm = (double)rec->nabs_ion * P.m_ion + (double)rec->nabs_e * MASS_E;
 	const double m = rec->grain_m + dm;
 	double dp[3];
@@ -423,6 +433,12 @@ __global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel
 	h.pad = (int)rec->warn;
 	for (int k = 0; k < 3; k++) h.epe[k] = epe ? rec->epe[k] : 0.0;
 	hist[rec->t_steps % HIST] = h;
+}
+
+__global__ void k_grain_end(double4* __restrict__ pos, double4* __restrict__ vel, StepHist* hist, Params P,
+                            RunRec* rec, int epe)
+{
+	grain_end_body(GridSelf {}, pos, vel, hist, P, rec, epe);
 }
 
 // ---------------------------------------------------------------------------
@@ -523,8 +539,9 @@ __device__ __forceinline__ double spheroid_phi_at(const Params& P, const RunRec*
 // it (pot.c:2409-2418): rank k samples phi at azimuth 2 pi k / P in the x-y
 // plane through the grain, the samples are summed and divided by P; every 20
 // steps.  Four warps share the samples; the sum is taken in rank order.
-__global__ void __launch_bounds__(128) k_chi_b(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec,
-                                              int force)
+template <class G>
+__device__ __forceinline__ void chi_b_body(G grd, const TreeDev& T, const double4* __restrict__ src64,
+                                           const Params& P, RunRec* rec, int force)
 {
 	__shared__ int32_t stack[4][PHI_STACK];
 	__shared__ double sample[64];
@@ -557,6 +574,12 @@ __global__ void __launch_bounds__(128) k_chi_b(TreeDev T, const double4* __restr
 			rec->chi_b = sum / P.chi_ranks;
 		}
 	}
+}
+
+__global__ void __launch_bounds__(128) k_chi_b(TreeDev T, const double4* __restrict__ src64, Params P, RunRec* rec,
+                                               int force)
+{
+	chi_b_body(GridSelf {}, T, src64, P, rec, force);
 }
 
 __global__ void k_phi_query(TreeDev T, const double4* __restrict__ src64, const double* __restrict__ xyz,
@@ -689,6 +712,51 @@ void launch_phi_query(const TreeDev& T, const double4* src64, const double* xyz,
 	ScopedKernel k(tm, "phi_query");
 	const uint32_t nb = (nq + 3) / 4;
 	k_phi_query<<<nb < 4096 ? nb : 4096, 128, 0, s>>>(T, src64, xyz, nq, phi, P, rec);
+}
+
+}  // namespace pot
+
+// ---------------------------------------------------------------------------
+// packed batch: chi_b, late absorption and the grain update of every member
+// ---------------------------------------------------------------------------
+namespace pot {
+
+__global__ void __launch_bounds__(128) kp_chi_b(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_ONE], B.M);
+	const MemberView& v = B.mv[sb.m];
+	chi_b_body(GridSeg { sb.id, sb.n }, v.T, v.src64, v.P, v.rec, 0);
+}
+
+__global__ void kp_absorb_late(PackDev B, int k)
+{
+	const SegBlock sb = seg_block(B.pre[PS_SMALL], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const uint32_t b = pack_out(v, k);
+	absorb_late_body(GridSeg { sb.id, sb.n }, v.pos[b], v.vel[b], v.src64, v.due_list, v.rein_list, v.P, v.rec);
+}
+
+__global__ void kp_grain_end(PackDev B, int k)
+{
+	const SegBlock sb = seg_block(B.pre[PS_ONE], B.M);
+	const MemberView& v = B.mv[sb.m];
+	const uint32_t b = pack_out(v, k);
+	grain_end_body(GridSeg { sb.id, sb.n }, v.pos[b], v.vel[b], v.hist, v.P, v.rec, 0);
+}
+
+void pack_chi_b(const PackDev& B, cudaStream_t s)
+{
+	kp_chi_b<<<B.blocks[PS_ONE], 128, 0, s>>>(B);
+}
+
+void pack_absorb_late(const PackDev& B, int k, cudaStream_t s)
+{
+	kp_absorb_late<<<B.blocks[PS_SMALL], 256, 0, s>>>(B, k);
+}
+
+void pack_grain_end(const PackDev& B, int k, cudaStream_t s)
+{
+	kp_grain_end<<<B.blocks[PS_ONE], 32, 0, s>>>(B, k);
 }
 
 }  // namespace pot

@@ -649,12 +649,14 @@ __device__ __forceinline__ uint32_t dpre_at(const uint32_t* __restrict__ dpre, u
 	return dpre ? dpre[s] : s;
 }
 
-__global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __restrict__ groups,
-                         unsigned int* ctr, uint32_t gmax, Params P, RunRec* rec)
+template <class G>
+__device__ __forceinline__ void groups_body(G grd, const TreeDev& T, const uint32_t* __restrict__ dpre,
+                                            uint2* __restrict__ groups, unsigned int* ctr, uint32_t gmax,
+                                            const Params& P, RunRec* rec)
 {
 	if (rec->status != POT_OK) return;
 	const uint32_t M = rec->n_nodes;
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+	for (uint32_t k = grd.id() * blockDim.x + threadIdx.x; k < M; k += grd.n() * blockDim.x) {
 		const uint32_t a = T.first[k], b = T.last[k] + 1;
 		const uint32_t d = dpre_at(dpre, b) - dpre_at(dpre, a);
 		if (d == 0) continue;
@@ -685,130 +687,160 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 		emit_groups(ctr, groups, run_start, run, gmax);
 	}
 	// slots after the tree's (a spheroidal grain) are a group of their own
-	if (blockIdx.x == 0 && threadIdx.x == 0 && P.n_tree < P.n) {
+	if (grd.id() == 0 && threadIdx.x == 0 && P.n_tree < P.n) {
 		const uint32_t a = dpre_at(dpre, P.n_tree), b = dpre_at(dpre, P.n);
 		if (b > a) emit_groups(ctr, groups, a, b - a, gmax);
 	}
 }
 
-// STG as in k_push_plain: 0 the Boris step; 1 and 2 the two halves of the
-// non-Boris integrators (stage 2 walks over the intermediate sources).
-template <int TPL, int STG, bool DIP = false>
-__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel,
-                                                            TreeDev T, const float4* __restrict__ src32,
-                                                            const uint32_t* __restrict__ due_list,
-                                                            const uint2* __restrict__ groups,
-                                                            uint32_t* __restrict__ rein_list, Params P,
-                                                            RunRec* rec, const double4* __restrict__ src64,
-                                                            StageBufs sb)
+__global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __restrict__ groups, unsigned int* ctr,
+                         uint32_t gmax, Params P, RunRec* rec)
 {
-	__shared__ FastSmem<TPL, DIP> smem[FW_WARPS];
-	FastSmem<TPL, DIP>& sm = smem[threadIdx.x >> 5];
-	if (rec->status != POT_OK) return;
-	const uint32_t n_groups = rec->n_groups;
+	groups_body(GridSelf {}, T, dpre, groups, ctr, gmax, P, rec);
+}
+
+// The point where a target's field is evaluated: for the Boris step the
+// position drifted half a step, x + (dt tss / 2) v (pot.c:2478-2485); for
+// the stages of the other integrators the position itself.
+template <int STG>
+__device__ __forceinline__ double3 eval_point(const double4 p, const double4* __restrict__ vel, uint32_t s,
+                                              const Params& P)
+{
+	if (STG == 0) {
+		const double4 v = vel[s];
+		const double half = 0.5 * (P.dt * (double)P.tss[(int)p.w]);
+		return make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
+	}
+	return make_double3(p.x, p.y, p.z);
+}
+
+// Per-launch state of one run's push: the grain (its position for the
+// absorption test, its charge) and the scale of the walk's FP32 sums.
+struct PushCtx {
+	const float4* srcf;
+	double gx, gy, gz, qg, escale;
+	bool grain_due, absorb_on;
+};
+
+template <int STG>
+__device__ __forceinline__ PushCtx push_ctx(const double4* __restrict__ pos, const float4* __restrict__ src32,
+                                            const Params& P, const RunRec* rec, const StageBufs& sb)
+{
+	PushCtx c;
 	const unsigned long long t_step = rec->t_steps;
-	const bool grain_due = rec->grain_due != 0;
-	const bool absorb_on = !(P.flags & FLAG_NO_GRAIN) && t_step >= P.t_settle;
-	double gx = rec->grain_pos[0], gy = rec->grain_pos[1], gz = rec->grain_pos[2];
-	if (STG == 2 && grain_due && rec->grain_slot < P.n) {
+	c.grain_due = rec->grain_due != 0;
+	c.absorb_on = !(P.flags & FLAG_NO_GRAIN) && t_step >= P.t_settle;
+	c.gx = rec->grain_pos[0];
+	c.gy = rec->grain_pos[1];
+	c.gz = rec->grain_pos[2];
+	if (STG == 2 && c.grain_due && rec->grain_slot < P.n) {
 		const double4 gp = pos[rec->grain_slot];  // the grain's intermediate position
-		gx = gp.x; gy = gp.y; gz = gp.z;
+		c.gx = gp.x; c.gy = gp.y; c.gz = gp.z;
 	}
-	const float4* __restrict__ srcf = STG == 2 ? sb.src32b : src32;
-	const double qg = (double)rec->grain_q;
-	const double escale = QE / (P.k4 * P.rad * P.rad);
-	unsigned long long n_inter = 0, n_push = 0;
-	uint32_t stack_max = 0;
-	for (;;) {
-		uint32_t g = 0;
-		if (lane_f() == 0) g = atomicAdd(&rec->work_ctr, 1u);
-		g = __shfl_sync(0xffffffffu, g, 0);
-		if (g >= n_groups) break;
-		const uint2 grp = groups[g];
-		Targets<TPL> tg;
-		uint32_t slot[TPL];
-		double3 h[TPL];
-		// small groups split the warp (see group_walk): lanes past the
-		// first 32 / split hold copies of members and push nothing
-		const int split = TPL == 1 ? (grp.y <= 8 ? 4 : (grp.y <= 16 ? 2 : 1)) : 1;
-		const uint32_t width = 32u / (uint32_t)split;
-		const bool owner = lane_f() < width;
+	c.srcf = STG == 2 ? sb.src32b : src32;
+	c.qg = (double)rec->grain_q;
+	c.escale = QE / (P.k4 * P.rad * P.rad);
+	return c;
+}
+
+// One target group grp = (first entry of the due list, count): the warp's
+// walk for the whole group, then each member's push, absorption and boundary
+// test.  Adds to the lane's interaction and push counts and the deepest
+// stack; returns the walk's status (a member that fails leaves the group's
+// pushes undone).
+template <int TPL, int STG, bool DIP>
+__device__ __forceinline__ int push_group(uint2 grp, double4* __restrict__ pos, double4* __restrict__ vel,
+                                          const TreeDev& T, const float4* __restrict__ src32,
+                                          const uint32_t* __restrict__ due_list, uint32_t* __restrict__ rein_list,
+                                          const Params& P, RunRec* rec, const double4* __restrict__ src64,
+                                          const StageBufs& sb, const PushCtx& pc, FastSmem<TPL, DIP>& sm,
+                                          unsigned long long& n_inter, unsigned long long& n_push,
+                                          uint32_t& stack_max)
+{
+	Targets<TPL> tg;
+	uint32_t slot[TPL];
+	// small groups split the warp (see group_walk): lanes past the
+	// first 32 / split hold copies of members and push nothing
+	const int split = TPL == 1 ? (grp.y <= 8 ? 4 : (grp.y <= 16 ? 2 : 1)) : 1;
+	const uint32_t width = 32u / (uint32_t)split;
+	const bool owner = lane_f() < width;
+	// the FP64 evaluation point (half-drifted for the Boris step) is
+	// recomputed after the walk from the same state with the same
+	// operations, so it is not held in registers through the walk
 #pragma unroll
-		for (int k = 0; k < TPL; k++) {
-			const uint32_t m = (lane_f() & (width - 1u)) + 32u * k;
-			tg.valid[k] = m < grp.y;
-			slot[k] = 0xFFFFFFFFu;
-			h[k] = make_double3(P.rad, P.rad, P.rad);
-			if (tg.valid[k]) {
-				slot[k] = due_list[grp.x + m];
-				const double4 p = pos[slot[k]];
-				if (STG == 0) {
-					const double4 v = vel[slot[k]];
-					const double half = 0.5 * (P.dt * (double)P.tss[(int)p.w]);
-					h[k] = make_double3(fma(half, v.x, p.x), fma(half, v.y, p.y), fma(half, v.z, p.z));
-				} else {
-					h[k] = make_double3(p.x, p.y, p.z);
-				}
-			}
-			tg.self[k] = slot[k];
-			tg.t[k] = make_float3((float)((h[k].x - P.rad) * P.inv_rad), (float)((h[k].y - P.rad) * P.inv_rad),
-			                      (float)((h[k].z - P.rad) * P.inv_rad));
+	for (int k = 0; k < TPL; k++) {
+		const uint32_t m = (lane_f() & (width - 1u)) + 32u * k;
+		tg.valid[k] = m < grp.y;
+		slot[k] = 0xFFFFFFFFu;
+		double3 h = make_double3(P.rad, P.rad, P.rad);
+		if (tg.valid[k]) {
+			slot[k] = due_list[grp.x + m];
+			h = eval_point<STG>(pos[slot[k]], vel, slot[k], P);
 		}
-		uint32_t ne = 0, depth = 0;
-		int err = POT_OK;
-		const Field<TPL> ef = group_walk<TPL, false, DIP>(tg, T, srcf, P, sm, ne, depth, err, split);
-		stack_max = max(stack_max, depth);
-		if (err != POT_OK) {
-			if (lane_f() == 0) set_status(rec, err);
-			break;
-		}
+		tg.self[k] = slot[k];
+		tg.t[k] = make_float3((float)((h.x - P.rad) * P.inv_rad), (float)((h.y - P.rad) * P.inv_rad),
+		                      (float)((h.z - P.rad) * P.inv_rad));
+	}
+	uint32_t ne = 0, depth = 0;
+	int err = POT_OK;
+	const Field<TPL> ef = group_walk<TPL, false, DIP>(tg, T, pc.srcf, P, sm, ne, depth, err, split);
+	stack_max = max(stack_max, depth);
+	if (err != POT_OK) return err;
 #pragma unroll
-		for (int k = 0; k < TPL; k++) {
-			if (!tg.valid[k] || !owner) continue;
-			const uint32_t s = slot[k];
-			const double4 p = pos[s];
-			double4 v = vel[s];
-			const int sp = (int)p.w;
-			const double dt = P.dt * (double)P.tss[sp];
-			n_inter += ne;
-			if (STG != 1) n_push++;
-			double E[3] = { (double)ef.x[k] * escale, (double)ef.y[k] * escale, (double)ef.z[k] * escale };
-			if (P.shape && sp != SP_DUST) {
-				// the spheroid's own field in FP64 (pot-spheroid.c:1815-1819)
-				double Eg[3];
-				spheroid_field(P, qg, dsub(h[k].x, gx), dsub(h[k].y, gy), dsub(h[k].z, gz), Eg);
-				E[0] += Eg[0];
-				E[1] += Eg[1];
-				E[2] += Eg[2];
-			}
-			const double charge = sp == SP_DUST ? qg : (sp == SP_ION ? 1.0 : -1.0);
-			const double qom = (QE * charge) / mass_of(sp, P);
-			if (STG == 1) {
-				const double3 a1 = accel_lorentz(E, v, qom, P);
-				double4 pm = p;
-				half_first(pm, v, a1, dt, P);
-				pos[s] = pm;
-				vel[s] = v;
-				sb.acc[s] = make_double4(a1.x, a1.y, a1.z, 0.0);
-				sb.src32b[s] = make_float4((float)((pm.x - P.rad) * P.inv_rad), (float)((pm.y - P.rad) * P.inv_rad),
-				                           (float)((pm.z - P.rad) * P.inv_rad), src32[s].w);
-				sb.src64b[s] = make_double4(pm.x, pm.y, pm.z, src64[s].w);
-				continue;
-			}
-			double3 xn;
-			if (STG == 0) {
-				boris(v, h[k], E, qom, dt, P, xn);
-			} else {
-				const double4 a = sb.acc[s];
-				half_second(xn, v, p, make_double3(a.x, a.y, a.z), accel_lorentz(E, v, qom, P), dt, P);
-			}
-			uint32_t reason = 0;
-			if (!grain_due) reason = after_push(sp, STG == 0 ? p : src64[s], xn, v, P, rec, absorb_on, gx, gy, gz);
-			pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
+	for (int k = 0; k < TPL; k++) {
+		if (!tg.valid[k] || !owner) continue;
+		const uint32_t s = slot[k];
+		const double4 p = pos[s];
+		double4 v = vel[s];
+		const int sp = (int)p.w;
+		const double dt = P.dt * (double)P.tss[sp];
+		const double3 hk = eval_point<STG>(p, vel, s, P);
+		n_inter += ne;
+		if (STG != 1) n_push++;
+		double E[3] = { (double)ef.x[k] * pc.escale, (double)ef.y[k] * pc.escale, (double)ef.z[k] * pc.escale };
+		if (P.shape && sp != SP_DUST) {
+			// the spheroid's own field in FP64 (pot-spheroid.c:1815-1819)
+			double Eg[3];
+			spheroid_field(P, pc.qg, dsub(hk.x, pc.gx), dsub(hk.y, pc.gy), dsub(hk.z, pc.gz), Eg);
+			E[0] += Eg[0];
+			E[1] += Eg[1];
+			E[2] += Eg[2];
+		}
+		const double charge = sp == SP_DUST ? pc.qg : (sp == SP_ION ? 1.0 : -1.0);
+		const double qom = (QE * charge) / mass_of(sp, P);
+		if (STG == 1) {
+			const double3 a1 = accel_lorentz(E, v, qom, P);
+			double4 pm = p;
+			half_first(pm, v, a1, dt, P);
+			pos[s] = pm;
 			vel[s] = v;
-			if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
+			sb.acc[s] = make_double4(a1.x, a1.y, a1.z, 0.0);
+			sb.src32b[s] = make_float4((float)((pm.x - P.rad) * P.inv_rad), (float)((pm.y - P.rad) * P.inv_rad),
+			                           (float)((pm.z - P.rad) * P.inv_rad), src32[s].w);
+			sb.src64b[s] = make_double4(pm.x, pm.y, pm.z, src64[s].w);
+			continue;
 		}
+		double3 xn;
+		if (STG == 0) {
+			boris(v, hk, E, qom, dt, P, xn);
+		} else {
+			const double4 a = sb.acc[s];
+			half_second(xn, v, p, make_double3(a.x, a.y, a.z), accel_lorentz(E, v, qom, P), dt, P);
+		}
+		uint32_t reason = 0;
+		if (!pc.grain_due)
+			reason = after_push(sp, STG == 0 ? p : src64[s], xn, v, P, rec, pc.absorb_on, pc.gx, pc.gy, pc.gz);
+		pos[s] = make_double4(xn.x, xn.y, xn.z, p.w);
+		vel[s] = v;
+		if (reason) rein_list[atomicAdd(&rec->n_rein, 1u)] = s | (reason << 30);
 	}
+	return POT_OK;
+}
+
+// The lanes' interaction and push counts and deepest stack into the run record.
+__device__ __forceinline__ void push_stats(RunRec* rec, unsigned long long n_inter, unsigned long long n_push,
+                                           uint32_t stack_max)
+{
 	unsigned long long a = n_inter, b = n_push;
 #pragma unroll
 	for (int o = 16; o; o >>= 1) {
@@ -820,6 +852,38 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) k_push_fast(d
 		if (b) atomicAdd(&rec->n_pushed, b);
 		if (stack_max) atomicMax(&rec->stack_max, stack_max);
 	}
+}
+
+// STG as in k_push_plain: 0 the Boris step; 1 and 2 the two halves of the
+// non-Boris integrators (stage 2 walks over the intermediate sources).
+// Persistent: each warp takes the next group from the run's work counter.
+template <int TPL, int STG, bool DIP = false>
+__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 5)
+k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T, const float4* __restrict__ src32,
+            const uint32_t* __restrict__ due_list, const uint2* __restrict__ groups, uint32_t* __restrict__ rein_list,
+            Params P, RunRec* rec, const double4* __restrict__ src64, StageBufs sb)
+{
+	__shared__ FastSmem<TPL, DIP> smem[FW_WARPS];
+	FastSmem<TPL, DIP>& sm = smem[threadIdx.x >> 5];
+	// warp-uniform: another warp may set the status meanwhile
+	if (__shfl_sync(0xffffffffu, lane_f() == 0 ? rec->status : 0, 0) != POT_OK) return;
+	const uint32_t n_groups = rec->n_groups;
+	const PushCtx pc = push_ctx<STG>(pos, src32, P, rec, sb);
+	unsigned long long n_inter = 0, n_push = 0;
+	uint32_t stack_max = 0;
+	for (;;) {
+		uint32_t g = 0;
+		if (lane_f() == 0) g = atomicAdd(&rec->work_ctr, 1u);
+		g = __shfl_sync(0xffffffffu, g, 0);
+		if (g >= n_groups) break;
+		const int err = push_group<TPL, STG, DIP>(groups[g], pos, vel, T, src32, due_list, rein_list, P, rec, src64,
+		                                          sb, pc, sm, n_inter, n_push, stack_max);
+		if (err != POT_OK) {
+			if (lane_f() == 0) set_status(rec, err);
+			break;
+		}
+	}
+	push_stats(rec, n_inter, n_push, stack_max);
 }
 
 template <int TPL, bool DIP = false>
@@ -903,7 +967,8 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_epe_fast(const double4* __res
 {
 	__shared__ FastSmem<TPL, DIP> smem[FW_WARPS];
 	FastSmem<TPL, DIP>& sm = smem[threadIdx.x >> 5];
-	if (rec->status != POT_OK) return;
+	// warp-uniform: another warp may set the status meanwhile
+	if (__shfl_sync(0xffffffffu, lane_f() == 0 ? rec->status : 0, 0) != POT_OK) return;
 	const uint32_t n_groups = rec->n_groups_all;
 	const uint32_t gs = rec->grain_slot;
 	const double pscale = QE / (P.k4 * P.rad);
@@ -1028,6 +1093,115 @@ void launch_field_query_fast(const TreeDev& T, const float4* src32, const double
 		else
 			k_field_query_fast<1><<<nb, FW_WARPS * 32, 0, s>>>(T, src32, xyz, self_slot, nq, E, P, rec);
 	}
+}
+
+}  // namespace pot
+
+// ---------------------------------------------------------------------------
+// packed batch: target groups and the walk of every member in one launch
+// ---------------------------------------------------------------------------
+namespace pot {
+
+__global__ void kp_groups(PackDev B)
+{
+	const SegBlock sb = seg_block(B.pre[PS_GROUPS], B.M);
+	const MemberView& v = B.mv[sb.m];
+	groups_body(GridSeg { sb.id, sb.n }, v.T, v.due_prefix, v.groups, &v.rec->n_groups, v.P.group_max, v.P, v.rec);
+}
+
+// gpre[m] = target groups of members 0..m-1 (a member whose status is set
+// contributes none); the walk's work counter is reset.  One block.
+__global__ void __launch_bounds__(1024) kp_group_prefix(PackDev B)
+{
+	__shared__ uint32_t carry;
+	if (threadIdx.x == 0) {
+		carry = 0;
+		*B.ctr = 0u;
+	}
+	__syncthreads();
+	for (uint32_t base = 0; base < B.M; base += blockDim.x) {
+		const uint32_t m = base + threadIdx.x;
+		uint32_t c = 0;
+		if (m < B.M) {
+			const RunRec* r = B.mv[m].rec;
+			c = r->status == POT_OK ? r->n_groups : 0u;
+		}
+		// block-wide inclusive scan of c, warp by warp
+		__shared__ uint32_t wsum[32];
+		uint32_t x = c;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+			if ((threadIdx.x & 31) >= (unsigned)o) x += t;
+		}
+		if ((threadIdx.x & 31) == 31) wsum[threadIdx.x >> 5] = x;
+		__syncthreads();
+		if (threadIdx.x < 32) {
+			uint32_t y = threadIdx.x < (blockDim.x >> 5) ? wsum[threadIdx.x] : 0u;
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const uint32_t t = __shfl_up_sync(0xffffffffu, y, o);
+				if (threadIdx.x >= (unsigned)o) y += t;
+			}
+			wsum[threadIdx.x] = y;
+		}
+		__syncthreads();
+		const uint32_t incl = x + ((threadIdx.x >> 5) ? wsum[(threadIdx.x >> 5) - 1] : 0u) + carry;
+		if (m < B.M) B.gpre[m] = incl - c;
+		__syncthreads();
+		if (threadIdx.x == blockDim.x - 1) carry = incl;
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) B.gpre[B.M] = carry;
+}
+
+// The walk and push of every member's groups: each warp takes the next
+// group of the whole batch, finds its member in gpre and runs it with that
+// member's tree, state and record; counts go to the member's record.
+template <int TPL>
+__global__ void __launch_bounds__(FW_WARPS * 32, 5) kp_push_fast(PackDev B, int k)
+{
+	__shared__ FastSmem<TPL, false> smem[FW_WARPS];
+	FastSmem<TPL, false>& sm = smem[threadIdx.x >> 5];
+	const uint32_t total = B.gpre[B.M];
+	const StageBufs sb { 0, nullptr, nullptr, nullptr };
+	for (;;) {
+		uint32_t g = 0;
+		if (lane_f() == 0) g = atomicAdd(B.ctr, 1u);
+		g = __shfl_sync(0xffffffffu, g, 0);
+		if (g >= total) break;
+		uint32_t lo = 0, hi = B.M;  // gpre[lo] <= g < gpre[hi]
+		while (hi - lo > 1) {
+			const uint32_t mid = (lo + hi) >> 1;
+			if (B.gpre[mid] <= g) lo = mid; else hi = mid;
+		}
+		const MemberView& v = B.mv[lo];
+		RunRec* rec = v.rec;
+		// warp-uniform: another warp may set the status meanwhile
+		if (__shfl_sync(0xffffffffu, lane_f() == 0 ? rec->status : 0, 0) != POT_OK) continue;
+		const uint32_t b = pack_out(v, k);
+		const PushCtx pc = push_ctx<0>(v.pos[b], v.src32, v.P, rec, sb);
+		unsigned long long n_inter = 0, n_push = 0;
+		uint32_t stack_max = 0;
+		const int err = push_group<TPL, 0, false>(v.groups[g - B.gpre[lo]], v.pos[b], v.vel[b], v.T, v.src32,
+		                                          v.due_list, v.rein_list, v.P, rec, v.src64, sb, pc, sm, n_inter,
+		                                          n_push, stack_max);
+		if (err != POT_OK && lane_f() == 0) set_status(rec, err);
+		push_stats(rec, n_inter, n_push, stack_max);
+	}
+}
+
+void pack_groups(const PackDev& B, cudaStream_t s)
+{
+	kp_groups<<<B.blocks[PS_GROUPS], 256, 0, s>>>(B);
+	kp_group_prefix<<<1, 1024, 0, s>>>(B);
+}
+
+void pack_push(const PackDev& B, int k, uint32_t tpl, cudaStream_t s)
+{
+	const int nb = sm_count_fast() * 5;
+	if (tpl == 2) kp_push_fast<2><<<nb, FW_WARPS * 32, 0, s>>>(B, k);
+	else kp_push_fast<1><<<nb, FW_WARPS * 32, 0, s>>>(B, k);
 }
 
 }  // namespace pot

@@ -41,6 +41,9 @@ STEP_EPE = 0x1
 CFG_SCEPTIC, CFG_DISABLE_GRAIN, CFG_DIPOLES, CFG_POIS_IONS = 0x1, 0x2, 0x4, 0x8
 INT_BORIS, INT_VERLET, INT_EULER_RICHARDSON = 0, 1, 2
 OPT_TIMING = 0x1
+OPT_CHI_CAP = 0x2
+WARN_CHI_CAP = 512
+BATCH_NO_PACK = 0x1
 
 
 class PotError(RuntimeError):
@@ -167,7 +170,8 @@ class _MacroSums(C.Structure):
 
 
 class _BatchOpts(C.Structure):
-    _fields_ = [("device", C.c_int32), ("steps_per_launch", C.c_uint32), ("reserve_bytes", C.c_uint64)]
+    _fields_ = [("device", C.c_int32), ("steps_per_launch", C.c_uint32), ("reserve_bytes", C.c_uint64),
+                ("flags", C.c_uint32), ("pad", C.c_uint32)]
 
 
 BATCH_ROW_DTYPE = np.dtype([("slot", "<i4"), ("status", "<i4"), ("t_steps", "<u8"), ("grain_q", "<i8"),
@@ -251,14 +255,14 @@ class Run:
 
     def __init__(self, cfg: RunConfig, form: str = "plain", leaf_size: int = 0, group_size: int = 0,
                  seed: int = 1, device: int = 0, stream: Optional[int] = None, timing: bool = False,
-                 chi_b_ranks: int = 0):
+                 chi_b_ranks: int = 0, chi_cap: bool = False):
         self.lib = load_library()
         self.cfg = cfg
         o = _Opts()
         o.form = FORM_PLAIN if form == "plain" else FORM_FAST
         o.leaf_size = int(leaf_size)
         o.group_size = int(group_size)
-        o.flags = OPT_TIMING if timing else 0
+        o.flags = (OPT_TIMING if timing else 0) | (OPT_CHI_CAP if chi_cap else 0)
         o.device = int(device)
         o.seed = int(seed) & ((1 << 64) - 1)
         o.stream = stream
@@ -303,7 +307,11 @@ class Run:
     def step(self, n: int = 1, epe: bool = False) -> dict:
         """Run n steps; epe=True also computes the potential energies."""
         st = _Stats()
-        self._check(self.lib.pot_gpu_step(self.h, int(n), STEP_EPE if epe else 0, C.byref(st)), "pot_gpu_step")
+        rc = self.lib.pot_gpu_step(self.h, int(n), STEP_EPE if epe else 0, C.byref(st))
+        if rc != POT_OK:
+            e = PotError(rc, "pot_gpu_step", self.lib.pot_gpu_strerror(rc).decode())
+            e.stats = _stats_dict(st)  # the run record at the failure (the library fills it)
+            raise e
         return _stats_dict(st)
 
     def step_async(self, n: int = 1, epe: bool = False):
@@ -420,8 +428,9 @@ class Run:
         self._check(self.lib.pot_gpu_sync(self.h), "pot_gpu_sync")
 
 
-def _opts(form="fast", leaf_size=0, group_size=0, seed=1, device=0) -> _Opts:
+def _opts(form="fast", leaf_size=0, group_size=0, seed=1, device=0, chi_cap=False) -> _Opts:
     o = _Opts()
+    o.flags = OPT_CHI_CAP if chi_cap else 0
     o.form = FORM_PLAIN if form == "plain" else FORM_FAST
     o.leaf_size = int(leaf_size)
     o.group_size = int(group_size)
@@ -456,10 +465,11 @@ class Batch:
     """Many independent runs stepped by one CUDA-graph launch
     (``pot_batch``)."""
 
-    def __init__(self, device: int = 0, steps_per_launch: int = 2, reserve_bytes: int = 0):
+    def __init__(self, device: int = 0, steps_per_launch: int = 2, reserve_bytes: int = 0, pack: bool = True):
         self.lib = load_library()
         o = _BatchOpts()
         o.device, o.steps_per_launch, o.reserve_bytes = int(device), int(steps_per_launch), int(reserve_bytes)
+        o.flags = 0 if pack else BATCH_NO_PACK
         self.h = C.c_void_p()
         self.cfgs = {}
         self._check(self.lib.pot_batch_create(C.byref(o), C.byref(self.h)), "pot_batch_create")
@@ -486,9 +496,10 @@ class Batch:
     def __exit__(self, *a):
         self.close()
 
-    def admit(self, cfg: RunConfig, form="fast", leaf_size=0, group_size=0, seed=1, parts=None, grain=None) -> int:
+    def admit(self, cfg: RunConfig, form="fast", leaf_size=0, group_size=0, seed=1, parts=None, grain=None,
+              chi_cap=False) -> int:
         slot = C.c_int32(-1)
-        o = _opts(form, leaf_size, group_size, seed)
+        o = _opts(form, leaf_size, group_size, seed, chi_cap=chi_cap)
         pp = None
         if parts is not None:
             parts = np.ascontiguousarray(parts, dtype=PARTICLE_DTYPE)

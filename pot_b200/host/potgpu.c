@@ -88,6 +88,7 @@ typedef struct {
 	uint64_t seed;
 	bool have_seed;
 	bool host_macro;  /* summary sums from downloaded particles instead of on the device */
+	bool phi_start;   /* pot-phi.dat rows for the starting state as well */
 	char out_dir[4096];
 } Run;
 
@@ -163,6 +164,7 @@ static void usage(const char* prog)
 	e_puts("GPU execution:");
 	e_puts("  --form fast|plain  --leaf N  --group 8|16|32|64  --seed S  --axis X,Y,Z  --output-dir DIR");
 	e_puts("  --host-macro  compute the summary from downloaded particles (default: on the device)");
+	e_puts("  --phi-start   also write pot-phi.dat rows for the starting (or resumed) state");
 }
 
 static int want(int* n, int argc) { return ++(*n) < argc; }
@@ -185,6 +187,7 @@ static int parse_args(int argc, char** argv, Run* ru)
 			if (!strcmp(f, "--no-sceptic")) { ru->sceptic = false; continue; }
 			if (!strcmp(f, "--disable-grain")) { ru->disable_grain = true; continue; }
 			if (!strcmp(f, "--host-macro")) { ru->host_macro = true; continue; }
+			if (!strcmp(f, "--phi-start")) { ru->phi_start = true; continue; }
 			if (!strcmp(f, "--dipoles")) { ru->dipoles = true; continue; }
 			if (!strcmp(f, "--pois-ions")) { ru->pois_ions = true; continue; }
 			if (!want(&n, argc)) return 1;
@@ -941,6 +944,18 @@ int main(int argc, char** argv)
 		free(P);
 		free(ru.sw_path);
 		return EXIT_FAILURE;
+	}
+	if (ru.phi_start) {
+		/* the potential profile of the starting state (write_phi_data_to_file
+		   as pot.c:4397-4403 calls it, at the resumed step) over its own tree */
+		if ((rc = pot_gpu_build_tree(ctx, NULL)) != POT_OK || (rc = pot_gpu_download(ctx, P, &g)) != POT_OK ||
+		    (rc = write_phi(&ru, ctx, &g, g.t_steps)) != POT_OK) {
+			fail(ctx, g.t_steps, rc);
+			pot_gpu_destroy(ctx);
+			free(P);
+			free(ru.sw_path);
+			return EXIT_FAILURE;
+		}
 	}
 	FILE* fp_macro = NULL;
 	if (ru.N >= 6) {

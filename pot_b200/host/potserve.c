@@ -28,7 +28,13 @@
  * charge, aggregate particle-steps/s, queue depth, and (with
  * --plain-sample K) the first K jobs run one at a time in the plain FP64
  * form for comparison.  --tune picks leaf and group sizes per size class
- * with the library's autotuner.
+ * with the library's autotuner.  The batch packs its fast-form runs (one
+ * launch per kernel of the step over all of them); --no-pack steps each run
+ * as its own kernel sequence instead, for comparison.  Jobs run with
+ * POT_OPT_CHI_CAP (the sampler's edge potential capped where the
+ * reference's inverse CDF is undefined, so a cold-ion job with a noisy edge
+ * potential goes on instead of stopping with POT_E_ITER); --strict-sampler
+ * runs them as the reference would, stopping such jobs.
  */
 #define _POSIX_C_SOURCE 200809L
 #include <math.h>
@@ -178,7 +184,7 @@ int main(int argc, char** argv)
 	double nmin = 16000, nmax = 256000, rate = 20.0, duration = 600.0, bmax = 0.0, reserve_gb = 8.0;
 	uint64_t max_steps = 20000, seed0 = 1000, gen_seed = 12345;
 	uint32_t epoch = 50;
-	bool tune = false;
+	bool tune = false, pack = true, chi_cap = true;
 	for (int k = 1; k < argc; k++) {
 		const char* f = argv[k];
 		const char* v = k + 1 < argc ? argv[k + 1] : "";
@@ -198,10 +204,14 @@ int main(int argc, char** argv)
 		else if (!strcmp(f, "--plain-sample")) { plain_sample = atoi(v); k++; }
 		else if (!strcmp(f, "--device")) { device = atoi(v); k++; }
 		else if (!strcmp(f, "--tune")) { tune = true; }
+		else if (!strcmp(f, "--no-pack")) { pack = false; }
+		else if (!strcmp(f, "--strict-sampler")) { chi_cap = false; }
 		else {
 			fprintf(stderr, "usage: %s [--mode sweep|serve] [--runs N] [--nmin N] [--nmax N] [--rate R] "
 			                "[--duration S] [--bmax T] [--max-steps N] [--max-runs N] [--epoch N] [--seed S] "
-			                "[--gen-seed S] [--reserve-gb G] [--plain-sample K] [--tune] [--device D]\n", argv[0]);
+			                "[--gen-seed S] [--reserve-gb G] [--plain-sample K] [--tune] [--no-pack] [--strict-sampler] "
+			        "[--device D]\n",
+			        argv[0]);
 			return 2;
 		}
 	}
@@ -239,6 +249,7 @@ int main(int argc, char** argv)
 	bo.device = device;
 	bo.steps_per_launch = 2;
 	bo.reserve_bytes = (uint64_t)(reserve_gb * 1073741824.0);
+	bo.flags = pack ? 0u : POT_BATCH_NO_PACK;
 	int rc = pot_batch_create(&bo, &b);
 	if (rc != POT_OK) {
 		fprintf(stderr, "pot_batch_create: %s\n", pot_gpu_strerror(rc));
@@ -250,7 +261,7 @@ int main(int argc, char** argv)
 	double tune_s = 0.0;
 	pot_batch_row* rows = calloc((size_t)(n_jobs > 0 ? n_jobs : 1), sizeof(pot_batch_row));
 	int* slot_job = calloc((size_t)(n_jobs + 4096), sizeof(int));
-	int next = 0, active = 0, finished = 0, max_active = 0, converged_n = 0, failed_n = 0;
+	int next = 0, active = 0, finished = 0, max_active = 0, converged_n = 0, failed_n = 0, capped_n = 0;
 	double ps = 0.0, queue_sum = 0.0, queue_max = 0.0;
 	uint64_t n_epochs = 0;
 	const double t_start = now_s();
@@ -264,6 +275,7 @@ int main(int argc, char** argv)
 			o.form = POT_FORM_FAST;
 			o.device = device;
 			o.seed = j->seed;
+			o.flags = chi_cap ? POT_OPT_CHI_CAP : 0u;
 			if (tune) {
 				const double cls = pow(2.0, floor(log2((double)j->cfg.N) + 0.5));
 				int e = 0;
@@ -354,6 +366,7 @@ int main(int argc, char** argv)
 			if (conv || st >= max_steps || rows[r].status != POT_OK) {
 				j->converged = conv;
 				converged_n += conv;
+				capped_n += (rows[r].warn & 512u) != 0;
 				j->done = tnow;
 				j->state = 2;
 				pot_batch_evict(b, rows[r].slot);
@@ -380,12 +393,14 @@ int main(int argc, char** argv)
 	       "\"latency_s\": {\"p50\": %s, \"p99\": %s, \"max\": %s}, "
 	       "\"latency_converged_s\": {\"p50\": %s, \"p99\": %s}, \"mean_steps\": %.1f, "
 	       "\"max_concurrent_runs\": %d, \"queue_depth\": {\"mean\": %.2f, \"max\": %.0f}, \"epochs\": %lu, "
-	       "\"epoch_steps\": %u, \"tuned_classes\": %d, \"tune_s\": %.3f",
+	       "\"epoch_steps\": %u, \"tuned_classes\": %d, \"tune_s\": %.3f, \"packed\": %s, \"chi_cap\": %s, "
+	       "\"runs_chi_capped\": %d",
 	       mode, n_jobs, finished, failed_n, converged_n, finished - converged_n - failed_n, (unsigned long)max_steps, wall, ps,
 	       wall > 0 ? ps / wall : 0.0, jnum(b1, pct(lat, nl, 0.5)), jnum(b2, pct(lat, nl, 0.99)),
 	       jnum(b3, pct(lat, nl, 1.0)), jnum(b4, pct(lat_c, nlc, 0.5)), jnum(b5, pct(lat_c, nlc, 0.99)),
 	       nl ? steps_sum / nl : 0.0, max_active,
-	       n_epochs ? queue_sum / (double)n_epochs : 0.0, queue_max, (unsigned long)n_epochs, epoch, n_tc, tune_s);
+	       n_epochs ? queue_sum / (double)n_epochs : 0.0, queue_max, (unsigned long)n_epochs, epoch, n_tc, tune_s,
+	       pack ? "true" : "false", chi_cap ? "true" : "false", capped_n);
 	if (serve) printf(", \"rate_per_s\": %g, \"duration_s\": %g", rate, duration);
 	printf(", \"n_range\": [%g, %g]", nmin, nmax);
 	if (tune && n_tc) {
@@ -411,6 +426,7 @@ int main(int argc, char** argv)
 			o.form = POT_FORM_PLAIN;
 			o.device = device;
 			o.seed = j->seed;
+			o.flags = chi_cap ? POT_OPT_CHI_CAP : 0u;
 			pot_gpu_ctx* c = NULL;
 			const double t0 = now_s();
 			if (pot_gpu_create(&j->cfg, &o, &c) != POT_OK || pot_gpu_init_particles(c) != POT_OK) {

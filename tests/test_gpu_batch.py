@@ -34,12 +34,13 @@ def test_bytes_needed_grows_with_n():
 
 
 @pytest.mark.gpu
-def test_batch_matches_runs_alone():
+@pytest.mark.parametrize("pack", [True, False])
+def test_batch_matches_runs_alone(pack):
     cfgs = [job(12001, 0.3, 10, 1.0), job(30001, 0.05, 1, 0.0, B=0.4), job(20001, 0.5, 30, 2.0, A=3.0),
             job(16001, 0.1, 3, 0.5)]
     forms = ["fast", "fast", "plain", "fast"]
     seeds = [1001, 1002, 1003, 1004]
-    with Batch(steps_per_launch=2) as b:
+    with Batch(steps_per_launch=2, pack=pack) as b:
         s0 = b.admit(cfgs[0], forms[0], seed=seeds[0])
         s1 = b.admit(cfgs[1], forms[1], seed=seeds[1])
         b.step(10)
@@ -65,6 +66,40 @@ def test_batch_matches_runs_alone():
         assert row["t_steps"] == steps[k] and row["grain_q"] == ga["q"]
         assert row["q_sum"] == sum(qs)
         assert row["particles"] == cfgs[k].N
+
+
+@pytest.mark.gpu
+def test_packed_batch_of_many_runs_matches_runs_alone():
+    """Twelve fast-form runs of 8k-70k particles -- leaf sizes 8, 16 and 32,
+    groups of 32 and 64 (two packed classes), a spheroidal grain, a
+    magnetic field -- stepped 12 steps in packed launches, one run admitted
+    after 4 steps and one evicted after 8: each run's particles and grain
+    bit for bit as stepped alone."""
+    rng = np.random.default_rng(5)
+    specs = []
+    for i in range(12):
+        N = int(np.exp(rng.uniform(np.log(8001), np.log(70001)))) | 1
+        cfg = job(N, float(np.exp(rng.uniform(np.log(0.05), np.log(0.8)))), [1, 3, 10, 30][i % 4],
+                  float(rng.uniform(0, 2)), B=0.6 if i == 3 else 0.0, A=3.0 if i == 5 else 0.0)
+        specs.append((cfg, [8, 16, 32][i % 3], 64 if i % 4 == 1 else 32, 2000 + i))
+    with Batch(steps_per_launch=2) as b:
+        slots = {i: b.admit(c, "fast", leaf_size=L, group_size=G, seed=sd) for i, (c, L, G, sd) in enumerate(specs)
+                 if i != 11}
+        b.step(4)
+        slots[11] = b.admit(specs[11][0], "fast", leaf_size=specs[11][1], group_size=specs[11][2], seed=specs[11][3])
+        b.step(4)
+        b.evict(slots.pop(7))
+        b.step(4)
+        b.sync()
+        got = {i: b.download(s) for i, s in slots.items()}
+    for i, (P, g) in got.items():
+        c, L, G, sd = specs[i]
+        with Run(c, form="fast", leaf_size=L, group_size=G, seed=sd) as r:
+            r.init_particles()
+            r.step(8 if i == 11 else 12)
+            Pa, ga = r.download()
+        assert np.array_equal(P.view(np.uint8), Pa.view(np.uint8)), i
+        assert g["q"] == ga["q"] and g["t_steps"] == ga["t_steps"], i
 
 
 @pytest.mark.gpu

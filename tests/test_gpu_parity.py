@@ -386,31 +386,50 @@ def test_fast_push_field_accuracy(leaf, group):
 
 
 @pytest.mark.parametrize("N,form", [(300001, "fast"), (8193, "fast"), (8193, "plain")])
-def test_move_particles_matches_upload_step_download(N, form):
-    """The drop-in call (chunked transfers overlapping the conversions, one
-    host wait) gives bit for bit what pot_gpu_upload, one step and
-    pot_gpu_download give, twice in a row."""
+@pytest.mark.parametrize("across_ion_step", [False, True])
+def test_move_particles_matches_upload_step_download(N, form, across_ion_step):
+    """The drop-in call (chunked transfers overlapping the conversions, a
+    download of only the records the step can change) gives bit for bit what
+    pot_gpu_upload, one step and pot_gpu_download give, twice in a row; with
+    across_ion_step the two calls are the steps just before and at an ion
+    step (t = tss_ion - 1, tss_ion).  The records not copied back keep the
+    caller's bytes: a marker written into every record's padding survives in
+    the ions' records on a step with no ion due and nowhere else."""
     cfg = run_config(dict(SMALL, N=N))
+    tss_ion = int(np.sqrt(cfg.Te * 1836.15 / cfg.Ti))
     kw = dict(leaf_size=16) if form == "fast" else {}
     with Run(cfg, form=form, seed=3, **kw) as r0:
         r0.init_particles()
-        r0.step(2)
+        r0.step(tss_ion - 2 if across_ion_step else 2)
         P0, g0 = r0.download()
     a_parts, a_grain = P0.copy(), dict(g0)
     b_parts, b_grain = P0.copy(), dict(g0)
+    fields = [k for k in P0.dtype.names if k != "_pad"]
+    mark = 0x5A5A5A5A
     with Run(cfg, form=form, seed=3, **kw) as ra, Run(cfg, form=form, seed=3, **kw) as rb:
         for _ in range(2):
+            a_parts["_pad"] = mark
             a_grain, sa = ra.move_particles(a_parts, a_grain)
             rb.upload(b_parts, b_grain)
             sb = rb.step(1)
             b_parts, b_grain = rb.download()
-            assert a_parts.tobytes() == b_parts.tobytes()
+            for k in fields:
+                assert a_parts[k].tobytes() == b_parts[k].tobytes(), k
+            ion_due = sa["t_steps"] % tss_ion == 0
+            ions = a_parts["species"] == 1
+            kept = a_parts["_pad"] == mark
+            assert not kept[0] and not kept[a_parts["species"] == 2].any()
+            if ion_due:
+                assert not kept[ions].any()
+            else:
+                assert kept[ions].all()
             for k in ("q", "m", "tot_absor_e", "t_steps", "chi_b"):
                 assert a_grain[k] == b_grain[k], k
             assert np.array_equal(a_grain["pos"], b_grain["pos"]) and np.array_equal(a_grain["vel"], b_grain["vel"])
             for k in ("t_steps", "grain_q", "dq", "de", "n_absorbed", "n_reinjected", "n_pushed", "interactions",
                       "n_nodes", "chi_b", "status", "q_sum"):
                 assert sa[k] == sb[k], k
+        assert across_ion_step == (sa["t_steps"] == tss_ion)
 
 
 def test_bad_species_is_reported():

@@ -44,6 +44,44 @@ def test_noalloc_matches_allocating_query_twice(form, leaf):
             assert np.max(np.abs(got - want).max(1) / mag) < 1e-12
 
 
+@pytest.mark.parametrize("form,leaf", [("plain", 0), ("fast", 16)])
+def test_noalloc_first_on_a_fresh_run_allocates_nothing(form, leaf):
+    """On a run that has never answered a field query (no query buffers
+    exist yet), two no-alloc calls leave the device's free memory as it was;
+    the allocating query afterwards gives the same fields."""
+    import torch
+    d = dict(SMALL, N=30001)
+    o = oracle_snapshot(d, seed=8, mode="gpu")
+    o.set_grain(q=-250)
+    P = o.particles()
+    g = dict(q=-250, pos=(P[0]["x"], P[0]["y"], P[0]["z"]))
+    rng = np.random.default_rng(23)
+    pts = [_points(o, rng, k) for k in (3000, 2000)]
+    # another run answers one query first, so that every kernel the query
+    # uses is already loaded on the device (module loading is not the call's)
+    with Run(run_config(d), form=form, leaf_size=leaf, seed=8) as w:
+        w.upload(P, g)
+        w.build_tree()
+        w.field_at(*pts[1])
+        w.field_at_noalloc(*pts[1])
+    torch.cuda.synchronize()
+    with Run(run_config(d), form=form, leaf_size=leaf, seed=8) as r:
+        r.upload(P, g)
+        r.build_tree()
+        r.sync()
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        got = [r.field_at_noalloc(idx, xyz) for idx, xyz in pts]
+        torch.cuda.synchronize()
+        free1 = torch.cuda.mem_get_info()[0]
+        assert free1 >= free0, "the no-alloc query took %d bytes of device memory" % (free0 - free1)
+        for (idx, xyz), e in zip(pts, got):
+            want = r.field_at(idx, xyz)
+            mag = np.sqrt((want ** 2).sum(1))
+            assert np.all(np.isfinite(e))
+            assert np.max(np.abs(e - want).max(1) / mag) < 1e-12
+
+
 def test_noalloc_rejects_oversized_requests():
     d = dict(SMALL, N=2049)
     o = oracle_snapshot(d, seed=6, mode="gpu")
