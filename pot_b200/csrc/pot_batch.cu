@@ -265,7 +265,7 @@ static void member_blocks(const MemberView& v, uint32_t out[PS_COUNT])
 	out[PS_MOMPRE] = div_up(nt / 4 + 1, 256);
 	out[PS_GROUPS] = std::min<uint32_t>(592u, std::max<uint32_t>(1u, div_up(nt, 2048)));
 	out[PS_ONE] = 1;
-	out[PS_SMALL] = std::max<uint32_t>(1u, std::min<uint32_t>(148u, n / 16384u));
+	out[PS_SMALL] = std::max<uint32_t>(4u, std::min<uint32_t>(148u, n / 8192u));
 }
 
 // Sort the batch's live members into packed classes (left in b->packs,

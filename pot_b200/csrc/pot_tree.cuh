@@ -88,7 +88,8 @@ struct MemberView {
 //   PS_MOMPRE  blocks_for(n_tree / 4 + 1, 256): cell moments from the sums
 //   PS_GROUPS  target groups
 //   PS_ONE     one block per member: digit offsets, scan tops, chi_b, grain
-//   PS_SMALL   a few blocks per member: late absorption, reinjection
+//   PS_SMALL   4-148 blocks per member (one per 8,192 particles): late
+//              absorption, reinjection (one warp per reinjected particle)
 enum PackStage : int {
 	PS_N256, PS_HIST, PS_TILES, PS_CMP, PS_PAIRS, PS_NODES, PS_FILL, PS_FINISH, PS_MOM, PS_MOMPRE, PS_GROUPS,
 	PS_ONE, PS_SMALL, PS_COUNT
