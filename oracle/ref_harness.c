@@ -394,7 +394,7 @@ double potref_integrate_for_alpha(double s, double chi_b, double u2, double Rol)
 
 /* The reference's own state-file writer and reader (pot.c:3816-3901,
    3904-4019), on the harness's run: format C, one worker record.  read
-   returns 0 on success (read_sim_state_from_file's nonzero is success). */
+   returns 0 on success, as read_sim_state_from_file does. */
 void potref_write_state(const char* path)
 {
 	/* run() writes at the top of an iteration, after its t_steps++
@@ -404,7 +404,7 @@ void potref_write_state(const char* path)
 	write_sim_state_to_file((unsigned int) R.N, &H, path);
 	H.t_steps--;
 }
-int potref_read_state(const char* path) { return read_sim_state_from_file((unsigned int) R.N, &H, path) ? 0 : -1; }
+int potref_read_state(const char* path) { return read_sim_state_from_file((unsigned int) R.N, &H, path) ? -1 : 0; }
 
 #ifdef RECORD_PHI_DATA
 /* write_phi_data_to_file (pot.c:3001-3042) for the tree last built, the

@@ -36,6 +36,7 @@ struct pot_gpu_ctx {
 	uint32_t* counts = nullptr;
 	uint32_t* block_sums = nullptr;
 	uint8_t* due = nullptr;
+	uint32_t* due_tiles = nullptr;   // due flags per scan tile (counted by the reorder)
 	uint32_t* due_list = nullptr;
 	uint32_t* due_prefix = nullptr;  // n + 1
 	uint2* groups = nullptr;
@@ -588,6 +589,7 @@ bool ctx_member_view(pot_gpu_ctx* c, MemberView* v)
 	v->counts = c->counts;
 	v->block_sums = c->block_sums;
 	v->due = c->due;
+	v->due_tiles = c->due_tiles;
 	v->due_list = c->due_list;
 	v->due_prefix = c->due_prefix;
 	v->groups = c->groups;
@@ -734,6 +736,7 @@ static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu
 	AL(c->counts, radix_counts_words(n));
 	AL(c->block_sums, nsum);
 	AL(c->due, n);
+	AL(c->due_tiles, scan_blocks(n) + 1);
 	AL(c->due_list, n);
 	AL(c->due_prefix, (size_t)n + 1);
 	if (fast) AL(c->groups, n);
@@ -885,13 +888,15 @@ static void enqueue_tree(pot_gpu_ctx* c, int begin_step)
 {
 	Params& P = c->P;
 	cudaStream_t s = c->stream;
-	launch_keys(c->pos[c->cur], c->keys[0], c->vals[0], P, c->rec, begin_step, s, c->timer);
+	uint32_t* hist = radix_sort_begin(c->counts, c->n, (int)P.key_bits, s);
+	launch_keys(c->pos[c->cur], c->keys[0], c->vals[0], P, c->rec, begin_step, hist, s, c->timer);
 	const int kb = radix_sort_pairs(c->keys, c->vals, c->n, c->counts, c->block_sums, (int)P.key_bits, s, c->timer,
 	                                &c->rec->status);
 	c->kb = kb;
 	const int nx = c->cur ^ 1;
+	cudaMemsetAsync(c->due_tiles, 0, sizeof(uint32_t) * scan_blocks(c->n), s);
 	launch_reorder(c->vals[kb], c->pos[c->cur], c->vel[c->cur], c->pid[c->cur], c->pos[nx], c->vel[nx], c->pid[nx],
-	               c->src64, c->src32, c->due, P, c->rec, s, c->timer);
+	               c->src64, c->src32, c->due, P, c->rec, c->due_tiles, s, c->timer);
 	c->cur = nx;
 	launch_build(c->keys[kb], c->T, c->src64, P, c->rec, c->block_sums, s, c->timer);
 }
@@ -902,7 +907,7 @@ static void enqueue_step(pot_gpu_ctx* c, uint32_t flags)
 	Params& P = c->P;
 	cudaStream_t s = c->stream;
 	enqueue_tree(c, 1);
-	compact_flags(c->due, c->n, c->due_list, c->block_sums, &c->rec->n_due, s, c->timer, c->due_prefix);
+	compact_flags(c->due, c->n, c->due_list, c->due_tiles, &c->rec->n_due, s, c->timer, c->due_prefix, true);
 	if (P.form == POT_FORM_FAST) launch_groups(c->T, c->due_prefix, c->groups, P, c->rec, s, c->timer);
 	launch_chi_b(c->T, c->src64, P, c->rec, 0, s, c->timer);
 	if (P.integrator == POT_INT_BORIS) {

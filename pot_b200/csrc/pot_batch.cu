@@ -253,8 +253,8 @@ static inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b
 static void member_blocks(const MemberView& v, uint32_t out[PS_COUNT])
 {
 	const uint32_t n = v.P.n, nt = v.P.n_tree, L = v.P.leaf_size;
+	out[PS_KEYS] = keys_blocks(n);
 	out[PS_N256] = div_up(n, 256);
-	out[PS_HIST] = std::min<uint32_t>(v.tiles, 1024u);
 	out[PS_TILES] = v.tiles;
 	out[PS_CMP] = pack_scan_blocks(n);
 	out[PS_PAIRS] = div_up(nt - 1, 256);
@@ -333,6 +333,7 @@ static void enqueue_pack(const PackClass& pc, uint32_t spl)
 	const PackDev& B = pc.B;
 	cudaStream_t s = pc.st;
 	for (uint32_t k = 0; k < spl; k++) {
+		pack_sort_begin(B, s);
 		pack_keys(B, (int)k, s);
 		pack_sort(B, s);
 		pack_reorder(B, (int)k, s);

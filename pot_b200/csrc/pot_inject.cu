@@ -38,6 +38,7 @@ constexpr int REJECT_CAP = 10000;
 // without bound).
 constexpr int RETRY_CAP = 100000;
 constexpr int SIMPSON_CAP = 100000;
+constexpr int NAN_SPEED_CAP = 64;  // NaN speeds in a row taken as "every draw is NaN"
 
 __device__ double d_u_no_flow_icdf(double chi, double q, uint32_t& fail)
 {
@@ -316,6 +317,7 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 	const double v_n = sp == SP_E ? P.vn_e : P.vn_i;
 	double chi_b = chi_b_in;
 	double u_mag = 0.0, u2 = 0.0, cz = 0.0, b = 0.0, alpha = 0.0, u[3];
+	int nan_speeds = 0;
 	for (int attempt = 0;; attempt++) {
 		chi_b = chi_b_in;
 		if (sp == SP_E) chi_b *= -P.Ti / P.Te;
@@ -350,11 +352,20 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 			cz = st.rnd(2.0) - 1.0;
 		}
 		if (isnan(u2)) {
-			// the reference would retry forever: every speed it can draw is NaN
-			fail |= FAIL_SPEED;
-			alpha = 0.0;
-			break;
+			// A NaN speed makes alpha NaN in the reference, which retries
+			// (pot.c:582-599): the same here.  When every speed it can draw is
+			// NaN (chi above about U^2 + 1/2) it would retry without end: a run
+			// of NAN_SPEED_CAP NaN speeds in a row stops the sampler instead.
+			if (++nan_speeds >= NAN_SPEED_CAP) {
+				fail |= FAIL_SPEED;
+				alpha = 0.0;
+				break;
+			}
+			alpha = NAN;
+			if (attempt + 1 >= RETRY_CAP) break;
+			continue;
 		}
+		nan_speeds = 0;
 		u[0] = 0.0;
 		u[1] = 0.0;
 		u[2] = u_mag;

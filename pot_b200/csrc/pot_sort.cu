@@ -160,11 +160,11 @@ void scan_exclusive(const uint32_t* in, uint32_t* out, size_t n, uint32_t* block
 }
 
 void compact_flags(const uint8_t* flags, size_t n, uint32_t* list, uint32_t* block_sums,
-                   unsigned int* count, cudaStream_t s, Timer& tm, uint32_t* prefix)
+                   unsigned int* count, cudaStream_t s, Timer& tm, uint32_t* prefix, bool tiles_counted)
 {
 	const size_t nb = scan_blocks(n ? n : 1);
-	ScopedKernel k(tm, "compact", 3);
-	k_scan_reduce<uint8_t><<<nb, SCAN_THREADS, 0, s>>>(flags, n, block_sums);
+	ScopedKernel k(tm, "compact", tiles_counted ? 2 : 3);
+	if (!tiles_counted) k_scan_reduce<uint8_t><<<nb, SCAN_THREADS, 0, s>>>(flags, n, block_sums);
 	k_scan_top<<<1, SCAN_THREADS, 0, s>>>(block_sums, nb, count);
 	k_scan_down<uint8_t, true><<<nb, SCAN_THREADS, 0, s>>>(flags, n, block_sums, list, prefix);
 }
@@ -183,37 +183,11 @@ void compact_flags(const uint8_t* flags, size_t n, uint32_t* list, uint32_t* blo
 constexpr int OS_THREADS = 256;
 constexpr int OS_ITEMS = 8;
 constexpr int OS_TILE = OS_THREADS * OS_ITEMS;
-constexpr int OS_MAX_PASSES = 8;
 constexpr uint32_t OS_FLAG_AGG = 1u << 30;
 constexpr uint32_t OS_FLAG_PRE = 2u << 30;
 constexpr uint32_t OS_COUNT = (1u << 30) - 1u;
 constexpr long OS_SPIN_CAP = 1L << 24;
 constexpr int OS_LOOKBACK = 8;      // earlier tiles read per round of the look-back
-
-// Digit counts of every pass in one read of the keys: hist[p * 256 + d].
-template <class G>
-__device__ __forceinline__ void os_hist_body(G grd, const uint64_t* __restrict__ keys, size_t n, int low_bit,
-                                             int npass, uint32_t* __restrict__ hist)
-{
-	__shared__ uint32_t h[OS_MAX_PASSES][RS_BINS];
-	for (int i = threadIdx.x; i < OS_MAX_PASSES * RS_BINS; i += OS_THREADS) (&h[0][0])[i] = 0;
-	__syncthreads();
-	for (size_t i = (size_t)grd.id() * OS_THREADS + threadIdx.x; i < n; i += (size_t)grd.n() * OS_THREADS) {
-		const uint64_t k = keys[i];
-		for (int p = 0; p < npass; p++) atomicAdd(&h[p][(k >> (low_bit + 8 * p)) & 0xFF], 1u);
-	}
-	__syncthreads();
-	for (int p = 0; p < npass; p++) {
-		const uint32_t c = h[p][threadIdx.x];
-		if (c) atomicAdd(&hist[p * RS_BINS + threadIdx.x], c);
-	}
-}
-
-__global__ void __launch_bounds__(OS_THREADS) k_os_hist(const uint64_t* __restrict__ keys, size_t n, int low_bit,
-                                                        int npass, uint32_t* __restrict__ hist)
-{
-	os_hist_body(GridSelf {}, keys, n, low_bit, npass, hist);
-}
 
 // In place: hist[p * 256 + d] <- exclusive prefix over digits (one block).
 template <class G>
@@ -380,6 +354,16 @@ size_t radix_counts_words(size_t n)
 	return (size_t)OS_MAX_PASSES * (tiles ? tiles : 1) * RS_BINS + (size_t)OS_MAX_PASSES * RS_BINS + OS_MAX_PASSES;
 }
 
+uint32_t* radix_sort_begin(uint32_t* counts, size_t n, int low_bit, cudaStream_t s)
+{
+	const uint32_t tiles = (uint32_t)((n + OS_TILE - 1) / OS_TILE);
+	const int npass = os_passes(low_bit);
+	uint32_t* hist = counts + (size_t)OS_MAX_PASSES * tiles * RS_BINS;
+	cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)npass * tiles * RS_BINS, s);
+	cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (OS_MAX_PASSES * RS_BINS + OS_MAX_PASSES), s);
+	return hist;
+}
+
 int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* counts, uint32_t* block_sums,
                      int low_bit, cudaStream_t s, Timer& tm, int* err)
 {
@@ -390,13 +374,8 @@ int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* c
 	uint32_t* status = counts;
 	uint32_t* hist = counts + (size_t)OS_MAX_PASSES * tiles * RS_BINS;
 	unsigned int* ctr = hist + OS_MAX_PASSES * RS_BINS;
-	const size_t words = (size_t)npass * tiles * RS_BINS;
-	cudaMemsetAsync(status, 0, sizeof(uint32_t) * words, s);
-	cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (OS_MAX_PASSES * RS_BINS + OS_MAX_PASSES), s);
 	{
-		ScopedKernel k(tm, "sort_hist", 2);
-		uint32_t nb = tiles < 1024 ? tiles : 1024;
-		k_os_hist<<<nb, OS_THREADS, 0, s>>>(keys[0], n, low_bit, npass, hist);
+		ScopedKernel k(tm, "sort_offsets");
 		k_os_offsets<<<1, RS_BINS, 0, s>>>(hist, npass);
 	}
 	int src = 0;
@@ -441,7 +420,7 @@ struct OsLayout {
 
 // What the single run clears with memsets before its sort, tree and groups:
 // each tile's status words of every pass; block 0 of a member the digit
-// counts, tile counters, overflow count and group count.
+// counts, tile counters, due-flag tile counts, overflow count and group count.
 __global__ void __launch_bounds__(OS_THREADS) kp_sort_clear(PackDev B)
 {
 	const SegBlock sb = seg_block(B.pre[PS_TILES], B.M);
@@ -451,19 +430,13 @@ __global__ void __launch_bounds__(OS_THREADS) kp_sort_clear(PackDev B)
 		L.status[((size_t)p * v.tiles + sb.id) * RS_BINS + threadIdx.x] = 0u;
 	if (sb.id == 0) {
 		for (int i = threadIdx.x; i < OS_MAX_PASSES * RS_BINS + OS_MAX_PASSES; i += OS_THREADS) L.hist[i] = 0u;
+		const uint32_t nt = (uint32_t)dev_scan_blocks(v.P.n);
+		for (uint32_t i = threadIdx.x; i < nt; i += OS_THREADS) v.due_tiles[i] = 0u;
 		if (threadIdx.x == 0) {
 			v.rec->n_overflow = 0;
 			v.rec->n_groups = 0;
 		}
 	}
-}
-
-__global__ void __launch_bounds__(OS_THREADS) kp_os_hist(PackDev B)
-{
-	const SegBlock sb = seg_block(B.pre[PS_HIST], B.M);
-	const MemberView& v = B.mv[sb.m];
-	os_hist_body(GridSeg { sb.id, sb.n }, v.keys[0], (size_t)v.P.n, (int)v.P.key_bits, (int)B.npass,
-	             OsLayout(v).hist);
 }
 
 __global__ void __launch_bounds__(RS_BINS) kp_os_offsets(PackDev B)
@@ -487,40 +460,35 @@ __global__ void __launch_bounds__(OS_THREADS) kp_os_pass(PackDev B, int p)
 	             v.vals[src ^ 1], &v.rec->status);
 }
 
-void pack_sort(const PackDev& B, cudaStream_t s)
+void pack_sort_begin(const PackDev& B, cudaStream_t s)
 {
 	kp_sort_clear<<<B.blocks[PS_TILES], OS_THREADS, 0, s>>>(B);
-	kp_os_hist<<<B.blocks[PS_HIST], OS_THREADS, 0, s>>>(B);
+}
+
+void pack_sort(const PackDev& B, cudaStream_t s)
+{
 	kp_os_offsets<<<B.blocks[PS_ONE], RS_BINS, 0, s>>>(B);
 	for (uint32_t p = 0; p < B.npass; p++) kp_os_pass<<<B.blocks[PS_TILES], OS_THREADS, 0, s>>>(B, (int)p);
 }
 
-// the due list and its prefix (compact_flags)
-__global__ void __launch_bounds__(SCAN_THREADS) kp_cmp_reduce(PackDev B)
-{
-	const SegBlock sb = seg_block(B.pre[PS_CMP], B.M);
-	const MemberView& v = B.mv[sb.m];
-	scan_reduce_body<uint8_t>(GridSeg { sb.id, sb.n }, v.due, (size_t)v.P.n, v.block_sums);
-}
-
+// the due list and its prefix (compact_flags; the reorder counted each tile)
 __global__ void __launch_bounds__(SCAN_THREADS) kp_cmp_top(PackDev B)
 {
 	const SegBlock sb = seg_block(B.pre[PS_ONE], B.M);
 	const MemberView& v = B.mv[sb.m];
-	scan_top_body(GridSeg { sb.id, sb.n }, v.block_sums, dev_scan_blocks(v.P.n), &v.rec->n_due);
+	scan_top_body(GridSeg { sb.id, sb.n }, v.due_tiles, dev_scan_blocks(v.P.n), &v.rec->n_due);
 }
 
 __global__ void __launch_bounds__(SCAN_THREADS) kp_cmp_down(PackDev B)
 {
 	const SegBlock sb = seg_block(B.pre[PS_CMP], B.M);
 	const MemberView& v = B.mv[sb.m];
-	scan_down_body<uint8_t, true>(GridSeg { sb.id, sb.n }, v.due, (size_t)v.P.n, v.block_sums, v.due_list,
+	scan_down_body<uint8_t, true>(GridSeg { sb.id, sb.n }, v.due, (size_t)v.P.n, v.due_tiles, v.due_list,
 	                              v.due_prefix);
 }
 
 void pack_compact(const PackDev& B, cudaStream_t s)
 {
-	kp_cmp_reduce<<<B.blocks[PS_CMP], SCAN_THREADS, 0, s>>>(B);
 	kp_cmp_top<<<B.blocks[PS_ONE], SCAN_THREADS, 0, s>>>(B);
 	kp_cmp_down<<<B.blocks[PS_CMP], SCAN_THREADS, 0, s>>>(B);
 }

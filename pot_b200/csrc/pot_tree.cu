@@ -72,10 +72,20 @@ __device__ __forceinline__ uint64_t scaled_key(double x, double y, double z, dou
 	return (spread3(ix) << 2) | (spread3(iy) << 1) | spread3(iz);
 }
 
+// Keys of every particle (grid-stride) and, when hist is given, the digit
+// counts of each of the radix sort's npass 8-bit passes from low_bit,
+// hist[p * 256 + d], counted in shared memory and added once per block: the
+// sort then needs no read of the keys of its own for them.
 template <class G>
 __device__ __forceinline__ void keys_body(G grd, const double4* __restrict__ pos, uint64_t* __restrict__ keys,
-                                          uint32_t* __restrict__ vals, const Params& P, RunRec* rec, int begin_step)
+                                          uint32_t* __restrict__ vals, const Params& P, RunRec* rec, int begin_step,
+                                          uint32_t* __restrict__ hist, int low_bit, int npass)
 {
+	__shared__ uint32_t h[OS_MAX_PASSES][RS_BINS];
+	if (hist) {
+		for (int i = threadIdx.x; i < npass * RS_BINS; i += blockDim.x) (&h[0][0])[i] = 0;
+		__syncthreads();
+	}
 	if (begin_step && grd.id() == 0 && threadIdx.x == 0) {
 		const unsigned long long t = rec->t_steps + 1;
 		rec->t_steps = t;
@@ -98,42 +108,50 @@ __device__ __forceinline__ void keys_body(G grd, const double4* __restrict__ pos
 		rec->n_bounced = 0;
 		rec->grain_slot = 0xFFFFFFFFu;
 	}
-	const uint32_t s = grd.id() * blockDim.x + threadIdx.x;
-	if (s >= P.n) return;
-	const double4 p = pos[s];
-	if (isnan(p.x) || isnan(p.y) || isnan(p.z)) {
-		set_status(rec, POT_E_NONFINITE);
-	} else if (p.x < 0.0 || p.x > P.root_w || p.y < 0.0 || p.y > P.root_w || p.z < 0.0 || p.z > P.root_w) {
-		set_status(rec, POT_E_DOMAIN);  // build_tree returns NULL, pot.c:1491-1500
+	for (uint32_t s = grd.id() * blockDim.x + threadIdx.x; s < P.n; s += grd.n() * blockDim.x) {
+		const double4 p = pos[s];
+		if (isnan(p.x) || isnan(p.y) || isnan(p.z)) {
+			set_status(rec, POT_E_NONFINITE);
+		} else if (p.x < 0.0 || p.x > P.root_w || p.y < 0.0 || p.y > P.root_w || p.z < 0.0 || p.z > P.root_w) {
+			set_status(rec, POT_E_DOMAIN);  // build_tree returns NULL, pot.c:1491-1500
+		}
+		// A spheroidal grain is not a tree source (pot-spheroid.c:1516-1518): the
+		// largest key sorts it to the last slot, outside [0, n_tree).  No
+		// particle of the spherical domain lies in that corner cell.
+		const uint64_t k = (P.shape && (int)p.w == SP_DUST) ? 0x7FFFFFFFFFFFFFFFull
+		                   : P.form == POT_FORM_FAST       ? scaled_key(p.x, p.y, p.z, 2097152.0 / P.root_w)
+		                                                   : morton_key(p.x, p.y, p.z, P.root_w);
+		keys[s] = k;
+		vals[s] = s;
+		if (hist)
+			for (int q = 0; q < npass; q++) atomicAdd(&h[q][(k >> (low_bit + 8 * q)) & 0xFF], 1u);
 	}
-	// A spheroidal grain is not a tree source (pot-spheroid.c:1516-1518): the
-	// largest key sorts it to the last slot, outside [0, n_tree).  No
-	// particle of the spherical domain lies in that corner cell.
-	keys[s] = (P.shape && (int)p.w == SP_DUST) ? 0x7FFFFFFFFFFFFFFFull
-	          : P.form == POT_FORM_FAST       ? scaled_key(p.x, p.y, p.z, 2097152.0 / P.root_w)
-	                                          : morton_key(p.x, p.y, p.z, P.root_w);
-	vals[s] = s;
+	if (hist) {
+		__syncthreads();
+		for (int i = threadIdx.x; i < npass * RS_BINS; i += blockDim.x) {
+			const uint32_t c = (&h[0][0])[i];
+			if (c) atomicAdd(&hist[i], c);
+		}
+	}
 }
 
 __global__ void k_keys(const double4* __restrict__ pos, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                       Params P, RunRec* rec, int begin_step)
+                       Params P, RunRec* rec, int begin_step, uint32_t* __restrict__ hist, int low_bit, int npass)
 {
-	keys_body(GridSelf {}, pos, keys, vals, P, rec, begin_step);
+	keys_body(GridSelf {}, pos, keys, vals, P, rec, begin_step, hist, low_bit, npass);
 }
 
 // Gather the state into the new Morton order, write the tree sources and
 // mark the particles due this step (electrons every step, ions every
 // tss[ION] steps, the grain every tss[DUST] steps, pot.c:2430-2434).
-template <class G>
-__device__ __forceinline__ void reorder_body(G grd, const uint32_t* __restrict__ perm,
-                                             const double4* __restrict__ pos_in, const double4* __restrict__ vel_in,
-                                             const uint32_t* __restrict__ pid_in, double4* __restrict__ pos_out,
-                                             double4* __restrict__ vel_out, uint32_t* __restrict__ pid_out,
-                                             double4* __restrict__ src64, float4* __restrict__ src32,
-                                             uint8_t* __restrict__ due, const Params& P, RunRec* rec)
+// One slot of the reorder; returns whether the particle is due.
+__device__ __forceinline__ bool reorder_one(uint32_t s, const uint32_t* __restrict__ perm,
+                                            const double4* __restrict__ pos_in, const double4* __restrict__ vel_in,
+                                            const uint32_t* __restrict__ pid_in, double4* __restrict__ pos_out,
+                                            double4* __restrict__ vel_out, uint32_t* __restrict__ pid_out,
+                                            double4* __restrict__ src64, float4* __restrict__ src32,
+                                            uint8_t* __restrict__ due, const Params& P, RunRec* rec)
 {
-	const uint32_t s = grd.id() * blockDim.x + threadIdx.x;
-	if (s >= P.n) return;
 	const uint32_t j = perm[s];
 	const double4 p = pos_in[j];
 	const double4 v = vel_in[j];
@@ -148,17 +166,49 @@ __device__ __forceinline__ void reorder_body(G grd, const uint32_t* __restrict__
 		src32[s] = make_float4((float)((p.x - P.rad) * P.inv_rad), (float)((p.y - P.rad) * P.inv_rad),
 		                       (float)((p.z - P.rad) * P.inv_rad), (float)q);
 	}
-	due[s] = (rec->t_steps % P.tss[sp]) == 0 ? 1 : 0;
+	const bool d = (rec->t_steps % P.tss[sp]) == 0;
+	due[s] = d ? 1 : 0;
 	if (sp == SP_DUST) rec->grain_slot = s;
+	return d;
+}
+
+
+template <class G>
+__device__ __forceinline__ void reorder_body(G grd, const uint32_t* __restrict__ perm,
+                                             const double4* __restrict__ pos_in, const double4* __restrict__ vel_in,
+                                             const uint32_t* __restrict__ pid_in, double4* __restrict__ pos_out,
+                                             double4* __restrict__ vel_out, uint32_t* __restrict__ pid_out,
+                                             double4* __restrict__ src64, float4* __restrict__ src32,
+                                             uint8_t* __restrict__ due, const Params& P, RunRec* rec,
+                                             uint32_t* __restrict__ due_tiles)
+{
+	const uint32_t s = grd.id() * blockDim.x + threadIdx.x;
+	// the due flags' count per scan tile of SCAN_TILE slots (the compaction's
+	// first stage; a 256-thread block lies inside one tile)
+	bool is_due = false;
+	if (s < P.n) is_due = reorder_one(s, perm, pos_in, vel_in, pid_in, pos_out, vel_out, pid_out, src64, src32, due,
+	                                  P, rec);
+	if (due_tiles) {
+		__shared__ uint32_t wcnt[32];
+		const uint32_t c = __popc(__ballot_sync(0xffffffffu, is_due));
+		if ((threadIdx.x & 31) == 0) wcnt[threadIdx.x >> 5] = c;
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			uint32_t t = 0;
+			for (uint32_t w = 0; w < (blockDim.x >> 5); w++) t += wcnt[w];
+			if (t) atomicAdd(&due_tiles[(grd.id() * blockDim.x) / SCAN_TILE], t);
+		}
+	}
 }
 
 __global__ void k_reorder(const uint32_t* __restrict__ perm, const double4* __restrict__ pos_in,
                           const double4* __restrict__ vel_in, const uint32_t* __restrict__ pid_in,
                           double4* __restrict__ pos_out, double4* __restrict__ vel_out,
                           uint32_t* __restrict__ pid_out, double4* __restrict__ src64, float4* __restrict__ src32,
-                          uint8_t* __restrict__ due, Params P, RunRec* rec)
+                          uint8_t* __restrict__ due, Params P, RunRec* rec, uint32_t* __restrict__ due_tiles)
 {
-	reorder_body(GridSelf {}, perm, pos_in, vel_in, pid_in, pos_out, vel_out, pid_out, src64, src32, due, P, rec);
+	reorder_body(GridSelf {}, perm, pos_in, vel_in, pid_in, pos_out, vel_out, pid_out, src64, src32, due, P, rec,
+	             due_tiles);
 }
 
 __device__ __forceinline__ int lcp_levels(uint64_t a, uint64_t b)
@@ -881,20 +931,25 @@ size_t mom_block_entries(size_t n) { return (n + MOM_TILE - 1) / MOM_TILE + 1; }
 // ---------------------------------------------------------------------------
 static inline uint32_t blocks_for(size_t n, int threads) { return (uint32_t)((n + threads - 1) / threads); }
 
+// The keys kernel's grid: a block per 256 particles up to eight blocks per
+// SM, then grid-stride (each block adds its digit counts once).
+uint32_t keys_blocks(size_t n) { return std::min<uint32_t>(blocks_for(n, 256), 148u * 8u); }
+
 void launch_keys(const double4* pos, uint64_t* keys, uint32_t* vals, const Params& P, RunRec* rec,
-                 int begin_step, cudaStream_t s, Timer& tm)
+                 int begin_step, uint32_t* hist, cudaStream_t s, Timer& tm)
 {
 	ScopedKernel k(tm, "keys");
-	k_keys<<<blocks_for(P.n, 256), 256, 0, s>>>(pos, keys, vals, P, rec, begin_step);
+	k_keys<<<keys_blocks(P.n), 256, 0, s>>>(pos, keys, vals, P, rec, begin_step, hist, (int)P.key_bits,
+	                                        radix_passes((int)P.key_bits));
 }
 
 void launch_reorder(const uint32_t* perm, const double4* pos_in, const double4* vel_in, const uint32_t* pid_in,
                     double4* pos_out, double4* vel_out, uint32_t* pid_out, double4* src64, float4* src32,
-                    uint8_t* due, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
+                    uint8_t* due, const Params& P, RunRec* rec, uint32_t* due_tiles, cudaStream_t s, Timer& tm)
 {
 	ScopedKernel k(tm, "reorder");
 	k_reorder<<<blocks_for(P.n, 256), 256, 0, s>>>(perm, pos_in, vel_in, pid_in, pos_out, vel_out, pid_out,
-	                                               src64, src32, due, P, rec);
+	                                               src64, src32, due, P, rec, due_tiles);
 }
 
 void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const Params& P, RunRec* rec,
@@ -954,9 +1009,10 @@ namespace pot {
 
 __global__ void kp_keys(PackDev B, int k)
 {
-	const SegBlock sb = seg_block(B.pre[PS_N256], B.M);
+	const SegBlock sb = seg_block(B.pre[PS_KEYS], B.M);
 	const MemberView& v = B.mv[sb.m];
-	keys_body(GridSeg { sb.id, sb.n }, v.pos[pack_in(v, k)], v.keys[0], v.vals[0], v.P, v.rec, 1);
+	keys_body(GridSeg { sb.id, sb.n }, v.pos[pack_in(v, k)], v.keys[0], v.vals[0], v.P, v.rec, 1,
+	          v.counts + (size_t)OS_MAX_PASSES * v.tiles * RS_BINS, (int)v.P.key_bits, (int)B.npass);
 }
 
 __global__ void kp_reorder(PackDev B, int k)
@@ -965,7 +1021,7 @@ __global__ void kp_reorder(PackDev B, int k)
 	const MemberView& v = B.mv[sb.m];
 	const uint32_t a = pack_in(v, k), b = pack_out(v, k);
 	reorder_body(GridSeg { sb.id, sb.n }, v.vals[v.kb], v.pos[a], v.vel[a], v.pid[a], v.pos[b], v.vel[b], v.pid[b],
-	             v.src64, v.src32, v.due, v.P, v.rec);
+	             v.src64, v.src32, v.due, v.P, v.rec, v.due_tiles);
 }
 
 __global__ void kp_pairs(PackDev B)
@@ -1027,7 +1083,7 @@ static_assert(MOM_TILE == (int)PACK_MOM_TILE, "moment tile");
 
 void pack_keys(const PackDev& B, int k, cudaStream_t s)
 {
-	kp_keys<<<B.blocks[PS_N256], 256, 0, s>>>(B, k);
+	kp_keys<<<B.blocks[PS_KEYS], 256, 0, s>>>(B, k);
 }
 
 void pack_reorder(const PackDev& B, int k, cudaStream_t s)

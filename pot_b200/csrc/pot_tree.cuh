@@ -62,6 +62,7 @@ struct MemberView {
 	uint32_t* counts;      // radix-sort status words, histograms and tile counters
 	uint32_t* block_sums;  // scan block sums
 	uint8_t* due;
+	uint32_t* due_tiles;   // due flags per scan tile, counted by the reorder
 	uint32_t* due_list;
 	uint32_t* due_prefix;
 	uint2* groups;
@@ -76,8 +77,8 @@ struct MemberView {
 // member (pot_batch.cu builds this).  pre[stage] is the exclusive prefix of
 // the members' block counts for that stage's kernels (device, M + 1
 // entries), blocks[stage] its total.  Stages:
-//   PS_N256    blocks_for(n, 256): keys, reorder
-//   PS_HIST    min(tiles, 1024): the sort's histogram
+//   PS_KEYS    keys_blocks(n): keys and the sort's digit counts
+//   PS_N256    blocks_for(n, 256): reorder
 //   PS_TILES   the sort's tiles: clearing the status words, each pass
 //   PS_CMP     scan tiles over n: the due list
 //   PS_PAIRS   blocks_for(n_tree - 1, 256)
@@ -91,7 +92,7 @@ struct MemberView {
 //   PS_SMALL   4-148 blocks per member (one per 8,192 particles): late
 //              absorption, reinjection (one warp per reinjected particle)
 enum PackStage : int {
-	PS_N256, PS_HIST, PS_TILES, PS_CMP, PS_PAIRS, PS_NODES, PS_FILL, PS_FINISH, PS_MOM, PS_MOMPRE, PS_GROUPS,
+	PS_KEYS, PS_N256, PS_TILES, PS_CMP, PS_PAIRS, PS_NODES, PS_FILL, PS_FINISH, PS_MOM, PS_MOMPRE, PS_GROUPS,
 	PS_ONE, PS_SMALL, PS_COUNT
 };
 struct PackDev {
@@ -110,6 +111,7 @@ __device__ __forceinline__ uint32_t pack_out(const MemberView& v, int k) { retur
 
 // the packed step's launches, in stream order (tree.cu, sort.cu, walk.cu,
 // walk_fast.cu, inject.cu)
+void pack_sort_begin(const PackDev& B, cudaStream_t s);
 void pack_keys(const PackDev& B, int k, cudaStream_t s);
 void pack_sort(const PackDev& B, cudaStream_t s);
 void pack_reorder(const PackDev& B, int k, cudaStream_t s);
@@ -128,10 +130,11 @@ uint32_t pack_scan_blocks(uint32_t n);        // scan tiles over n items
 size_t mom_prefix_entries(size_t n);
 size_t mom_block_entries(size_t n);
 void launch_keys(const double4* pos, uint64_t* keys, uint32_t* vals, const Params& P, RunRec* rec,
-                 int begin_step, cudaStream_t s, Timer& tm);
+                 int begin_step, uint32_t* hist, cudaStream_t s, Timer& tm);
+uint32_t keys_blocks(size_t n);
 void launch_reorder(const uint32_t* perm, const double4* pos_in, const double4* vel_in, const uint32_t* pid_in,
                     double4* pos_out, double4* vel_out, uint32_t* pid_out, double4* src64, float4* src32,
-                    uint8_t* due, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
+                    uint8_t* due, const Params& P, RunRec* rec, uint32_t* due_tiles, cudaStream_t s, Timer& tm);
 void launch_build(const uint64_t* keys, TreeDev& T, const double4* src64, const Params& P, RunRec* rec,
                   uint32_t* block_sums, cudaStream_t s, Timer& tm);
 

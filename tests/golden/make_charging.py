@@ -9,7 +9,7 @@ electrons in a sphere of 5 Debye lengths, Te = Ti, no flow, no field, theta
 
 * ``small``    the grain of radius 0.1 Debye lengths (8 seeds, 1..8);
 * ``grain05``  a grain of radius 0.5 Debye lengths, which collects about
-  25 times more charge in the same time (16 seeds, 1..16).
+  16 times more charge in the same time (16 seeds, 1..16).
 
 WELL512 is seeded from splitmix64 of the seed.  After every step the grain
 charge (e) is recorded: build_tree and move_particles exactly as run()

@@ -4,7 +4,7 @@ tests/golden/charging.npz holds the grain charge after each of 2,000 steps
 of the reference pot.c itself (SCEPTIC reinjection, 8,193 particles, Te =
 Ti, no flow, theta 0.5), written by tests/golden/make_charging.py for two
 grains: radius 0.1 Debye lengths (the benchmark's small plasma, seeds 1..8)
-and 0.5 Debye lengths (seeds 1..16; it collects about 25 times more charge,
+and 0.5 Debye lengths (seeds 1..16; it collects about 16 times more charge,
 so the comparison is sharper).  The GPU runs the same plasmas in both forms
 from its own init_particles (Philox streams, so only the statistics can
 agree), and the mean charge over steps 1,001-2,000 (from the device's

@@ -102,16 +102,18 @@ def test_one_plain_step_1m_vs_oracle(a_debye):
     assert gg["q"] == go["q"] and gg["tot_absor_e"] == go["tot_absor_e"]
     assert st["dq"] == so["dq"] and st["de"] == so["de"]
     assert st["n_absorbed"] == so["n_absorbed"]
-    assert st["n_reinjected"] == so["n_reinjected"] and st["n_pushed"] == so["n_pushed"]
+    assert st["n_pushed"] == so["n_pushed"]
+    # a particle absorbed and reinjected onto the boundary sphere is tested
+    # against the boundary again (pot.c:2676 then 2691), an ulp-level coin
+    # flip of libm: either side may reinject it once more
+    assert abs(st["n_reinjected"] - so["n_reinjected"]) <= so["n_absorbed"]
     if a_debye >= 1.0:
         assert st["n_absorbed"] > 0
     assert np.array_equal(Pg["species"], Po["species"])
     R = p["r"] * p["mpp"]
     pos_g = np.stack([Pg["x"], Pg["y"], Pg["z"]], 1)
     pos_o = np.stack([Po["x"], Po["y"], Po["z"]], 1)
-    # a particle absorbed and reinjected onto the boundary sphere is tested
-    # against the boundary again (pot.c:2676 then 2691): an ulp-level coin flip
-    # of libm, so the two may reinject it differently; each such particle lies
+    # such a particle may end up reinjected differently by the two; it lies
     # on the sphere in both results, at most one per absorption
     bad = np.nonzero(np.abs(pos_g - pos_o).max(1) >= 1e-12 * R)[0]
     assert len(bad) <= so["n_absorbed"]
