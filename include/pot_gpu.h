@@ -117,10 +117,11 @@ typedef struct pot_gpu_opts {
 
 #define POT_OPT_TIMING 0x1u  /* record CUDA events around each kernel (pot_gpu_kernel_times) */
 /* SCEPTIC reinjection with the edge potential capped (no counterpart in the
-   reference): the speed sampler is given min(chi, 0.9 (U^2 + 1/2)) for each
-   species, U its drift in units of its normalisation speed.  Above about
-   U^2 + 1/2 the reference's inverse CDF is NaN for every draw
-   (prng.c:171-214) and sceptically_reinject retries without end
+   reference): the speed sampler is given min(chi, 0.95 chi*) for each
+   species, chi* = U^2 + 1/2 + U exp(-U^2) / (sqrt(pi) erf(U)) (1 as U -> 0),
+   U its drift in units of its normalisation speed.  Above chi* the
+   reference's inverse CDF is NaN for every draw (its normaliser vanishes
+   there, prng.c:171-214) and sceptically_reinject retries without end
    (pot.c:582-599); a noisy single-point edge potential of a small grain in
    cold ions can read that high.  Off, such a run stops with POT_E_ITER and
    warn bit 64 (the reference's behaviour made finite); on, it goes on and

@@ -24,7 +24,11 @@ LIB = os.path.join(PKG, "libpotgpu.so")
 BUILD_DIR = os.path.join(PKG, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+# -fmad=false: a multiply and an add written separately stay two roundings
+# (fused multiply-adds are written as fma() where they are meant), so no
+# result depends on how the compiler contracts one kernel or another: a run
+# stepped by its own kernels and by a packed batch's gives the same bits.
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-fmad=false", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-Wall", "-Xcudafe", "--diag_suppress=177"]
 
 

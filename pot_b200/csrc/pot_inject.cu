@@ -322,10 +322,13 @@ __device__ void sceptic_reinject(Stream& st, int sp, double chi_b_in, const Para
 		chi_b = chi_b_in;
 		if (sp == SP_E) chi_b *= -P.Ti / P.Te;
 		if (P.flags & FLAG_CHI_CAP) {
-			// POT_OPT_CHI_CAP: keep the speed distribution defined (its inverse
-			// CDF needs chi below about U^2 + 1/2); nine tenths of that
+			// POT_OPT_CHI_CAP: keep the speed distribution defined.  The inverse
+			// CDF's normaliser 2 (U exp(-U^2) + psi erf(U)), psi = sqrt(pi)
+			// (1 + 2 (U^2 - chi)) / 2, vanishes at chi* = U^2 + 1/2 +
+			// U exp(-U^2) / (sqrt(pi) erf(U)) (1 in the limit U -> 0, the no-flow
+			// form's 1 - chi > 0); above it every draw is NaN.  The cap is 0.95 chi*.
 			const double U = P.x_drift / v_n;
-			const double cap = 0.9 * ((U * U) + 0.5);
+			const double cap = 0.95 * ((U * U) + 0.5 + (U > 1e-8 ? U * exp(-U * U) / (SQRT_PI_REF * erf(U)) : 0.5));
 			if (chi_b > cap) {
 				chi_b = cap;
 				fail |= FAIL_CAPPED;

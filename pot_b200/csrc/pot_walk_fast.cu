@@ -364,88 +364,37 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 	__syncwarp();
 	for (;;) {
 		const bool done = (len == 0);
+		// This round's cells are popped and their moments, child codes and
+		// leaf ranges requested first; the flushes below evaluate what earlier
+		// rounds staged while those loads are in flight, and the cells are
+		// tested and staged after them.
+		int32_t code = CH_EMPTY;
+		float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
+		float4 dipole = make_float4(0.f, 0.f, 0.f, 0.f);
+		float r2 = 0.f;
+		int4 c0 = make_int4(CH_EMPTY, CH_EMPTY, CH_EMPTY, CH_EMPTY), c1 = c0;
+		uint2 lr = make_uint2(0u, 0u);
 		if (!done) {
 			const int take = len < 32 ? len : 32;
-			const int32_t code = (int)lane < take ? sm.stack[len - 1 - (int)lane] : CH_EMPTY;
+			code = (int)lane < take ? sm.stack[len - 1 - (int)lane] : CH_EMPTY;
 			__syncwarp();
 			len -= take;
-			bool acc = false, leafr = false;
-			float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
-			float4 dipole = make_float4(0.f, 0.f, 0.f, 0.f);
-			uint2 range = make_uint2(0u, 0u);
-			int nch = 0;
-			int32_t cc[8];
-#pragma unroll
-			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
 			if (code >= 0) {
 				// the child codes are loaded with the cell's moments, before the
 				// test, so an opened cell costs one round trip to L2, not two
 				const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * (uint32_t)code]);
-				cell = T.f[code];
-				const float r2 = T.r2[code];
-				const int4 c0 = cp[0], c1 = cp[1];
-				if (DIP) dipole = T.fd[code];
-				if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
-					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
-				} else {
-					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
-					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
-#pragma unroll
-					for (int d = 0; d < 8; d++) nch += cc[d] != CH_EMPTY;
-				}
-			} else if (code != CH_EMPTY) {
+				cell = __ldg(&T.f[code]);
+				r2 = __ldg(&T.r2[code]);
+				c0 = __ldg(cp);
+				c1 = __ldg(cp + 1);
+				if (DIP) dipole = __ldg(&T.fd[code]);
+			} else if (code != CH_EMPTY && !single_leaves) {
 				const uint32_t e = leaf_payload(code);
-				if (single_leaves) {
-					leafr = true;
-					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
-				} else {
-					cell = T.lf[e];
-					const float r2 = T.lr2[e];
-					const uint2 lr = T.lrange[e];  // with the moments, as for cells
-					if (DIP) dipole = T.lfd[e];
-					if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
-						acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
-					} else {
-						leafr = true;
-						range = lr;
-					}
-				}
+				cell = __ldg(&T.lf[e]);
+				r2 = __ldg(&T.lr2[e]);
+				lr = __ldg(&T.lrange[e]);  // with the moments, as for cells
+				if (DIP) dipole = __ldg(&T.lfd[e]);
 			}
-			leafr = leafr && range.y > 0u;  // the leaf flush relies on no staged leaf being empty
-			// one warp scan for the three appends: accepted cells in bits 0-9,
-			// leaf ranges in bits 10-19, children in bits 20-31 (totals <= 32,
-			// <= 32 and <= 256 fit)
-			int tot;
-			const int packed = (acc ? 1 : 0) | ((leafr ? 1 : 0) << 10) | (nch << 20);
-			const int off = warp_excl(packed, tot);
-			const int co = off & 0x3FF, lo = (off >> 10) & 0x3FF, po = off >> 20;
-			const int tcell = tot & 0x3FF, tleaf = (tot >> 10) & 0x3FF, tch = tot >> 20;
-			if (acc) stage_src(sm.cells, ncell + co, cell, tag);
-			if (DIP && acc) sm.cells[FW_CELLS + ncell + co] = dipole;
-			ncell += tcell;
-			if (leafr) sm.leaves[nleaf + lo] = range;
-			nleaf += tleaf;
-			// opened leaves that may hold members' own particles
-			unsigned int hits = __ballot_sync(0xffffffffu, leafr && range.x <= smax && range.x + range.y > smin);
-			while (hits) {
-				const int b = __ffs(hits) - 1;
-				hits &= hits - 1;
-				const uint32_t rx = __shfl_sync(0xffffffffu, range.x, b);
-				const uint32_t ry = __shfl_sync(0xffffffffu, range.y, b);
-#pragma unroll
-				for (int k = 0; k < TPL; k++) seen[k] = seen[k] || (tg.self[k] - rx < ry);
-			}
-			if (len + tch > FW_STACK) {
-				err = POT_E_WALK;
-				break;
-			}
-			int w = len + po;
-#pragma unroll
-			for (int d = 0; d < 8; d++)
-				if (cc[d] != CH_EMPTY) sm.stack[w++] = cc[d];
-			len += tch;
-			maxlen = max(maxlen, len);
-			__syncwarp();
 		}
 		// flush staged monopoles in whole units of the unrolled loop, so it
 		// needs no remainder: a flush during the walk evaluates the whole units
@@ -563,6 +512,70 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			__syncwarp();
 		}
 		if (done) break;
+		{
+			bool acc = false, leafr = false;
+			uint2 range = make_uint2(0u, 0u);
+			int nch = 0;
+			int32_t cc[8];
+#pragma unroll
+			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
+			if (code >= 0) {
+				if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
+					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
+				} else {
+					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
+					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
+#pragma unroll
+					for (int d = 0; d < 8; d++) nch += cc[d] != CH_EMPTY;
+				}
+			} else if (code != CH_EMPTY) {
+				const uint32_t e = leaf_payload(code);
+				if (single_leaves) {
+					leafr = true;
+					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
+				} else if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
+					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
+				} else {
+					leafr = true;
+					range = lr;
+				}
+			}
+			leafr = leafr && range.y > 0u;  // the leaf flush relies on no staged leaf being empty
+			// one warp scan for the three appends: accepted cells in bits 0-9,
+			// leaf ranges in bits 10-19, children in bits 20-31 (totals <= 32,
+			// <= 32 and <= 256 fit)
+			int tot;
+			const int packed = (acc ? 1 : 0) | ((leafr ? 1 : 0) << 10) | (nch << 20);
+			const int off = warp_excl(packed, tot);
+			const int co = off & 0x3FF, lo = (off >> 10) & 0x3FF, po = off >> 20;
+			const int tcell = tot & 0x3FF, tleaf = (tot >> 10) & 0x3FF, tch = tot >> 20;
+			if (acc) stage_src(sm.cells, ncell + co, cell, tag);
+			if (DIP && acc) sm.cells[FW_CELLS + ncell + co] = dipole;
+			ncell += tcell;
+			if (leafr) sm.leaves[nleaf + lo] = range;
+			nleaf += tleaf;
+			// opened leaves that may hold members' own particles
+			unsigned int hits = __ballot_sync(0xffffffffu, leafr && range.x <= smax && range.x + range.y > smin);
+			while (hits) {
+				const int b = __ffs(hits) - 1;
+				hits &= hits - 1;
+				const uint32_t rx = __shfl_sync(0xffffffffu, range.x, b);
+				const uint32_t ry = __shfl_sync(0xffffffffu, range.y, b);
+#pragma unroll
+				for (int k = 0; k < TPL; k++) seen[k] = seen[k] || (tg.self[k] - rx < ry);
+			}
+			if (len + tch > FW_STACK) {
+				err = POT_E_WALK;
+				break;
+			}
+			int w = len + po;
+#pragma unroll
+			for (int d = 0; d < 8; d++)
+				if (cc[d] != CH_EMPTY) sm.stack[w++] = cc[d];
+			len += tch;
+			maxlen = max(maxlen, len);
+			__syncwarp();
+		}
 	}
 	Field<TPL> F;
 	if constexpr (TPL == 1) {
@@ -858,7 +871,7 @@ __device__ __forceinline__ void push_stats(RunRec* rec, unsigned long long n_int
 // non-Boris integrators (stage 2 walks over the intermediate sources).
 // Persistent: each warp takes the next group from the run's work counter.
 template <int TPL, int STG, bool DIP = false>
-__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 5)
+__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4)
 k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T, const float4* __restrict__ src32,
             const uint32_t* __restrict__ due_list, const uint2* __restrict__ groups, uint32_t* __restrict__ rein_list,
             Params P, RunRec* rec, const double4* __restrict__ src64, StageBufs sb)
@@ -1159,7 +1172,7 @@ __global__ void __launch_bounds__(1024) kp_group_prefix(PackDev B)
 // group of the whole batch, finds its member in gpre and runs it with that
 // member's tree, state and record; counts go to the member's record.
 template <int TPL>
-__global__ void __launch_bounds__(FW_WARPS * 32, 5) kp_push_fast(PackDev B, int k)
+__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) kp_push_fast(PackDev B, int k)
 {
 	__shared__ FastSmem<TPL, false> smem[FW_WARPS];
 	FastSmem<TPL, false>& sm = smem[threadIdx.x >> 5];

@@ -30,7 +30,9 @@
  * form for comparison.  --tune picks leaf and group sizes per size class
  * with the library's autotuner.  The batch packs its fast-form runs (one
  * launch per kernel of the step over all of them); --no-pack steps each run
- * as its own kernel sequence instead, for comparison.  Jobs run with
+ * as its own kernel sequence instead, for comparison.  --wall-limit S stops
+ * after S seconds and reports the jobs finished inside that window, and the
+ * jobs running and waiting at the stop.  Jobs run with
  * POT_OPT_CHI_CAP (the sampler's edge potential capped where the
  * reference's inverse CDF is undefined, so a cold-ion job with a noisy edge
  * potential goes on instead of stopping with POT_E_ITER); --strict-sampler
@@ -185,6 +187,7 @@ int main(int argc, char** argv)
 	uint64_t max_steps = 20000, seed0 = 1000, gen_seed = 12345;
 	uint32_t epoch = 50;
 	bool tune = false, pack = true, chi_cap = true;
+	double wall_limit = 0.0;  /* stop after this many seconds (0: when every job is done) */
 	for (int k = 1; k < argc; k++) {
 		const char* f = argv[k];
 		const char* v = k + 1 < argc ? argv[k + 1] : "";
@@ -206,11 +209,12 @@ int main(int argc, char** argv)
 		else if (!strcmp(f, "--tune")) { tune = true; }
 		else if (!strcmp(f, "--no-pack")) { pack = false; }
 		else if (!strcmp(f, "--strict-sampler")) { chi_cap = false; }
+		else if (!strcmp(f, "--wall-limit")) { wall_limit = atof(v); k++; }
 		else {
 			fprintf(stderr, "usage: %s [--mode sweep|serve] [--runs N] [--nmin N] [--nmax N] [--rate R] "
 			                "[--duration S] [--bmax T] [--max-steps N] [--max-runs N] [--epoch N] [--seed S] "
 			                "[--gen-seed S] [--reserve-gb G] [--plain-sample K] [--tune] [--no-pack] [--strict-sampler] "
-			        "[--device D]\n",
+			        "[--wall-limit S] [--device D]\n",
 			        argv[0]);
 			return 2;
 		}
@@ -265,8 +269,13 @@ int main(int argc, char** argv)
 	double ps = 0.0, queue_sum = 0.0, queue_max = 0.0;
 	uint64_t n_epochs = 0;
 	const double t_start = now_s();
+	bool stopped = false;
 	while (finished < n_jobs) {
 		const double t = now_s() - t_start;
+		if (wall_limit > 0.0 && t >= wall_limit) {
+			stopped = true;  /* the window is over: report what finished inside it */
+			break;
+		}
 		/* admission (FIFO) */
 		while (next < n_jobs && (!serve || jobs[next].arrival <= t) && active < max_runs) {
 			Job* j = &jobs[next];
@@ -402,6 +411,12 @@ int main(int argc, char** argv)
 	       n_epochs ? queue_sum / (double)n_epochs : 0.0, queue_max, (unsigned long)n_epochs, epoch, n_tc, tune_s,
 	       pack ? "true" : "false", chi_cap ? "true" : "false", capped_n);
 	if (serve) printf(", \"rate_per_s\": %g, \"duration_s\": %g", rate, duration);
+	if (wall_limit > 0.0) {
+		int arrived = 0;
+		for (int i = 0; i < n_jobs; i++) arrived += !serve || jobs[i].arrival <= wall;
+		printf(", \"wall_limit_s\": %g, \"stopped_at_wall_limit\": %s, \"arrived\": %d, \"running_at_stop\": %d, "
+		       "\"waiting_at_stop\": %d", wall_limit, stopped ? "true" : "false", arrived, active, arrived - next);
+	}
 	printf(", \"n_range\": [%g, %g]", nmin, nmax);
 	if (tune && n_tc) {
 		printf(", \"tuned\": [");
