@@ -250,6 +250,62 @@ def force_accuracy(run, cfg_name: str, cfg, dev, n_targets: int = 8192):
     return out
 
 
+def push_field_accuracy(run, cfg_name: str, cfg, dev, n_targets: int = 8192):
+    """The field the fast form's push actually applied in one step, against
+    an FP64 direct sum (plus the spheroid's analytic field) and against the
+    reference's own tree, at the same positions: the half-drifted positions
+    x0 + v0 dt / 2 of n_targets sampled electrons that the step neither
+    absorbed nor reinjected.  The field comes back from the velocity change
+    through the Boris step (pot.c:2475-2532): v1 = e + R(v0 + e), e = q E dt
+    / (2 m), R the rotation about the field's direction by 2 atan(q B dt /
+    (2 m)), so E = (2 m / (q dt)) (I + R)^-1 (v1 - R v0)."""
+    P0, g0 = run.download()
+    run.step(1)
+    P1, _ = run.download()
+    qe, me = 1.6021766e-19, 9.109383e-31
+    qom = -qe / me
+    dt = cfg.dt  # electrons move every step
+    B = np.asarray(cfg.B, float)
+    bmag = float(np.sqrt((B * B).sum()))
+    R = np.eye(3)
+    if bmag > 0.0:
+        b = B / bmag
+        ang = 2.0 * np.arctan(0.5 * dt * qom * bmag)
+        K = np.array([[0.0, -b[2], b[1]], [b[2], 0.0, -b[0]], [-b[1], b[0], 0.0]])  # K v = b x v
+        # rotate_vec_about_dir (coord.c:45-59): v cos + (b x v) sin + b (b.v)(1 - cos)
+        R = np.cos(ang) * np.eye(3) + np.sin(ang) * K + (1.0 - np.cos(ang)) * np.outer(b, b)
+    Rad = cfg.r * cfg.mpp
+    moved = np.sqrt((P1["x"] - P0["x"]) ** 2 + (P1["y"] - P0["y"]) ** 2 + (P1["z"] - P0["z"]) ** 2)
+    cand = np.nonzero((P0["species"] == 2) & (moved < 1e-3 * Rad))[0]
+    rng = np.random.default_rng(4321)
+    idx = np.sort(rng.choice(cand, min(n_targets, len(cand)), replace=False)).astype(np.uint32)
+    v0 = np.stack([P0["vx"][idx], P0["vy"][idx], P0["vz"][idx]], 1)
+    v1 = np.stack([P1["vx"][idx], P1["vy"][idx], P1["vz"][idx]], 1)
+    e = np.linalg.solve(np.eye(3) + R, (v1 - v0 @ R.T).T).T
+    E_push = e * 2.0 / (qom * dt)
+    h = np.stack([P0["x"][idx] + 0.5 * dt * P0["vx"][idx], P0["y"][idx] + 0.5 * dt * P0["vy"][idx],
+                  P0["z"][idx] + 0.5 * dt * P0["vz"][idx]], 1)
+    spheroid = bool(cfg.A)
+    e_dir = direct_field_fp64(P0, g0, idx, h, cfg.soft, dev, grain_source=not spheroid)
+    if spheroid:
+        g = dict(g0, x=P0[0]["x"], y=P0[0]["y"], z=P0[0]["z"])
+        e_dir = e_dir + grain_field_fp64(cfg_name, g, h)
+    e_ref = reference_tree_field(cfg_name, P0, g0, idx, h)
+    mag2 = (e_dir ** 2).sum(1)
+
+    def stat(ev):
+        rel = np.sqrt(((ev - e_dir) ** 2).sum(1) / mag2)
+        return {"rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99))}
+
+    out = {"targets": int(len(idx)), "state": "one step after the timed steps",
+           "field": "recovered from the push's velocity change through the Boris step",
+           "direct": "FP64, every pair softened" + (", plus the spheroid's analytic field" if spheroid else ""),
+           "push_vs_direct": stat(E_push)}
+    if e_ref is not None:
+        out["reference_tree_vs_direct"] = stat(e_ref)
+    return out
+
+
 def cpu_baseline_reference(cfg_name: str):
     """The reference program (compiled from its own sources, one MPI rank on
     one core) on a bounded sample of the same configuration.
@@ -465,28 +521,32 @@ def kernel_table(kt, N, pushes, hbm_peak):
     return out
 
 
-def roofline(kernel, interactions, launch_s, clk, alg_bytes, hbm_achieved, hbm_peak, peak_kind, traffic, share,
-             timing):
+def roofline(kernel, interactions, far_cells, pushes, launch_s, clk, alg_bytes, hbm_achieved, hbm_peak, peak_kind,
+             traffic, share, timing):
     """The dominant kernel against its bound.  The fast walk is bound by
-    FP32 arithmetic and instruction issue, not HBM: 17 FP32 flops (and one
-    reciprocal square root) per target-source interaction, interactions per
-    launch from the device counter, over the launch's CUDA-event time,
-    against 148 SMs x 128 FP32 lanes x 2 flops x the median SM clock sampled
-    during the timed region (a nominal peak: no measured FP32 figure
-    exists).  Its HBM figures (96 B per push: the FP64 state read and
-    written) sit beside it; `traffic` is the DRAM bytes of one launch from
-    an ncu capture of the same workload."""
+    FP32 arithmetic and instruction issue, not HBM.  Its arithmetic per
+    launch: 17 FP32 flops (and one reciprocal square root) per
+    target-source interaction, 60 per far cell expanded about its group's
+    centre (field, first and second derivatives, once per group) and 45 per
+    push (the expansion evaluated at the target), counts from the device
+    counters, over the launch's CUDA-event time; against 148 SMs x 128 FP32
+    lanes x 2 flops x the median SM clock sampled during the timed region
+    (a nominal peak: no measured FP32 figure exists).  Its HBM figures (96 B
+    per push: the FP64 state read and written) sit beside it; `traffic` is
+    the DRAM bytes of one launch from an ncu capture of the same workload."""
     mhz = (clk or {}).get("sm_mhz") or 1965.0
     out = {"kernel": kernel, "ms_per_launch": launch_s * 1e3, "share_of_step": share, "timing": timing,
            "alg_bytes_per_launch": alg_bytes, "traffic": traffic,
            "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
                    "frac": hbm_achieved / hbm_peak}}
     if interactions and kernel.startswith("walk_push") and launch_s:
-        achieved = interactions * 17.0 / launch_s / 1e12
+        flops = interactions * 17.0 + (far_cells * 60.0 + pushes * 45.0 if far_cells else 0.0)
+        achieved = flops / launch_s / 1e12
         peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
         out.update({"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                     "peak_kind": "nominal FP32 at the sampled SM clock (%.0f MHz)" % mhz,
-                    "flop_per_interaction": 17, "interactions_per_launch": interactions})
+                    "flop_per_interaction": 17, "interactions_per_launch": interactions,
+                    "far_cells_per_launch": far_cells, "flop_per_far_cell": 60, "flop_per_push_expansion": 45})
     else:
         out.update({"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
                     "frac": hbm_achieved / hbm_peak, "peak_kind": peak_kind})
@@ -582,7 +642,7 @@ def run_ours(args):
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
-        sums = {"interactions": 0, "n_pushed": 0, "n_groups": 0}
+        sums = {"interactions": 0, "n_pushed": 0, "n_groups": 0, "far_cells": 0}
         for k in range(args.steps):
             ev[k][0].record(stream)
             r.step_async(1)
@@ -641,8 +701,11 @@ def run_ours(args):
                 traffic = tj.get(dom_name)
         except Exception:
             traffic = None
-    # interactions per walk launch, averaged over the instrumented pass's steps
+    # interactions, far cells and pushes per walk launch, averaged over the
+    # instrumented pass's steps
     inter = stk["sum_interactions"] / args.steps if stk.get("sum_interactions") else st["interactions"]
+    far = stk.get("sum_far_cells", 0) / args.steps
+    pushes_launch = stk.get("sum_n_pushed", 0) / args.steps
 
     # plain FP64 form on the same workload (fewer steps: it is the slow form)
     plain = None
@@ -709,6 +772,7 @@ def run_ours(args):
         # its own tree for the force comparison
         cpu = cpu_baseline_reference(args.config)
         accuracy = force_accuracy(run, args.config, cfg, dev)
+        accuracy["push"] = push_field_accuracy(run, args.config, cfg, dev)
 
     batch = None
     if ws == 1 and args.batch_runs > 0:
@@ -727,13 +791,14 @@ def run_ours(args):
                        "group_size": group,
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
                        "parallelism": "replicas" if ws > 1 else "1 GPU"},
-            "roofline": roofline(dom_name, inter, per_launch_s, clk, alg_bytes, achieved, hbm_peak, peak_kind,
-                                 traffic, dom_ms / tk_ms if tk_ms else None,
+            "roofline": roofline(dom_name, inter, far, pushes_launch, per_launch_s, clk, alg_bytes, achieved,
+                                 hbm_peak, peak_kind, traffic, dom_ms / tk_ms if tk_ms else None,
                                  "per-kernel CUDA events in a second, instrumented pass over the same %d steps "
                                  "(%.4f ms per step with the events)" % (args.steps, tk_ms / args.steps)),
             "interactions_per_s": (inter * ws / (t_ms / args.steps / 1e3)) if inter else None,
             "interactions_per_push": (stk["sum_interactions"] / stk["sum_n_pushed"])
             if stk.get("sum_n_pushed") else None,
+            "far_cells_per_group": (stk["sum_far_cells"] / stk["sum_n_groups"]) if stk.get("sum_n_groups") else None,
             "kernels": kernels,
             "gpu_launches": launches, "clocks": clk, "plain_fp64": plain, "e2e": e2e, "cpu_baseline": cpu,
             "walk_stack_max": st.get("stack_max"),

@@ -151,7 +151,7 @@ typedef struct pot_step_stats {
 	uint64_t n_absorbed;   /* particles absorbed this step */
 	uint64_t n_reinjected; /* reinjections this step (absorption + boundary) */
 	uint64_t n_pushed;     /* particles advanced this step */
-	uint64_t interactions; /* cell + pair interactions evaluated this step */
+	uint64_t interactions; /* cell + pair terms evaluated for each target this step */
 	uint64_t n_nodes;      /* internal tree nodes this step */
 	double chi_b;          /* edge potential in force after the step */
 	int32_t status;        /* POT_OK or the first device-side error */
@@ -177,6 +177,9 @@ typedef struct pot_step_stats {
 	uint32_t n_groups;     /* fast form: target groups the walk ran this step, one warp each
 	                          (n_pushed / n_groups targets per group on average); 0 in the plain form */
 	uint32_t pad;
+	uint64_t far_cells;    /* fast form: accepted cells far from their group that were expanded
+	                          once about the group's centre instead of evaluated for each target
+	                          (not counted in interactions); 0 in the plain form */
 } pot_step_stats;
 
 /* capacity of the fast form's per-warp stack of cells awaiting a test;

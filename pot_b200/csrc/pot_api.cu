@@ -1013,6 +1013,7 @@ int pot_gpu_step(pot_gpu_ctx* c, uint32_t nsteps, uint32_t flags, pot_step_stats
 		out->n_reinjected = h.n_reinjected;
 		out->n_pushed = h.n_pushed;
 		out->interactions = h.interactions;
+		out->far_cells = h.far_cells;
 		out->n_nodes = h.n_nodes;
 		out->chi_b = r.chi_b;
 		out->status = r.status;
@@ -1239,6 +1240,7 @@ int pot_gpu_move_particles(pot_gpu_ctx* c, pot_particle* parts, uint64_t N, pot_
 		out->n_reinjected = h.n_reinjected;
 		out->n_pushed = h.n_pushed;
 		out->interactions = h.interactions;
+		out->far_cells = h.far_cells;
 		out->n_nodes = h.n_nodes;
 		out->chi_b = r.chi_b;
 		out->status = r.status;

@@ -97,6 +97,7 @@ struct RunRec {
 	long long sumv_e[3];
 	unsigned long long interactions;
 	unsigned long long n_pushed;
+	unsigned long long far_cells;  // fast form: far cells expanded about their group's centre
 	double epe[3];           // potential energies of the last step that computed them (J)
 	double phi_grain;        // potential at the grain from every other particle (V)
 	unsigned int epe_step;   // 1 when this step computes them
@@ -122,6 +123,7 @@ struct StepHist {
 	unsigned long long n_pushed;
 	unsigned long long interactions;
 	unsigned long long n_nodes;
+	unsigned long long far_cells;
 	double chi_b;
 	int status;
 	int pad;

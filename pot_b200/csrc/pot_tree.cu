@@ -102,6 +102,7 @@ __device__ __forceinline__ void keys_body(G grd, const double4* __restrict__ pos
 		rec->nabs_e = 0;
 		for (int k = 0; k < 3; k++) { rec->sumv_ion[k] = 0; rec->sumv_e[k] = 0; }
 		rec->interactions = 0;
+		rec->far_cells = 0;
 		rec->n_pushed = 0;
 		rec->n_collected = 0;
 		rec->n_wall = 0;

@@ -427,6 +427,7 @@ __device__ __forceinline__ void grain_end_body(G grd, double4* __restrict__ pos,
 	h.n_reinjected = rec->n_rein;
 	h.n_pushed = rec->n_pushed;
 	h.interactions = rec->interactions;
+	h.far_cells = rec->far_cells;
 	h.n_nodes = rec->n_nodes;
 	h.chi_b = rec->chi_b;
 	h.status = rec->status;

@@ -275,6 +275,97 @@ __device__ __forceinline__ Field<2> from_eval(const Acc<2>& E)
 	return f;
 }
 
+// Far cells of a group.  An accepted cell whose centre of charge is farther
+// from the centre c of the group's box than FAR_RATIO times the box's half
+// diagonal h is not staged for every target: the lane that tested it adds
+// its field at c and the field's first and second derivatives there to the
+// lane's expansion (monopole field E = q d / r^3, d = t - s):
+//   E_a     = w d_a,                                  w = q / r^3
+//   J_ab    = w (delta_ab - 3 d_a d_b / r^2)          (symmetric, traceless)
+//   H_abc   = w / r^2 (15 d_a d_b d_c / r^2 - 3 (delta_ab d_c + delta_ac d_b
+//             + delta_bc d_a))                        (symmetric, traceless)
+// J keeps 5 components, H 7 (J_zz = -J_xx - J_yy, H_xzz = -H_xxx - H_xyy,
+// H_yzz = -H_xxy - H_yyy, H_zzz = -H_xxz - H_yyz: a monopole's field is
+// divergence-free away from it).  After the walk the lanes' expansions are
+// summed by shuffles and each target adds E + J delta + H delta delta / 2,
+// delta = t - c.  The remainder is of third order: at most 4 (|delta| / d)^3
+// ~ 4 / FAR_RATIO^3 of the cell's field along the axis (1.9 % for 6), below
+// the monopole's own truncation of the cell's dipole and quadrupole, which
+// the opening test bounds by theta.
+constexpr float FAR_RATIO = 6.0f;
+
+struct FarExp {
+	float ex, ey, ez;
+	float jxx, jyy, jxy, jxz, jyz;
+	float hxxx, hyyy, hxxy, hxxz, hxyy, hyyz, hxyz;
+	__device__ __forceinline__ void zero()
+	{
+		ex = ey = ez = 0.f;
+		jxx = jyy = jxy = jxz = jyz = 0.f;
+		hxxx = hyyy = hxxy = hxxz = hxyy = hyyz = hxyz = 0.f;
+	}
+	// a monopole of charge q at (sx, sy, sz), expanded about c
+	__device__ __forceinline__ void add(float3 c, float4 s)
+	{
+		const float dx = c.x - s.x, dy = c.y - s.y, dz = c.z - s.z;
+		const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+		const float ri = rsqrt_ftz(r2);
+		const float ri2 = ri * ri;
+		const float w = (s.w * ri2) * ri;
+		ex = fmaf(w, dx, ex);
+		ey = fmaf(w, dy, ey);
+		ez = fmaf(w, dz, ez);
+		const float w3 = -3.f * w * ri2;  // -3 w / r^2
+		jxx += fmaf(w3, dx * dx, w);
+		jyy += fmaf(w3, dy * dy, w);
+		jxy = fmaf(w3, dx * dy, jxy);
+		jxz = fmaf(w3, dx * dz, jxz);
+		jyz = fmaf(w3, dy * dz, jyz);
+		const float v3 = w3 * ri2;         // -3 w / r^4
+		const float v15 = -5.f * v3 * ri2; // 15 w / r^6
+		hxxx += dx * fmaf(v15, dx * dx, 3.f * v3);
+		hyyy += dy * fmaf(v15, dy * dy, 3.f * v3);
+		hxxy += dy * fmaf(v15, dx * dx, v3);
+		hxxz += dz * fmaf(v15, dx * dx, v3);
+		hxyy += dx * fmaf(v15, dy * dy, v3);
+		hyyz += dz * fmaf(v15, dy * dy, v3);
+		hxyz = fmaf(v15 * dx, dy * dz, hxyz);
+	}
+	__device__ __forceinline__ void warp_sum()
+	{
+#pragma unroll
+		for (int o = 16; o; o >>= 1) {
+			ex += __shfl_xor_sync(0xffffffffu, ex, o);
+			ey += __shfl_xor_sync(0xffffffffu, ey, o);
+			ez += __shfl_xor_sync(0xffffffffu, ez, o);
+			jxx += __shfl_xor_sync(0xffffffffu, jxx, o);
+			jyy += __shfl_xor_sync(0xffffffffu, jyy, o);
+			jxy += __shfl_xor_sync(0xffffffffu, jxy, o);
+			jxz += __shfl_xor_sync(0xffffffffu, jxz, o);
+			jyz += __shfl_xor_sync(0xffffffffu, jyz, o);
+			hxxx += __shfl_xor_sync(0xffffffffu, hxxx, o);
+			hyyy += __shfl_xor_sync(0xffffffffu, hyyy, o);
+			hxxy += __shfl_xor_sync(0xffffffffu, hxxy, o);
+			hxxz += __shfl_xor_sync(0xffffffffu, hxxz, o);
+			hxyy += __shfl_xor_sync(0xffffffffu, hxyy, o);
+			hyyz += __shfl_xor_sync(0xffffffffu, hyyz, o);
+			hxyz += __shfl_xor_sync(0xffffffffu, hxyz, o);
+		}
+	}
+	// the expansion's field at c + (x, y, z)
+	__device__ __forceinline__ float3 at(float x, float y, float z) const
+	{
+		const float jzz = -jxx - jyy;
+		const float hxzz = -hxxx - hxyy, hyzz = -hxxy - hyyy, hzzz = -hxxz - hyyz;
+		const float xx = 0.5f * x * x, yy = 0.5f * y * y, zz = 0.5f * z * z, xy = x * y, xz = x * z, yz = y * z;
+		float3 e;
+		e.x = ex + jxx * x + jxy * y + jxz * z + hxxx * xx + hxyy * yy + hxzz * zz + hxxy * xy + hxxz * xz + hxyz * yz;
+		e.y = ey + jxy * x + jyy * y + jyz * z + hxxy * xx + hyyy * yy + hyzz * zz + hxyy * xy + hxyz * xz + hyyz * yz;
+		e.z = ez + jxz * x + jyz * y + jzz * z + hxxz * xx + hyyz * yy + hzzz * zz + hxyz * xy + hxzz * xz + hyzz * yz;
+		return e;
+	}
+};
+
 // Group walk.  Returns the fields in units of q / R^2 (multiply by
 // QE / (4 pi eps0 R^2) for V/m) and the number of entries evaluated per
 // target.
@@ -296,7 +387,7 @@ __device__ __forceinline__ Field<2> from_eval(const Acc<2>& E)
 template <int TPL, bool POT = false, bool DIP = false>
 __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const float4* __restrict__ src32,
                                  const Params& P, FastSmem<TPL, DIP>& sm, uint32_t& n_eval, uint32_t& stack_max,
-                                 int& err, int split = 1)
+                                 int& err, int split = 1, uint32_t* n_far_cells = nullptr)
 {
 	const uint32_t lane = lane_f();
 	uint32_t smin = 0xFFFFFFFFu, smax = 0u;
@@ -337,6 +428,15 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 	const float eps2 = fmaxf(P.soft2_f, 1e-20f);
 	const float3 bc = make_float3(0.5f * (bmin.x + bmax.x), 0.5f * (bmin.y + bmax.y), 0.5f * (bmin.z + bmax.z));
 	const bool single_leaves = P.leaf_size == 1;
+	// far cells (fields of monopoles only): expanded about bc instead of staged
+	constexpr bool USE_FAR = !POT && !DIP;
+	float far2 = 3.0e38f;
+	FarExp far;
+	if constexpr (USE_FAR) {
+		const float hx = 0.5f * (bmax.x - bmin.x), hy = 0.5f * (bmax.y - bmin.y), hz = 0.5f * (bmax.z - bmin.z);
+		far2 = (FAR_RATIO * FAR_RATIO) * fmaf(hx, hx, fmaf(hy, hy, hz * hz));
+		far.zero();
+	}
 	const int sub = (int)lane / (32 / split);  // this lane's share of each staged list
 	// Evaluation is FP32x2 in both forms.  Two targets per lane: each pair is
 	// the lane's two targets against one duplicated source.  One target per
@@ -359,42 +459,109 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 	// (so that the padded list fits the cell buffer)
 	const int cell_unroll = (TPL == 1 && split > 1) ? 4 : 8;
 	int len = 1, ncell = 0, nleaf = 0;
-	uint32_t n_cells_ev = 0, n_parts_ev = 0;
+	uint32_t n_cells_ev = 0, n_parts_ev = 0, n_far = 0;
 	if (lane == 0) sm.stack[0] = 0;
 	__syncwarp();
 	for (;;) {
 		const bool done = (len == 0);
-		// This round's cells are popped and their moments, child codes and
-		// leaf ranges requested first; the flushes below evaluate what earlier
-		// rounds staged while those loads are in flight, and the cells are
-		// tested and staged after them.
-		int32_t code = CH_EMPTY;
-		float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
-		float4 dipole = make_float4(0.f, 0.f, 0.f, 0.f);
-		float r2 = 0.f;
-		int4 c0 = make_int4(CH_EMPTY, CH_EMPTY, CH_EMPTY, CH_EMPTY), c1 = c0;
-		uint2 lr = make_uint2(0u, 0u);
 		if (!done) {
 			const int take = len < 32 ? len : 32;
-			code = (int)lane < take ? sm.stack[len - 1 - (int)lane] : CH_EMPTY;
+			const int32_t code = (int)lane < take ? sm.stack[len - 1 - (int)lane] : CH_EMPTY;
 			__syncwarp();
 			len -= take;
+			bool acc = false, leafr = false;
+			float4 cell = make_float4(0.f, 0.f, 0.f, 0.f);
+			float4 dipole = make_float4(0.f, 0.f, 0.f, 0.f);
+			uint2 range = make_uint2(0u, 0u);
+			int nch = 0;
+			int32_t cc[8];
+#pragma unroll
+			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
 			if (code >= 0) {
 				// the child codes are loaded with the cell's moments, before the
 				// test, so an opened cell costs one round trip to L2, not two
 				const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * (uint32_t)code]);
-				cell = __ldg(&T.f[code]);
-				r2 = __ldg(&T.r2[code]);
-				c0 = __ldg(cp);
-				c1 = __ldg(cp + 1);
-				if (DIP) dipole = __ldg(&T.fd[code]);
-			} else if (code != CH_EMPTY && !single_leaves) {
+				cell = T.f[code];
+				const float r2 = T.r2[code];
+				const int4 c0 = cp[0], c1 = cp[1];
+				if (DIP) dipole = T.fd[code];
+				if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
+					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
+					if (USE_FAR && acc) {
+						const float fx = bc.x - cell.x, fy = bc.y - cell.y, fz = bc.z - cell.z;
+						if (fmaf(fx, fx, fmaf(fy, fy, fz * fz)) > far2) {
+							far.add(bc, cell);
+							acc = false;
+							n_far++;
+						}
+					}
+				} else {
+					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
+					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
+#pragma unroll
+					for (int d = 0; d < 8; d++) nch += cc[d] != CH_EMPTY;
+				}
+			} else if (code != CH_EMPTY) {
 				const uint32_t e = leaf_payload(code);
-				cell = __ldg(&T.lf[e]);
-				r2 = __ldg(&T.lr2[e]);
-				lr = __ldg(&T.lrange[e]);  // with the moments, as for cells
-				if (DIP) dipole = __ldg(&T.lfd[e]);
+				if (single_leaves) {
+					leafr = true;
+					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
+				} else {
+					cell = T.lf[e];
+					const float r2 = T.lr2[e];
+					const uint2 lr = T.lrange[e];  // with the moments, as for cells
+					if (DIP) dipole = T.lfd[e];
+					if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
+						acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
+						if (USE_FAR && acc) {
+							const float fx = bc.x - cell.x, fy = bc.y - cell.y, fz = bc.z - cell.z;
+							if (fmaf(fx, fx, fmaf(fy, fy, fz * fz)) > far2) {
+								far.add(bc, cell);
+								acc = false;
+								n_far++;
+							}
+						}
+					} else {
+						leafr = true;
+						range = lr;
+					}
+				}
 			}
+			leafr = leafr && range.y > 0u;  // the leaf flush relies on no staged leaf being empty
+			// one warp scan for the three appends: accepted cells in bits 0-9,
+			// leaf ranges in bits 10-19, children in bits 20-31 (totals <= 32,
+			// <= 32 and <= 256 fit)
+			int tot;
+			const int packed = (acc ? 1 : 0) | ((leafr ? 1 : 0) << 10) | (nch << 20);
+			const int off = warp_excl(packed, tot);
+			const int co = off & 0x3FF, lo = (off >> 10) & 0x3FF, po = off >> 20;
+			const int tcell = tot & 0x3FF, tleaf = (tot >> 10) & 0x3FF, tch = tot >> 20;
+			if (acc) stage_src(sm.cells, ncell + co, cell, tag);
+			if (DIP && acc) sm.cells[FW_CELLS + ncell + co] = dipole;
+			ncell += tcell;
+			if (leafr) sm.leaves[nleaf + lo] = range;
+			nleaf += tleaf;
+			// opened leaves that may hold members' own particles
+			unsigned int hits = __ballot_sync(0xffffffffu, leafr && range.x <= smax && range.x + range.y > smin);
+			while (hits) {
+				const int b = __ffs(hits) - 1;
+				hits &= hits - 1;
+				const uint32_t rx = __shfl_sync(0xffffffffu, range.x, b);
+				const uint32_t ry = __shfl_sync(0xffffffffu, range.y, b);
+#pragma unroll
+				for (int k = 0; k < TPL; k++) seen[k] = seen[k] || (tg.self[k] - rx < ry);
+			}
+			if (len + tch > FW_STACK) {
+				err = POT_E_WALK;
+				break;
+			}
+			int w = len + po;
+#pragma unroll
+			for (int d = 0; d < 8; d++)
+				if (cc[d] != CH_EMPTY) sm.stack[w++] = cc[d];
+			len += tch;
+			maxlen = max(maxlen, len);
+			__syncwarp();
 		}
 		// flush staged monopoles in whole units of the unrolled loop, so it
 		// needs no remainder: a flush during the walk evaluates the whole units
@@ -512,70 +679,6 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			__syncwarp();
 		}
 		if (done) break;
-		{
-			bool acc = false, leafr = false;
-			uint2 range = make_uint2(0u, 0u);
-			int nch = 0;
-			int32_t cc[8];
-#pragma unroll
-			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
-			if (code >= 0) {
-				if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
-					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
-				} else {
-					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
-					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
-#pragma unroll
-					for (int d = 0; d < 8; d++) nch += cc[d] != CH_EMPTY;
-				}
-			} else if (code != CH_EMPTY) {
-				const uint32_t e = leaf_payload(code);
-				if (single_leaves) {
-					leafr = true;
-					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
-				} else if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
-					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
-				} else {
-					leafr = true;
-					range = lr;
-				}
-			}
-			leafr = leafr && range.y > 0u;  // the leaf flush relies on no staged leaf being empty
-			// one warp scan for the three appends: accepted cells in bits 0-9,
-			// leaf ranges in bits 10-19, children in bits 20-31 (totals <= 32,
-			// <= 32 and <= 256 fit)
-			int tot;
-			const int packed = (acc ? 1 : 0) | ((leafr ? 1 : 0) << 10) | (nch << 20);
-			const int off = warp_excl(packed, tot);
-			const int co = off & 0x3FF, lo = (off >> 10) & 0x3FF, po = off >> 20;
-			const int tcell = tot & 0x3FF, tleaf = (tot >> 10) & 0x3FF, tch = tot >> 20;
-			if (acc) stage_src(sm.cells, ncell + co, cell, tag);
-			if (DIP && acc) sm.cells[FW_CELLS + ncell + co] = dipole;
-			ncell += tcell;
-			if (leafr) sm.leaves[nleaf + lo] = range;
-			nleaf += tleaf;
-			// opened leaves that may hold members' own particles
-			unsigned int hits = __ballot_sync(0xffffffffu, leafr && range.x <= smax && range.x + range.y > smin);
-			while (hits) {
-				const int b = __ffs(hits) - 1;
-				hits &= hits - 1;
-				const uint32_t rx = __shfl_sync(0xffffffffu, range.x, b);
-				const uint32_t ry = __shfl_sync(0xffffffffu, range.y, b);
-#pragma unroll
-				for (int k = 0; k < TPL; k++) seen[k] = seen[k] || (tg.self[k] - rx < ry);
-			}
-			if (len + tch > FW_STACK) {
-				err = POT_E_WALK;
-				break;
-			}
-			int w = len + po;
-#pragma unroll
-			for (int d = 0; d < 8; d++)
-				if (cc[d] != CH_EMPTY) sm.stack[w++] = cc[d];
-			len += tch;
-			maxlen = max(maxlen, len);
-			__syncwarp();
-		}
 	}
 	Field<TPL> F;
 	if constexpr (TPL == 1) {
@@ -589,6 +692,19 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 		F = from_eval(e1);
 	} else {
 		F = from_eval(E);
+	}
+	if constexpr (USE_FAR) {
+		far.warp_sum();
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			const float3 e = far.at(tg.t[k].x - bc.x, tg.t[k].y - bc.y, tg.t[k].z - bc.z);
+			F.x[k] += e.x;
+			F.y[k] += e.y;
+			F.z[k] += e.z;
+		}
+		// the group's far cells, each expanded once
+		for (int o = 16; o; o >>= 1) n_far += __shfl_xor_sync(0xffffffffu, n_far, o);
+		if (n_far_cells) *n_far_cells = n_far;
 	}
 	// take back the members' own terms
 #pragma unroll
@@ -768,7 +884,7 @@ __device__ __forceinline__ int push_group(uint2 grp, double4* __restrict__ pos, 
                                           const Params& P, RunRec* rec, const double4* __restrict__ src64,
                                           const StageBufs& sb, const PushCtx& pc, FastSmem<TPL, DIP>& sm,
                                           unsigned long long& n_inter, unsigned long long& n_push,
-                                          uint32_t& stack_max)
+                                          uint32_t& stack_max, unsigned long long& n_far)
 {
 	Targets<TPL> tg;
 	uint32_t slot[TPL];
@@ -794,11 +910,12 @@ __device__ __forceinline__ int push_group(uint2 grp, double4* __restrict__ pos, 
 		tg.t[k] = make_float3((float)((h.x - P.rad) * P.inv_rad), (float)((h.y - P.rad) * P.inv_rad),
 		                      (float)((h.z - P.rad) * P.inv_rad));
 	}
-	uint32_t ne = 0, depth = 0;
+	uint32_t ne = 0, depth = 0, nf = 0;
 	int err = POT_OK;
-	const Field<TPL> ef = group_walk<TPL, false, DIP>(tg, T, pc.srcf, P, sm, ne, depth, err, split);
+	const Field<TPL> ef = group_walk<TPL, false, DIP>(tg, T, pc.srcf, P, sm, ne, depth, err, split, &nf);
 	stack_max = max(stack_max, depth);
 	if (err != POT_OK) return err;
+	if (lane_f() == 0) n_far += nf;
 #pragma unroll
 	for (int k = 0; k < TPL; k++) {
 		if (!tg.valid[k] || !owner) continue;
@@ -850,19 +967,22 @@ __device__ __forceinline__ int push_group(uint2 grp, double4* __restrict__ pos, 
 	return POT_OK;
 }
 
-// The lanes' interaction and push counts and deepest stack into the run record.
+// The lanes' interaction and push counts, far cells and deepest stack into
+// the run record.
 __device__ __forceinline__ void push_stats(RunRec* rec, unsigned long long n_inter, unsigned long long n_push,
-                                           uint32_t stack_max)
+                                           uint32_t stack_max, unsigned long long n_far)
 {
-	unsigned long long a = n_inter, b = n_push;
+	unsigned long long a = n_inter, b = n_push, f = n_far;
 #pragma unroll
 	for (int o = 16; o; o >>= 1) {
 		a += __shfl_xor_sync(0xffffffffu, a, o);
 		b += __shfl_xor_sync(0xffffffffu, b, o);
+		f += __shfl_xor_sync(0xffffffffu, f, o);
 	}
 	if (lane_f() == 0) {
 		if (a) atomicAdd(&rec->interactions, a);
 		if (b) atomicAdd(&rec->n_pushed, b);
+		if (f) atomicAdd(&rec->far_cells, f);
 		if (stack_max) atomicMax(&rec->stack_max, stack_max);
 	}
 }
@@ -871,7 +991,7 @@ __device__ __forceinline__ void push_stats(RunRec* rec, unsigned long long n_int
 // non-Boris integrators (stage 2 walks over the intermediate sources).
 // Persistent: each warp takes the next group from the run's work counter.
 template <int TPL, int STG, bool DIP = false>
-__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4)
+__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 5)
 k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T, const float4* __restrict__ src32,
             const uint32_t* __restrict__ due_list, const uint2* __restrict__ groups, uint32_t* __restrict__ rein_list,
             Params P, RunRec* rec, const double4* __restrict__ src64, StageBufs sb)
@@ -882,7 +1002,7 @@ k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T, con
 	if (__shfl_sync(0xffffffffu, lane_f() == 0 ? rec->status : 0, 0) != POT_OK) return;
 	const uint32_t n_groups = rec->n_groups;
 	const PushCtx pc = push_ctx<STG>(pos, src32, P, rec, sb);
-	unsigned long long n_inter = 0, n_push = 0;
+	unsigned long long n_inter = 0, n_push = 0, n_far = 0;
 	uint32_t stack_max = 0;
 	for (;;) {
 		uint32_t g = 0;
@@ -890,13 +1010,13 @@ k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T, con
 		g = __shfl_sync(0xffffffffu, g, 0);
 		if (g >= n_groups) break;
 		const int err = push_group<TPL, STG, DIP>(groups[g], pos, vel, T, src32, due_list, rein_list, P, rec, src64,
-		                                          sb, pc, sm, n_inter, n_push, stack_max);
+		                                          sb, pc, sm, n_inter, n_push, stack_max, n_far);
 		if (err != POT_OK) {
 			if (lane_f() == 0) set_status(rec, err);
 			break;
 		}
 	}
-	push_stats(rec, n_inter, n_push, stack_max);
+	push_stats(rec, n_inter, n_push, stack_max, n_far);
 }
 
 template <int TPL, bool DIP = false>
@@ -1172,7 +1292,7 @@ __global__ void __launch_bounds__(1024) kp_group_prefix(PackDev B)
 // group of the whole batch, finds its member in gpre and runs it with that
 // member's tree, state and record; counts go to the member's record.
 template <int TPL>
-__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) kp_push_fast(PackDev B, int k)
+__global__ void __launch_bounds__(FW_WARPS * 32, 5) kp_push_fast(PackDev B, int k)
 {
 	__shared__ FastSmem<TPL, false> smem[FW_WARPS];
 	FastSmem<TPL, false>& sm = smem[threadIdx.x >> 5];
@@ -1194,13 +1314,13 @@ __global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 4) kp_push_fast(
 		if (__shfl_sync(0xffffffffu, lane_f() == 0 ? rec->status : 0, 0) != POT_OK) continue;
 		const uint32_t b = pack_out(v, k);
 		const PushCtx pc = push_ctx<0>(v.pos[b], v.src32, v.P, rec, sb);
-		unsigned long long n_inter = 0, n_push = 0;
+		unsigned long long n_inter = 0, n_push = 0, n_far = 0;
 		uint32_t stack_max = 0;
 		const int err = push_group<TPL, 0, false>(v.groups[g - B.gpre[lo]], v.pos[b], v.vel[b], v.T, v.src32,
 		                                          v.due_list, v.rein_list, v.P, rec, v.src64, sb, pc, sm, n_inter,
-		                                          n_push, stack_max);
+		                                          n_push, stack_max, n_far);
 		if (err != POT_OK && lane_f() == 0) set_status(rec, err);
-		push_stats(rec, n_inter, n_push, stack_max);
+		push_stats(rec, n_inter, n_push, stack_max, n_far);
 	}
 }
 

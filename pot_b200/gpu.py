@@ -79,7 +79,8 @@ class _Stats(C.Structure):
                 ("interactions", C.c_uint64), ("n_nodes", C.c_uint64), ("chi_b", C.c_double),
                 ("status", C.c_int32), ("stack_max", C.c_uint32), ("epe", C.c_double * 3),
                 ("q_sum", C.c_int64), ("warn", C.c_uint32), ("n_collected", C.c_uint32),
-                ("n_wall", C.c_uint32), ("n_bounced", C.c_uint32), ("n_groups", C.c_uint32), ("pad", C.c_uint32)]
+                ("n_wall", C.c_uint32), ("n_bounced", C.c_uint32), ("n_groups", C.c_uint32), ("pad", C.c_uint32),
+                ("far_cells", C.c_uint64)]
 
 
 _LIB = None

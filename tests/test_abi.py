@@ -27,7 +27,7 @@ def test_struct_sizes():
     assert C.sizeof(gpu._RunCfg) == 8 + 4 + 4 + 8 * 9 + 24 + 8 + 24 + 8 + 4 + 4
     assert C.sizeof(gpu._Opts) == 40
     assert C.sizeof(gpu._Grain) == 88
-    assert C.sizeof(gpu._Stats) == 88 + 24 + 8 + 16 + 8
+    assert C.sizeof(gpu._Stats) == 88 + 24 + 8 + 16 + 8 + 8
 
 
 def test_strerror_covers_every_status():
