@@ -276,8 +276,9 @@ __device__ __forceinline__ Field<2> from_eval(const Acc<2>& E)
 }
 
 // Far cells of a group.  An accepted cell whose centre of charge is farther
-// from the centre c of the group's box than FAR_RATIO times the box's half
-// diagonal h is not staged for every target: the lane that tested it adds
+// from the centre c of the group's box than FAR_RATIO times h, the largest
+// distance of a member from c, is not staged for every target: the lane
+// that tested it adds
 // its field at c and the field's first and second derivatives there to the
 // lane's expansion (monopole field E = q d / r^3, d = t - s):
 //   E_a     = w d_a,                                  w = q / r^3
@@ -433,8 +434,17 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 	float far2 = 3.0e38f;
 	FarExp far;
 	if constexpr (USE_FAR) {
-		const float hx = 0.5f * (bmax.x - bmin.x), hy = 0.5f * (bmax.y - bmin.y), hz = 0.5f * (bmax.z - bmin.z);
-		far2 = (FAR_RATIO * FAR_RATIO) * fmaf(hx, hx, fmaf(hy, hy, hz * hz));
+		float h2 = 0.f;  // the largest squared distance of a member from bc
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			if (tg.valid[k]) {
+				const float dx = tg.t[k].x - bc.x, dy = tg.t[k].y - bc.y, dz = tg.t[k].z - bc.z;
+				h2 = fmaxf(h2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+			}
+		}
+#pragma unroll
+		for (int o = 16; o; o >>= 1) h2 = fmaxf(h2, __shfl_xor_sync(0xffffffffu, h2, o));
+		far2 = (FAR_RATIO * FAR_RATIO) * h2;
 		far.zero();
 	}
 	const int sub = (int)lane / (32 / split);  // this lane's share of each staged list
@@ -924,7 +934,10 @@ __device__ __forceinline__ int push_group(uint2 grp, double4* __restrict__ pos, 
 		double4 v = vel[s];
 		const int sp = (int)p.w;
 		const double dt = P.dt * (double)P.tss[sp];
-		const double3 hk = eval_point<STG>(p, vel, s, P);
+		// the evaluation point as eval_point computes it, from the same values
+		const double3 hk = STG == 0 ? make_double3(fma(0.5 * dt, v.x, p.x), fma(0.5 * dt, v.y, p.y),
+		                                           fma(0.5 * dt, v.z, p.z))
+		                            : make_double3(p.x, p.y, p.z);
 		n_inter += ne;
 		if (STG != 1) n_push++;
 		double E[3] = { (double)ef.x[k] * pc.escale, (double)ef.y[k] * pc.escale, (double)ef.z[k] * pc.escale };
@@ -991,7 +1004,7 @@ __device__ __forceinline__ void push_stats(RunRec* rec, unsigned long long n_int
 // non-Boris integrators (stage 2 walks over the intermediate sources).
 // Persistent: each warp takes the next group from the run's work counter.
 template <int TPL, int STG, bool DIP = false>
-__global__ void __launch_bounds__(FW_WARPS * 32, TPL == 1 ? 5 : 5)
+__global__ void __launch_bounds__(FW_WARPS * 32, 5)
 k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T, const float4* __restrict__ src32,
             const uint32_t* __restrict__ due_list, const uint2* __restrict__ groups, uint32_t* __restrict__ rein_list,
             Params P, RunRec* rec, const double4* __restrict__ src64, StageBufs sb)
