@@ -41,6 +41,8 @@ struct pot_gpu_ctx {
 	uint32_t* due_prefix = nullptr;  // n + 1
 	uint2* groups = nullptr;
 	uint2* groups_all = nullptr;     // fast form, potential energies
+	uint8_t* gcell = nullptr;        // fast form: groups per tree cell (pre-order group build)
+	uint32_t* gblk = nullptr;        // fast form: groups per build block, then their prefix
 	double* epe_partial = nullptr;   // per-block / per-group partial sums
 	double* macro = nullptr;         // macroscopic-summary partials and sums
 	uint32_t* rein_list = nullptr;
@@ -317,6 +319,15 @@ static int dalloc(pot_gpu_ctx* c, T** p, size_t count)
 }
 
 static inline uint32_t nblk(size_t n, int t) { return (uint32_t)((n + t - 1) / t); }
+
+// From this many particles on, a single run builds its target groups in tree
+// pre-order (two more launches).  The walk's warps then share the tree nodes
+// they read in L2: on the 4,000,001-particle plasma the walk's L2 hit rate
+// went from 79 % to 92 %, its DRAM traffic from 1.28 GB to 0.48 GB a launch
+// and the step from 4.80 to 4.66 ms.  On the 1,000,001-particle plasma, whose
+// tree and sources (about 30 MB) stay in L2 in any order, the two launches
+// only cost time (1.188 against 1.204 ms).
+constexpr uint32_t ORDERED_GROUPS_MIN_N = 2000000u;
 
 static int fill_params(pot_gpu_ctx* c)
 {
@@ -741,6 +752,10 @@ static int create_impl(const pot_run_cfg* cfg, const pot_gpu_opts* opts, pot_gpu
 	AL(c->due_prefix, (size_t)n + 1);
 	if (fast) AL(c->groups, n);
 	if (fast) AL(c->groups_all, n);
+	if (fast && n >= ORDERED_GROUPS_MIN_N) {
+		AL(c->gcell, cap);
+		AL(c->gblk, (size_t)group_blocks() + 1);
+	}
 	AL(c->epe_partial, 3 * (size_t)(n > (uint32_t)EPE_BLOCKS ? n : (uint32_t)EPE_BLOCKS));
 	AL(c->rein_list, 2 * (size_t)n);
 	AL(c->macro, macro_scratch_doubles());
@@ -908,7 +923,8 @@ static void enqueue_step(pot_gpu_ctx* c, uint32_t flags)
 	cudaStream_t s = c->stream;
 	enqueue_tree(c, 1);
 	compact_flags(c->due, c->n, c->due_list, c->due_tiles, &c->rec->n_due, s, c->timer, c->due_prefix, true);
-	if (P.form == POT_FORM_FAST) launch_groups(c->T, c->due_prefix, c->groups, P, c->rec, s, c->timer);
+	if (P.form == POT_FORM_FAST)
+		launch_groups(c->T, c->due_prefix, c->groups, c->gcell, c->gblk, P, c->rec, s, c->timer);
 	launch_chi_b(c->T, c->src64, P, c->rec, 0, s, c->timer);
 	if (P.integrator == POT_INT_BORIS) {
 		launch_push(c->pos[c->cur], c->vel[c->cur], c->T, c->src64, c->src32, c->due_list, c->groups, c->rein_list,

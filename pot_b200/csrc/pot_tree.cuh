@@ -157,8 +157,14 @@ struct StageBufs {
 void launch_push(double4* pos, double4* vel, const TreeDev& T, const double4* src64, const float4* src32,
                  const uint32_t* due_list, const uint2* groups, uint32_t* rein_list, const Params& P, RunRec* rec,
                  const StageBufs& sb, cudaStream_t s, Timer& tm);
-void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const Params& P, RunRec* rec,
-                   cudaStream_t s, Timer& tm);
+// Target groups of at most P.group_max due particles, each inside one tree
+// cell.  With gcell (a byte per tree cell) and gblk (group_blocks() + 1
+// words) the groups are laid out in tree pre-order, so that the walk's
+// concurrent warps work on neighbouring groups; with gcell == nullptr they
+// are built by one launch, in the order their cells finish.
+uint32_t group_blocks();
+void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, uint8_t* gcell, uint32_t* gblk,
+                   const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 void launch_absorb_late(double4* pos, double4* vel, const double4* src64, const uint32_t* due_list,
                         uint32_t* rein_list, const Params& P, RunRec* rec, cudaStream_t s, Timer& tm);
 void launch_grain_end(double4* pos, double4* vel, StepHist* hist, const Params& P, RunRec* rec, int epe,

@@ -838,6 +838,164 @@ __global__ void k_groups(TreeDev T, const uint32_t* __restrict__ dpre, uint2* __
 	groups_body(GridSelf {}, T, dpre, groups, ctr, gmax, P, rec);
 }
 
+// The same groups in tree pre-order, so that the walk's warps, which take
+// groups in array order, work on neighbouring groups at any one time and
+// share the tree nodes they read in L2.  Three launches: each of
+// GROUP_BLOCKS blocks owns a contiguous range of cells (pre-order) and counts
+// the groups each cell emits (gcell, one byte a cell, and the block's total);
+// one block turns the block totals into a prefix; each block then emits its
+// cells' groups at the prefix plus a block scan of the cell counts, in cell
+// order.  A cell's groups are the ones groups_body emits for it.
+constexpr int GROUP_THREADS = 256;
+
+template <bool EMIT>
+__device__ __forceinline__ uint32_t put_groups(uint2* out, uint32_t at, uint32_t start, uint32_t count, uint32_t gmax)
+{
+	uint32_t k = 0;
+	while (count > 0) {
+		const uint32_t c = count < gmax ? count : gmax;
+		if (EMIT) out[at + k] = make_uint2(start, c);
+		start += c;
+		count -= c;
+		k++;
+	}
+	return k;
+}
+
+template <bool EMIT>
+__device__ __forceinline__ uint32_t cell_groups(uint32_t k, const TreeDev& T, const uint32_t* __restrict__ dpre,
+                                                uint32_t gmax, const Params& P, uint2* out)
+{
+	const uint32_t a = T.first[k], b = T.last[k] + 1;
+	const uint32_t d = dpre_at(dpre, b) - dpre_at(dpre, a);
+	if (d == 0) return 0;
+	if (d <= gmax) return k == 0 ? put_groups<EMIT>(out, 0, dpre_at(dpre, a), d, gmax) : 0;
+	uint32_t n = 0, run_start = 0, run = 0;
+	for (int c = 0; c < 8; c++) {
+		const int32_t code = T.child[8u * k + (uint32_t)c];
+		if (code == CH_EMPTY) continue;
+		uint32_t ca, cb;
+		child_range(T, code, P, ca, cb);
+		const uint32_t dc = dpre_at(dpre, cb) - dpre_at(dpre, ca);
+		if (dc == 0) continue;
+		if (code >= 0 && dc > gmax) {
+			n += put_groups<EMIT>(out, n, run_start, run, gmax);
+			run = 0;
+			continue;
+		}
+		if (run + dc > gmax) {
+			n += put_groups<EMIT>(out, n, run_start, run, gmax);
+			run = 0;
+		}
+		if (run == 0) run_start = dpre_at(dpre, ca);
+		run += dc;
+	}
+	n += put_groups<EMIT>(out, n, run_start, run, gmax);
+	return n;
+}
+
+// exclusive scan over a GROUP_THREADS-thread block; *total = block sum
+__device__ __forceinline__ uint32_t group_block_scan(uint32_t v, uint32_t* total)
+{
+	__shared__ uint32_t ws[GROUP_THREADS / 32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	uint32_t x = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+		if (lane >= o) x += y;
+	}
+	if (lane == 31) ws[w] = x;
+	__syncthreads();
+	uint32_t before = 0, tot = 0;
+#pragma unroll
+	for (int k = 0; k < GROUP_THREADS / 32; k++) {
+		const uint32_t t = ws[k];
+		if (k < w) before += t;
+		tot += t;
+	}
+	__syncthreads();
+	*total = tot;
+	return before + x - v;
+}
+
+__device__ __forceinline__ void block_cells(uint32_t M, uint32_t& k0, uint32_t& k1)
+{
+	k0 = (uint32_t)((uint64_t)M * blockIdx.x / gridDim.x);
+	k1 = (uint32_t)((uint64_t)M * (blockIdx.x + 1) / gridDim.x);
+}
+
+__global__ void __launch_bounds__(GROUP_THREADS) k_groups_count(TreeDev T, const uint32_t* __restrict__ dpre,
+                                                                uint8_t* __restrict__ gcell,
+                                                                uint32_t* __restrict__ gblk, uint32_t gmax, Params P,
+                                                                RunRec* rec)
+{
+	if (rec->status != POT_OK) return;
+	uint32_t k0, k1, sum = 0;
+	block_cells(rec->n_nodes, k0, k1);
+	for (uint32_t k = k0 + threadIdx.x; k < k1; k += GROUP_THREADS) {
+		const uint32_t n = cell_groups<false>(k, T, dpre, gmax, P, nullptr);
+		gcell[k] = (uint8_t)(n < 255u ? n : 255u);  // 255: count again when emitting
+		sum += n;
+	}
+	uint32_t tot;
+	group_block_scan(sum, &tot);
+	if (threadIdx.x == 0) gblk[blockIdx.x] = tot;
+}
+
+// One block: gblk[b] <- groups of the blocks before b; the slots after the
+// tree's (a spheroidal grain) make the last groups; rec->n_groups the total.
+__global__ void __launch_bounds__(GROUP_THREADS) k_groups_prefix(uint32_t* __restrict__ gblk, uint32_t nb,
+                                                                 const uint32_t* __restrict__ dpre,
+                                                                 uint2* __restrict__ groups, uint32_t gmax, Params P,
+                                                                 RunRec* rec)
+{
+	if (rec->status != POT_OK) return;
+	__shared__ uint32_t carry;
+	if (threadIdx.x == 0) carry = 0;
+	__syncthreads();
+	for (uint32_t base = 0; base < nb; base += GROUP_THREADS) {
+		const uint32_t i = base + threadIdx.x;
+		const uint32_t v = i < nb ? gblk[i] : 0u;
+		uint32_t tot;
+		const uint32_t e = group_block_scan(v, &tot);
+		const uint32_t c = carry;
+		if (i < nb) gblk[i] = c + e;
+		__syncthreads();
+		if (threadIdx.x == 0) carry = c + tot;
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		uint32_t total = carry;
+		if (P.n_tree < P.n) {
+			const uint32_t a = dpre_at(dpre, P.n_tree), b = dpre_at(dpre, P.n);
+			if (b > a) total += put_groups<true>(groups, total, a, b - a, gmax);
+		}
+		rec->n_groups = total;
+	}
+}
+
+__global__ void __launch_bounds__(GROUP_THREADS) k_groups_emit(TreeDev T, const uint32_t* __restrict__ dpre,
+                                                               const uint8_t* __restrict__ gcell,
+                                                               const uint32_t* __restrict__ gblk,
+                                                               uint2* __restrict__ groups, uint32_t gmax, Params P,
+                                                               RunRec* rec)
+{
+	if (rec->status != POT_OK) return;
+	uint32_t k0, k1;
+	block_cells(rec->n_nodes, k0, k1);
+	uint32_t at = gblk[blockIdx.x];
+	for (uint32_t base = k0; base < k1; base += GROUP_THREADS) {
+		const uint32_t k = base + threadIdx.x;
+		uint32_t n = k < k1 ? gcell[k] : 0u;
+		if (n == 255u) n = cell_groups<false>(k, T, dpre, gmax, P, nullptr);
+		uint32_t tot;
+		const uint32_t off = group_block_scan(n, &tot);
+		if (n) cell_groups<true>(k, T, dpre, gmax, P, groups + at + off);
+		at += tot;
+	}
+}
+
 // The point where a target's field is evaluated: for the Boris step the
 // position drifted half a step, x + (dt tss / 2) v (pot.c:2478-2485); for
 // the stages of the other integrators the position itself.
@@ -1093,12 +1251,22 @@ static int sm_count_fast()
 	return n;
 }
 
-void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, const Params& P, RunRec* rec,
-                   cudaStream_t s, Timer& tm)
+uint32_t group_blocks() { return (uint32_t)sm_count_fast() * 4u; }
+
+void launch_groups(const TreeDev& T, const uint32_t* dpre, uint2* groups, uint8_t* gcell, uint32_t* gblk,
+                   const Params& P, RunRec* rec, cudaStream_t s, Timer& tm)
 {
 	cudaMemsetAsync(&rec->n_groups, 0, sizeof(unsigned int), s);
-	ScopedKernel k(tm, "groups");
-	k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, dpre, groups, &rec->n_groups, P.group_max, P, rec);
+	if (!gcell) {  // one launch, groups in the order their cells finish
+		ScopedKernel k(tm, "groups");
+		k_groups<<<sm_count_fast() * 4, 256, 0, s>>>(T, dpre, groups, &rec->n_groups, P.group_max, P, rec);
+		return;
+	}
+	const uint32_t nb = group_blocks();
+	ScopedKernel k(tm, "groups", 3);
+	k_groups_count<<<nb, GROUP_THREADS, 0, s>>>(T, dpre, gcell, gblk, P.group_max, P, rec);
+	k_groups_prefix<<<1, GROUP_THREADS, 0, s>>>(gblk, nb, dpre, groups, P.group_max, P, rec);
+	k_groups_emit<<<nb, GROUP_THREADS, 0, s>>>(T, dpre, gcell, gblk, groups, P.group_max, P, rec);
 }
 
 // compute_epe (pot.c:2771-2804), fast form: groups of up to 32 TPL over

@@ -69,6 +69,28 @@ def test_batch_matches_runs_alone(pack):
 
 
 @pytest.mark.gpu
+def test_large_run_pre_order_groups_match_packed():
+    """From 2,000,000 particles on, a run alone builds its target groups in
+    tree pre-order (three launches); the packed batch builds the same groups
+    in one launch, in whatever order their cells finish.  The groups are the
+    same set, so four steps of a 2,000,001-particle run, alone and as the
+    one member of a packed batch, leave the same particles bit for bit."""
+    cfg = job(2000001, 0.3, 10, 1.0, B=0.3)
+    with Batch(steps_per_launch=2, pack=True) as b:
+        s = b.admit(cfg, "fast", seed=77)
+        b.step(4)
+        b.sync()
+        P, g = b.download(s)
+    with Run(cfg, form="fast", seed=77) as r:
+        r.init_particles()
+        st = r.step(4)
+        Pa, ga = r.download()
+    assert st["status"] == 0 and st["n_groups"] > 0
+    assert np.array_equal(P.view(np.uint8), Pa.view(np.uint8))
+    assert g["q"] == ga["q"] and g["t_steps"] == 4
+
+
+@pytest.mark.gpu
 def test_packed_batch_of_many_runs_matches_runs_alone():
     """Twelve fast-form runs of 8k-70k particles -- leaf sizes 8, 16 and 32,
     groups of 32 and 64 (two packed classes), a spheroidal grain, a
