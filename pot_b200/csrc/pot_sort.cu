@@ -172,8 +172,9 @@ void compact_flags(const uint8_t* flags, size_t n, uint32_t* list, uint32_t* blo
 // ---------------------------------------------------------------------------
 // radix sort: one kernel per 8-bit pass with decoupled look-back
 // ---------------------------------------------------------------------------
-// Tiles of OS_TILE keys.  A block takes the next tile index from a counter
-// (so tiles start in index order), ranks its keys stably per digit, publishes
+// Tiles of OS_TILE keys.  The grid is the blocks the device holds at once;
+// each block takes the next tile index from a counter (so tiles start in
+// index order) until none is left, ranks its keys stably per digit, publishes
 // its per-digit counts, and obtains the exclusive prefix of each digit over
 // all earlier tiles by looking back at their published words (aggregate or
 // inclusive prefix).  Every wait has an iteration cap; reaching it records
@@ -223,12 +224,14 @@ __device__ __forceinline__ void os_pass_body(G grd, const uint64_t* __restrict__
 	__shared__ uint32_t s_val[OS_TILE];
 	const int t = threadIdx.x, w = t >> 5, lane = t & 31;
 	const uint32_t lt_mask = (1u << lane) - 1u;
+	for (;;) {  // tiles in ticket order until none is left
 	if (t == 0) s_tile = atomicAdd(tile_ctr, 1u);
 #pragma unroll
 	for (int k = 0; k < NW; k++) s_wcnt[k][t] = 0;
 	__syncthreads();
 	const uint32_t tile = s_tile;
 	const size_t base = (size_t)tile * OS_TILE;
+	if (base >= n) return;
 	// warp w holds the tile's keys [256 w, 256 w + 256), round r the 32 at
 	// 256 w + 32 r, so a key's index in the tile is (warp, round, lane) in order
 	uint64_t key[OS_ITEMS];
@@ -330,6 +333,8 @@ __device__ __forceinline__ void os_pass_body(G grd, const uint64_t* __restrict__
 		kout[o] = k;
 		vout[o] = s_val[i];
 	}
+	__syncthreads();  // the next tile reuses the shared arrays
+	}
 }
 
 __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restrict__ kin,
@@ -344,6 +349,21 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const uint64_t* __restri
 }
 
 static inline int os_passes(int low_bit) { return (63 - low_bit + 7) / 8; }
+
+// Blocks of k_os_pass resident on the device at once: the pass's grid, each
+// block taking tiles until none is left (no second wave of blocks).
+static uint32_t os_resident()
+{
+	static uint32_t n = 0;
+	if (!n) {
+		int dev = 0, sms = 0, per = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_os_pass, OS_THREADS, 0);
+		n = (uint32_t)std::max(1, sms) * (uint32_t)std::max(1, per);
+	}
+	return n;
+}
 
 uint32_t radix_tiles(size_t n) { return (uint32_t)((n + OS_TILE - 1) / OS_TILE); }
 int radix_passes(int low_bit) { return os_passes(low_bit); }
@@ -381,7 +401,7 @@ int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* c
 	int src = 0;
 	for (int p = 0; p < npass; p++) {
 		ScopedKernel k(tm, "sort_pass");
-		k_os_pass<<<tiles, OS_THREADS, 0, s>>>(keys[src], vals[src], n, low_bit + 8 * p, hist + p * RS_BINS,
+		k_os_pass<<<std::min<uint32_t>(tiles, os_resident()), OS_THREADS, 0, s>>>(keys[src], vals[src], n, low_bit + 8 * p, hist + p * RS_BINS,
 		                                      status + (size_t)p * tiles * RS_BINS, ctr + p, keys[src ^ 1],
 		                                      vals[src ^ 1], err);
 		src ^= 1;
