@@ -37,6 +37,12 @@ constexpr int FW_CELL_FLUSH = 64;
 constexpr int FW_LEAVES = 64;      // staged leaf ranges (flush at >= 32)
 constexpr int FW_LEAF_FLUSH = 32;
 static_assert(GROUP_MAX == 32 * FW_TPL_MAX, "one group per warp, at most FW_TPL_MAX targets per lane");
+// Blocks per SM the push kernels are compiled for.  With two targets per
+// lane the walk holds both targets' sums and operands: at four blocks (128
+// registers a thread) it needs no spills and runs faster than at five (96
+// registers, spilling), 4.51 against 4.65 ms per step on the 4m plasma.  One
+// target per lane fits 96 registers, and five blocks hide more latency.
+constexpr int fw_push_blocks(int tpl) { return tpl == 2 ? 4 : 5; }
 
 // Per-warp shared memory.  A staged source (accepted cell or gathered
 // particle) takes TPL float4s: with one target per lane it is (x, y, z, q);
@@ -1162,7 +1168,7 @@ __device__ __forceinline__ void push_stats(RunRec* rec, unsigned long long n_int
 // non-Boris integrators (stage 2 walks over the intermediate sources).
 // Persistent: each warp takes the next group from the run's work counter.
 template <int TPL, int STG, bool DIP = false>
-__global__ void __launch_bounds__(FW_WARPS * 32, 5)
+__global__ void __launch_bounds__(FW_WARPS * 32, fw_push_blocks(TPL))
 k_push_fast(double4* __restrict__ pos, double4* __restrict__ vel, TreeDev T, const float4* __restrict__ src32,
             const uint32_t* __restrict__ due_list, const uint2* __restrict__ groups, uint32_t* __restrict__ rein_list,
             Params P, RunRec* rec, const double4* __restrict__ src64, StageBufs sb)
@@ -1473,7 +1479,7 @@ __global__ void __launch_bounds__(1024) kp_group_prefix(PackDev B)
 // group of the whole batch, finds its member in gpre and runs it with that
 // member's tree, state and record; counts go to the member's record.
 template <int TPL>
-__global__ void __launch_bounds__(FW_WARPS * 32, 5) kp_push_fast(PackDev B, int k)
+__global__ void __launch_bounds__(FW_WARPS * 32, fw_push_blocks(TPL)) kp_push_fast(PackDev B, int k)
 {
 	__shared__ FastSmem<TPL, false> smem[FW_WARPS];
 	FastSmem<TPL, false>& sm = smem[threadIdx.x >> 5];
