@@ -493,14 +493,40 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 			int32_t cc[8];
 #pragma unroll
 			for (int d = 0; d < 8; d++) cc[d] = CH_EMPTY;
-			if (code >= 0) {
+			// Cells and bucket leaves load their moments from their own arrays
+			// but share one opening test and one far expansion: a round whose
+			// lanes hold both kinds runs that code once, not once per kind.  A
+			// leaf's particle range travels in c0.x, c0.y.
+			const bool is_cell = code >= 0;
+			bool tested = false, opened = false;
+			float r2 = 0.f;
+			int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
+			if (is_cell) {
 				// the child codes are loaded with the cell's moments, before the
 				// test, so an opened cell costs one round trip to L2, not two
 				const int4* cp = reinterpret_cast<const int4*>(&T.child[8u * (uint32_t)code]);
 				cell = T.f[code];
-				const float r2 = T.r2[code];
-				const int4 c0 = cp[0], c1 = cp[1];
+				r2 = T.r2[code];
+				c0 = cp[0];
+				c1 = cp[1];
 				if (DIP) dipole = T.fd[code];
+				tested = true;
+			} else if (code != CH_EMPTY) {
+				const uint32_t e = leaf_payload(code);
+				if (single_leaves) {
+					leafr = true;
+					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
+				} else {
+					cell = T.lf[e];
+					r2 = T.lr2[e];
+					const uint2 lr = T.lrange[e];  // with the moments, as for cells
+					c0.x = (int)lr.x;
+					c0.y = (int)lr.y;
+					if (DIP) dipole = T.lfd[e];
+					tested = true;
+				}
+			}
+			if (tested) {
 				if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
 					acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
 					if (USE_FAR && acc) {
@@ -511,37 +537,18 @@ __device__ Field<TPL> group_walk(const Targets<TPL>& tg, const TreeDev& T, const
 							n_far++;
 						}
 					}
+				} else if (is_cell) {
+					opened = true;
+					nch = (c0.x != CH_EMPTY) + (c0.y != CH_EMPTY) + (c0.z != CH_EMPTY) + (c0.w != CH_EMPTY) +
+					      (c1.x != CH_EMPTY) + (c1.y != CH_EMPTY) + (c1.z != CH_EMPTY) + (c1.w != CH_EMPTY);
 				} else {
-					cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
-					cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
-#pragma unroll
-					for (int d = 0; d < 8; d++) nch += cc[d] != CH_EMPTY;
-				}
-			} else if (code != CH_EMPTY) {
-				const uint32_t e = leaf_payload(code);
-				if (single_leaves) {
 					leafr = true;
-					range = e < P.n_tree ? make_uint2(e, 1u) : T.ovf[e - P.n_tree];
-				} else {
-					cell = T.lf[e];
-					const float r2 = T.lr2[e];
-					const uint2 lr = T.lrange[e];  // with the moments, as for cells
-					if (DIP) dipole = T.lfd[e];
-					if (group_accepts(bmin, bmax, bc, cell, r2, P.oap2_f)) {
-						acc = cell.w != 0.f || (DIP && (dipole.x != 0.f || dipole.y != 0.f || dipole.z != 0.f));
-						if (USE_FAR && acc) {
-							const float fx = bc.x - cell.x, fy = bc.y - cell.y, fz = bc.z - cell.z;
-							if (fmaf(fx, fx, fmaf(fy, fy, fz * fz)) > far2) {
-								far.add(bc, cell);
-								acc = false;
-								n_far++;
-							}
-						}
-					} else {
-						leafr = true;
-						range = lr;
-					}
+					range = make_uint2((uint32_t)c0.x, (uint32_t)c0.y);
 				}
+			}
+			if (opened) {
+				cc[0] = c0.x; cc[1] = c0.y; cc[2] = c0.z; cc[3] = c0.w;
+				cc[4] = c1.x; cc[5] = c1.y; cc[6] = c1.z; cc[7] = c1.w;
 			}
 			leafr = leafr && range.y > 0u;  // the leaf flush relies on no staged leaf being empty
 			// one warp scan for the three appends: accepted cells in bits 0-9,
