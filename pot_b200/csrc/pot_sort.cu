@@ -225,115 +225,115 @@ __device__ __forceinline__ void os_pass_body(G grd, const uint64_t* __restrict__
 	const int t = threadIdx.x, w = t >> 5, lane = t & 31;
 	const uint32_t lt_mask = (1u << lane) - 1u;
 	for (;;) {  // tiles in ticket order until none is left
-	if (t == 0) s_tile = atomicAdd(tile_ctr, 1u);
+		if (t == 0) s_tile = atomicAdd(tile_ctr, 1u);
 #pragma unroll
-	for (int k = 0; k < NW; k++) s_wcnt[k][t] = 0;
-	__syncthreads();
-	const uint32_t tile = s_tile;
-	const size_t base = (size_t)tile * OS_TILE;
-	if (base >= n) return;
-	// warp w holds the tile's keys [256 w, 256 w + 256), round r the 32 at
-	// 256 w + 32 r, so a key's index in the tile is (warp, round, lane) in order
-	uint64_t key[OS_ITEMS];
-	uint32_t val[OS_ITEMS];
-	uint32_t rank[OS_ITEMS];
-	int dig[OS_ITEMS];
+		for (int k = 0; k < NW; k++) s_wcnt[k][t] = 0;
+		__syncthreads();
+		const uint32_t tile = s_tile;
+		const size_t base = (size_t)tile * OS_TILE;
+		if (base >= n) return;
+		// warp w holds the tile's keys [256 w, 256 w + 256), round r the 32 at
+		// 256 w + 32 r, so a key's index in the tile is (warp, round, lane) in order
+		uint64_t key[OS_ITEMS];
+		uint32_t val[OS_ITEMS];
+		uint32_t rank[OS_ITEMS];
+		int dig[OS_ITEMS];
 #pragma unroll
-	for (int r = 0; r < OS_ITEMS; r++) {
-		const size_t i = base + (size_t)(w * 32 * OS_ITEMS + r * 32 + lane);
-		dig[r] = RS_BINS;
-		key[r] = 0;
-		val[r] = 0;
-		if (i < n) {
-			key[r] = kin[i];
-			val[r] = vin[i];
-			dig[r] = (int)((key[r] >> shift) & 0xFF);
+		for (int r = 0; r < OS_ITEMS; r++) {
+			const size_t i = base + (size_t)(w * 32 * OS_ITEMS + r * 32 + lane);
+			dig[r] = RS_BINS;
+			key[r] = 0;
+			val[r] = 0;
+			if (i < n) {
+				key[r] = kin[i];
+				val[r] = vin[i];
+				dig[r] = (int)((key[r] >> shift) & 0xFF);
+			}
 		}
-	}
-	// stable ranks inside the warp: a running count per digit in the warp's
-	// own row, updated once per round by the lowest lane of each digit
+		// stable ranks inside the warp: a running count per digit in the warp's
+		// own row, updated once per round by the lowest lane of each digit
 #pragma unroll
-	for (int r = 0; r < OS_ITEMS; r++) {
-		const int d = dig[r];
-		const uint32_t peers = __match_any_sync(0xffffffffu, d);
-		const uint32_t before = d < RS_BINS ? s_wcnt[w][d] : 0u;
-		rank[r] = before + __popc(peers & lt_mask);
-		__syncwarp();
-		if (d < RS_BINS && (peers & lt_mask) == 0u) s_wcnt[w][d] = before + __popc(peers);
-		__syncwarp();
-	}
-	__syncthreads();
-	// digit t: each warp's exclusive prefix over the warps before it, and
-	// the tile's count
-	uint32_t cnt = 0;
+		for (int r = 0; r < OS_ITEMS; r++) {
+			const int d = dig[r];
+			const uint32_t peers = __match_any_sync(0xffffffffu, d);
+			const uint32_t before = d < RS_BINS ? s_wcnt[w][d] : 0u;
+			rank[r] = before + __popc(peers & lt_mask);
+			__syncwarp();
+			if (d < RS_BINS && (peers & lt_mask) == 0u) s_wcnt[w][d] = before + __popc(peers);
+			__syncwarp();
+		}
+		__syncthreads();
+		// digit t: each warp's exclusive prefix over the warps before it, and
+		// the tile's count
+		uint32_t cnt = 0;
 #pragma unroll
-	for (int k = 0; k < NW; k++) {
-		const uint32_t c = s_wcnt[k][t];
-		s_wcnt[k][t] = cnt;
-		cnt += c;
-	}
-	// publish this tile's count of digit t, then look back for its prefix,
-	// OS_LOOKBACK earlier tiles per round of reads
-	volatile uint32_t* st = status;
-	st[(size_t)tile * RS_BINS + t] = (tile == 0 ? OS_FLAG_PRE : OS_FLAG_AGG) | cnt;
-	uint32_t excl = 0;
-	if (tile > 0) {
-		long spins = 0;
-		int64_t j = (int64_t)tile - 1;  // next tile to read
-		bool found = false;
-		while (!found) {
-			uint32_t v[OS_LOOKBACK];
+		for (int k = 0; k < NW; k++) {
+			const uint32_t c = s_wcnt[k][t];
+			s_wcnt[k][t] = cnt;
+			cnt += c;
+		}
+		// publish this tile's count of digit t, then look back for its prefix,
+		// OS_LOOKBACK earlier tiles per round of reads
+		volatile uint32_t* st = status;
+		st[(size_t)tile * RS_BINS + t] = (tile == 0 ? OS_FLAG_PRE : OS_FLAG_AGG) | cnt;
+		uint32_t excl = 0;
+		if (tile > 0) {
+			long spins = 0;
+			int64_t j = (int64_t)tile - 1;  // next tile to read
+			bool found = false;
+			while (!found) {
+				uint32_t v[OS_LOOKBACK];
 #pragma unroll
-			for (int q = 0; q < OS_LOOKBACK; q++) v[q] = j - q >= 0 ? st[(size_t)(j - q) * RS_BINS + t] : 0u;
-			int used = 0;
-			bool stalled = false;
+				for (int q = 0; q < OS_LOOKBACK; q++) v[q] = j - q >= 0 ? st[(size_t)(j - q) * RS_BINS + t] : 0u;
+				int used = 0;
+				bool stalled = false;
 #pragma unroll
-			for (int q = 0; q < OS_LOOKBACK; q++) {
-				if (found || stalled) continue;
-				const uint32_t flag = v[q] & ~OS_COUNT;
-				if (flag == 0) {  // not yet published (tile 0 always is, so j - q >= 0 here)
-					stalled = true;
-					continue;
+				for (int q = 0; q < OS_LOOKBACK; q++) {
+					if (found || stalled) continue;
+					const uint32_t flag = v[q] & ~OS_COUNT;
+					if (flag == 0) {  // not yet published (tile 0 always is, so j - q >= 0 here)
+						stalled = true;
+						continue;
+					}
+					excl += v[q] & OS_COUNT;
+					used++;
+					if (flag == OS_FLAG_PRE) found = true;
 				}
-				excl += v[q] & OS_COUNT;
-				used++;
-				if (flag == OS_FLAG_PRE) found = true;
+				if (found) break;
+				j -= used;
+				if (used == 0 && ++spins > OS_SPIN_CAP) {
+					atomicCAS(err, 0, POT_E_ITER);
+					break;
+				}
 			}
-			if (found) break;
-			j -= used;
-			if (used == 0 && ++spins > OS_SPIN_CAP) {
-				atomicCAS(err, 0, POT_E_ITER);
-				break;
-			}
+			st[(size_t)tile * RS_BINS + t] = OS_FLAG_PRE | (excl + cnt);
 		}
-		st[(size_t)tile * RS_BINS + t] = OS_FLAG_PRE | (excl + cnt);
-	}
-	s_glob[t] = goff[t] + excl;
-	// digit starts inside the tile
-	{
-		uint32_t tot;
-		const uint32_t e = block_excl_scan(cnt, &tot);
-		s_loc[t] = e;
-	}
-	__syncthreads();
+		s_glob[t] = goff[t] + excl;
+		// digit starts inside the tile
+		{
+			uint32_t tot;
+			const uint32_t e = block_excl_scan(cnt, &tot);
+			s_loc[t] = e;
+		}
+		__syncthreads();
 #pragma unroll
-	for (int r = 0; r < OS_ITEMS; r++) {
-		if (dig[r] < RS_BINS) {
-			const uint32_t p = s_loc[dig[r]] + s_wcnt[w][dig[r]] + rank[r];
-			s_key[p] = key[r];
-			s_val[p] = val[r];
+		for (int r = 0; r < OS_ITEMS; r++) {
+			if (dig[r] < RS_BINS) {
+				const uint32_t p = s_loc[dig[r]] + s_wcnt[w][dig[r]] + rank[r];
+				s_key[p] = key[r];
+				s_val[p] = val[r];
+			}
 		}
-	}
-	__syncthreads();
-	const uint32_t nt = (uint32_t)((n - base) < (size_t)OS_TILE ? (n - base) : (size_t)OS_TILE);
-	for (uint32_t i = t; i < nt; i += OS_THREADS) {
-		const uint64_t k = s_key[i];
-		const int d = (int)((k >> shift) & 0xFF);
-		const uint32_t o = s_glob[d] + (i - s_loc[d]);
-		kout[o] = k;
-		vout[o] = s_val[i];
-	}
-	__syncthreads();  // the next tile reuses the shared arrays
+		__syncthreads();
+		const uint32_t nt = (uint32_t)((n - base) < (size_t)OS_TILE ? (n - base) : (size_t)OS_TILE);
+		for (uint32_t i = t; i < nt; i += OS_THREADS) {
+			const uint64_t k = s_key[i];
+			const int d = (int)((k >> shift) & 0xFF);
+			const uint32_t o = s_glob[d] + (i - s_loc[d]);
+			kout[o] = k;
+			vout[o] = s_val[i];
+		}
+		__syncthreads();  // the next tile reuses the shared arrays
 	}
 }
 
@@ -401,7 +401,8 @@ int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], size_t n, uint32_t* c
 	int src = 0;
 	for (int p = 0; p < npass; p++) {
 		ScopedKernel k(tm, "sort_pass");
-		k_os_pass<<<std::min<uint32_t>(tiles, os_resident()), OS_THREADS, 0, s>>>(keys[src], vals[src], n, low_bit + 8 * p, hist + p * RS_BINS,
+		const uint32_t grid = std::min<uint32_t>(tiles, os_resident());
+		k_os_pass<<<grid, OS_THREADS, 0, s>>>(keys[src], vals[src], n, low_bit + 8 * p, hist + p * RS_BINS,
 		                                      status + (size_t)p * tiles * RS_BINS, ctr + p, keys[src ^ 1],
 		                                      vals[src ^ 1], err);
 		src ^= 1;
