@@ -61,3 +61,68 @@ def onesweep_pass(keys, vals, shift):
             out_v[o] = s_val[p]
         before_tiles += cnt
     return out_k, out_v
+
+
+AGG, PRE, LOOKBACK = 1, 2, 8  # status flags and tiles read per look-back round (OS_FLAG_*, OS_LOOKBACK)
+
+
+def lookback_schedule(counts, grid, seed, max_events=10_000_000):
+    """The pass's tile scheduling and decoupled look-back for one digit, with
+    `grid` resident blocks interleaved at random.  A block takes the next
+    ticket (tile), publishes its count (AGG; tile 0 publishes PRE), then reads
+    LOOKBACK earlier status words per round, adding counts until it meets an
+    inclusive prefix (PRE) and stopping the round at a word not yet published;
+    it then publishes PRE with its inclusive prefix and takes the next ticket
+    until none is left.  Each scheduling event advances one block by one
+    step (a publish or one round of reads).  Returns each tile's exclusive
+    prefix and the most rounds any tile spent looking back; raises if the
+    blocks stop making progress."""
+    rng = np.random.default_rng(seed)
+    n = len(counts)
+    st_flag = np.zeros(n, dtype=np.int64)
+    st_val = np.zeros(n, dtype=np.int64)
+    excl_out = np.full(n, -1, dtype=np.int64)
+    ticket = 0
+    blocks = [{"state": "take"} for _ in range(grid)]
+    live = list(range(grid))
+    max_rounds = 0
+    events = 0
+    while live:
+        events += 1
+        if events > max_events:
+            raise RuntimeError("no progress")
+        i = live[rng.integers(len(live))]
+        b = blocks[i]
+        if b["state"] == "take":
+            if ticket >= n:
+                live.remove(i)
+                continue
+            b.update(state="publish", tile=ticket, excl=0, j=ticket - 1, rounds=0)
+            ticket += 1
+        elif b["state"] == "publish":
+            t = b["tile"]
+            st_flag[t], st_val[t] = (PRE if t == 0 else AGG), counts[t]
+            b["state"] = "done" if t == 0 else "look"
+        elif b["state"] == "look":
+            j = b["j"]
+            reads = [(st_flag[j - q], st_val[j - q]) if j - q >= 0 else (0, 0) for q in range(LOOKBACK)]
+            b["rounds"] += 1
+            used, found = 0, False
+            for flag, val in reads:
+                if flag == 0:
+                    break
+                b["excl"] += val
+                used += 1
+                if flag == PRE:
+                    found = True
+                    break
+            b["j"] = j - used
+            if found:
+                t = b["tile"]
+                st_flag[t], st_val[t] = PRE, b["excl"] + counts[t]
+                b["state"] = "done"
+        if b["state"] == "done":
+            excl_out[b["tile"]] = b["excl"]
+            max_rounds = max(max_rounds, b.get("rounds", 0))
+            b["state"] = "take"
+    return excl_out, max_rounds

@@ -36,3 +36,18 @@ def test_passes_compose_to_a_full_sort():
         k, v = sm.onesweep_pass(k, v, 8 * p)
     order = np.argsort(keys, kind="stable")
     assert np.array_equal(k, keys[order]) and np.array_equal(v, order.astype(np.uint32))
+
+
+@pytest.mark.parametrize("tiles,grid", [(1, 4), (37, 1), (200, 8), (977, 64), (1954, 444)])
+def test_persistent_lookback_is_exact_and_ends(tiles, grid):
+    """The pass's grid is the blocks resident at once, each taking tiles in
+    ticket order until none is left (1,954 tiles of the 4m plasma on 444
+    resident blocks).  Under random interleavings every tile's look-back ends
+    with the exact count of its digit over all earlier tiles: a block waits
+    only on tiles with earlier tickets, which running blocks hold."""
+    rng = np.random.default_rng(tiles)
+    counts = rng.integers(0, 9, size=tiles)
+    for seed in range(3):
+        excl, rounds = sm.lookback_schedule(counts, grid, seed)
+        assert np.array_equal(excl, np.concatenate([[0], np.cumsum(counts)[:-1]]))
+        assert rounds >= (1 if tiles > 1 else 0)
