@@ -2,8 +2,10 @@
 kernel's expressions: it is the monopole field's Taylor expansion to second
 order about the group centre, and its error at an offset delta is bounded by
 the on-axis remainder 1/(1-e)^2 - (1 + 2e + 3e^2), e = |delta| / d, of the
-field at the centre (leading term 4 e^3; 2.3 % at the walk's FAR_RATIO of 6,
-where a target lies at most h from the centre and the cell at least 6 h)."""
+field at the centre (leading term 4 e^3; 9.0 % at the walk's FAR_RATIO of 4,
+where a target lies at most h from the centre and the cell at least 4 h).
+This test found the first build's second-derivative coefficients off by a
+factor 1 / r^2."""
 import numpy as np
 import pytest
 
@@ -79,13 +81,13 @@ def test_error_is_third_order():
 
 def test_far_cells_of_a_group_add():
     """Many far cells folded into one expansion: the group's error is at most
-    the sum of each cell's bound, with every cell at least 6 h from the
+    the sum of each cell's bound, with every cell at least 4 h from the
     centre and every target within h of it."""
     rng = np.random.default_rng(11)
     h = 0.05
     src, bound = [], 0.0
     for _ in range(200):
-        d = rng.uniform(6 * h, 40 * h)
+        d = rng.uniform(4 * h, 40 * h)
         u = _unit(rng)
         q = float(rng.choice([-2.0, -1.0, 1.0, 3.0]))
         src.append((d * u[0], d * u[1], d * u[2], q))
